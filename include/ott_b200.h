@@ -1,0 +1,135 @@
+/*
+ * ott_b200 C ABI: log-domain Sinkhorn on squared-Euclidean point clouds for
+ * NVIDIA B200 (sm_100a).
+ *
+ * Plain C: pointers, sizes and an int status; no C++ or torch types cross the
+ * boundary, nothing throws, and the library allocates no device memory. The
+ * caller owns every buffer, including a workspace sized by
+ * ottb_sinkhorn_workspace_size(). Every call is stream-ordered on the stream
+ * it is given; calls on different streams with distinct buffers may overlap.
+ *
+ * Reference interfaces replaced (paths inside the ott-jax source tree):
+ *   ottb_sinkhorn_pointcloud  <- ott/solvers/linear/_solve.py:29-64 (solve)
+ *                                -> sinkhorn.py:782-801 (Sinkhorn.__call__),
+ *                                sinkhorn.py:1052-1099 (run / iterations),
+ *                                math/fixed_point_loop.py:23-93 (fixpoint_iter),
+ *                                geometry/geometry.py:376-398 (update_potential),
+ *                                geometry/pointcloud.py:74-103 (apply_lse_kernel),
+ *                                sinkhorn.py:191-221 (marginal_error),
+ *                                sinkhorn.py:224-277 (compute_kl_reg_cost)
+ *   ottb_cost_stats           <- geometry/geometry.py:113-135
+ *                                (mean_cost_matrix / std_cost_matrix) through
+ *                                geometry/pointcloud.py:170-186 (sqeucl form)
+ */
+#ifndef OTT_B200_H_
+#define OTT_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes returned by every entry point. */
+enum {
+  OTTB_OK = 0,
+  OTTB_ERR_INVALID = 1,     /* bad argument (null pointer, size, config)   */
+  OTTB_ERR_UNSUPPORTED = 2, /* valid in the reference, not on this path    */
+  OTTB_ERR_CUDA = 3,        /* a CUDA runtime call failed                  */
+  OTTB_ERR_TIMEOUT = 4,     /* a device-side wait hit its time limit       */
+  OTTB_ERR_WORKSPACE = 5,   /* workspace missing or too small              */
+  OTTB_ERR_NO_DEVICE = 6    /* no sm_100 device visible                    */
+};
+
+/* Arithmetic used for the inner products <x_i, y_j>. */
+enum {
+  OTTB_PRECISION_AUTO = -1,       /* BF16 split-3 for d >= 32, else FP32   */
+  OTTB_PRECISION_FP32 = 0,        /* FP32 FMAs on the CUDA cores           */
+  OTTB_PRECISION_BF16_SPLIT3 = 1  /* tcgen05 BF16 hi/lo, 3 products, TMEM  */
+};
+
+/* One point-cloud problem. All pointers are device pointers. */
+typedef struct ottb_problem {
+  const float* x;      /* [n, d] row-major                                  */
+  const float* y;      /* [m, d] row-major                                  */
+  const float* a;      /* [n] first marginal (>= 0)                         */
+  const float* b;      /* [m] second marginal (>= 0)                        */
+  const float* f_init; /* [n] initial f, or NULL                            */
+  const float* g_init; /* [m] initial g, or NULL                            */
+  float* f;            /* [n] out: first potential                          */
+  float* g;            /* [m] out: second potential                         */
+  float* errors;       /* [ceil(max_iterations / inner_iterations)] out     */
+  int64_t n;
+  int64_t m;
+  float epsilon;        /* target epsilon (already resolved)                */
+  float inv_scale_cost; /* cost multiplier, 1 / scale_cost                  */
+} ottb_problem;
+
+/* Solver configuration shared by every problem of one call
+ * (sinkhorn.py:718-780 defaults: threshold 1e-3, norm_error 1,
+ * inner_iterations 10, min_iterations 0, max_iterations 2000). */
+typedef struct ottb_solver_cfg {
+  float threshold;
+  int32_t norm_error;       /* p of the p-norm marginal error (>= 1)        */
+  int32_t inner_iterations;
+  int32_t min_iterations;
+  int32_t max_iterations;
+  float eps_init;           /* epsilon_scheduler.py:43-60 (init, decay)     */
+  float eps_decay;
+  int32_t precision;        /* OTTB_PRECISION_*                             */
+  int32_t mask_init;        /* 1: f_init/g_init set to -inf where weight 0  */
+  int32_t timeout_ms;       /* device wait limit, 0 = default (60 s)        */
+  int32_t phantom_arrivals; /* extra grid-barrier arrivals to wait for; 0 in
+                               normal use, > 0 only to exercise the timeout */
+} ottb_solver_cfg;
+
+/* Per-problem scalar results, written to device memory. */
+typedef struct ottb_result {
+  double reg_ot_cost;  /* sinkhorn.py:224-277, FP64 sums                    */
+  double marginal_sum; /* sum_j of the column marginal of the final state   */
+  int32_t n_iters;     /* sinkhorn.py:432-434                               */
+  int32_t converged;   /* sinkhorn.py:1020-1023                             */
+  int32_t status;      /* OTTB_OK or OTTB_ERR_TIMEOUT                       */
+  int32_t reserved;
+} ottb_result;
+
+/* Bytes of workspace ottb_sinkhorn_pointcloud needs for these problems.
+ * Only n, m of each problem are read. Returns 0 on invalid input. */
+size_t ottb_sinkhorn_workspace_size(const ottb_problem* problems,
+                                    int32_t num_problems, int32_t d,
+                                    const ottb_solver_cfg* cfg);
+
+/* Solve num_problems independent problems of dimension d in one persistent
+ * launch. problems and cfg are host memory; results is a device array of
+ * num_problems ottb_result. Returns OTTB_OK once the work is enqueued;
+ * per-problem device-side status is in results[k].status. */
+int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems,
+                                 int32_t num_problems, int32_t d,
+                                 const ottb_solver_cfg* cfg,
+                                 ottb_result* results, void* workspace,
+                                 size_t workspace_bytes, void* stream);
+
+/* Bytes of workspace ottb_cost_stats needs. */
+size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d);
+
+/* Cost-matrix statistics of one problem without materialising it.
+ * out (device, 2 doubles): mean(C) and mean(C^2) of
+ * C_ij = inv_scale_cost * |x_i - y_j|^2 over uniform weights, from FP64
+ * moments of x and y (fixed-order reductions, deterministic). */
+int32_t ottb_cost_stats(const float* x, const float* y, int64_t n, int64_t m,
+                        int32_t d, float inv_scale_cost, double* out,
+                        void* workspace, size_t workspace_bytes,
+                        void* stream);
+
+/* Human-readable text of a status code. */
+const char* ottb_status_string(int32_t status);
+
+/* Library version, e.g. "0.1.0". */
+const char* ottb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* OTT_B200_H_ */

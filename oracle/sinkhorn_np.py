@@ -1,0 +1,432 @@
+"""CPU oracle: NumPy restatement of ott-jax's log-domain Sinkhorn on PointClouds.
+
+TEST INFRASTRUCTURE ONLY. Nothing in the ``ott_b200`` package imports this
+module; it is used by ``tests/``, ``__graft_entry__.smoke()`` and the CPU
+baseline leg of ``bench.py`` as the checker, never as the thing measured or
+shipped.
+
+Every function restates, in plain NumPy, the reference function it names
+(paths are relative to the ott-jax source tree, ``src/ott/...``).  The op
+order of the reference is kept (centre ``f + g - C``, divide by epsilon,
+max-shifted logsumexp, multiply by epsilon, subtract the finite potential) so
+that the float32 mode reproduces the reference's FP32 rounding behaviour as
+closely as a different backend can, and the float64 mode is the accuracy
+judge (the reference run with ``jax_enable_x64``).
+
+The arithmetic core of the reference lives in a third-party dependency that is
+absent here: ``jax.scipy.special.logsumexp`` (jax, unpinned ``jax>=0.4.0`` in
+``pyproject.toml``).  Its published algorithm is restated in
+:func:`logsumexp`.  The oracle is pinned against the reference's own Python
+executed over a NumPy stand-in for ``jax`` (``oracle/jaxshim``); the golden
+fixtures it produced live in ``tests/golden``.
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+DEFAULT_EPSILON_SCALE = 0.05  # geometry/epsilon_scheduler.py:22
+
+
+# ---------------------------------------------------------------------------
+# math/utils.py:132-136 -> jax.scipy.special.logsumexp (restated)
+# ---------------------------------------------------------------------------
+def logsumexp(mat: np.ndarray, axis: Optional[int] = None, b=None,
+              return_sign: bool = False):
+  """Max-shifted log-sum-exp, as jax.scipy.special.logsumexp computes it.
+
+  Published algorithm: weights ``b == 0`` mask the entry to ``-inf``; the
+  shift is the max over the reduced axis, replaced by 0 when it is not finite;
+  ``out = log(|sum(b * exp(a - shift))|) + shift``; with ``b`` given and no
+  sign requested, a negative sum yields NaN.
+  """
+  a = np.asarray(mat)
+  if b is not None:
+    b = np.asarray(b, dtype=a.dtype)
+    a, b = np.broadcast_arrays(a, b)
+    a = np.where(b != 0, a, -np.inf).astype(a.dtype)
+  with np.errstate(invalid="ignore", over="ignore"):
+    amax = np.max(a, axis=axis, keepdims=True, initial=-np.inf)
+    amax = np.where(np.isfinite(amax), amax, 0).astype(a.dtype)
+    exp_a = np.exp(a - amax)
+    if b is not None:
+      exp_a = exp_a * b
+    sumexp = np.sum(exp_a, axis=axis, keepdims=True)
+    sign = np.sign(sumexp)
+    with np.errstate(divide="ignore"):
+      out = np.log(np.abs(sumexp)) + amax
+  if axis is not None:
+    out = np.squeeze(out, axis=axis)
+    sign = np.squeeze(sign, axis=axis)
+  else:
+    out = out.reshape(())
+    sign = sign.reshape(())
+  if return_sign:
+    return out, sign
+  if b is not None:
+    out = np.where(sign < 0, np.nan, out)
+  return out
+
+
+# ---------------------------------------------------------------------------
+# geometry/costs.py:548-573 (SqEuclidean) and costs.py:82-92 (all_pairs)
+# ---------------------------------------------------------------------------
+def sq_norm(x: np.ndarray) -> np.ndarray:
+  """costs.py:554-556: ``sum(x ** 2, axis=-1)``."""
+  return np.sum(x * x, axis=-1)
+
+
+def sqeuclidean_all_pairs(x: np.ndarray, y: np.ndarray) -> np.ndarray:
+  """costs.py:558-561 applied to all pairs: ``|x|^2 + |y|^2 + (-2 <x, y>)``."""
+  cross = -2.0 * (x @ y.T)
+  return (sq_norm(x)[:, None] + sq_norm(y)[None, :]) + cross.astype(x.dtype)
+
+
+# ---------------------------------------------------------------------------
+# Geometry: epsilon and cost statistics
+# ---------------------------------------------------------------------------
+def mean_cost_matrix(x, y, inv_scale_cost=1.0) -> float:
+  """geometry.py:113-117 through pointcloud.py:170-186 (sqeucl closed form).
+
+  ``tmp = |x|^2 . vec + |y|^2 * sum(vec) - 2 y (x^T vec)`` with
+  ``vec = 1/n``, then ``sum(tmp / m)``; uniform weights by construction.
+  """
+  n, m = x.shape[0], y.shape[0]
+  vec = np.full((n,), 1.0 / n, dtype=x.dtype)
+  nx, ny = sq_norm(x), sq_norm(y)
+  applied = np.dot(nx, vec) + ny * np.sum(vec)
+  applied = applied - 2.0 * (y @ (x.T @ vec))
+  applied = inv_scale_cost * applied
+  return np.sum((1.0 / m) * applied)
+
+
+def std_cost_matrix(x, y, inv_scale_cost=1.0) -> float:
+  """geometry.py:120-135: ``sqrt(relu(mean(C^2) - mean(C)^2))``."""
+  n, m = x.shape[0], y.shape[0]
+  c = inv_scale_cost * sqeuclidean_all_pairs(x, y)
+  vec = np.full((n,), 1.0 / n, dtype=x.dtype)
+  tmp = (c * c).T @ vec
+  tmp = np.sum((1.0 / m) * tmp) - mean_cost_matrix(x, y, inv_scale_cost) ** 2
+  return np.sqrt(max(tmp, 0.0))
+
+
+def inv_scale_cost(x, y, scale_cost) -> float:
+  """pointcloud.py:343-383 for the scalings that do not need the full cost."""
+  if isinstance(scale_cost, (int, float)):
+    return 1.0 / scale_cost
+  if scale_cost == "mean":
+    return 1.0 / np.mean(sqeuclidean_all_pairs(x, y))
+  if scale_cost == "max_cost":
+    return 1.0 / np.max(sqeuclidean_all_pairs(x, y))
+  if scale_cost == "median":
+    return 1.0 / np.median(sqeuclidean_all_pairs(x, y))
+  nx, ny = sq_norm(x), sq_norm(y)
+  if scale_cost == "max_norm":
+    return 1.0 / max(nx.max(), ny.max())
+  if scale_cost == "max_bound":
+    xm, ym = nx.max(), ny.max()
+    return 1.0 / (xm + ym + 2 * np.sqrt(xm * ym))
+  raise ValueError(f"Scaling {scale_cost} not implemented.")
+
+
+def resolve_epsilon(x, y, epsilon=None, relative_epsilon=None,
+                    inv_scale=1.0) -> float:
+  """geometry.py:148-176: target epsilon of the scheduler."""
+  if relative_epsilon is None:
+    if epsilon is not None:
+      return epsilon
+    return DEFAULT_EPSILON_SCALE * std_cost_matrix(x, y, inv_scale)
+  if relative_epsilon == "std":
+    scale = std_cost_matrix(x, y, inv_scale)
+  elif relative_epsilon == "mean":
+    scale = mean_cost_matrix(x, y, inv_scale)
+  else:
+    raise ValueError(f"Invalid relative epsilon: {relative_epsilon}.")
+  mult = DEFAULT_EPSILON_SCALE if epsilon is None else epsilon
+  return mult * scale
+
+
+def epsilon_at(target, it, init=1.0, decay=1.0):
+  """epsilon_scheduler.py:47-60: ``max(init * decay**it, 1) * target``."""
+  if it is None:
+    return target
+  return max(init * (decay ** it), 1.0) * target
+
+
+# ---------------------------------------------------------------------------
+# Dense (or row/column-blocked) geometry with the lse kernel
+# ---------------------------------------------------------------------------
+@dataclass
+class Geom:
+  """A point-cloud geometry with squared-Euclidean cost.
+
+  ``batch_size`` follows pointcloud.py:438-448: ``None`` materialises the
+  cost (geometry.py:260-299); an integer recomputes it in blocks
+  (pointcloud.py:85-103), which is what lets the oracle run large inputs.
+  """
+  x: np.ndarray
+  y: np.ndarray
+  epsilon: float
+  inv_scale: float = 1.0
+  eps_init: float = 1.0
+  eps_decay: float = 1.0
+  batch_size: Optional[int] = None
+  _cost: Optional[np.ndarray] = field(default=None, repr=False)
+
+  @property
+  def dtype(self):
+    return self.x.dtype
+
+  @property
+  def shape(self):
+    return self.x.shape[0], self.y.shape[0]
+
+  def cost_block(self, rows=slice(None), cols=slice(None)):
+    if self.batch_size is None:
+      if self._cost is None:
+        self._cost = (self.inv_scale * sqeuclidean_all_pairs(self.x, self.y)
+                      ).astype(self.dtype)
+      return self._cost[rows, cols]
+    c = sqeuclidean_all_pairs(self.x[rows], self.y[cols])
+    return (self.inv_scale * c).astype(self.dtype)
+
+  def eps_at(self, it):
+    return self.dtype.type(
+        epsilon_at(self.epsilon, it, self.eps_init, self.eps_decay))
+
+  def apply_lse_kernel(self, f, g, eps, axis, vec=None):
+    """geometry.py:260-299 + _softmax :426-442 + _center :423-424.
+
+    Returns ``eps * lse((f + g - C) / eps) - finite(f or g)`` and the sign.
+    """
+    dt = self.dtype
+    eps = dt.type(eps)
+    n, m = self.shape
+    bs = self.batch_size or (m if axis == 0 else n)
+    if axis == 0:
+      out = np.empty((m,), dt)
+      sgn = np.ones((m,), dt)
+      for s in range(0, m, bs):
+        cols = slice(s, min(s + bs, m))
+        center = (f[:, None] + g[None, cols]) - self.cost_block(cols=cols)
+        r, sg = logsumexp(center / eps, axis=0,
+                          b=None if vec is None else vec[:, None],
+                          return_sign=True)
+        out[cols] = eps * r
+        sgn[cols] = sg
+      remove = g
+    else:
+      out = np.empty((n,), dt)
+      sgn = np.ones((n,), dt)
+      for s in range(0, n, bs):
+        rows = slice(s, min(s + bs, n))
+        center = (f[rows, None] + g[None, :]) - self.cost_block(rows=rows)
+        r, sg = logsumexp(center / eps, axis=1,
+                          b=None if vec is None else vec[None, :],
+                          return_sign=True)
+        out[rows] = eps * r
+        sgn[rows] = sg
+      remove = f
+    with np.errstate(invalid="ignore"):
+      res = out - np.where(np.isfinite(remove), remove, 0).astype(dt)
+    return res.astype(dt), sgn
+
+  def update_potential(self, f, g, log_marginal, iteration, axis):
+    """geometry.py:376-398."""
+    eps = self.eps_at(iteration)
+    app = self.apply_lse_kernel(f, g, eps, axis)[0]
+    with np.errstate(invalid="ignore"):
+      return (eps * log_marginal
+              - np.where(np.isfinite(app), app, 0)).astype(self.dtype)
+
+  def marginal_from_potentials(self, f, g, axis=0):
+    """geometry.py:326-349 (uses the target epsilon)."""
+    eps = self.dtype.type(self.epsilon)
+    h = f if axis == 1 else g
+    z = self.apply_lse_kernel(f, g, eps, axis)[0]
+    with np.errstate(over="ignore", invalid="ignore"):
+      return np.exp((z + h) / eps).astype(self.dtype)
+
+  def apply_transport_from_potentials(self, f, g, vec, axis=0):
+    """geometry.py:444-486: signed-weight lse applied to ``vec``."""
+    eps = self.dtype.type(self.epsilon)
+    res, sgn = self.apply_lse_kernel(f, g, eps, axis, vec=vec)
+    res = res + (f if axis == 1 else g)
+    with np.errstate(over="ignore", invalid="ignore"):
+      return (sgn * np.exp(res / eps)).astype(self.dtype)
+
+
+# ---------------------------------------------------------------------------
+# solvers/linear/sinkhorn.py
+# ---------------------------------------------------------------------------
+def marginal_error(f, g, target, geom: Geom, axis=0, norm_error=1):
+  """sinkhorn.py:191-221 (lse mode)."""
+  marginal = geom.marginal_from_potentials(f, g, axis=axis)
+  with np.errstate(invalid="ignore", over="ignore"):
+    return np.sum(np.abs(marginal - target) ** norm_error) ** (1.0 / norm_error)
+
+
+def compute_kl_reg_cost(f, g, a, b, geom: Geom):
+  """sinkhorn.py:224-277, balanced branch (tau_a == tau_b == 1)."""
+  dt = geom.dtype
+  with np.errstate(divide="ignore", invalid="ignore"):
+    fa = geom.dtype.type(geom.epsilon) * np.log(a)
+    div_a = np.sum(np.where(a > 0, a * (f - fa), 0.0).astype(dt))
+    gb = geom.dtype.type(geom.epsilon) * np.log(b)
+    div_b = np.sum(np.where(b > 0, b * (g - gb), 0.0).astype(dt))
+  total_sum = np.sum(geom.marginal_from_potentials(f, g))
+  return dt.type(div_a + div_b + geom.dtype.type(geom.epsilon)
+                 * (np.sum(a) * np.sum(b) - total_sum))
+
+
+def entr(p):
+  """jax.scipy.special.entr: ``-p log p`` (0 at 0, -inf below)."""
+  with np.errstate(divide="ignore", invalid="ignore"):
+    return np.where(p > 0, -p * np.log(np.where(p > 0, p, 1)),
+                    np.where(p == 0, 0.0, -np.inf))
+
+
+@dataclass
+class SinkhornResult:
+  f: np.ndarray
+  g: np.ndarray
+  errors: np.ndarray
+  reg_ot_cost: float
+  converged: bool
+  inner_iterations: int
+  threshold: float
+  a: np.ndarray
+  b: np.ndarray
+  epsilon: float
+
+  @property
+  def n_iters(self) -> int:
+    """sinkhorn.py:432-434."""
+    return int(np.sum(self.errors != -1) * self.inner_iterations)
+
+  @property
+  def dual_cost(self):
+    """sinkhorn.py:337-343."""
+    return (np.sum(np.where(self.a > 0, self.a * self.f, 0))
+            + np.sum(np.where(self.b > 0, self.b * self.g, 0)))
+
+  @property
+  def ent_reg_cost(self):
+    """sinkhorn.py:351-370."""
+    return self.reg_ot_cost - self.epsilon * (np.sum(entr(self.a))
+                                              + np.sum(entr(self.b)))
+
+
+def default_init(a, b, dtype):
+  """initializers.py:70-131: zeros, ``-inf`` where the weight is 0."""
+  f = np.where(a > 0, 0.0, -np.inf).astype(dtype)
+  g = np.where(b > 0, 0.0, -np.inf).astype(dtype)
+  return f, g
+
+
+def sinkhorn(geom: Geom, a=None, b=None, *, threshold=1e-3, norm_error=1,
+             inner_iterations=10, min_iterations=0, max_iterations=2000,
+             init: Optional[Tuple[np.ndarray, np.ndarray]] = None,
+             progress=None) -> SinkhornResult:
+  """sinkhorn.py:782-801 (__call__), :1052-1099 (run/iterations).
+
+  Loop: math/fixed_point_loop.py:23-93.  One iteration: sinkhorn.py:879-938
+  with the default ``Momentum()`` (weight 1, acceleration.py:161-172) and
+  sequential updates (``parallel_dual_updates=False``, :836-855).
+  """
+  dt = geom.dtype
+  n, m = geom.shape
+  a = np.full((n,), 1.0 / n, dt) if a is None else np.asarray(a, dt)
+  b = np.full((m,), 1.0 / m, dt) if b is None else np.asarray(b, dt)
+  if init is None:
+    f, g = default_init(a, b, dt)
+  else:
+    f, g = (np.asarray(init[0], dt).copy(), np.asarray(init[1], dt).copy())
+  with np.errstate(divide="ignore"):
+    log_a, log_b = np.log(a), np.log(b)
+  outer = int(math.ceil(max_iterations / inner_iterations))
+  errors = -np.ones((outer,), dt)
+
+  def momentum(old, new):
+    # acceleration.py:168-170 with weight 1
+    with np.errstate(invalid="ignore"):
+      old = np.where(np.isfinite(old), old, 0.0).astype(dt)
+      return ((dt.type(1.0) - dt.type(1.0)) * old + dt.type(1.0) * new).astype(dt)
+
+  def one_iteration(f, g, it, compute_error):
+    new_g = geom.update_potential(f, g, log_b, it, axis=0)
+    g = momentum(g, new_g)
+    new_f = geom.update_potential(f, g, log_a, it, axis=1)
+    f = momentum(f, new_f)
+    if it == max_iterations - 1 or (compute_error and it >= min_iterations):
+      err = marginal_error(f, g, b, geom, 0, norm_error)
+    else:
+      err = np.inf
+    errors[it // inner_iterations] = err
+    if progress is not None:
+      progress(it, f, g, errors)
+    return f, g
+
+  def cond(it):
+    # sinkhorn.py:940-953
+    err = errors[it // inner_iterations - 1]
+    converged = it > 0 and err < threshold
+    diverged = not np.isfinite(err)
+    return (not diverged) and (not converged)
+
+  it = 0
+  force_scan = min_iterations == max_iterations
+  if force_scan:
+    for _ in range(max_iterations // inner_iterations):
+      for k in range(inner_iterations):
+        f, g = one_iteration(f, g, it, k == inner_iterations - 1)
+        it += 1
+  else:
+    while it < max_iterations and (it < min_iterations or cond(it)):
+      for k in range(inner_iterations):
+        f, g = one_iteration(f, g, it, k == inner_iterations - 1)
+        it += 1
+  # sinkhorn.py:1020-1023
+  converged = bool((not np.any(np.isnan(errors))) and errors[-1] < threshold)
+  cost = compute_kl_reg_cost(f, g, a, b, geom)
+  return SinkhornResult(f=f, g=g, errors=errors, reg_ot_cost=cost,
+                        converged=converged, inner_iterations=inner_iterations,
+                        threshold=threshold, a=a, b=b, epsilon=geom.epsilon)
+
+
+def solve(x, y=None, a=None, b=None, *, epsilon=None, relative_epsilon=None,
+          scale_cost=1.0, batch_size=None, eps_init=1.0, eps_decay=1.0,
+          dtype=np.float64, **kw) -> SinkhornResult:
+  """_solve.py:29-64 on ``PointCloud(x, y, epsilon, relative_epsilon)``."""
+  x = np.asarray(x, dtype)
+  y = x if y is None else np.asarray(y, dtype)
+  inv = inv_scale_cost(x, y, scale_cost)
+  eps = resolve_epsilon(x, y, epsilon, relative_epsilon, inv)
+  geom = Geom(x, y, float(eps), inv_scale=float(inv), eps_init=eps_init,
+              eps_decay=eps_decay, batch_size=batch_size)
+  return sinkhorn(geom, a, b, **kw)
+
+
+# ---------------------------------------------------------------------------
+# Learned initializer objective (initializers/neural/meta_initializer.py)
+# ---------------------------------------------------------------------------
+def meta_dual_loss(f_pred, a, b, geom: Geom):
+  """meta_initializer.py:163-175: ``-compute_kl_reg_cost(f, g(f))``.
+
+  ``g(f) = update_potential(f, 0, log b, 0, axis=0)`` with non-finite entries
+  replaced by 0.  Returns ``(loss, dloss/df)``; the gradient follows from
+  ``g(f)`` being the exact maximiser of the dual in ``g`` (envelope theorem):
+  ``d(-J)/df = -(a - rowmarginal(f, g(f)))`` on the support of ``a``.
+  """
+  dt = geom.dtype
+  with np.errstate(divide="ignore"):
+    log_b = np.log(b)
+  g = geom.update_potential(f_pred, np.zeros_like(b), log_b, 0, axis=0)
+  g = np.where(np.isfinite(g), g, 0.0).astype(dt)
+  loss = -compute_kl_reg_cost(f_pred, g, a, b, geom)
+  row_marg = geom.marginal_from_potentials(f_pred, g, axis=1)
+  grad = -(np.where(a > 0, a, 0.0) - row_marg)
+  return loss, grad

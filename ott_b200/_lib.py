@@ -1,0 +1,138 @@
+"""ctypes binding of the ott_b200 C ABI (``include/ott_b200.h``).
+
+The shared library is built in-tree (``ott_b200/_lib/libottb200.so``) by
+``ott_b200.build``. There is no fallback: if the library or a CUDA device is
+missing, calls raise.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from typing import Optional
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libottb200.so")
+
+OTTB_OK = 0
+OTTB_ERR_INVALID = 1
+OTTB_ERR_UNSUPPORTED = 2
+OTTB_ERR_CUDA = 3
+OTTB_ERR_TIMEOUT = 4
+OTTB_ERR_WORKSPACE = 5
+OTTB_ERR_NO_DEVICE = 6
+
+PRECISION_AUTO = -1
+PRECISION_FP32 = 0
+PRECISION_BF16_SPLIT3 = 1
+
+EXPORTED_SYMBOLS = (
+    "ottb_sinkhorn_workspace_size",
+    "ottb_sinkhorn_pointcloud",
+    "ottb_cost_stats_workspace_size",
+    "ottb_cost_stats",
+    "ottb_status_string",
+    "ottb_version",
+)
+
+
+class OttbProblem(ctypes.Structure):
+  _fields_ = [
+      ("x", ctypes.c_void_p),
+      ("y", ctypes.c_void_p),
+      ("a", ctypes.c_void_p),
+      ("b", ctypes.c_void_p),
+      ("f_init", ctypes.c_void_p),
+      ("g_init", ctypes.c_void_p),
+      ("f", ctypes.c_void_p),
+      ("g", ctypes.c_void_p),
+      ("errors", ctypes.c_void_p),
+      ("n", ctypes.c_int64),
+      ("m", ctypes.c_int64),
+      ("epsilon", ctypes.c_float),
+      ("inv_scale_cost", ctypes.c_float),
+  ]
+
+
+class OttbSolverCfg(ctypes.Structure):
+  _fields_ = [
+      ("threshold", ctypes.c_float),
+      ("norm_error", ctypes.c_int32),
+      ("inner_iterations", ctypes.c_int32),
+      ("min_iterations", ctypes.c_int32),
+      ("max_iterations", ctypes.c_int32),
+      ("eps_init", ctypes.c_float),
+      ("eps_decay", ctypes.c_float),
+      ("precision", ctypes.c_int32),
+      ("mask_init", ctypes.c_int32),
+      ("timeout_ms", ctypes.c_int32),
+      ("phantom_arrivals", ctypes.c_int32),
+  ]
+
+
+class OttbResult(ctypes.Structure):
+  _fields_ = [
+      ("reg_ot_cost", ctypes.c_double),
+      ("marginal_sum", ctypes.c_double),
+      ("n_iters", ctypes.c_int32),
+      ("converged", ctypes.c_int32),
+      ("status", ctypes.c_int32),
+      ("reserved", ctypes.c_int32),
+  ]
+
+
+RESULT_BYTES = ctypes.sizeof(OttbResult)
+
+_lock = threading.Lock()
+_lib: Optional[ctypes.CDLL] = None
+
+
+class OttbError(RuntimeError):
+  """A C-ABI call returned a non-OK status."""
+
+  def __init__(self, status: int, what: str):
+    self.status = status
+    super().__init__(f"{what}: {status_string(status)} (status {status})")
+
+
+def load() -> ctypes.CDLL:
+  """Loads the library (once). Raises if it has not been built."""
+  global _lib
+  with _lock:
+    if _lib is not None:
+      return _lib
+    if not os.path.exists(LIB_PATH):
+      raise RuntimeError(
+          f"libottb200.so not found at {LIB_PATH}; build it with "
+          "`python -m ott_b200.build`")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp, sz, i32, i64 = ctypes.c_void_p, ctypes.c_size_t, ctypes.c_int32, ctypes.c_int64
+    lib.ottb_sinkhorn_workspace_size.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg)]
+    lib.ottb_sinkhorn_workspace_size.restype = sz
+    lib.ottb_sinkhorn_pointcloud.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg),
+        vp, vp, sz, vp]
+    lib.ottb_sinkhorn_pointcloud.restype = i32
+    lib.ottb_cost_stats_workspace_size.argtypes = [i64, i64, i32]
+    lib.ottb_cost_stats_workspace_size.restype = sz
+    lib.ottb_cost_stats.argtypes = [vp, vp, i64, i64, i32, ctypes.c_float, vp, vp, sz, vp]
+    lib.ottb_cost_stats.restype = i32
+    lib.ottb_status_string.argtypes = [i32]
+    lib.ottb_status_string.restype = ctypes.c_char_p
+    lib.ottb_version.argtypes = []
+    lib.ottb_version.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def status_string(status: int) -> str:
+  try:
+    return load().ottb_status_string(int(status)).decode()
+  except Exception:  # library not loadable: still give a message
+    return f"status {status}"
+
+
+def check(status: int, what: str) -> None:
+  if status != OTTB_OK:
+    raise OttbError(status, what)

@@ -1,0 +1,60 @@
+"""Builds libottb200.so in-tree for sm_100a.
+
+``python -m ott_b200.build`` compiles ``ott_b200/csrc/capi.cu`` (which
+includes every kernel) with nvcc into ``ott_b200/_lib/libottb200.so``.
+Runs without a GPU (nvcc cross-compiles).
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+CSRC = os.path.join(HERE, "csrc")
+OUT_DIR = os.path.join(HERE, "_lib")
+OUT = os.path.join(OUT_DIR, "libottb200.so")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def nvcc() -> str:
+  for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+    if cand and os.path.exists(cand):
+      return cand
+  raise RuntimeError("nvcc not found")
+
+
+def sources():
+  return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
+                if f.endswith((".cu", ".cuh", ".h")))
+
+
+def up_to_date() -> bool:
+  if not os.path.exists(OUT):
+    return False
+  t = os.path.getmtime(OUT)
+  deps = sources() + [os.path.join(HERE, "..", "include", "ott_b200.h"), __file__]
+  return all(os.path.getmtime(s) <= t for s in deps if os.path.exists(s))
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+  if not force and up_to_date():
+    return OUT
+  os.makedirs(OUT_DIR, exist_ok=True)
+  cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+         "-shared", "-o", OUT + ".tmp", os.path.join(CSRC, "capi.cu")]
+  if verbose:
+    cmd.insert(1, "-Xptxas=-v")
+  r = subprocess.run(cmd, capture_output=True, text=True)
+  if r.returncode != 0:
+    sys.stderr.write(r.stdout + r.stderr)
+    raise RuntimeError("nvcc failed building libottb200.so")
+  if verbose:
+    sys.stderr.write(r.stderr)
+  os.replace(OUT + ".tmp", OUT)
+  return OUT
+
+
+if __name__ == "__main__":
+  print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

@@ -1,0 +1,429 @@
+// C-ABI entry points of libottb200 (declared in include/ott_b200.h).
+//
+// Host side of the solve: argument checks, the work plan (padding, column
+// splits, workspace layout), the device tables and the launch sequence
+//   fill errors -> prep points -> init potentials -> persistent loop
+//   (cooperative) -> finalize.
+// Nothing here allocates device memory: all scratch lives in the caller's
+// workspace.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "aux_kernels.cuh"
+#include "kernel_simt.cuh"
+
+using namespace ottb;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+inline int64_t round_up(int64_t v, int64_t a) { return (v + a - 1) / a * a; }
+
+struct DeviceInfo {
+  int sms = 0;
+  int major = 0;
+  int minor = 0;
+};
+
+DeviceInfo device_info() {
+  static std::mutex mu;
+  static DeviceInfo cache[64];
+  static bool have[64] = {false};
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return DeviceInfo{};
+  std::lock_guard<std::mutex> lock(mu);
+  if (!have[dev]) {
+    DeviceInfo di;
+    cudaDeviceGetAttribute(&di.sms, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&di.major, cudaDevAttrComputeCapabilityMajor, dev);
+    cudaDeviceGetAttribute(&di.minor, cudaDevAttrComputeCapabilityMinor, dev);
+    cache[dev] = di;
+    have[dev] = true;
+  }
+  return cache[dev];
+}
+
+int simt_dp(int d) {
+  int dp = 2;
+  while (dp < d) dp <<= 1;
+  return dp;
+}
+
+// Kernel table for the CUDA-core engine.
+template <int DP>
+struct SimtKernel {
+  static void* fn() { return (void*)&sinkhorn_simt_kernel<DP>; }
+  static size_t smem() { return sizeof(SimtKernelSmem<DP>); }
+};
+
+struct KernelChoice {
+  void* fn = nullptr;
+  size_t smem = 0;
+  int threads = 256;
+};
+
+KernelChoice pick_simt(int dp) {
+  KernelChoice k;
+  switch (dp) {
+    case 2: k.fn = SimtKernel<2>::fn(); k.smem = SimtKernel<2>::smem(); break;
+    case 4: k.fn = SimtKernel<4>::fn(); k.smem = SimtKernel<4>::smem(); break;
+    case 8: k.fn = SimtKernel<8>::fn(); k.smem = SimtKernel<8>::smem(); break;
+    case 16: k.fn = SimtKernel<16>::fn(); k.smem = SimtKernel<16>::smem(); break;
+    case 32: k.fn = SimtKernel<32>::fn(); k.smem = SimtKernel<32>::smem(); break;
+    case 64: k.fn = SimtKernel<64>::fn(); k.smem = SimtKernel<64>::smem(); break;
+    case 128: k.fn = SimtKernel<128>::fn(); k.smem = SimtKernel<128>::smem(); break;
+    default: break;
+  }
+  return k;
+}
+
+// Grid size of the persistent launch: all CTAs co-resident.
+int persistent_grid(const KernelChoice& k, int sms) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  if (cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           (int)k.smem) != cudaSuccess)
+    return 0;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem) !=
+      cudaSuccess)
+    return 0;
+  return per_sm * sms;
+}
+
+// Column splits of one sweep: enough units to keep every CTA busy with
+// little tail (efficiency = units / (waves * grid)).
+int choose_split(int rb, int ntiles, int grid, int num_problems) {
+  if (num_problems > 1 || grid <= 0) return 1;
+  int best = 1;
+  double best_score = -1.0;
+  const int smax = std::max(1, std::min(ntiles, 32));
+  for (int s = 1; s <= smax; ++s) {
+    const double units = (double)rb * s;
+    const double waves = std::ceil(units / grid);
+    const double eff = units / (waves * grid);
+    const double score = eff - 0.004 * s;
+    if (score > best_score + 1e-9) {
+      best_score = score;
+      best = s;
+    }
+  }
+  return best;
+}
+
+struct ProbPlan {
+  int64_t n, m, n_pad, m_pad;
+  int rb_f, rb_g, split_f, split_g;
+  size_t off_xt, off_yt, off_nx, off_ny, off_galt, off_pm, off_pl, off_arr, off_err,
+      off_msum;
+};
+
+struct Plan {
+  int num = 0;
+  int dp = 0;
+  int grid = 0;
+  KernelChoice kern;
+  size_t off_globals = 0, off_sched = 0, off_probs = 0, off_state = 0, off_ids = 0,
+         off_prefix = 0, off_eval_ids = 0, off_eval_prefix = 0, off_ptrs = 0;
+  size_t header_bytes = 0;
+  size_t total = 0;
+  std::vector<ProbPlan> probs;
+  std::vector<int> order;  // table position -> caller index
+};
+
+int validate_cfg(const ottb_solver_cfg* cfg) {
+  if (!cfg) return OTTB_ERR_INVALID;
+  if (cfg->inner_iterations < 1 || cfg->max_iterations < 0 || cfg->min_iterations < 0)
+    return OTTB_ERR_INVALID;
+  if (cfg->norm_error < 1) return OTTB_ERR_UNSUPPORTED;
+  if (!(cfg->eps_decay <= 1.0f) || !(cfg->eps_init > 0.0f)) return OTTB_ERR_INVALID;
+  return OTTB_OK;
+}
+
+int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* cfg,
+              bool need_grid, Plan& plan) {
+  if (!probs || num < 1 || d < 1) return OTTB_ERR_INVALID;
+  int st = validate_cfg(cfg);
+  if (st != OTTB_OK) return st;
+  if (d > 128) return OTTB_ERR_UNSUPPORTED;
+  if (cfg->precision == OTTB_PRECISION_BF16_SPLIT3) return OTTB_ERR_UNSUPPORTED;
+  plan.num = num;
+  plan.dp = simt_dp(d);
+  plan.kern = pick_simt(plan.dp);
+  if (!plan.kern.fn) return OTTB_ERR_UNSUPPORTED;
+  if (need_grid) {
+    DeviceInfo di = device_info();
+    if (di.sms <= 0) return OTTB_ERR_NO_DEVICE;
+    if (di.major < 10) return OTTB_ERR_NO_DEVICE;
+    plan.grid = persistent_grid(plan.kern, di.sms);
+    if (plan.grid <= 0) return OTTB_ERR_CUDA;
+  } else {
+    plan.grid = 148;
+  }
+  // Problems ordered by decreasing work so the atomic queue deals the
+  // largest units first.
+  plan.order.resize(num);
+  for (int i = 0; i < num; ++i) {
+    if (probs[i].n < 1 || probs[i].m < 1) return OTTB_ERR_INVALID;
+    if (probs[i].n > (int64_t)1 << 31 || probs[i].m > (int64_t)1 << 31) return OTTB_ERR_UNSUPPORTED;
+    plan.order[i] = i;
+  }
+  std::stable_sort(plan.order.begin(), plan.order.end(), [&](int a, int b) {
+    return (double)probs[a].n * probs[a].m > (double)probs[b].n * probs[b].m;
+  });
+  size_t off = 0;
+  plan.off_globals = off; off = align_up(off + sizeof(Globals));
+  plan.off_sched = off; off = align_up(off + sizeof(Sched));
+  plan.off_probs = off; off = align_up(off + sizeof(ProbDev) * num);
+  plan.off_state = off; off = align_up(off + sizeof(ProbState) * num);
+  plan.off_ids = off; off = align_up(off + sizeof(int) * num);
+  plan.off_prefix = off; off = align_up(off + sizeof(int) * 2 * (num + 1));
+  plan.off_eval_ids = off; off = align_up(off + sizeof(int) * num);
+  plan.off_eval_prefix = off; off = align_up(off + sizeof(int) * (num + 1));
+  plan.off_ptrs = off; off = align_up(off + sizeof(float*) * 4 * num);
+  plan.header_bytes = off;
+  plan.probs.resize(num);
+  for (int t = 0; t < num; ++t) {
+    const ottb_problem& q = probs[plan.order[t]];
+    ProbPlan& pp = plan.probs[t];
+    pp.n = q.n;
+    pp.m = q.m;
+    pp.n_pad = round_up(q.n, kBM);
+    pp.m_pad = round_up(q.m, kBM);
+    pp.rb_f = (int)(pp.n_pad / kBM);
+    pp.rb_g = (int)(pp.m_pad / kBM);
+    pp.split_f = choose_split(pp.rb_f, (int)(pp.m_pad / kBN), plan.grid, num);
+    pp.split_g = choose_split(pp.rb_g, (int)(pp.n_pad / kBN), plan.grid, num);
+    const size_t fsz = sizeof(float);
+    pp.off_xt = off; off = align_up(off + fsz * plan.dp * pp.n_pad);
+    pp.off_yt = off; off = align_up(off + fsz * plan.dp * pp.m_pad);
+    pp.off_nx = off; off = align_up(off + fsz * pp.n_pad);
+    pp.off_ny = off; off = align_up(off + fsz * pp.m_pad);
+    pp.off_galt = off; off = align_up(off + fsz * pp.m);
+    // Partials are sized for the largest split any grid could choose, so the
+    // workspace size does not depend on the device the call runs on.
+    const int64_t smax_f = num > 1 ? 1 : std::min<int64_t>(32, pp.m_pad / kBN);
+    const int64_t smax_g = num > 1 ? 1 : std::min<int64_t>(32, pp.n_pad / kBN);
+    const int64_t parts = std::max(smax_f * pp.n, smax_g * pp.m);
+    const bool split = smax_f > 1 || smax_g > 1;
+    pp.off_pm = off; off = align_up(off + (split ? fsz * parts : 0));
+    pp.off_pl = off; off = align_up(off + (split ? fsz * parts : 0));
+    pp.off_arr = off; off = align_up(off + sizeof(int) * std::max(pp.rb_f, pp.rb_g));
+    pp.off_err = off; off = align_up(off + sizeof(double) * pp.rb_g);
+    pp.off_msum = off; off = align_up(off + sizeof(double) * pp.rb_g);
+  }
+  plan.total = off;
+  return OTTB_OK;
+}
+
+inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA; }
+
+}  // namespace
+
+extern "C" {
+
+const char* ottb_version(void) { return "0.1.0"; }
+
+const char* ottb_status_string(int32_t status) {
+  switch (status) {
+    case OTTB_OK: return "ok";
+    case OTTB_ERR_INVALID: return "invalid argument";
+    case OTTB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case OTTB_ERR_CUDA: return "CUDA runtime error";
+    case OTTB_ERR_TIMEOUT: return "device wait timed out";
+    case OTTB_ERR_WORKSPACE: return "workspace missing or too small";
+    case OTTB_ERR_NO_DEVICE: return "no sm_100 device";
+    default: return "unknown status";
+  }
+}
+
+size_t ottb_sinkhorn_workspace_size(const ottb_problem* problems, int32_t num_problems,
+                                    int32_t d, const ottb_solver_cfg* cfg) {
+  Plan plan;
+  // The split choice depends on the grid; size for the largest grid this
+  // device can run so the plan at solve time always fits.
+  if (make_plan(problems, num_problems, d, cfg, true, plan) != OTTB_OK) {
+    if (make_plan(problems, num_problems, d, cfg, false, plan) != OTTB_OK) return 0;
+  }
+  return plan.total;
+}
+
+int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_problems,
+                                 int32_t d, const ottb_solver_cfg* cfg,
+                                 ottb_result* results, void* workspace,
+                                 size_t workspace_bytes, void* stream_ptr) {
+  if (!results) return OTTB_ERR_INVALID;
+  for (int i = 0; i < num_problems && problems; ++i) {
+    const ottb_problem& q = problems[i];
+    if (!q.x || !q.y || !q.a || !q.b || !q.f || !q.g || !q.errors) return OTTB_ERR_INVALID;
+    if (!(q.epsilon > 0.0f) || !std::isfinite(q.epsilon)) return OTTB_ERR_INVALID;
+    if (!(q.inv_scale_cost > 0.0f) || !std::isfinite(q.inv_scale_cost)) return OTTB_ERR_INVALID;
+  }
+  Plan plan;
+  int st = make_plan(problems, num_problems, d, cfg, true, plan);
+  if (st != OTTB_OK) return st;
+  if (!workspace || workspace_bytes < plan.total) return OTTB_ERR_WORKSPACE;
+  if (((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  char* ws = (char*)workspace;
+  const int outer = (int)std::ceil((double)cfg->max_iterations / cfg->inner_iterations);
+
+  // Host image of the header: globals, schedule, tables.
+  std::vector<char> host(plan.header_bytes, 0);
+  Sched* sched = (Sched*)(host.data() + plan.off_sched);
+  ProbDev* pd = (ProbDev*)(host.data() + plan.off_probs);
+  ProbState* ps = (ProbState*)(host.data() + plan.off_state);
+  int* ids = (int*)(host.data() + plan.off_ids);
+  int* prefix = (int*)(host.data() + plan.off_prefix);
+  const float** ptrs = (const float**)(host.data() + plan.off_ptrs);
+  int ug = 0, uf = 0;
+  for (int t = 0; t < num_problems; ++t) {
+    const ottb_problem& q = problems[plan.order[t]];
+    const ProbPlan& pp = plan.probs[t];
+    ProbDev P;
+    std::memset(&P, 0, sizeof(P));
+    P.a = q.a;
+    P.b = q.b;
+    P.f = q.f;
+    P.gbuf[0] = q.g;
+    P.gbuf[1] = (float*)(ws + pp.off_galt);
+    P.errors = q.errors;
+    P.xt = (const float*)(ws + pp.off_xt);
+    P.yt = (const float*)(ws + pp.off_yt);
+    P.nx = (const float*)(ws + pp.off_nx);
+    P.ny = (const float*)(ws + pp.off_ny);
+    P.part_m = (float*)(ws + pp.off_pm);
+    P.part_l = (float*)(ws + pp.off_pl);
+    P.arrive = (int*)(ws + pp.off_arr);
+    P.err_part = (double*)(ws + pp.off_err);
+    P.msum_part = (double*)(ws + pp.off_msum);
+    P.n = pp.n;
+    P.m = pp.m;
+    P.n_pad = pp.n_pad;
+    P.m_pad = pp.m_pad;
+    P.rb_f = pp.rb_f;
+    P.rb_g = pp.rb_g;
+    P.split_f = pp.split_f;
+    P.split_g = pp.split_g;
+    P.eps_target = q.epsilon;
+    P.inv_scale = q.inv_scale_cost;
+    P.uid = plan.order[t];
+    P.outer = outer;
+    pd[t] = P;
+    ps[t].active = 1;
+    ids[t] = t;
+    prefix[t] = ug;
+    prefix[num_problems + 1 + t] = uf;
+    ug += pp.rb_g * pp.split_g;
+    uf += pp.rb_f * pp.split_f;
+    ptrs[2 * t] = q.x;
+    ptrs[2 * t + 1] = q.y;
+    ptrs[2 * num_problems + 2 * t] = q.f_init;
+    ptrs[2 * num_problems + 2 * t + 1] = q.g_init;
+  }
+  prefix[num_problems] = ug;
+  prefix[2 * num_problems + 1] = uf;
+  sched->num_active = num_problems;
+  sched->total_units[0] = ug;
+  sched->total_units[1] = uf;
+  sched->status = OTTB_OK;
+
+  cudaError_t e;
+  e = cudaMemcpyAsync(ws, host.data(), plan.header_bytes, cudaMemcpyHostToDevice, stream);
+  if (e != cudaSuccess) return OTTB_ERR_CUDA;
+  for (int t = 0; t < num_problems; ++t) {
+    const ProbPlan& pp = plan.probs[t];
+    e = cudaMemsetAsync(ws + pp.off_arr, 0, sizeof(int) * std::max(pp.rb_f, pp.rb_g), stream);
+    if (e != cudaSuccess) return OTTB_ERR_CUDA;
+  }
+  ProbDev* d_probs = (ProbDev*)(ws + plan.off_probs);
+  const float* const* d_ptrs = (const float* const*)(ws + plan.off_ptrs);
+  int64_t maxpts = 1;
+  for (const ProbPlan& pp : plan.probs) maxpts = std::max(maxpts, std::max(pp.n_pad, pp.m_pad) + pp.n + pp.m);
+
+  {
+    dim3 grid(std::max(1, (outer + 255) / 256), num_problems);
+    fill_errors_kernel<<<grid, 256, 0, stream>>>(d_probs);
+  }
+  {
+    PrepArgs pa{d_ptrs, d_probs, d, plan.dp};
+    int64_t mx = 1;
+    for (const ProbPlan& pp : plan.probs) mx = std::max(mx, std::max(pp.n_pad, pp.m_pad));
+    dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, 1024), num_problems, 2);
+    prep_points_kernel<<<grid, 256, 0, stream>>>(pa);
+  }
+  {
+    InitArgs ia{d_ptrs + 2 * num_problems, d_probs, cfg->mask_init};
+    dim3 grid((unsigned)std::min<int64_t>((maxpts + 255) / 256, 1024), num_problems);
+    init_potentials_kernel<<<grid, 256, 0, stream>>>(ia);
+  }
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return OTTB_ERR_CUDA;
+
+  KernelArgs ka;
+  std::memset(&ka, 0, sizeof(ka));
+  ka.probs = d_probs;
+  ka.state = (ProbState*)(ws + plan.off_state);
+  ka.sched = (Sched*)(ws + plan.off_sched);
+  ka.gl = (Globals*)(ws + plan.off_globals);
+  ka.active_ids = (int*)(ws + plan.off_ids);
+  ka.prefix = (int*)(ws + plan.off_prefix);
+  ka.eval_ids = (int*)(ws + plan.off_eval_ids);
+  ka.eval_prefix = (int*)(ws + plan.off_eval_prefix);
+  ka.num_problems = num_problems;
+  ka.dynamic_units = num_problems > 1 ? 1 : 0;
+  ka.expected_arrivals = (unsigned)plan.grid + (unsigned)std::max(0, cfg->phantom_arrivals);
+  const int tmo = cfg->timeout_ms > 0 ? cfg->timeout_ms : 60000;
+  ka.timeout_ns = (uint64_t)tmo * 1000000ull;
+  ka.cfg = *cfg;
+  void* kargs[] = {&ka};
+  e = cudaLaunchCooperativeKernel(plan.kern.fn, dim3(plan.grid), dim3(plan.kern.threads), kargs,
+                                  plan.kern.smem, stream);
+  if (e != cudaSuccess) return OTTB_ERR_CUDA;
+
+  FinalArgs fa{d_probs, ka.state, ka.sched, results, *cfg};
+  finalize_kernel<<<num_problems, 512, 0, stream>>>(fa);
+  return cuda_status(cudaGetLastError());
+}
+
+size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {
+  if (n < 1 || m < 1 || d < 1 || d > 128) return 0;
+  const size_t K = 3 + 2 * (size_t)d + (size_t)d * d;
+  return align_up(sizeof(double) * K * 2 * 148) + align_up(sizeof(double) * 2 * K);
+}
+
+int32_t ottb_cost_stats(const float* x, const float* y, int64_t n, int64_t m, int32_t d,
+                        float inv_scale_cost, double* out, void* workspace,
+                        size_t workspace_bytes, void* stream_ptr) {
+  if (!x || !y || !out || n < 1 || m < 1 || d < 1) return OTTB_ERR_INVALID;
+  if (d > 128) return OTTB_ERR_UNSUPPORTED;
+  const size_t need = ottb_cost_stats_workspace_size(n, m, d);
+  if (!workspace || workspace_bytes < need) return OTTB_ERR_WORKSPACE;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  const int K = 3 + 2 * d + d * d;
+  const int nblk = 148;
+  double* px = (double*)workspace;
+  double* py = px + (size_t)K * nblk;
+  double* mom = (double*)((char*)workspace + align_up(sizeof(double) * K * 2 * 148));
+  const size_t smem = sizeof(double) * K + sizeof(float) * 64 * d;
+  static std::mutex mu;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    if (cudaFuncSetAttribute((void*)moments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess)
+      return OTTB_ERR_CUDA;
+  }
+  moments_kernel<<<nblk, 256, smem, stream>>>(x, n, d, px);
+  moments_kernel<<<nblk, 256, smem, stream>>>(y, m, d, py);
+  cost_stats_reduce_kernel<<<1, 256, 0, stream>>>(px, py, nblk, d, (double)inv_scale_cost, mom,
+                                                  out);
+  return cuda_status(cudaGetLastError());
+}
+
+}  // extern "C"

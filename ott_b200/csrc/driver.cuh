@@ -1,0 +1,135 @@
+// Persistent Sinkhorn driver: the whole fixed-point loop of every problem of
+// a call runs inside one cooperative launch.
+//
+// Mirrors ott/math/fixed_point_loop.py:23-93 (blocks of inner_iterations,
+// stop test between blocks, scan mode when min == max) and
+// ott/solvers/linear/sinkhorn.py:879-953 (g-update then f-update, the error
+// of a block's last iteration, converged / diverged tests). The marginal
+// error of the state after a block is read off the next g-sweep, which
+// computes the same column log-sum-exp: b_hat_j = 2^(lse2_j + (g_j -
+// inv |y_j|^2) log2(e) / eps). That sweep's new g goes to a second buffer
+// and is dropped if the problem stops, so the returned (f, g) is exactly
+// the state the reference returns.
+#pragma once
+
+#include "common.cuh"
+
+namespace ottb {
+
+struct KernelArgs {
+  ProbDev* probs;
+  ProbState* state;
+  Sched* sched;
+  Globals* gl;
+  int* active_ids;   // [P] problems in schedule order
+  int* prefix;       // [2][P + 1] unit prefix sums (g-sweep, f-sweep)
+  int* eval_ids;     // [P]
+  int* eval_prefix;  // [P + 1]
+  int num_problems;
+  int dynamic_units;
+  unsigned expected_arrivals;
+  uint64_t timeout_ns;
+  ottb_solver_cfg cfg;
+};
+
+struct SweepParams {
+  int kind;      // kSweepG / kSweepF
+  float mult;    // epsilon multiplier of this sweep
+  int eval;      // compute the column marginal (g-sweeps only)
+  int write;     // write the new potential
+  int final_eval;  // use the eval list and each problem's final parity
+  int parity;    // g parity of active problems
+};
+
+__device__ __forceinline__ float eps_mult(const ottb_solver_cfg& c, int it) {
+  // epsilon_scheduler.py:47-60: max(init * decay^it, 1)
+  float mlt = c.eps_init * powf(c.eps_decay, (float)it);
+  return fmaxf(mlt, 1.0f);
+}
+
+// Exponent scale of a sweep, log2(e) / eps in FP32; the single source of
+// this value for the sweep engines and the potential update.
+__device__ __forceinline__ float sweep_wscale(const ProbDev& P, float mult) {
+  return (float)(kLog2eD / ((double)P.eps_target * (double)mult));
+}
+
+__device__ __forceinline__ SweepOperands make_operands(const ProbDev& P, int kind,
+                                                       const float* gcur) {
+  SweepOperands op;
+  if (kind == kSweepG) {
+    op.At = P.yt; op.a_pad = P.m_pad; op.rows = P.m;
+    op.Bt = P.xt; op.b_pad = P.n_pad; op.cols = P.n;
+    op.potB = P.f; op.nb = P.nx;
+  } else {
+    op.At = P.xt; op.a_pad = P.n_pad; op.rows = P.n;
+    op.Bt = P.yt; op.b_pad = P.m_pad; op.cols = P.m;
+    op.potB = gcur; op.nb = P.ny;
+  }
+  return op;
+}
+
+// Block-wide sum of one double per thread (threads 0..kBM-1 contribute),
+// fixed-order tree so the result is deterministic.
+__device__ __forceinline__ double block_sum_128(double v, double* red) {
+  int t = threadIdx.x;
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  if (t < kBM && (t & 31) == 0) red[t >> 5] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (t == 0) r = (red[0] + red[1]) + (red[2] + red[3]);
+  __syncthreads();
+  return r;
+}
+
+// Potential update and (optionally) marginal for the rows of one row block,
+// from their base-2 LSE state. geometry.py:376-398 / :326-349.
+__device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parity,
+                              int rb, const float* rm, const float* rl,
+                              int norm_error, double* red) {
+  const int t = threadIdx.x;
+  const bool isG = sp.kind == kSweepG;
+  const int64_t R = isG ? P.m : P.n;
+  const float* marg = isG ? P.b : P.a;
+  const float* na = isG ? P.ny : P.nx;
+  const float* oldp = isG ? P.gbuf[parity] : P.f;
+  float* outp = isG ? P.gbuf[parity ^ 1] : P.f;
+  // The sweep scaled every exponent by the FP32 value ws = log2(e) / eps;
+  // the update uses the epsilon that ws stands for, eps = log2(e) / ws, in
+  // both of its terms. A mismatch between the two would bias the f- and
+  // g-updates differently, and such a bias accumulates along the neutral
+  // direction (f + c, g - c) of the iteration.
+  const float ws = sweep_wscale(P, sp.mult);
+  const double eps = kLog2eD / (double)ws;
+  double err_t = 0.0, msum_t = 0.0;
+  const int64_t r = (int64_t)rb * kBM + t;
+  if (t < kBM && r < R) {
+    const float mv = rm[t], lv = rl[t];
+    double lse2 = (lv > 0.f) ? (double)mv + log2((double)lv)
+                             : (lv == 0.f ? -INFINITY : (double)NAN);
+    const double nrm = (double)na[r];
+    const double app = eps * kLn2 * lse2 - nrm;
+    const double old = (double)__ldcg(oldp + r);
+    const double mg = (double)marg[r];
+    const double logm = log(mg);
+    const bool keep = isfinite(old) && isfinite(app);
+    const double newp = eps * logm - (keep ? app : 0.0);
+    if (sp.write) outp[r] = (float)newp;
+    if (sp.eval) {
+      double bh = 0.0;
+      if (!(old == -INFINITY)) bh = exp2(lse2 + (old - nrm) * (double)ws);
+      double dv = fabs(bh - mg);
+      err_t = (norm_error == 1) ? dv : pow(dv, (double)norm_error);
+      msum_t = bh;
+    }
+  }
+  if (sp.eval) {
+    double e = block_sum_128(err_t, red);
+    double s = block_sum_128(msum_t, red);
+    if (t == 0) {
+      P.err_part[rb] = e;
+      P.msum_part[rb] = s;
+    }
+  }
+}
+
+}  // namespace ottb

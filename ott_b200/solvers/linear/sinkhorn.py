@@ -1,0 +1,317 @@
+"""Sinkhorn solver (ott/solvers/linear/sinkhorn.py), log-domain, on B200.
+
+``Sinkhorn.__call__`` mirrors sinkhorn.py:782-801: run the initializer (or
+take ``init``), then one C-ABI call (``ottb_sinkhorn_pointcloud``) runs the
+whole fixed-point loop of fixed_point_loop.py:23-93 in one persistent
+launch and fills ``f``, ``g``, ``errors`` and the scalar results
+(``reg_ot_cost``, ``n_iters``, ``converged``).
+
+Supported: balanced problems, ``lse_mode=True``, default ``Momentum()``
+(weight 1), sequential updates, ``norm_error >= 1``, epsilon schedules,
+``min_iterations`` / ``max_iterations`` / ``inner_iterations``, warm starts
+through ``init=(f, g)`` or an initializer. Everything else raises
+``NotImplementedError`` rather than silently changing the algorithm.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+from typing import Any, List, NamedTuple, Optional, Sequence, Tuple
+
+import torch
+
+from ott_b200 import _arrays, _lib
+from ott_b200.geometry import epsilon_scheduler as eps_scheduler
+from ott_b200.initializers.linear import initializers as init_lib
+from ott_b200.problems.linear import linear_problem
+
+__all__ = ["Sinkhorn", "SinkhornOutput", "run_batch"]
+
+_PRECISIONS = {
+    "auto": _lib.PRECISION_AUTO,
+    "fp32": _lib.PRECISION_FP32,
+    "bf16_split3": _lib.PRECISION_BF16_SPLIT3,
+}
+
+
+class _Results:
+  """Device-side ``ottb_result`` records, read back to the host once."""
+
+  def __init__(self, buf: torch.Tensor, num: int):
+    self._buf = buf
+    self._num = num
+    self._host: Optional[List[_lib.OttbResult]] = None
+
+  def get(self, k: int) -> _lib.OttbResult:
+    if self._host is None:
+      raw = self._buf.cpu().numpy().tobytes()
+      sz = _lib.RESULT_BYTES
+      self._host = [_lib.OttbResult.from_buffer_copy(raw[i * sz:(i + 1) * sz])
+                    for i in range(self._num)]
+      for r in self._host:
+        if r.status != _lib.OTTB_OK:
+          raise _lib.OttbError(r.status, "ottb_sinkhorn_pointcloud (device)")
+    return self._host[k]
+
+
+class SinkhornOutput(NamedTuple):
+  """Output of the solver (sinkhorn.py:280-538).
+
+  ``potentials`` are torch CUDA tensors; ``errors`` has length
+  ``ceil(max_iterations / inner_iterations)`` with the reference's
+  conventions (-1: not reached, inf: not computed).
+  """
+
+  potentials: Tuple[torch.Tensor, torch.Tensor]
+  errors: Optional[torch.Tensor] = None
+  reg_ot_cost_: Optional[Any] = None  # (_Results, index)
+  ot_prob: Optional[linear_problem.LinearProblem] = None
+  threshold: Optional[float] = None
+  inner_iterations: Optional[int] = None
+
+  def _res(self) -> _lib.OttbResult:
+    results, k = self.reg_ot_cost_
+    return results.get(k)
+
+  @property
+  def f(self) -> torch.Tensor:
+    return self.potentials[0]
+
+  @property
+  def g(self) -> torch.Tensor:
+    return self.potentials[1]
+
+  @property
+  def reg_ot_cost(self) -> float:
+    """sinkhorn.py:224-277 (balanced), FP64 sums on the device."""
+    return self._res().reg_ot_cost
+
+  @property
+  def kl_reg_cost(self) -> float:
+    return self.reg_ot_cost
+
+  @property
+  def converged(self) -> bool:
+    """sinkhorn.py:1020-1023."""
+    return bool(self._res().converged)
+
+  @property
+  def n_iters(self) -> int:
+    """sinkhorn.py:432-434."""
+    return int(self._res().n_iters)
+
+  @property
+  def geom(self):
+    return self.ot_prob.geom
+
+  @property
+  def a(self) -> torch.Tensor:
+    return self.ot_prob.a
+
+  @property
+  def b(self) -> torch.Tensor:
+    return self.ot_prob.b
+
+  @property
+  def dual_cost(self) -> float:
+    """sinkhorn.py:337-343."""
+    a, b = self.a.double(), self.b.double()
+    f, g = self.f.double(), self.g.double()
+    zero = torch.zeros((), dtype=torch.float64, device=a.device)
+    return float(torch.where(a > 0, a * f, zero).sum() + torch.where(b > 0, b * g, zero).sum())
+
+  @property
+  def ent_reg_cost(self) -> float:
+    """sinkhorn.py:351-370: ``reg_ot_cost - eps * (H(a) + H(b))``."""
+    def entr(p):
+      p = p.double()
+      safe = torch.where(p > 0, p, torch.ones_like(p))
+      return torch.where(p > 0, -p * torch.log(safe), torch.zeros_like(p)).sum()
+    return self.reg_ot_cost - self.geom.epsilon * float(entr(self.a) + entr(self.b))
+
+  @property
+  def transport_mass(self) -> float:
+    """Sum of the transport matrix of the final state (column marginal sum)."""
+    return float(self._res().marginal_sum)
+
+
+class Sinkhorn:
+  """Sinkhorn solver (sinkhorn.py:542-780), same constructor arguments.
+
+  Extra keyword: ``precision`` in ``{"auto", "fp32", "bf16_split3"}``
+  selects the arithmetic of the cost inner products.
+  """
+
+  def __init__(
+      self,
+      lse_mode: bool = True,
+      threshold: float = 1e-3,
+      norm_error: int = 1,
+      inner_iterations: int = 10,
+      min_iterations: int = 0,
+      max_iterations: int = 2000,
+      momentum: Optional[Any] = None,
+      anderson: Optional[Any] = None,
+      parallel_dual_updates: bool = False,
+      recenter_potentials: bool = False,
+      use_danskin: Optional[bool] = None,
+      implicit_diff: Optional[Any] = "default",
+      initializer: Optional[init_lib.SinkhornInitializer] = None,
+      progress_fn: Optional[Any] = None,
+      precision: str = "auto",
+      timeout_ms: int = 0,
+  ):
+    if not lse_mode:
+      raise NotImplementedError("kernel mode (lse_mode=False) is not on this path")
+    if momentum is not None and getattr(momentum, "value", 1.0) != 1.0:
+      raise NotImplementedError("momentum other than weight 1 is not on this path")
+    if anderson is not None:
+      raise NotImplementedError("Anderson acceleration is not on this path")
+    if parallel_dual_updates:
+      raise NotImplementedError("parallel dual updates are not on this path")
+    if recenter_potentials:
+      raise NotImplementedError("recentred potentials are not on this path")
+    if precision not in _PRECISIONS:
+      raise ValueError(f"precision must be one of {sorted(_PRECISIONS)}")
+    self.lse_mode = lse_mode
+    self.threshold = threshold
+    self.norm_error = norm_error
+    self.inner_iterations = inner_iterations
+    self.min_iterations = min_iterations
+    self.max_iterations = max_iterations
+    self.parallel_dual_updates = parallel_dual_updates
+    self.recenter_potentials = recenter_potentials
+    self.use_danskin = use_danskin
+    self.implicit_diff = implicit_diff
+    self.initializer = (init_lib.DefaultInitializer()
+                        if initializer is None else initializer)
+    self.progress_fn = progress_fn
+    self.precision = precision
+    self.timeout_ms = timeout_ms
+    self._phantom_arrivals = 0
+
+  @property
+  def outer_iterations(self) -> int:
+    """sinkhorn.py:956-962."""
+    return int(math.ceil(self.max_iterations / self.inner_iterations))
+
+  def _cfg(self, mask_init: bool, eps: eps_scheduler.Epsilon) -> _lib.OttbSolverCfg:
+    c = _lib.OttbSolverCfg()
+    c.threshold = float(self.threshold)
+    c.norm_error = int(self.norm_error)
+    c.inner_iterations = int(self.inner_iterations)
+    c.min_iterations = int(self.min_iterations)
+    c.max_iterations = int(self.max_iterations)
+    c.eps_init = float(eps.init)
+    c.eps_decay = float(eps.decay)
+    c.precision = _PRECISIONS[self.precision]
+    c.mask_init = 1 if mask_init else 0
+    c.timeout_ms = int(self.timeout_ms)
+    c.phantom_arrivals = int(self._phantom_arrivals)
+    return c
+
+  def __call__(self, ot_prob: linear_problem.LinearProblem,
+               init: Optional[Tuple[Any, Any]] = None, **kwargs: Any) -> SinkhornOutput:
+    return run_batch([ot_prob], self, [init], **kwargs)[0]
+
+
+def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
+              inits: Optional[Sequence[Optional[Tuple[Any, Any]]]] = None,
+              **init_kwargs: Any) -> List[SinkhornOutput]:
+  """Solves independent problems of the same dimension in ONE persistent
+  launch (the batched form of ``jax.vmap`` over ``Sinkhorn``)."""
+  if not probs:
+    return []
+  lib = _lib.load()
+  inits = list(inits) if inits is not None else [None] * len(probs)
+  d = probs[0].geom.dim
+  dev = probs[0].geom.x.device
+  scheds = []
+  for p in probs:
+    if not p.is_balanced:
+      raise NotImplementedError("unbalanced problems (tau < 1) are not on this path")
+    if p.geom.dim != d:
+      raise ValueError("all problems of one batch must have the same dimension")
+    scheds.append(p.geom.epsilon_scheduler)
+  s0 = scheds[0]
+  for s in scheds:
+    if (s.init, s.decay) != (s0.init, s0.decay):
+      raise ValueError("all problems of one batch must share the epsilon schedule")
+
+  outer = solver.outer_iterations
+  arr = (_lib.OttbProblem * len(probs))()
+  keep: List[torch.Tensor] = []
+  outs = []
+  mask_init = False
+  for k, p in enumerate(probs):
+    n, m = p.geom.shape
+    a, b = p.a, p.b
+    init = inits[k]
+    if init is None:
+      fi, gi = solver.initializer(p, lse_mode=True, **init_kwargs)
+      if fi is not None or gi is not None:
+        mask_init = True
+    else:
+      fi, gi = init
+    fi = None if fi is None else _arrays.as_f32(fi, dev)
+    gi = None if gi is None else _arrays.as_f32(gi, dev)
+    f = torch.empty(n, dtype=torch.float32, device=dev)
+    g = torch.empty(m, dtype=torch.float32, device=dev)
+    errors = torch.empty(max(outer, 1), dtype=torch.float32, device=dev)
+    keep += [t for t in (fi, gi) if t is not None]
+    q = arr[k]
+    q.x = p.geom.x.data_ptr()
+    q.y = p.geom.y.data_ptr()
+    q.a = a.data_ptr()
+    q.b = b.data_ptr()
+    q.f_init = None if fi is None else fi.data_ptr()
+    q.g_init = None if gi is None else gi.data_ptr()
+    q.f = f.data_ptr()
+    q.g = g.data_ptr()
+    q.errors = errors.data_ptr()
+    q.n = n
+    q.m = m
+    q.epsilon = float(p.geom.epsilon)
+    q.inv_scale_cost = float(p.geom.inv_scale_cost)
+    outs.append((f, g, errors[:outer]))
+  cfg = solver._cfg(mask_init, s0)
+  nprob = len(probs)
+  ws_bytes = lib.ottb_sinkhorn_workspace_size(arr, nprob, d, ctypes.byref(cfg))
+  if ws_bytes == 0:
+    raise NotImplementedError("problem sizes or configuration not supported")
+  ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+  res = torch.empty(nprob * _lib.RESULT_BYTES, dtype=torch.uint8, device=dev)
+  st = lib.ottb_sinkhorn_pointcloud(arr, nprob, d, ctypes.byref(cfg), res.data_ptr(),
+                                    ws.data_ptr(), ws_bytes, _arrays.stream_handle())
+  if st == _lib.OTTB_ERR_UNSUPPORTED:
+    raise NotImplementedError(_lib.status_string(st))
+  _lib.check(st, "ottb_sinkhorn_pointcloud")
+  results = _Results(res, nprob)
+  out = []
+  for k, p in enumerate(probs):
+    f, g, errors = outs[k]
+    out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
+                              ot_prob=p, threshold=solver.threshold,
+                              inner_iterations=solver.inner_iterations))
+  # The workspace must outlive the kernels: record it on the stream.
+  ws.record_stream(torch.cuda.current_stream())
+  for t in keep:
+    t.record_stream(torch.cuda.current_stream())
+  if solver.progress_fn is not None:
+    _replay_progress(solver, out)
+  return out
+
+
+def _replay_progress(solver: Sinkhorn, outs: List[SinkhornOutput]) -> None:
+  """Calls ``progress_fn`` once per recorded block after the solve.
+
+  The reference calls it from inside the loop every iteration
+  (sinkhorn.py:933-937); the persistent kernel does not return to the host
+  mid-solve, so the per-block errors are replayed afterwards with the final
+  potentials in the state.
+  """
+  for o in outs:
+    errs = o.errors.cpu()
+    for blk in range(int((errs != -1).sum())):
+      it = (blk + 1) * solver.inner_iterations - 1
+      solver.progress_fn((it, solver.inner_iterations, solver.max_iterations, o))

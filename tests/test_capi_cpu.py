@@ -1,0 +1,56 @@
+"""Host-side checks of the C ABI that need no GPU: the library loads and
+exports every function include/ott_b200.h declares."""
+import ctypes
+import os
+import re
+
+from ott_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+  text = open(os.path.join(ROOT, "include", "ott_b200.h")).read()
+  text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+  names = re.findall(r"^\s*(?:const\s+)?[a-z_0-9]+\s*\*?\s*(ottb_[a-z_0-9]+)\s*\(",
+                     text, flags=re.M)
+  return sorted(set(names))
+
+
+def test_header_declares_expected_functions():
+  names = declared_functions()
+  assert set(_lib.EXPORTED_SYMBOLS) <= set(names), names
+
+
+def test_library_exports_every_declared_symbol():
+  lib = _lib.load()
+  for name in declared_functions():
+    assert hasattr(lib, name), name
+
+
+def test_status_strings_and_version():
+  lib = _lib.load()
+  assert lib.ottb_version().decode().count(".") == 2
+  for st in range(7):
+    assert lib.ottb_status_string(st)
+  assert _lib.status_string(_lib.OTTB_ERR_TIMEOUT) == "device wait timed out"
+
+
+def test_struct_layouts_match_header():
+  # sizes follow from the C declarations on LP64
+  assert ctypes.sizeof(_lib.OttbProblem) == 9 * 8 + 2 * 8 + 2 * 4
+  assert ctypes.sizeof(_lib.OttbSolverCfg) == 11 * 4
+  assert ctypes.sizeof(_lib.OttbResult) == 2 * 8 + 4 * 4
+
+
+def test_invalid_arguments_rejected_without_device():
+  lib = _lib.load()
+  cfg = _lib.OttbSolverCfg(threshold=1e-3, norm_error=1, inner_iterations=10,
+                           min_iterations=0, max_iterations=100, eps_init=1.0,
+                           eps_decay=1.0, precision=-1)
+  # null problem array / zero problems -> 0 workspace
+  assert lib.ottb_sinkhorn_workspace_size(None, 0, 2, ctypes.byref(cfg)) == 0
+  st = lib.ottb_sinkhorn_pointcloud(None, 1, 2, ctypes.byref(cfg), None, None, 0, None)
+  assert st == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_cost_stats(None, None, 0, 0, 2, ctypes.c_float(1.0), None, None, 0,
+                             None) == _lib.OTTB_ERR_INVALID

@@ -1,0 +1,162 @@
+"""Parity of the CUDA path (through the C ABI) with the float64 oracle.
+
+Tolerances: f and g within 1e-4 * epsilon absolute, reg_ot_cost within
+1e-5 relative, n_iters equal (within one block where a stopping test sits
+on the threshold). Relations mirror the reference's own tests
+(tests/solvers/linear/sinkhorn_test.py).
+"""
+import numpy as np
+import pytest
+
+from tests import helpers, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def test_reference_problem_zero_weights():
+  """sinkhorn_test.py:38-54 problem (a[0] = b[3] = 0), epsilon 0.1."""
+  x, y, a, b = problems.ref_test_problem()
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1)
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.1)
+  assert np.isneginf(out.f.cpu().numpy()[0]) and np.isneginf(out.g.cpu().numpy()[3])
+  helpers.assert_parity(geom, out, ref)
+
+
+@pytest.mark.parametrize("n,m,d", [(1, 1, 1), (2, 3, 2), (17, 29, 3), (127, 129, 31),
+                                   (129, 127, 33), (300, 257, 2), (1000, 1100, 16),
+                                   (513, 200, 64), (130, 140, 128)])
+def test_ragged_shapes(n, m, d):
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + m + d)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_uniform_2048_d2():
+  """n = m = 2048, d = 2, epsilon = 0.05 mean(C), threshold 1e-3."""
+  x, y, a, b = problems.uniform_cloud_problem(2048, 2048, 2, seed=0)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  assert out.converged
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_min_iterations_pattern():
+  """sinkhorn_test.py:248-265: errors inf, inf, inf, then > 0."""
+  x, y, a, b = problems.ref_test_problem()
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1, threshold=1e-3,
+                                min_iterations=34)
+  errs = out.errors.cpu().numpy()
+  assert np.isinf(errs[:3]).all() and errs[3] > 0
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.1, threshold=1e-3, min_iterations=34)
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_scan_loop():
+  """sinkhorn_test.py:267-284: min == max runs a scan, last error computed."""
+  x, y, a, b = problems.ref_test_problem()
+  kw = dict(threshold=1e-3, min_iterations=50, max_iterations=50)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1, **kw)
+  errs = out.errors.cpu().numpy()
+  assert out.converged and 0 < errs[-1] < 1e-3
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.1, **kw)
+  helpers.assert_parity(geom, out, ref)
+
+
+@pytest.mark.parametrize("kw", [dict(max_iterations=25), dict(max_iterations=7),
+                                dict(min_iterations=10), dict(max_iterations=5),
+                                dict(inner_iterations=3, max_iterations=40),
+                                dict(norm_error=2), dict(threshold=1e-6, max_iterations=60)])
+def test_loop_edge_cases(kw):
+  x, y, a, b = problems.ref_test_problem()
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1, **dict(kw))
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.1, **dict(kw))
+  assert out.n_iters == ref.n_iters
+  helpers.assert_parity(geom, out, ref, iter_blocks=0)
+
+
+def test_epsilon_decay_schedule():
+  import torch
+  from ott_b200.geometry import epsilon_scheduler, pointcloud
+  from ott_b200.solvers import linear
+  from oracle import sinkhorn_np as oracle
+  x, y, a, b = problems.uniform_cloud_problem(200, 300, 3, seed=3)
+  eps = epsilon_scheduler.Epsilon(target=0.01, init=20.0, decay=0.8)
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=eps)
+  out = linear.solve(geom, torch.as_tensor(a).cuda(), torch.as_tensor(b).cuda())
+  ref = oracle.solve(x, y, a, b, epsilon=0.01, eps_init=20.0, eps_decay=0.8)
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_warm_restart_converges_in_one_block():
+  """sinkhorn_test.py:491-546: restarting from (f, g) stops after one block
+  with a smaller error."""
+  x, y, a, b = problems.ref_test_problem()
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1, threshold=1e-3)
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers.linear import sinkhorn
+  prob = linear_problem.LinearProblem(geom, out.a, out.b)
+  out2 = sinkhorn.Sinkhorn(threshold=1e-3)(prob, init=(out.f, out.g))
+  assert out2.n_iters == 10
+  e1 = out.errors.cpu().numpy()
+  e2 = out2.errors.cpu().numpy()
+  assert e2[0] < e1[e1 > -1][-1]
+
+
+def test_default_epsilon_std_and_scale_mean():
+  x, y, a, b = problems.uniform_cloud_problem(300, 200, 5, seed=5)
+  geom, out = helpers.gpu_solve(x, y, a, b)  # epsilon = 0.05 * std(C)
+  ref = helpers.oracle_solve(x, y, a, b)
+  np.testing.assert_allclose(geom.epsilon, ref.epsilon, rtol=1e-6)
+  helpers.assert_parity(geom, out, ref)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.1, relative_epsilon="mean",
+                                scale_cost="mean")
+  ref = helpers.oracle_solve(x, y, a, b, epsilon=0.1, relative_epsilon="mean",
+                             scale_cost="mean")
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_uniform_default_marginals_and_self_cloud():
+  x, _, _, _ = problems.uniform_cloud_problem(400, 400, 2, seed=7)
+  geom, out = helpers.gpu_solve(x, None, None, None, epsilon=0.01)
+  ref = helpers.oracle_solve(x, None, None, None, epsilon=0.01)
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_batched_matches_single():
+  """One persistent launch over uneven problems equals one solve each."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  probs = problems.batched_uneven_problems(12, d=8, lo=16, hi=700, seed=1)
+  geoms = [pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                                 epsilon=0.05, relative_epsilon="mean")
+           for x, y, _, _ in probs]
+  outs = linear.solve_batch(geoms, [torch.as_tensor(p[2]).cuda() for p in probs],
+                            [torch.as_tensor(p[3]).cuda() for p in probs])
+  for (x, y, a, b), geom, out in zip(probs, geoms, outs):
+    ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+    helpers.assert_parity(geom, out, ref)
+
+
+def test_device_wait_timeout_reports_status():
+  """A grid barrier waiting for arrivals that never come gives up after its
+  time limit and reports OTTB_ERR_TIMEOUT; the context stays usable."""
+  import torch
+  from ott_b200 import _lib
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers.linear import sinkhorn
+  x, y, a, b = problems.ref_test_problem()
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=0.1)
+  solver = sinkhorn.Sinkhorn(timeout_ms=200)
+  solver._phantom_arrivals = 1
+  out = solver(linear_problem.LinearProblem(geom, torch.as_tensor(a).cuda(),
+                                            torch.as_tensor(b).cuda()))
+  with pytest.raises(_lib.OttbError) as e:
+    _ = out.n_iters
+  assert e.value.status == _lib.OTTB_ERR_TIMEOUT
+  geom2, out2 = helpers.gpu_solve(x, y, a, b, epsilon=0.1)
+  assert out2.converged
