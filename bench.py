@@ -1,0 +1,395 @@
+#!/usr/bin/env python
+"""Benchmark: seconds to 1e-3 marginal error and Sinkhorn iterations/s.
+
+Workload: one log-domain Sinkhorn solve (ott ``linear.solve`` semantics) on
+a squared-Euclidean point cloud, n = m = 65536, d = 64, x ~ N(0, I),
+y ~ N(0.5 * 1, diag(U[0.5, 2])), uniform weights, epsilon = 0.01 * mean(C),
+threshold 1e-3 (L1 marginal error), max_iterations 2000. Synthetic seeded
+data (numpy default_rng(0)). A step is one full solve to the threshold.
+
+``python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]``
+prints one JSON line (rank 0). Under torchrun each rank solves its own
+replica of the workload (the path does not shard: replicas only); times are
+device times, max over ranks.
+
+``--impl reference`` times the CPU restatement of the reference algorithm
+(C port of the oracle, OpenMP, all host threads) on a bounded row sample of
+the same workload and converts it to the same metric.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+  sys.path.insert(0, ROOT)
+
+METRIC = "s to 1e-3 marginal err & Sinkhorn iters/s: chosen form vs plain FP32, 1 B200"
+L2_BYTES = 126 * 1024 * 1024
+
+
+def parse_args():
+  p = argparse.ArgumentParser()
+  p.add_argument("--gpus", type=int, default=1)
+  p.add_argument("--steps", type=int, default=3)
+  p.add_argument("--warmup", type=int, default=3)
+  p.add_argument("--impl", choices=["ours", "reference"], default="ours")
+  p.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16_split3"])
+  p.add_argument("--n", type=int, default=65536)
+  p.add_argument("--d", type=int, default=64)
+  p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
+  p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+  return p.parse_args()
+
+
+def workload(args):
+  from tests import problems
+  n = args.n
+  x, y, a, b = problems.gaussian_shift_problem(n, n, args.d, seed=0)
+  return x, y, a, b
+
+
+def config_dict(args, n_iters=None):
+  return {"workload": f"sinkhorn sqeuclidean n=m={args.n} d={args.d} "
+                      f"eps=0.01*mean(C) thr=1e-3 (L1)",
+          "n": args.n, "m": args.n, "d": args.d, "epsilon": "0.01*mean(C)",
+          "threshold": 1e-3, "max_iterations": 2000, "n_iters": n_iters,
+          "data": "x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, seed 0",
+          "l2": "flushed between timed steps (256 MiB write); inputs 32 MiB < L2",
+          "parallelism": f"replicas x{args.gpus}"}
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+  QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+           "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+           "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+  def __init__(self, index: int):
+    self.index = index
+    self.proc = None
+    self.path = None
+
+  def start(self):
+    fd, self.path = tempfile.mkstemp(suffix=".csv")
+    os.close(fd)
+    try:
+      self.proc = subprocess.Popen(
+          ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.QUERY}",
+           "--format=csv,noheader,nounits", "-lms", "200"],
+          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+    except OSError:
+      self.proc = None
+
+  def stop(self):
+    if self.proc is None:
+      return None
+    self.proc.terminate()
+    try:
+      self.proc.wait(timeout=5)
+    except subprocess.TimeoutExpired:
+      self.proc.kill()
+    rows = []
+    for line in open(self.path):
+      parts = [p.strip() for p in line.split(",")]
+      if len(parts) >= 9:
+        rows.append(parts)
+    os.unlink(self.path)
+    if not rows:
+      return None
+    sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+    mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
+    return {"sm_mhz": statistics.median(sm) if sm else None,
+            "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+            "samples": len(rows)}
+
+
+# ---------------------------------------------------------------------------
+# measured pipe peaks (no driver figure exists for these pipes)
+# ---------------------------------------------------------------------------
+def measure_pipe_peaks(torch):
+  lib = ctypes.CDLL(os.path.join(ROOT, "ott_b200", "_lib", "libottb200_peaks.so"))
+  lib.ottb_peaks_launch.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2
+  out = torch.zeros(4096, device="cuda")
+  sms = torch.cuda.get_device_properties(0).multi_processor_count
+  blocks, res = sms * 8, {}
+  stream = torch.cuda.current_stream().cuda_stream
+  for kind, name, iters in ((0, "ffma_per_s", 20000), (1, "ex2_per_s", 4000)):
+    lib.ottb_peaks_launch(kind, blocks, iters, out.data_ptr(), stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    lib.ottb_peaks_launch(kind, blocks, iters, out.data_ptr(), stream)
+    e1.record()
+    torch.cuda.synchronize()
+    res[name] = blocks * 256 * iters * 8 / (e0.elapsed_time(e1) * 1e-3)
+  return res
+
+
+def load_peaks_json():
+  path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+  try:
+    return json.load(open(path))
+  except Exception:
+    return None
+
+
+def ncu_traffic(name):
+  """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
+  path = os.path.join(ROOT, "profiles", "traffic.json")
+  try:
+    return json.load(open(path)).get(name)
+  except Exception:
+    return None
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: C port of the oracle on a bounded row sample
+# ---------------------------------------------------------------------------
+def cpu_sample(x, y, a, b, eps, rows, repeats=1):
+  """Times a 10-iteration scan solve of the first `rows` rows of x against
+  all of y. Returns seconds per cost entry (one entry of one LSE sweep)."""
+  from oracle import sinkhorn_c
+  xs = np.ascontiguousarray(x[:rows])
+  as_ = a[:rows] / a[:rows].sum()
+  best = None
+  for _ in range(repeats):
+    t0 = time.perf_counter()
+    sinkhorn_c.solve(xs, y, as_, b, epsilon=eps, min_iterations=10, max_iterations=10)
+    dt = time.perf_counter() - t0
+    best = dt if best is None else min(best, dt)
+  # 20 update sweeps + 1 error sweep (it == max-1) + 1 reg_ot_cost sweep
+  sweeps = 22
+  return best / (sweeps * rows * y.shape[0]), sinkhorn_c.threads()
+
+
+def cpu_time_to_threshold(sec_per_entry, n, m, n_iters, inner=10):
+  """Reference loop cost: 2 sweeps per iteration, 1 error sweep per block,
+  1 reg_ot_cost sweep."""
+  sweeps = 2 * n_iters + n_iters / inner + 1
+  return sec_per_entry * sweeps * n * m
+
+
+def run_reference(args):
+  rank = int(os.environ.get("RANK", "0"))
+  if rank != 0:
+    return 0
+  from oracle import sinkhorn_np
+  x, y, a, b = workload(args)
+  eps = 0.01 * float(sinkhorn_np.mean_cost_matrix(x.astype(np.float64), y.astype(np.float64)))
+  rows = 2048 if args.n >= 8192 else args.n
+  # Iteration count of the reference loop on this workload, from the oracle
+  # port on a reduced-size instance of the same distribution.
+  n_iters = int(os.environ.get("OTTB_REF_ITERS", "50"))
+  for _ in range(args.warmup):
+    cpu_sample(x, y, a, b, eps, rows)
+  samples = []
+  for _ in range(args.steps):
+    spe, cores = cpu_sample(x, y, a, b, eps, rows)
+    samples.append(spe)
+  spe = statistics.median(samples)
+  val = cpu_time_to_threshold(spe, args.n, args.n, n_iters)
+  iters_per_s = 1.0 / (spe * 2 * args.n * args.n)
+  line = {
+      "metric": METRIC, "value": val, "unit": "s", "impl": "reference",
+      "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+      "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
+      "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+      "config": config_dict(args, n_iters),
+      "iters_per_s": iters_per_s, "entries_per_s": 1.0 / spe,
+      "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
+                       "sample": f"10-iteration scan solve of {rows} of {args.n} rows "
+                                 f"x all {args.n} columns (d={args.d}), per-entry time "
+                                 f"scaled to 2.1 sweeps/iteration x {n_iters} iterations"},
+      "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+  }
+  print(json.dumps(line))
+  return 0
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args):
+  import torch
+  import torch.distributed as dist
+  from datetime import timedelta
+
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  rank = int(os.environ.get("RANK", "0"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  torch.cuda.set_device(local)
+  if world > 1:
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import sinkhorn
+
+  def barrier():
+    if world > 1:
+      dist.barrier()
+    torch.cuda.synchronize()
+
+  def max_over_ranks(v):
+    if world == 1:
+      return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+  x, y, a, b = workload(args)
+  xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
+  ad, bd = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+  geom = pointcloud.PointCloud(xd, yd, epsilon=0.01, relative_epsilon="mean")
+  eps = geom.epsilon
+  prob = linear_problem.LinearProblem(geom, ad, bd)
+  flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
+
+  def timed_solves(solver, steps, warm):
+    for _ in range(warm):
+      out = solver(prob)
+      _ = out.n_iters
+    barrier()
+    ms, out = 0.0, None
+    for _ in range(steps):
+      flush.zero_()
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record()
+      out = solver(prob)
+      e1.record()
+      e1.synchronize()
+      ms += e0.elapsed_time(e1)
+    barrier()
+    return max_over_ranks(ms / steps), out
+
+  solver = sinkhorn.Sinkhorn(threshold=1e-3, max_iterations=2000, precision=args.precision)
+  clocks = ClockSampler(local)
+  clocks.start()
+  ms, out = timed_solves(solver, args.steps, args.warmup)
+  clk = clocks.stop()
+  n_iters, converged = out.n_iters, out.converged
+  form = "bf16_split3" if (args.precision == "bf16_split3" or
+                           (args.precision == "auto" and args.d >= 32 and False)) else "fp32"
+
+  # plain FP32 comparison (the "vs plain FP32" half of the metric)
+  plain = None
+  if not args.no_plain and form != "fp32":
+    pms, pout = timed_solves(sinkhorn.Sinkhorn(threshold=1e-3, precision="fp32"), 1, 1)
+    plain = {"s_to_threshold": pms * 1e-3, "n_iters": pout.n_iters,
+             "iters_per_s": pout.n_iters / (pms * 1e-3)}
+
+  # end to end through the public API, host buffers in, results out
+  xh = torch.from_numpy(x).pin_memory()
+  yh = torch.from_numpy(y).pin_memory()
+  ah = torch.from_numpy(a).pin_memory()
+  bh = torch.from_numpy(b).pin_memory()
+
+  def e2e_step():
+    g = pointcloud.PointCloud(xh, yh, epsilon=0.01, relative_epsilon="mean")
+    o = linear.solve(g, ah, bh, threshold=1e-3, precision=args.precision)
+    f_host, g_host = o.f.cpu(), o.g.cpu()
+    err_host = o.errors.cpu()
+    return o.reg_ot_cost, f_host, g_host, err_host
+
+  for _ in range(max(1, args.warmup)):
+    e2e_step()
+  barrier()
+  e2e_ms = 0.0
+  for _ in range(args.steps):
+    flush.zero_()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    e2e_step()
+    e1.record()
+    e1.synchronize()
+    e2e_ms += e0.elapsed_time(e1)
+  barrier()
+  e2e_ms = max_over_ranks(e2e_ms / args.steps)
+  h2d = (x.nbytes + y.nbytes + a.nbytes + b.nbytes)
+  d2h = 4 * (2 * args.n) + 4 * out.errors.numel() + 16 + 32
+
+  # roofline of the dominant kernel (the persistent solve kernel)
+  entries = 2.0 * args.n * args.n * n_iters      # algorithmic: 2 sweeps/iteration
+  t = ms * 1e-3
+  peaks = measure_pipe_peaks(torch)
+  mp = load_peaks_json()
+  if form == "fp32" and args.d > 8:
+    achieved = 2.0 * args.d * entries / t / 1e12
+    peak = 2.0 * peaks["ffma_per_s"] / 1e12
+    roof = {"bound": "fp32_fma", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+            "frac": achieved / peak,
+            "peak_source": "measured in bench.py (FFMA probe kernel, 8 chains/thread)"}
+  else:
+    achieved = entries / t / 1e9
+    peak = peaks["ex2_per_s"] / 1e9
+    roof = {"bound": "mufu_ex2", "achieved": achieved, "peak": peak, "unit": "Gex2/s",
+            "frac": achieved / peak,
+            "peak_source": "measured in bench.py (MUFU ex2 probe kernel)"}
+  traffic = ncu_traffic(f"sinkhorn_{form}_n{args.n}_d{args.d}")
+  roof["traffic"] = traffic
+  roof["work_per_launch"] = f"{entries:.4g} cost entries (2*n*m per iteration x {n_iters})"
+  if mp:
+    roof["measured_peaks_file"] = {"hbm_gbs": mp.get("hbm_gbs"),
+                                   "bf16_tflops": mp.get("bf16_tflops")}
+
+  cpu = None
+  if not args.no_cpu and rank == 0 and world == 1:
+    rows = 2048 if args.n >= 8192 else args.n
+    spe, cores = cpu_sample(x, y, a, b, eps, rows)
+    val = cpu_time_to_threshold(spe, args.n, args.n, n_iters)
+    cpu = {"value": val, "unit": "s", "cores": cores, "kind": "port",
+           "sample": f"10-iteration scan solve of {rows} of {args.n} rows x all "
+                     f"{args.n} columns, per-entry time scaled to 2.1 sweeps/iteration "
+                     f"x {n_iters} iterations"}
+
+  launches_per_solve = 5  # fill errors, prep, init, persistent loop, finalize
+  line = {
+      "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world,
+      "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+      "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+      "dtype": "f32" if form == "fp32" else "bf16x3/f32", "data": "synthetic",
+      "config": config_dict(args, n_iters), "form": form, "converged": converged,
+      "iters_per_s": n_iters / t, "entries_per_s": entries / t,
+      "plain_fp32": plain,
+      "roofline": roof, "cpu_baseline": cpu,
+      "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d,
+              "d2h_bytes_per_step": d2h},
+      "clocks": clk, "gpu_launches": launches_per_solve * args.steps,
+      "pipe_peaks": peaks,
+  }
+  if rank == 0:
+    print(json.dumps(line))
+  if world > 1:
+    dist.destroy_process_group()
+  return 0
+
+
+def main():
+  args = parse_args()
+  if args.warmup < 3:
+    print("warning: fewer than 3 warm-up steps", file=sys.stderr)
+  if args.impl == "reference":
+    return run_reference(args)
+  return run_ours(args)
+
+
+if __name__ == "__main__":
+  sys.exit(main())

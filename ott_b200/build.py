@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 OUT_DIR = os.path.join(HERE, "_lib")
 OUT = os.path.join(OUT_DIR, "libottb200.so")
+PEAKS_OUT = os.path.join(OUT_DIR, "libottb200_peaks.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -25,34 +26,41 @@ def nvcc() -> str:
   raise RuntimeError("nvcc not found")
 
 
-def sources():
-  return sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC)
+def sources(root=CSRC):
+  return sorted(os.path.join(root, f) for f in os.listdir(root)
                 if f.endswith((".cu", ".cuh", ".h")))
 
 
-def up_to_date() -> bool:
-  if not os.path.exists(OUT):
+def up_to_date(out, deps) -> bool:
+  if not os.path.exists(out):
     return False
-  t = os.path.getmtime(OUT)
-  deps = sources() + [os.path.join(HERE, "..", "include", "ott_b200.h"), __file__]
+  t = os.path.getmtime(out)
+  deps = list(deps) + [__file__]
   return all(os.path.getmtime(s) <= t for s in deps if os.path.exists(s))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-  if not force and up_to_date():
-    return OUT
+def _nvcc_shared(src, out, verbose):
   os.makedirs(OUT_DIR, exist_ok=True)
   cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-         "-shared", "-o", OUT + ".tmp", os.path.join(CSRC, "capi.cu")]
+         "-shared", "-o", out + ".tmp", src]
   if verbose:
     cmd.insert(1, "-Xptxas=-v")
   r = subprocess.run(cmd, capture_output=True, text=True)
   if r.returncode != 0:
     sys.stderr.write(r.stdout + r.stderr)
-    raise RuntimeError("nvcc failed building libottb200.so")
+    raise RuntimeError(f"nvcc failed building {os.path.basename(out)}")
   if verbose:
     sys.stderr.write(r.stderr)
-  os.replace(OUT + ".tmp", OUT)
+  os.replace(out + ".tmp", out)
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+  deps = sources() + [os.path.join(HERE, "..", "include", "ott_b200.h")]
+  if force or not up_to_date(OUT, deps):
+    _nvcc_shared(os.path.join(CSRC, "capi.cu"), OUT, verbose)
+  peaks = os.path.join(CSRC, "peaks", "peaks.cu")
+  if force or not up_to_date(PEAKS_OUT, [peaks]):
+    _nvcc_shared(peaks, PEAKS_OUT, verbose)
   return OUT
 
 
