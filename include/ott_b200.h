@@ -110,6 +110,27 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems,
                                  ottb_result* results, void* workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* Fixed device scratch of ottb_sinkhorn_pointcloud_noalloc, per device. */
+#define OTTB_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* No counterpart in the reference: ott-jax runs inside XLA, which owns all
+ * device memory. This is ottb_sinkhorn_pointcloud for callers that cannot
+ * allocate device memory where they call the solver (a handler inside a host
+ * framework that only passes it the input and output buffers, or a service
+ * whose GPU memory budget is fixed at start-up). It allocates nothing: its
+ * workspace is a 16 MiB (OTTB_NOALLOC_SCRATCH_BYTES) array compiled into the
+ * library, held in every GPU that loads the library until the process exits.
+ * Calls whose scratch need (ottb_sinkhorn_workspace_size) exceeds that return
+ * OTTB_ERR_WORKSPACE before enqueuing anything. The first call on a device
+ * looks up the array's device address; make that first call before any
+ * stream capture. All calls share the array: calls whose work overlaps on
+ * the GPU race, so order them (one stream). Inputs, outputs and status as for
+ * ottb_sinkhorn_pointcloud. */
+int32_t ottb_sinkhorn_pointcloud_noalloc(const ottb_problem* problems,
+                                         int32_t num_problems, int32_t d,
+                                         const ottb_solver_cfg* cfg,
+                                         ottb_result* results, void* stream);
+
 /* Bytes of workspace ottb_cost_stats needs. */
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d);
 

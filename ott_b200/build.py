@@ -39,10 +39,11 @@ def up_to_date(out, deps) -> bool:
   return all(os.path.getmtime(s) <= t for s in deps if os.path.exists(s))
 
 
-def _nvcc_shared(src, out, verbose):
+def _nvcc_shared(srcs, out, verbose):
   os.makedirs(OUT_DIR, exist_ok=True)
+  srcs = [srcs] if isinstance(srcs, str) else list(srcs)
   cmd = [nvcc(), *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
-         "-shared", "-o", out + ".tmp", src]
+         "-shared", "-o", out + ".tmp", *srcs]
   if verbose:
     cmd.insert(1, "-Xptxas=-v")
   r = subprocess.run(cmd, capture_output=True, text=True)
@@ -57,7 +58,8 @@ def _nvcc_shared(src, out, verbose):
 def build(force: bool = False, verbose: bool = False) -> str:
   deps = sources() + [os.path.join(HERE, "..", "include", "ott_b200.h")]
   if force or not up_to_date(OUT, deps):
-    _nvcc_shared(os.path.join(CSRC, "capi.cu"), OUT, verbose)
+    _nvcc_shared([os.path.join(CSRC, "capi.cu"), os.path.join(CSRC, "noalloc.cu")], OUT,
+                 verbose)
   peaks = os.path.join(CSRC, "peaks", "peaks.cu")
   if force or not up_to_date(PEAKS_OUT, [peaks]):
     _nvcc_shared(peaks, PEAKS_OUT, verbose)
