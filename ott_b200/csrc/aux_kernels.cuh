@@ -2,6 +2,8 @@
 // initialisation, result finalisation and cost statistics.
 #pragma once
 
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 #include "driver.cuh"
 
@@ -259,6 +261,50 @@ __global__ void cost_stats_reduce_kernel(const double* px, const double* py, int
         (mnx2 + mny2 + 2.0 * mnx * mny + 4.0 * tr - 4.0 * nxy - 4.0 * xny);
     out[0] = mean;
     out[1] = msq;
+  }
+}
+
+}  // namespace ottb
+
+namespace ottb {
+
+// Tensor-core layout: centred points split into bf16 pairs, hi rows then lo
+// rows, [2][pad][dk] (zero padded in both dimensions), and scaled squared
+// norms of the centred FP32 points. blockIdx.y = problem, blockIdx.z = side.
+__global__ void prep_points_tc_kernel(PrepArgs args) {
+  __shared__ float center[128];
+  const int p = blockIdx.y;
+  const int side = blockIdx.z;
+  const ProbDev& P = args.probs[p];
+  const float* src = args.src[2 * p + side];
+  const int64_t cnt = side ? P.m : P.n;
+  const int64_t pad = side ? P.m_pad : P.n_pad;
+  __nv_bfloat16* dst = (__nv_bfloat16*)(side ? P.yh : P.xh);
+  float* nrm = const_cast<float*>(side ? P.ny : P.nx);
+  const int d = args.d, dk = args.dp;
+  sample_center(args.src[2 * p], P.n, args.src[2 * p + 1], P.m, d, center);
+  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pad;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    __nv_bfloat16* hi = dst + i * dk;
+    __nv_bfloat16* lo = dst + (pad + i) * dk;
+    double s = 0.0;
+    int k = 0;
+    if (i < cnt) {
+      const float* row = src + i * d;
+      for (; k < d; ++k) {
+        const float v = row[k] - center[k];
+        s += (double)v * (double)v;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        hi[k] = h;
+        lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+      }
+    }
+    for (; k < dk; ++k) {
+      hi[k] = zero;
+      lo[k] = zero;
+    }
+    nrm[i] = (float)((double)P.inv_scale * s);
   }
 }
 

@@ -14,8 +14,11 @@
 #include <mutex>
 #include <vector>
 
+#include <cuda.h>
+
 #include "aux_kernels.cuh"
 #include "kernel_simt.cuh"
+#include "kernel_tc.cuh"
 
 using namespace ottb;
 
@@ -83,6 +86,57 @@ KernelChoice pick_simt(int dp) {
   return k;
 }
 
+// Tensor-core engine: DK = 64 or 128 (d padded with zeros).
+template <int DK>
+struct TcKernel {
+  static void* fn() { return (void*)&sinkhorn_tc_kernel<DK>; }
+  static size_t smem() { return sizeof(TcSmem<DK>) + 1024; }  // + alignment slack
+};
+
+KernelChoice pick_tc(int dk) {
+  KernelChoice k;
+  k.threads = 320;
+  if (dk == 64) { k.fn = TcKernel<64>::fn(); k.smem = TcKernel<64>::smem(); }
+  if (dk == 128) { k.fn = TcKernel<128>::fn(); k.smem = TcKernel<128>::smem(); }
+  return k;
+}
+
+// cuTensorMapEncodeTiled, resolved through the runtime (no libcuda link).
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_tiled_fn() {
+  static std::mutex mu;
+  static EncodeTiledFn fn = nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// Tensor map over a [2 * pad][dk] bf16 array (hi rows, then lo rows): boxes
+// of 64 elements (128 bytes) x 128 rows, 128-byte swizzle.
+bool encode_points_map(CUtensorMap* map, void* base, int64_t pad, int dk) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {(cuuint64_t)dk, (cuuint64_t)(2 * pad)};
+  const cuuint64_t strides[1] = {(cuuint64_t)dk * 2};
+  const cuuint32_t box[2] = {64, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 // Grid size of the persistent launch: all CTAs co-resident.
 int persistent_grid(const KernelChoice& k, int sms) {
   static std::mutex mu;
@@ -124,13 +178,18 @@ struct ProbPlan {
       off_msum;
 };
 
+bool wants_tc(const ottb_solver_cfg* cfg, int d) {
+  return cfg->precision == OTTB_PRECISION_BF16_SPLIT3;
+}
+
 struct Plan {
   int num = 0;
-  int dp = 0;
+  int dp = 0;        // FP32 engine: padded dimension; tensor cores: DK
+  bool tc = false;
   int grid = 0;
   KernelChoice kern;
   size_t off_globals = 0, off_sched = 0, off_probs = 0, off_state = 0, off_ids = 0,
-         off_prefix = 0, off_eval_ids = 0, off_eval_prefix = 0, off_ptrs = 0;
+         off_prefix = 0, off_eval_ids = 0, off_eval_prefix = 0, off_ptrs = 0, off_maps = 0;
   size_t header_bytes = 0;
   size_t total = 0;
   std::vector<ProbPlan> probs;
@@ -152,10 +211,15 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
   int st = validate_cfg(cfg);
   if (st != OTTB_OK) return st;
   if (d > 128) return OTTB_ERR_UNSUPPORTED;
-  if (cfg->precision == OTTB_PRECISION_BF16_SPLIT3) return OTTB_ERR_UNSUPPORTED;
   plan.num = num;
-  plan.dp = simt_dp(d);
-  plan.kern = pick_simt(plan.dp);
+  plan.tc = wants_tc(cfg, d);
+  if (plan.tc) {
+    plan.dp = d <= 64 ? 64 : 128;
+    plan.kern = pick_tc(plan.dp);
+  } else {
+    plan.dp = simt_dp(d);
+    plan.kern = pick_simt(plan.dp);
+  }
   if (!plan.kern.fn) return OTTB_ERR_UNSUPPORTED;
   if (need_grid) {
     DeviceInfo di = device_info();
@@ -187,6 +251,7 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
   plan.off_eval_ids = off; off = align_up(off + sizeof(int) * num);
   plan.off_eval_prefix = off; off = align_up(off + sizeof(int) * (num + 1));
   plan.off_ptrs = off; off = align_up(off + sizeof(float*) * 4 * num);
+  plan.off_maps = off; off = align_up(off + (plan.tc ? sizeof(TcMaps) * num : 0));
   plan.header_bytes = off;
   plan.probs.resize(num);
   for (int t = 0; t < num; ++t) {
@@ -201,8 +266,10 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.split_f = choose_split(pp.rb_f, (int)(pp.m_pad / kBN), plan.grid, num);
     pp.split_g = choose_split(pp.rb_g, (int)(pp.n_pad / kBN), plan.grid, num);
     const size_t fsz = sizeof(float);
-    pp.off_xt = off; off = align_up(off + fsz * plan.dp * pp.n_pad);
-    pp.off_yt = off; off = align_up(off + fsz * plan.dp * pp.m_pad);
+    // FP32 engine: transposed [DP][pad] floats; tensor cores: [2][pad][DK] bf16
+    const size_t elt = plan.tc ? 2 * 2 : fsz;
+    pp.off_xt = off; off = align_up(off + elt * plan.dp * pp.n_pad);
+    pp.off_yt = off; off = align_up(off + elt * plan.dp * pp.m_pad);
     pp.off_nx = off; off = align_up(off + fsz * pp.n_pad);
     pp.off_ny = off; off = align_up(off + fsz * pp.m_pad);
     pp.off_galt = off; off = align_up(off + fsz * pp.m);
@@ -294,8 +361,19 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
     P.gbuf[0] = q.g;
     P.gbuf[1] = (float*)(ws + pp.off_galt);
     P.errors = q.errors;
-    P.xt = (const float*)(ws + pp.off_xt);
-    P.yt = (const float*)(ws + pp.off_yt);
+    if (plan.tc) {
+      P.xh = ws + pp.off_xt;
+      P.yh = ws + pp.off_yt;
+      TcMaps maps;  // 64-byte aligned, then copied into the header image
+      if (!encode_points_map(&maps.x, ws + pp.off_xt, pp.n_pad, plan.dp) ||
+          !encode_points_map(&maps.y, ws + pp.off_yt, pp.m_pad, plan.dp))
+        return OTTB_ERR_CUDA;
+      std::memcpy(host.data() + plan.off_maps + sizeof(TcMaps) * t, &maps, sizeof(TcMaps));
+      P.maps = ws + plan.off_maps + sizeof(TcMaps) * t;
+    } else {
+      P.xt = (const float*)(ws + pp.off_xt);
+      P.yt = (const float*)(ws + pp.off_yt);
+    }
     P.nx = (const float*)(ws + pp.off_nx);
     P.ny = (const float*)(ws + pp.off_ny);
     P.part_m = (float*)(ws + pp.off_pm);
@@ -356,7 +434,10 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
     int64_t mx = 1;
     for (const ProbPlan& pp : plan.probs) mx = std::max(mx, std::max(pp.n_pad, pp.m_pad));
     dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, 1024), num_problems, 2);
-    prep_points_kernel<<<grid, 256, 0, stream>>>(pa);
+    if (plan.tc)
+      prep_points_tc_kernel<<<grid, 256, 0, stream>>>(pa);
+    else
+      prep_points_kernel<<<grid, 256, 0, stream>>>(pa);
   }
   {
     InitArgs ia{d_ptrs + 2 * num_problems, d_probs, cfg->mask_init};

@@ -43,9 +43,11 @@ struct ProbDev {
   const float* yt;
   const float* nx;
   const float* ny;
-  // workspace: bf16 hi/lo copies for the tensor-core path, [pad][DPK]
+  // workspace, tensor-core path: bf16 hi/lo copies [2][pad][DK] and the
+  // TMA tensor maps over them (TcMaps, in the call header)
   const void* xh;
   const void* yh;
+  const void* maps;
   // workspace: split partials (m, l) [S][rows] and per-row-block data
   float* part_m;
   float* part_l;
@@ -107,6 +109,21 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   uint64_t t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
+}
+
+// Compensated accumulation s + c += x (Knuth's TwoSum: c collects the exact
+// rounding error of every addition). Each tile's terms are first summed in a
+// short tree; adding that tile sum to a long-running FP32 total would
+// otherwise drop every contribution below half an ulp of the total, a
+// one-signed error that, at small epsilon (many negligible terms per row),
+// biases the log-sum-exp low and, differing between the f- and g-sweeps,
+// accumulates along the neutral direction (f + c, g - c) of the iteration.
+__device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
+  const float t = s + x;
+  const float bb = t - s;
+  const float err = (s - (t - bb)) + (x - bb);
+  s = t;
+  c += err;
 }
 
 // Merge two (shift, sum) log-sum-exp states in base 2.

@@ -62,11 +62,12 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
     sm.As[k][r] = s * op.At[(int64_t)k * op.a_pad + row0 + r];
   }
 
-  float mrow[8], lrow[8];
+  float mrow[8], lrow[8], lcmp[8];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     mrow[i] = kNegSentinel;
     lrow[i] = 0.f;
+    lcmp[i] = 0.f;
   }
 
   // Prologue: tile t0 into buffer 0 (points via cp.async, w computed here).
@@ -128,13 +129,16 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
 #pragma unroll
       for (int j = 1; j < 8; ++j) cm = fmaxf(cm, acc[i][j]);
       if (cm > mrow[i] + kTau) {
-        lrow[i] *= ex2_approx(mrow[i] - cm);
+        const float sc = ex2_approx(mrow[i] - cm);
+        lrow[i] *= sc;
+        lcmp[i] *= sc;
         mrow[i] = cm;
       }
-      float sum = 0.f;
+      float e[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) sum += ex2_approx(acc[i][j] - mrow[i]);
-      lrow[i] += sum;
+      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(acc[i][j] - mrow[i]);
+      const float sum = ((e[0] + e[1]) + (e[2] + e[3])) + ((e[4] + e[5]) + (e[6] + e[7]));
+      two_sum_acc(lrow[i], lcmp[i], sum);
     }
     __syncthreads();
     if (has_next && tid < kBN) sm.ws[buf ^ 1][tid] = wnext;
@@ -143,6 +147,7 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
   // Merge the 16 column-partial states of each row (lanes sharing ty).
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
+    lrow[i] += lcmp[i];
 #pragma unroll
     for (int off = 1; off < 16; off <<= 1) {
       float m2 = __shfl_xor_sync(0xffffffffu, mrow[i], off);

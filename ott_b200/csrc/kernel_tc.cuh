@@ -1,0 +1,93 @@
+// Persistent Sinkhorn kernel on the tensor-core (tcgen05, BF16 split-3)
+// engine. One CTA per SM (its shared memory exceeds half an SM), so the
+// 256-column TMEM allocation never waits on another CTA.
+#pragma once
+
+#include "engine_tc.cuh"
+#include "persistent.cuh"
+
+namespace ottb {
+
+__device__ __forceinline__ TcOperands make_tc_operands(const ProbDev& P, int kind,
+                                                       const float* gcur) {
+  const TcMaps* maps = reinterpret_cast<const TcMaps*>(P.maps);
+  TcOperands op;
+  if (kind == kSweepG) {
+    op.mapA = &maps->y; op.padA = (int32_t)P.m_pad; op.rows = P.m;
+    op.mapB = &maps->x; op.padB = (int32_t)P.n_pad; op.cols = P.n;
+    op.potB = P.f; op.nb = P.nx;
+  } else {
+    op.mapA = &maps->x; op.padA = (int32_t)P.n_pad; op.rows = P.n;
+    op.mapB = &maps->y; op.padB = (int32_t)P.m_pad; op.cols = P.m;
+    op.potB = gcur; op.nb = P.ny;
+  }
+  return op;
+}
+
+template <int DK>
+__global__ void __launch_bounds__(TcCfg<DK>::kThreads, 1)
+sinkhorn_tc_kernel(KernelArgs A) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // The 128-byte swizzled operand tiles need 1024-byte alignment.
+  const uint32_t base = tc::smem_u32(smem_raw);
+  unsigned char* aligned = smem_raw + ((1024u - (base & 1023u)) & 1023u);
+  TcSmem<DK>& sm = *reinterpret_cast<TcSmem<DK>*>(aligned);
+  constexpr int NS = TcCfg<DK>::kStages;
+  constexpr int NB = TcCfg<DK>::kTmemBufs;
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < NS; ++i) {
+      tc::mbar_init(&sm.full[i], 1);
+      tc::mbar_init(&sm.empty[i], 1);
+    }
+    for (int i = 0; i < NB; ++i) {
+      tc::mbar_init(&sm.tfull[i], 1);
+      tc::mbar_init(&sm.tempty[i], 8);
+    }
+    tc::mbar_init(&sm.a_full, 1);
+    tc::mbar_init(&sm.a_empty, 1);
+    tc::mbar_init(&sm.drain, 1);
+    sm.err = 0;
+    tc::fence_barrier_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&sm.tmem_base, TcCfg<DK>::kTmemCols);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+
+  TcPipe pp{0u, 0u, 0u, 0u, 0};
+  const CommonSmem cs{sm.rm, sm.rl, sm.red, &sm.unit, &sm.last};
+  auto sweep = [&](const SweepParams& sp, unsigned idx) -> bool {
+    auto unit = [&](const ProbDev& P, const float* gcur, int rb, int t0, int t1, float s,
+                    float wscale) -> bool {
+      const TcOperands op = make_tc_operands(P, sp.kind, gcur);
+      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, wscale, A.timeout_ns);
+    };
+    return sweep_units(A, sp, idx, cs, unit);
+  };
+  persistent_main(A, sweep);
+
+  // Teardown. After a timeout, wait (bounded) for this CTA's own MMAs and
+  // TMA loads still in flight before the TMEM and shared memory go away.
+  __syncthreads();
+  if (sm.err) {
+    const uint64_t limit = 1000000000ull;  // 1 s
+    if (warp == 1 && lane == 0) {
+      tc::mma_commit(&sm.drain);
+      tc::mbar_wait(&sm.drain, 0, limit);
+    }
+    if (warp == 0 && lane == 0 && pp.issued)
+      tc::mbar_wait(&sm.full[pp.last_full_stage], pp.last_full_parity, limit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  if (warp == 1) tc::tmem_dealloc(sm.tmem_base, TcCfg<DK>::kTmemCols);
+}
+
+}  // namespace ottb
