@@ -95,7 +95,7 @@ struct TcKernel {
 
 KernelChoice pick_tc(int dk) {
   KernelChoice k;
-  k.threads = 320;
+  k.threads = dk == 64 ? TcCfg<64>::kThreads : TcCfg<128>::kThreads;
   if (dk == 64) { k.fn = TcKernel<64>::fn(); k.smem = TcKernel<64>::smem(); }
   if (dk == 128) { k.fn = TcKernel<128>::fn(); k.smem = TcKernel<128>::smem(); }
   return k;
@@ -178,8 +178,11 @@ struct ProbPlan {
       off_msum;
 };
 
+// BF16 split-3 on tcgen05 when asked for, and by default where the inner
+// product is a real contraction (d >= 32); FP32 CUDA-core FMAs below.
 bool wants_tc(const ottb_solver_cfg* cfg, int d) {
-  return cfg->precision == OTTB_PRECISION_BF16_SPLIT3;
+  if (cfg->precision == OTTB_PRECISION_BF16_SPLIT3) return true;
+  return cfg->precision == OTTB_PRECISION_AUTO && d >= 32;
 }
 
 struct Plan {

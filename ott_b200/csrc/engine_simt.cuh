@@ -5,9 +5,9 @@
 // 8 x 8 micro-tile (rows ty*4+{0..3}, 64+ty*4+{0..3}; columns tx*4+{0..3},
 // 64+tx*4+{0..3}) of
 //   t_rc = w_c + s * <A_r, B_c>       (log2 units)
-// accumulated with FFMAs from shared-memory tiles (A scaled by s once per
-// unit, the accumulator seeded with w_c), followed by an online base-2
-// log-sum-exp with lazy rescaling and ex2.approx on the MUFU pipe.
+// from a d-step FFMA dot product over shared-memory tiles, scaled and
+// shifted with one FFMA, followed by an online base-2 log-sum-exp with lazy
+// rescaling and ex2.approx on the MUFU pipe.
 #pragma once
 
 #include "common.cuh"
@@ -56,10 +56,10 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
   const int tx = tid & 15;
   const int ty = tid >> 4;
 
-  // A tile, pre-scaled by s.
+  // A tile.
   for (int idx = tid; idx < DP * kBM; idx += blockDim.x) {
     int k = idx / kBM, r = idx % kBM;
-    sm.As[k][r] = s * op.At[(int64_t)k * op.a_pad + row0 + r];
+    sm.As[k][r] = op.At[(int64_t)k * op.a_pad + row0 + r];
   }
 
   float mrow[8], lrow[8], lcmp[8];
@@ -100,15 +100,10 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
     __syncthreads();
 
     float acc[8][8];
-    {
-      float4 w0 = *reinterpret_cast<const float4*>(&sm.ws[buf][tx * 4]);
-      float4 w1 = *reinterpret_cast<const float4*>(&sm.ws[buf][64 + tx * 4]);
-      float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+    for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = wv[j];
-    }
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
 #pragma unroll 4
     for (int k = 0; k < DP; ++k) {
       float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
@@ -123,6 +118,18 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
         for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
 
+    // t = s * <A_r, B_c> + w_c, one rounding. Seeding the FFMA chain with
+    // w_c instead would round every one of the DP steps at the magnitude of
+    // w_c (~|x|^2 / eps), an error 10x larger than the reference's FP32 path.
+    {
+      float4 w0 = *reinterpret_cast<const float4*>(&sm.ws[buf][tx * 4]);
+      float4 w1 = *reinterpret_cast<const float4*>(&sm.ws[buf][64 + tx * 4]);
+      float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(acc[i][j], s, wv[j]);
+    }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
       float cm = acc[i][0];

@@ -38,13 +38,14 @@ sinkhorn_tc_kernel(KernelArgs A) {
   const int lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
+    constexpr int NE = TcCfg<DK>::kEpiWarps;
     for (int i = 0; i < NS; ++i) {
-      tc::mbar_init(&sm.full[i], 1);
-      tc::mbar_init(&sm.empty[i], 1);
+      tc::mbar_init(&sm.full[i], 32);  // producer lanes (+ TMA bytes)
+      tc::mbar_init(&sm.empty[i], 1);  // MMA commit
     }
     for (int i = 0; i < NB; ++i) {
       tc::mbar_init(&sm.tfull[i], 1);
-      tc::mbar_init(&sm.tempty[i], 8);
+      tc::mbar_init(&sm.tempty[i], NE);
     }
     tc::mbar_init(&sm.a_full, 1);
     tc::mbar_init(&sm.a_empty, 1);
@@ -56,6 +57,22 @@ sinkhorn_tc_kernel(KernelArgs A) {
     tc::tmem_alloc(&sm.tmem_base, TcCfg<DK>::kTmemCols);
     tc::tmem_relinquish();
   }
+  // Extension blocks: zero everywhere; A's first 3 K columns are ones.
+  {
+    uint32_t* a32 = reinterpret_cast<uint32_t*>(sm.Aext);
+    for (int i = threadIdx.x; i < TcCfg<DK>::kExtBytes / 4; i += blockDim.x) a32[i] = 0u;
+    for (int st = 0; st < NS; ++st) {
+      uint32_t* b32 = reinterpret_cast<uint32_t*>(sm.Bext[st]);
+      for (int i = threadIdx.x; i < TcCfg<DK>::kExtBytes / 4; i += blockDim.x) b32[i] = 0u;
+    }
+    __syncthreads();
+    if (threadIdx.x < kBM) {
+      const __nv_bfloat16 one = __float2bfloat16_rn(1.f);
+      for (int k = 0; k < 3; ++k)
+        *reinterpret_cast<__nv_bfloat16*>(sm.Aext + ext_offset(threadIdx.x, k)) = one;
+    }
+    tc::fence_proxy_async_smem();
+  }
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -66,7 +83,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
     auto unit = [&](const ProbDev& P, const float* gcur, int rb, int t0, int t1, float s,
                     float wscale) -> bool {
       const TcOperands op = make_tc_operands(P, sp.kind, gcur);
-      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, wscale, A.timeout_ns);
+      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, 0.5f / P.inv_scale, A.timeout_ns);
     };
     return sweep_units(A, sp, idx, cs, unit);
   };

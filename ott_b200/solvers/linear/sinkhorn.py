@@ -139,7 +139,10 @@ class Sinkhorn:
   """Sinkhorn solver (sinkhorn.py:542-780), same constructor arguments.
 
   Extra keyword: ``precision`` in ``{"auto", "fp32", "bf16_split3"}``
-  selects the arithmetic of the cost inner products.
+  selects the arithmetic of the cost inner products: ``"fp32"`` FMAs on the
+  CUDA cores; ``"bf16_split3"`` tcgen05 tensor-core products of bf16 hi/lo
+  splits (hi*hi + hi*lo + lo*hi, FP32 accumulation); ``"auto"`` (default)
+  uses the tensor cores for d >= 32 and FP32 below.
   """
 
   def __init__(

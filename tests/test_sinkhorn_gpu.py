@@ -27,8 +27,19 @@ def test_reference_problem_zero_weights():
                                    (513, 200, 64), (130, 140, 128)])
 def test_ragged_shapes(n, m, d):
   x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + m + d)
-  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
   ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  helpers.assert_parity(geom, out, ref)
+
+
+def test_gaussian_shift_d64_fp32():
+  """The n=m=65536, d=64 workload's distribution at n=4096 (eps 0.01 mean(C),
+  potentials ~100 eps): the FP32 path holds 1e-4 eps."""
+  x, y, a, b = problems.gaussian_shift_problem(4096, 4096, 64, seed=0)
+  kw = dict(epsilon=0.01, relative_epsilon="mean")
+  geom, out = helpers.gpu_solve(x, y, a, b, precision="fp32", **kw)
+  ref = helpers.oracle_solve(x, y, a, b, batch_size=1024, **kw)
   helpers.assert_parity(geom, out, ref)
 
 
