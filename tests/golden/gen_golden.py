@@ -1,0 +1,98 @@
+"""Generates the golden vectors in this directory from the reference itself.
+
+Runs ott-jax's own source for the Sinkhorn path (``ott.solvers.linear.solve``
+on ``ott.geometry.pointcloud.PointCloud``) over the NumPy stand-in for jax
+(``oracle/jaxshim.py``, loaded by ``oracle/reference_loader.py``), in float64
+(``jax_enable_x64`` semantics) and in float32, on seeded inputs from
+``tests/problems.py``. Needs the reference source tree (default
+/root/reference/src); the GPU machine only reads the committed ``*.npz``.
+
+    python tests/golden/gen_golden.py [reference_src_root]
+"""
+import json
+import os
+import sys
+import warnings
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from tests import problems  # noqa: E402
+
+# name -> (inputs, geometry kwargs, solver kwargs, init: None or "restart")
+CASES = {
+    "refprob_eps0.1": ("ref", dict(epsilon=0.1), dict(), None),
+    "refprob_min34": ("ref", dict(epsilon=0.1), dict(min_iterations=34), None),
+    "refprob_scan50": ("ref", dict(epsilon=0.1), dict(min_iterations=50, max_iterations=50), None),
+    "refprob_max25": ("ref", dict(epsilon=0.1), dict(threshold=1e-9, max_iterations=25), None),
+    "refprob_norm2": ("ref", dict(epsilon=0.1), dict(norm_error=2), None),
+    "refprob_inner3": ("ref", dict(epsilon=0.1), dict(inner_iterations=3), None),
+    "refprob_restart": ("ref", dict(epsilon=0.1), dict(), "restart"),
+    "uniform_64x80_d2_relmean": ("unif:64:80:2", dict(epsilon=0.05, relative_epsilon="mean"), dict(), None),
+    "uniform_50x40_d3_defaulteps": ("unif:50:40:3", dict(), dict(), None),
+    "uniform_60x70_d5_scalemean": ("unif:60:70:5", dict(epsilon=0.1, relative_epsilon="mean",
+                                                        scale_cost="mean"), dict(), None),
+    "uniform_40x45_d3_decay": ("unif:40:45:3", dict(epsilon="decay"), dict(), None),
+    "uniform_31x47_d33_relmean": ("unif:31:47:33", dict(epsilon=0.05, relative_epsilon="mean"), dict(), None),
+    "gauss_96x96_d64_relmean0.01": ("gauss:96:96:64", dict(epsilon=0.01, relative_epsilon="mean"), dict(), None),
+}
+
+
+def make_inputs(spec):
+  if spec == "ref":
+    return problems.ref_test_problem()
+  kind, n, m, d = spec.split(":")
+  n, m, d = int(n), int(m), int(d)
+  if kind == "unif":
+    return problems.uniform_cloud_problem(n, m, d, seed=n + m + d)
+  return problems.gaussian_shift_problem(n, m, d, seed=0)
+
+
+def run(ref, case, dtype):
+  spec, gkw, skw, init = CASES[case]
+  x, y, a, b = [np.asarray(v, dtype) for v in make_inputs(spec)]
+  gkw = dict(gkw)
+  if gkw.get("epsilon") == "decay":
+    gkw["epsilon"] = ref.epsilon_scheduler.Epsilon(target=0.01, init=20.0, decay=0.8)
+  geom = ref.pointcloud.PointCloud(x, y, **gkw)
+  kw = dict(skw)
+  if init == "restart":
+    out0 = ref.solve(geom, a, b, **kw)
+    prob = ref.linear_problem.LinearProblem(geom, a, b)
+    out = ref.sinkhorn.Sinkhorn(**kw)(prob, init=(out0.f, out0.g))
+  else:
+    out = ref.solve(geom, a, b, **kw)
+  res = dict(f=np.asarray(out.f), g=np.asarray(out.g), errors=np.asarray(out.errors),
+             reg_ot_cost=np.asarray(out.reg_ot_cost), n_iters=np.asarray(out.n_iters),
+             converged=np.asarray(out.converged), epsilon=np.asarray(geom.epsilon))
+  if init == "restart":
+    res["f_init"] = np.asarray(out0.f)
+    res["g_init"] = np.asarray(out0.g)
+  return (x, y, a, b), res
+
+
+def main():
+  from oracle import reference_loader
+  root = sys.argv[1] if len(sys.argv) > 1 else reference_loader.DEFAULT_ROOT
+  warnings.filterwarnings("ignore")
+  manifest = {}
+  for x64, tag in ((True, "f64"), (False, "f32")):
+    ref = reference_loader.load(root, x64=x64)
+    import ott.geometry.epsilon_scheduler as es  # noqa: E402  (loaded module)
+    ref.epsilon_scheduler = es
+    for case in CASES:
+      (x, y, a, b), res = run(ref, case, np.float64 if x64 else np.float32)
+      np.savez_compressed(os.path.join(HERE, f"{case}.{tag}.npz"), x=x, y=y, a=a, b=b, **res)
+      spec, gkw, skw, init = CASES[case]
+      manifest[case] = dict(inputs=spec, geometry={k: str(v) for k, v in gkw.items()},
+                            solver=skw, init=init)
+      print(tag, case, "n_iters", int(res["n_iters"]), "reg_ot_cost", float(res["reg_ot_cost"]))
+  with open(os.path.join(HERE, "manifest.json"), "w") as fh:
+    json.dump(manifest, fh, indent=1, sort_keys=True)
+
+
+if __name__ == "__main__":
+  main()

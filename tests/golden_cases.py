@@ -1,0 +1,28 @@
+"""Loads the golden vectors of tests/golden (made by gen_golden.py from the
+reference's own code) and maps each case to solver arguments."""
+import json
+import os
+
+import numpy as np
+
+HERE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+  with open(os.path.join(HERE, "manifest.json")) as fh:
+    return sorted(json.load(fh))
+
+
+def load(name, tag="f64"):
+  with open(os.path.join(HERE, "manifest.json")) as fh:
+    meta = json.load(fh)[name]
+  data = dict(np.load(os.path.join(HERE, f"{name}.{tag}.npz")))
+  geom = {}
+  for k, v in meta["geometry"].items():
+    if k == "epsilon" and v == "decay":
+      geom.update(epsilon=0.01, eps_init=20.0, eps_decay=0.8)
+    elif k in ("epsilon",):
+      geom[k] = float(v)
+    else:
+      geom[k] = v
+  return data, geom, dict(meta["solver"]), meta["init"]
