@@ -343,6 +343,13 @@ def run_ours(args):
     roof = {"bound": "mufu_ex2", "achieved": achieved, "peak": peak, "unit": "Gex2/s",
             "frac": achieved / peak,
             "peak_source": "measured in bench.py (MUFU ex2 probe kernel)"}
+    if clk and clk.get("sm_mhz"):
+      # the solves run power-capped below the probe's clock: also against
+      # 16 ex2 / clk / SM at the median SM clock sampled during the solves
+      sms = torch.cuda.get_device_properties(0).multi_processor_count
+      at_clk = 16 * sms * clk["sm_mhz"] * 1e6 / 1e9
+      roof["peak_at_sampled_clock"] = at_clk
+      roof["frac_at_sampled_clock"] = achieved / at_clk
     if form != "fp32" and mp and mp.get("bf16_tflops"):
       dk = 64 if args.d <= 64 else 128
       tf = 3 * 2 * dk * entries / t / 1e12   # split-3 MMA flops

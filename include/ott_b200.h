@@ -135,12 +135,13 @@ int32_t ottb_sinkhorn_pointcloud_noalloc(const ottb_problem* problems,
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d);
 
 /* Cost-matrix statistics of one problem without materialising it.
- * out (device, 2 doubles): mean(C) and mean(C^2) of
- * C_ij = inv_scale_cost * |x_i - y_j|^2 over uniform weights, from FP64
- * moments of x and y (fixed-order reductions, deterministic). */
+ * out (device, 2 doubles): mean(C) and, when second != 0, mean(C^2) of
+ * C_ij = inv_scale_cost * |x_i - y_j|^2 over uniform weights (out[1] is NaN
+ * otherwise), from FP64 moments of x and y (fixed-order reductions,
+ * deterministic). mean(C) needs O((n + m) d) work, mean(C^2) O((n + m) d^2). */
 int32_t ottb_cost_stats(const float* x, const float* y, int64_t n, int64_t m,
-                        int32_t d, float inv_scale_cost, double* out,
-                        void* workspace, size_t workspace_bytes,
+                        int32_t d, float inv_scale_cost, int32_t second,
+                        double* out, void* workspace, size_t workspace_bytes,
                         void* stream);
 
 /* Human-readable text of a status code. */

@@ -116,7 +116,7 @@ def load() -> ctypes.CDLL:
     lib.ottb_sinkhorn_pointcloud.restype = i32
     lib.ottb_cost_stats_workspace_size.argtypes = [i64, i64, i32]
     lib.ottb_cost_stats_workspace_size.restype = sz
-    lib.ottb_cost_stats.argtypes = [vp, vp, i64, i64, i32, ctypes.c_float, vp, vp, sz, vp]
+    lib.ottb_cost_stats.argtypes = [vp, vp, i64, i64, i32, ctypes.c_float, i32, vp, vp, sz, vp]
     lib.ottb_cost_stats.restype = i32
     lib.ottb_status_string.argtypes = [i32]
     lib.ottb_status_string.restype = ctypes.c_char_p

@@ -85,18 +85,32 @@ __global__ void init_potentials_kernel(InitArgs args) {
   const ProbDev& P = args.probs[p];
   const float* fi = args.init[2 * p];
   const float* gi = args.init[2 * p + 1];
-  const int64_t tot = P.n + P.m;
+  const float wsh = 0.5f / P.inv_scale;
+  // f over n_pad, then g over both g buffers' m_pad rows (padding rows get
+  // the -inf column shift of the tensor-core path)
+  const int64_t tot = P.n_pad + 2 * P.m_pad;
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot;
        i += (int64_t)gridDim.x * blockDim.x) {
-    if (i < P.n) {
-      float v = fi ? fi[i] : 0.f;
-      if ((!fi || args.mask) && !(P.a[i] > 0.f)) v = -INFINITY;
-      P.f[i] = v;
+    if (i < P.n_pad) {
+      float v = -INFINITY;
+      if (i < P.n) {
+        v = fi ? fi[i] : 0.f;
+        if ((!fi || args.mask) && !(P.a[i] > 0.f)) v = -INFINITY;
+        P.f[i] = v;
+      }
+      if (P.extx) write_ext_row((char*)P.extx + i * 16, i < P.n ? (v - P.nx[i]) * wsh : -INFINITY);
     } else {
-      int64_t j = i - P.n;
-      float v = gi ? gi[j] : 0.f;
-      if ((!gi || args.mask) && !(P.b[j] > 0.f)) v = -INFINITY;
-      P.gbuf[0][j] = v;
+      const int64_t k = i - P.n_pad;
+      const int buf = (int)(k / P.m_pad);
+      const int64_t j = k % P.m_pad;
+      float v = -INFINITY;
+      if (j < P.m && buf == 0) {
+        v = gi ? gi[j] : 0.f;
+        if ((!gi || args.mask) && !(P.b[j] > 0.f)) v = -INFINITY;
+        P.gbuf[0][j] = v;
+      }
+      if (P.exty && (buf == 0 || j >= P.m))
+        write_ext_row((char*)P.exty + k * 16, (j < P.m) ? (v - P.ny[j]) * wsh : -INFINITY);
     }
   }
 }
@@ -178,44 +192,47 @@ __global__ void fill_errors_kernel(ProbDev* probs) {
 }
 
 // FP64 moments for the cost statistics. Each CTA writes a partial vector
-// [cnt, sum n, sum n^2, sum x (d), sum n x (d), sum x x^T (d*d)] for one
-// point set; the reduction kernel adds partials in a fixed order.
-__global__ void moments_kernel(const float* pts, int64_t cnt, int d, double* part) {
+// [cnt, sum n, sum n^2, sum x (d), sum n x (d), sum x x^T (d*d, when
+// second != 0)] for one point set, n = |x|^2; the reductions add partials in
+// a fixed order, so the statistics are deterministic.
+__host__ __device__ inline int moments_len(int d, int second) {
+  return 3 + 2 * d + (second ? d * d : 0);
+}
+
+__global__ void moments_kernel(const float* pts, int64_t cnt, int d, int second, double* part) {
   extern __shared__ double sh[];
-  const int K = 3 + 2 * d + d * d;
-  double* acc = sh;                  // [K] per-CTA accumulators
+  const int K = moments_len(d, second);
+  double* acc = sh;                                // [K] per-CTA accumulators
   float* tile = reinterpret_cast<float*>(sh + K);  // [64][d]
+  double* nrm = sh + K + 32 * d;                   // [64] squared norms (tile is 64*d floats)
   for (int k = threadIdx.x; k < K; k += blockDim.x) acc[k] = 0.0;
   __syncthreads();
   const int64_t per = (cnt + gridDim.x - 1) / gridDim.x;
   const int64_t beg = (int64_t)blockIdx.x * per;
   const int64_t end = min(cnt, beg + per);
-  // thread-private partials for the outer-product entries it owns
   for (int64_t c0 = beg; c0 < end; c0 += 64) {
     const int rows = (int)min((int64_t)64, end - c0);
     for (int idx = threadIdx.x; idx < rows * d; idx += blockDim.x)
       tile[idx] = pts[c0 * d + idx];
+    __syncthreads();
+    for (int r = threadIdx.x; r < rows; r += blockDim.x) {
+      double s = 0.0;
+      for (int k = 0; k < d; ++k) s += (double)tile[r * d + k] * tile[r * d + k];
+      nrm[r] = s;
+    }
     __syncthreads();
     for (int e = threadIdx.x; e < K; e += blockDim.x) {
       double s = 0.0;
       if (e == 0) {
         s = rows;
       } else if (e <= 2) {
-        for (int r = 0; r < rows; ++r) {
-          double nr = 0.0;
-          for (int k = 0; k < d; ++k) nr += (double)tile[r * d + k] * tile[r * d + k];
-          s += (e == 1) ? nr : nr * nr;
-        }
+        for (int r = 0; r < rows; ++r) s += (e == 1) ? nrm[r] : nrm[r] * nrm[r];
       } else if (e < 3 + d) {
         const int k = e - 3;
         for (int r = 0; r < rows; ++r) s += tile[r * d + k];
       } else if (e < 3 + 2 * d) {
         const int k = e - 3 - d;
-        for (int r = 0; r < rows; ++r) {
-          double nr = 0.0;
-          for (int q = 0; q < d; ++q) nr += (double)tile[r * d + q] * tile[r * d + q];
-          s += nr * tile[r * d + k];
-        }
+        for (int r = 0; r < rows; ++r) s += nrm[r] * tile[r * d + k];
       } else {
         const int q = e - 3 - 2 * d;
         const int k1 = q / d, k2 = q % d;
@@ -228,39 +245,45 @@ __global__ void moments_kernel(const float* pts, int64_t cnt, int d, double* par
   for (int k = threadIdx.x; k < K; k += blockDim.x) part[(int64_t)blockIdx.x * K + k] = acc[k];
 }
 
-// out[0] = mean(C), out[1] = mean(C^2) from the x and y moment partials.
-__global__ void cost_stats_reduce_kernel(const double* px, const double* py, int nblk,
-                                         int d, double inv, double* mom, double* out) {
-  const int K = 3 + 2 * d + d * d;
-  for (int k = threadIdx.x; k < 2 * K; k += blockDim.x) {
-    const double* src = k < K ? px : py;
-    const int e = k < K ? k : k - K;
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += src[(int64_t)b * K + e];
-    mom[k] = s;
+// mom[k] = sum over the nblk partials of entry k, one thread per entry, for
+// the concatenated x and y moment vectors.
+__global__ void moments_reduce_kernel(const double* px, const double* py, int nblk, int K,
+                                      double* mom) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= 2 * K) return;
+  const double* src = k < K ? px : py;
+  const int e = k < K ? k : k - K;
+  double s = 0.0;
+  for (int b = 0; b < nblk; ++b) s += src[(int64_t)b * K + e];
+  mom[k] = s;
+}
+
+// out[0] = mean(C), out[1] = mean(C^2) (when second != 0) from the moments.
+__global__ void cost_stats_final_kernel(const double* mom, int d, int second, double inv,
+                                        double* out) {
+  const int K = moments_len(d, second);
+  const double* X = mom;
+  const double* Y = mom + K;
+  const double n = X[0], m = Y[0];
+  const double mnx = X[1] / n, mny = Y[1] / m;
+  double xy = 0.0, nxy = 0.0, xny = 0.0;
+  for (int k = 0; k < d; ++k) {
+    xy += (X[3 + k] / n) * (Y[3 + k] / m);
+    nxy += (X[3 + d + k] / n) * (Y[3 + k] / m);
+    xny += (X[3 + k] / n) * (Y[3 + d + k] / m);
   }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    const double* X = mom;
-    const double* Y = mom + K;
-    const double n = X[0], m = Y[0];
-    const double mnx = X[1] / n, mny = Y[1] / m;
-    const double mnx2 = X[2] / n, mny2 = Y[2] / m;
-    double xy = 0.0, nxy = 0.0, xny = 0.0, tr = 0.0;
-    for (int k = 0; k < d; ++k) {
-      xy += (X[3 + k] / n) * (Y[3 + k] / m);
-      nxy += (X[3 + d + k] / n) * (Y[3 + k] / m);
-      xny += (X[3 + k] / n) * (Y[3 + d + k] / m);
-    }
+  out[0] = inv * (mnx + mny - 2.0 * xy);
+  if (second) {
+    double tr = 0.0;
     for (int k1 = 0; k1 < d; ++k1)
       for (int k2 = 0; k2 < d; ++k2)
         tr += X[3 + 2 * d + k1 * d + k2] * Y[3 + 2 * d + k2 * d + k1];
     tr /= (n * m);
-    const double mean = inv * (mnx + mny - 2.0 * xy);
-    const double msq = inv * inv *
-        (mnx2 + mny2 + 2.0 * mnx * mny + 4.0 * tr - 4.0 * nxy - 4.0 * xny);
-    out[0] = mean;
-    out[1] = msq;
+    const double mnx2 = X[2] / n, mny2 = Y[2] / m;
+    out[1] = inv * inv *
+             (mnx2 + mny2 + 2.0 * mnx * mny + 4.0 * tr - 4.0 * nxy - 4.0 * xny);
+  } else {
+    out[1] = NAN;
   }
 }
 

@@ -137,6 +137,21 @@ bool encode_points_map(CUtensorMap* map, void* base, int64_t pad, int dk) {
          CUDA_SUCCESS;
 }
 
+// Tensor map over column-shift rows [rows][8] bf16: boxes of 8 x 128, no
+// swizzle (the K-major core-matrix layout of an MMA extension block).
+bool encode_ext_map(CUtensorMap* map, void* base, int64_t rows) {
+  EncodeTiledFn fn = encode_tiled_fn();
+  if (!fn) return false;
+  const cuuint64_t dims[2] = {8, (cuuint64_t)rows};
+  const cuuint64_t strides[1] = {16};
+  const cuuint32_t box[2] = {8, 128};
+  const cuuint32_t estr[2] = {1, 1};
+  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 // Grid size of the persistent launch: all CTAs co-resident.
 int persistent_grid(const KernelChoice& k, int sms) {
   static std::mutex mu;
@@ -175,7 +190,7 @@ struct ProbPlan {
   int64_t n, m, n_pad, m_pad;
   int rb_f, rb_g, split_f, split_g;
   size_t off_xt, off_yt, off_nx, off_ny, off_galt, off_pm, off_pl, off_arr, off_err,
-      off_msum;
+      off_msum, off_extx, off_exty;
 };
 
 // BF16 split-3 on tcgen05 when asked for, and by default where the inner
@@ -287,6 +302,9 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.off_arr = off; off = align_up(off + sizeof(int) * std::max(pp.rb_f, pp.rb_g));
     pp.off_err = off; off = align_up(off + sizeof(double) * pp.rb_g);
     pp.off_msum = off; off = align_up(off + sizeof(double) * pp.rb_g);
+    // tensor-core path: column-shift rows, 16 bytes per point (y: per g buffer)
+    pp.off_extx = off; off = align_up(off + (plan.tc ? 16 * pp.n_pad : 0));
+    pp.off_exty = off; off = align_up(off + (plan.tc ? 16 * 2 * pp.m_pad : 0));
   }
   plan.total = off;
   return OTTB_OK;
@@ -369,8 +387,12 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
       P.yh = ws + pp.off_yt;
       TcMaps maps;  // 64-byte aligned, then copied into the header image
       if (!encode_points_map(&maps.x, ws + pp.off_xt, pp.n_pad, plan.dp) ||
-          !encode_points_map(&maps.y, ws + pp.off_yt, pp.m_pad, plan.dp))
+          !encode_points_map(&maps.y, ws + pp.off_yt, pp.m_pad, plan.dp) ||
+          !encode_ext_map(&maps.extx, ws + pp.off_extx, pp.n_pad) ||
+          !encode_ext_map(&maps.exty, ws + pp.off_exty, 2 * pp.m_pad))
         return OTTB_ERR_CUDA;
+      P.extx = ws + pp.off_extx;
+      P.exty = ws + pp.off_exty;
       std::memcpy(host.data() + plan.off_maps + sizeof(TcMaps) * t, &maps, sizeof(TcMaps));
       P.maps = ws + plan.off_maps + sizeof(TcMaps) * t;
     } else {
@@ -426,7 +448,7 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
   ProbDev* d_probs = (ProbDev*)(ws + plan.off_probs);
   const float* const* d_ptrs = (const float* const*)(ws + plan.off_ptrs);
   int64_t maxpts = 1;
-  for (const ProbPlan& pp : plan.probs) maxpts = std::max(maxpts, std::max(pp.n_pad, pp.m_pad) + pp.n + pp.m);
+  for (const ProbPlan& pp : plan.probs) maxpts = std::max(maxpts, pp.n_pad + 2 * pp.m_pad);
 
   {
     dim3 grid(std::max(1, (outer + 255) / 256), num_problems);
@@ -478,35 +500,38 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
 
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {
   if (n < 1 || m < 1 || d < 1 || d > 128) return 0;
-  const size_t K = 3 + 2 * (size_t)d + (size_t)d * d;
+  const size_t K = (size_t)moments_len(d, 1);
   return align_up(sizeof(double) * K * 2 * 148) + align_up(sizeof(double) * 2 * K);
 }
 
 int32_t ottb_cost_stats(const float* x, const float* y, int64_t n, int64_t m, int32_t d,
-                        float inv_scale_cost, double* out, void* workspace,
+                        float inv_scale_cost, int32_t second, double* out, void* workspace,
                         size_t workspace_bytes, void* stream_ptr) {
   if (!x || !y || !out || n < 1 || m < 1 || d < 1) return OTTB_ERR_INVALID;
   if (d > 128) return OTTB_ERR_UNSUPPORTED;
   const size_t need = ottb_cost_stats_workspace_size(n, m, d);
   if (!workspace || workspace_bytes < need) return OTTB_ERR_WORKSPACE;
   cudaStream_t stream = (cudaStream_t)stream_ptr;
-  const int K = 3 + 2 * d + d * d;
-  const int nblk = 148;
+  second = second ? 1 : 0;
+  const int K = moments_len(d, second);
+  const int64_t pts = std::max(n, m);
+  const int nblk = (int)std::min<int64_t>(148, (pts + 255) / 256);
   double* px = (double*)workspace;
   double* py = px + (size_t)K * nblk;
-  double* mom = (double*)((char*)workspace + align_up(sizeof(double) * K * 2 * 148));
-  const size_t smem = sizeof(double) * K + sizeof(float) * 64 * d;
+  double* mom = (double*)((char*)workspace + align_up(sizeof(double) * moments_len(d, 1) * 2 * 148));
+  const size_t smem = sizeof(double) * (K + 64) + sizeof(float) * 64 * d;
   static std::mutex mu;
   {
     std::lock_guard<std::mutex> lock(mu);
     if (cudaFuncSetAttribute((void*)moments_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
+                             (int)(sizeof(double) * (moments_len(128, 1) + 64) +
+                                   sizeof(float) * 64 * 128)) != cudaSuccess)
       return OTTB_ERR_CUDA;
   }
-  moments_kernel<<<nblk, 256, smem, stream>>>(x, n, d, px);
-  moments_kernel<<<nblk, 256, smem, stream>>>(y, m, d, py);
-  cost_stats_reduce_kernel<<<1, 256, 0, stream>>>(px, py, nblk, d, (double)inv_scale_cost, mom,
-                                                  out);
+  moments_kernel<<<nblk, 256, smem, stream>>>(x, n, d, second, px);
+  moments_kernel<<<nblk, 256, smem, stream>>>(y, m, d, second, py);
+  moments_reduce_kernel<<<(2 * K + 255) / 256, 256, 0, stream>>>(px, py, nblk, K, mom);
+  cost_stats_final_kernel<<<1, 1, 0, stream>>>(mom, d, second, (double)inv_scale_cost, out);
   return cuda_status(cudaGetLastError());
 }
 

@@ -4,6 +4,7 @@
 // is bounded by %globaltimer, and small numeric helpers.
 #pragma once
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -48,6 +49,10 @@ struct ProbDev {
   const void* xh;
   const void* yh;
   const void* maps;
+  // tensor-core path: column-shift rows [pad][8] bf16 of x and [2][pad][8]
+  // of y (one per g buffer), written by every potential update
+  void* extx;
+  void* exty;
   // workspace: split partials (m, l) [S][rows] and per-row-block data
   float* part_m;
   float* part_l;
@@ -111,6 +116,48 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
+// 2^x on the FMA pipe, to take part of the exponentials off the MUFU pipe.
+// Range reduction x = n + f, n = rint(x), f in [-1/2, 1/2] (exact for
+// |x| < 2^22: adding 1.5 * 2^23 rounds x to an integer in the low mantissa
+// bits); 2^f by a degree-5 polynomial minimising the maximum relative error
+// on [-1/2, 1/2], fitted by exp2_poly_fit.py (Remez exchange; 7.5e-8
+// minimax, 2.3e-7 evaluated in FP32); 2^n by adding n to the exponent
+// field. Inputs below -126 are clamped (the result, < 2^-125, is negligible
+// next to the running sum's leading term >= 1); callers keep x <= kTau + 1.
+__device__ __forceinline__ float exp2_poly(float x) {
+  x = fmaxf(x, -126.0f);
+  const float t = x + 12582912.0f;  // 1.5 * 2^23
+  const float f = x - (t - 12582912.0f);
+  float p = 1.327647245e-03f;
+  p = fmaf(p, f, 9.675540961e-03f);
+  p = fmaf(p, f, 5.550713092e-02f);
+  p = fmaf(p, f, 2.402212024e-01f);
+  p = fmaf(p, f, 6.931469440e-01f);
+  p = fmaf(p, f, 1.000000119e+00f);
+  // t's bits are 0x4B400000 + n; shifted left by 23 they are n << 23.
+  return __int_as_float(__float_as_int(p) + (__float_as_int(t) << 23));
+}
+
+// Of every 8 exponentials, this many go to exp2_poly: in the CUDA-core
+// engine at d <= 4, where the MUFU pipe binds (measured at n = m = 32768,
+// d = 2: 2 of 8 is 2 % faster than 0, 3 of 8 slower); and in the tensor-core
+// epilogue, where issue slots bind instead (n = m = 65536, d = 64: 0 of 8
+// fastest, every step to 4 of 8 slower by 4-10 %).
+#ifndef OTTB_POLY_OF_8
+#define OTTB_POLY_OF_8 2
+#endif
+#ifndef OTTB_POLY_OF_8_TC
+#define OTTB_POLY_OF_8_TC 0
+#endif
+
+// Three-input maximum (sm_100 max.f32 with three sources; NaN operands are
+// ignored as by fmaxf).
+__device__ __forceinline__ float fmax3(float a, float b, float c) {
+  float d;
+  asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+  return d;
+}
+
 // Compensated accumulation s + c += x (Knuth's TwoSum: c collects the exact
 // rounding error of every addition). Each tile's terms are first summed in a
 // short tree; adding that tile sum to a long-running FP32 total would
@@ -124,6 +171,24 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
   const float err = (s - (t - bb)) + (x - bb);
   s = t;
   c += err;
+}
+
+// One 16-byte column-shift row of the tensor-core path: w' = (pot - inv
+// |p|^2) / (2 inv) as three bf16 terms w1 + w2 + w3 (~24 bits) followed by
+// five zeros. A non-finite w' (zero-weight potentials, padding rows = -inf)
+// is carried by w1 alone, so no inf - inf = NaN appears.
+__device__ __forceinline__ void write_ext_row(void* row16, float w) {
+  const bool fin = isfinite(w);
+  const __nv_bfloat16 w1 = __float2bfloat16_rn(w);
+  const float r1 = fin ? w - __bfloat162float(w1) : 0.f;
+  const __nv_bfloat16 w2 = __float2bfloat16_rn(r1);
+  const __nv_bfloat16 w3 = __float2bfloat16_rn(fin ? r1 - __bfloat162float(w2) : 0.f);
+  uint4 v;
+  v.x = (uint32_t)__bfloat16_as_ushort(w1) | ((uint32_t)__bfloat16_as_ushort(w2) << 16);
+  v.y = (uint32_t)__bfloat16_as_ushort(w3);
+  v.z = 0u;
+  v.w = 0u;
+  *reinterpret_cast<uint4*>(row16) = v;
 }
 
 // Merge two (shift, sum) log-sum-exp states in base 2.

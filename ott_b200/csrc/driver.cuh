@@ -113,7 +113,16 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
     const double logm = log(mg);
     const bool keep = isfinite(old) && isfinite(app);
     const double newp = eps * logm - (keep ? app : 0.0);
-    if (sp.write) outp[r] = (float)newp;
+    if (sp.write) {
+      const float nf = (float)newp;
+      outp[r] = nf;
+      // tensor-core path: the updated point's column shift for the next sweep
+      void* ext = isG ? P.exty : P.extx;
+      if (ext) {
+        const int64_t row = isG ? (int64_t)(parity ^ 1) * P.m_pad + r : r;
+        write_ext_row((char*)ext + row * 16, (nf - na[r]) * (0.5f / P.inv_scale));
+      }
+    }
     if (sp.eval) {
       double bh = 0.0;
       if (!(old == -INFINITY)) bh = exp2(lse2 + (old - nrm) * (double)ws);

@@ -132,9 +132,8 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i) {
-      float cm = acc[i][0];
-#pragma unroll
-      for (int j = 1; j < 8; ++j) cm = fmaxf(cm, acc[i][j]);
+      const float cm = fmaxf(fmax3(acc[i][0], acc[i][1], acc[i][2]),
+                             fmax3(acc[i][3], acc[i][4], fmax3(acc[i][5], acc[i][6], acc[i][7])));
       if (cm > mrow[i] + kTau) {
         const float sc = ex2_approx(mrow[i] - cm);
         lrow[i] *= sc;
@@ -143,7 +142,11 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
       }
       float e[8];
 #pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(acc[i][j] - mrow[i]);
+      for (int j = 0; j < 8; ++j) {
+        const float xj = acc[i][j] - mrow[i];
+        // small d is MUFU-bound: part of the exponentials on the FMA pipe
+        e[j] = (DP <= 4 && j >= 8 - OTTB_POLY_OF_8) ? exp2_poly(xj) : ex2_approx(xj);
+      }
       const float sum = ((e[0] + e[1]) + (e[2] + e[3])) + ((e[4] + e[5]) + (e[6] + e[7]));
       two_sum_acc(lrow[i], lcmp[i], sum);
     }

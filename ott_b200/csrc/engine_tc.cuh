@@ -10,12 +10,15 @@
 // extension block holds ones in its first 3 K columns, B's holds
 // w'_c = (pot_c - inv |B_c|^2) / (2 inv) as 3 bf16 terms (~24 bits), so the
 // accumulator is acc = <a_r, b_c> + w'_c and the exponent is s * acc,
-// s = 2 inv log2(e) / eps. The epilogue needs no per-column data.
+// s = 2 inv log2(e) / eps. The epilogue needs no per-column data, and w' is
+// computed once per point per sweep: every potential update writes its
+// point's row of the global extension array (write_ext_row), which the
+// producer loads by TMA with the B tile.
 //
 // Warp roles in the 576-thread CTA:
-//   warp 0      producer: A tile once per unit; B tiles through a ring of
-//               kStages shared-memory stages (TMA, no multicast), and each
-//               stage's w' extension block.
+//   warp 0      producer (lane 0): A tile once per unit; B tiles and their
+//               column-shift rows through a ring of kStages shared-memory
+//               stages (TMA, no multicast).
 //   warp 1      TMEM owner and MMA issuer (lane 0): two 128-column
 //               accumulators, so MMAs of tile t+1 overlap the epilogue of t.
 //   warps 2-17  epilogue: warp w reads TMEM lanes 32*(w%4).. (its rows) and
@@ -43,17 +46,14 @@ struct TcCfg {
   static constexpr int kEpiWarps = 4 * kColGroups;
   static constexpr int kThreads = 64 + 32 * kEpiWarps;
   static constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, 128);
-  // extension block: 128 rows x 16 bf16, 8-row groups 256 B apart, K halves
-  // 128 B apart, rows 16 B apart
+  // extension block: 128 rows x 16 bf16, K-major without swizzle: K half 0
+  // (elements 0-7) of all rows first, rows 16 B apart (8-row groups 128 B
+  // apart), then K half 1 (all zeros) 2048 B on
   static constexpr int kExtBytes = 128 * 16 * 2;
-  static constexpr uint32_t kExtLbo = 128;
-  static constexpr uint32_t kExtSbo = 256;
+  static constexpr int kExtHalfBytes = 128 * 16;
+  static constexpr uint32_t kExtLbo = 2048;
+  static constexpr uint32_t kExtSbo = 128;
 };
-
-// Byte offset of element (row, k) in an extension block.
-__device__ __forceinline__ int ext_offset(int row, int k) {
-  return (row >> 3) * 256 + (k >> 3) * 128 + (row & 7) * 16 + (k & 7) * 2;
-}
 
 template <int DK>
 struct TcSmem {
@@ -91,11 +91,15 @@ struct TcPipe {
   int issued;
 };
 
-// Tensor maps of a problem's point sets, [2 * pad][DK] bf16 (hi rows, then
-// lo rows), box 64 x 128, 128-byte swizzle. Stored in global memory.
+// Tensor maps of a problem, stored in global memory: the point sets
+// [2 * pad][DK] bf16 (hi rows, then lo rows; box 64 x 128, 128-byte swizzle)
+// and their column-shift rows [pad][8] and [2 * pad][8] bf16 (box 8 x 128,
+// no swizzle).
 struct TcMaps {
   CUtensorMap x;
   CUtensorMap y;
+  CUtensorMap extx;
+  CUtensorMap exty;
 };
 
 template <int DK>
@@ -144,33 +148,13 @@ __device__ __forceinline__ void tc_issue_ext(uint32_t d_tmem, const uint8_t* Aex
   tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, 1);
 }
 
-// w' split into three bf16 terms, written at K = 0, 1, 2 of row `row`
-// (K = 3..15 stay zero).
-// A non-finite w' (padding columns and zero-weight potentials are -inf) is
-// carried by the first term alone, so no inf - inf = NaN appears.
-__device__ __forceinline__ void write_ext_shift(uint8_t* blk, int row, float w) {
-  const bool fin = isfinite(w);
-  const __nv_bfloat16 w1 = __float2bfloat16_rn(w);
-  const float r1 = fin ? w - __bfloat162float(w1) : 0.f;
-  const __nv_bfloat16 w2 = __float2bfloat16_rn(r1);
-  const __nv_bfloat16 w3 = __float2bfloat16_rn(fin ? r1 - __bfloat162float(w2) : 0.f);
-  __nv_bfloat162 p01;
-  p01.x = w1;
-  p01.y = w2;
-  __nv_bfloat162 p23;
-  p23.x = w3;
-  p23.y = __float2bfloat16_rn(0.f);
-  *reinterpret_cast<__nv_bfloat162*>(blk + ext_offset(row, 0)) = p01;
-  *reinterpret_cast<__nv_bfloat162*>(blk + ext_offset(row, 2)) = p23;
-}
-
 // Operands of one tensor-core sweep for one problem.
 struct TcOperands {
   const CUtensorMap* mapA;
   const CUtensorMap* mapB;
+  const CUtensorMap* mapBext;
   int32_t padA, padB;
-  const float* potB;
-  const float* nb;
+  int32_t extRow0;  // first row of B's column-shift rows (g buffer of y)
   int64_t rows, cols;
 };
 
@@ -178,14 +162,12 @@ struct TcOperands {
 // Leaves the per-row base-2 LSE state in sm.rm / sm.rl. Returns false if a
 // wait timed out.
 //
-// Per ring stage st the producer warp fills B's hi/lo tiles (TMA) and the
-// stage's w' extension block (plain loads of pot and |B|^2 one tile ahead in
-// registers, generic stores, then an async-proxy fence); full[st] completes
-// on the TMA bytes plus 32 lane arrivals, empty[st] on the MMA commit.
-// wshift = 1 / (2 inv).
+// Per ring stage st the producer fills B's hi/lo tiles and the first K half
+// of B's extension block (TMA); full[st] completes on those bytes,
+// empty[st] on the MMA commit.
 template <int DK>
 __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
-                        int t0, int t1, float s, float wshift, uint64_t timeout_ns) {
+                        int t0, int t1, float s, uint64_t timeout_ns) {
   constexpr int NS = TcCfg<DK>::kStages;
   constexpr int NB = TcCfg<DK>::kTmemBufs;
   constexpr int CG = TcCfg<DK>::kColGroups;
@@ -196,13 +178,6 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
   bool ok = true;
 
   if (warp == 0) {
-    // w' of the first tile, 4 columns per lane
-    float wreg[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-      const int64_t c = (int64_t)t0 * kBN + lane + 32 * k;
-      wreg[k] = c < op.cols ? (__ldcg(op.potB + c) - op.nb[c]) * wshift : -INFINITY;
-    }
     if (lane == 0) {
       // A tile: wait until the previous unit's MMAs released it.
       if (!tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns)) ok = false;
@@ -210,33 +185,18 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
         tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK>::kOperandBytes);
         tc_load_operand<DK>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
       }
-    }
-    ok = __shfl_sync(0xffffffffu, ok ? 1 : 0, 0) != 0;
-    for (int i = 0; ok && i < ntiles; ++i) {
-      const uint32_t g = pp.tile + i;
-      const uint32_t st = g % NS;
-      const bool got = tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns);
-      if (!__all_sync(0xffffffffu, got)) {
-        ok = false;
-        break;
-      }
-      if (lane == 0) {
-        tc::mbar_expect_tx(&sm.full[st], TcCfg<DK>::kOperandBytes);
-        tc_load_operand<DK>(sm.B[st], op.mapB, &sm.full[st], (t0 + i) * kBN, op.padB);
+      for (int i = 0; ok && i < ntiles; ++i) {
+        const uint32_t g = pp.tile + i;
+        const uint32_t st = g % NS;
+        if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
+        const int32_t brow = (t0 + i) * kBN;
+        tc::mbar_arrive_expect_tx(&sm.full[st],
+                                  TcCfg<DK>::kOperandBytes + TcCfg<DK>::kExtHalfBytes);
+        tc_load_operand<DK>(sm.B[st], op.mapB, &sm.full[st], brow, op.padB);
+        tc::tma_load_2d(sm.Bext[st], op.mapBext, &sm.full[st], 0, op.extRow0 + brow);
         pp.last_full_stage = st;
         pp.last_full_parity = (g / NS) & 1;
         pp.issued = 1;
-      }
-#pragma unroll
-      for (int k = 0; k < 4; ++k) write_ext_shift(sm.Bext[st], lane + 32 * k, wreg[k]);
-      tc::fence_proxy_async_smem();
-      tc::mbar_arrive(&sm.full[st]);
-      if (i + 1 < ntiles) {
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const int64_t c = (int64_t)(t0 + i + 1) * kBN + lane + 32 * k;
-          wreg[k] = c < op.cols ? (__ldcg(op.potB + c) - op.nb[c]) * wshift : -INFINITY;
-        }
       }
     }
     __syncwarp();
@@ -282,9 +242,15 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
       tc::fence_before_sync();
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
-      float amax = v[0];
+      // tree maximum (depth 4) instead of a 31-step dependent chain
+      float t11[11];
 #pragma unroll
-      for (int j = 1; j < CW; ++j) amax = fmaxf(amax, v[j]);
+      for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
+      t11[10] = fmaxf(v[30], v[31]);
+      const float u0 = fmax3(t11[0], t11[1], t11[2]);
+      const float u1 = fmax3(t11[3], t11[4], t11[5]);
+      const float u2 = fmax3(t11[6], t11[7], t11[8]);
+      const float amax = fmaxf(fmax3(u0, u1, u2), fmaxf(t11[9], t11[10]));
       const float cm = amax * s;  // s > 0
       if (cm > mrun + kTau) {
         const float sc = ex2_approx(mrun - cm);
@@ -293,15 +259,21 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
         mrun = cm;
       }
       const float negm = -mrun;
-      float acc4[4] = {0.f, 0.f, 0.f, 0.f};
+      // 8 accumulators; lanes k >= 8 - OTTB_POLY_OF_8_TC of each group of 8
+      // columns use exp2_poly (FMA pipe), the rest ex2.approx (MUFU).
+      float acc8[8];
 #pragma unroll
-      for (int j = 0; j < CW; j += 4) {
-        acc4[0] += ex2_approx(fmaf(v[j], s, negm));
-        acc4[1] += ex2_approx(fmaf(v[j + 1], s, negm));
-        acc4[2] += ex2_approx(fmaf(v[j + 2], s, negm));
-        acc4[3] += ex2_approx(fmaf(v[j + 3], s, negm));
+      for (int k = 0; k < 8; ++k) acc8[k] = 0.f;
+#pragma unroll
+      for (int j = 0; j < CW; j += 8) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float xk = fmaf(v[j + k], s, negm);
+          acc8[k] += (k >= 8 - OTTB_POLY_OF_8_TC) ? exp2_poly(xk) : ex2_approx(xk);
+        }
       }
-      two_sum_acc(lrun, lcmp, (acc4[0] + acc4[1]) + (acc4[2] + acc4[3]));
+      two_sum_acc(lrun, lcmp, ((acc8[0] + acc8[1]) + (acc8[2] + acc8[3])) +
+                                  ((acc8[4] + acc8[5]) + (acc8[6] + acc8[7])));
     }
     sm.part_m[cg][r] = mrun;
     sm.part_l[cg][r] = lrun + lcmp;

@@ -23,8 +23,8 @@ sinkhorn_simt_kernel(KernelArgs A) {
   SimtKernelSmem<DP>& sm = *reinterpret_cast<SimtKernelSmem<DP>*>(smem_raw);
   const CommonSmem cs{sm.rm, sm.rl, sm.red, &sm.unit, &sm.last};
   auto sweep = [&](const SweepParams& sp, unsigned idx) -> bool {
-    auto unit = [&](const ProbDev& P, const float* gcur, int rb, int t0, int t1, float s,
-                    float wscale) -> bool {
+    auto unit = [&](const ProbDev& P, const float* gcur, int parity, int rb, int t0, int t1,
+                    float s, float wscale) -> bool {
       const SweepOperands op = make_operands(P, sp.kind, gcur);
       simt_unit<DP>(sm.tiles, op, (int64_t)rb * kBM, t0, t1, s, wscale, sm.rm, sm.rl);
       return true;

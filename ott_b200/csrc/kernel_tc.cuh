@@ -9,17 +9,17 @@
 namespace ottb {
 
 __device__ __forceinline__ TcOperands make_tc_operands(const ProbDev& P, int kind,
-                                                       const float* gcur) {
+                                                       int parity) {
   const TcMaps* maps = reinterpret_cast<const TcMaps*>(P.maps);
   TcOperands op;
   if (kind == kSweepG) {
     op.mapA = &maps->y; op.padA = (int32_t)P.m_pad; op.rows = P.m;
     op.mapB = &maps->x; op.padB = (int32_t)P.n_pad; op.cols = P.n;
-    op.potB = P.f; op.nb = P.nx;
+    op.mapBext = &maps->extx; op.extRow0 = 0;
   } else {
     op.mapA = &maps->x; op.padA = (int32_t)P.n_pad; op.rows = P.n;
     op.mapB = &maps->y; op.padB = (int32_t)P.m_pad; op.cols = P.m;
-    op.potB = gcur; op.nb = P.ny;
+    op.mapBext = &maps->exty; op.extRow0 = (int32_t)(parity * P.m_pad);
   }
   return op;
 }
@@ -40,7 +40,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
   if (threadIdx.x == 0) {
     constexpr int NE = TcCfg<DK>::kEpiWarps;
     for (int i = 0; i < NS; ++i) {
-      tc::mbar_init(&sm.full[i], 32);  // producer lanes (+ TMA bytes)
+      tc::mbar_init(&sm.full[i], 1);   // producer arrival + TMA bytes
       tc::mbar_init(&sm.empty[i], 1);  // MMA commit
     }
     for (int i = 0; i < NB; ++i) {
@@ -69,7 +69,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
     if (threadIdx.x < kBM) {
       const __nv_bfloat16 one = __float2bfloat16_rn(1.f);
       for (int k = 0; k < 3; ++k)
-        *reinterpret_cast<__nv_bfloat16*>(sm.Aext + ext_offset(threadIdx.x, k)) = one;
+        reinterpret_cast<__nv_bfloat16*>(sm.Aext + threadIdx.x * 16)[k] = one;
     }
     tc::fence_proxy_async_smem();
   }
@@ -80,10 +80,10 @@ sinkhorn_tc_kernel(KernelArgs A) {
   TcPipe pp{0u, 0u, 0u, 0u, 0};
   const CommonSmem cs{sm.rm, sm.rl, sm.red, &sm.unit, &sm.last};
   auto sweep = [&](const SweepParams& sp, unsigned idx) -> bool {
-    auto unit = [&](const ProbDev& P, const float* gcur, int rb, int t0, int t1, float s,
-                    float wscale) -> bool {
-      const TcOperands op = make_tc_operands(P, sp.kind, gcur);
-      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, 0.5f / P.inv_scale, A.timeout_ns);
+    auto unit = [&](const ProbDev& P, const float* gcur, int parity, int rb, int t0, int t1,
+                    float s, float wscale) -> bool {
+      const TcOperands op = make_tc_operands(P, sp.kind, parity);
+      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, A.timeout_ns);
     };
     return sweep_units(A, sp, idx, cs, unit);
   };

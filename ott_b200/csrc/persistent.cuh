@@ -130,7 +130,7 @@ struct CommonSmem {
 };
 
 // One sweep over the units of the scheduled problems, common to both
-// engines. unit_fn(P, gcur, rb, t0, t1, s, wscale) computes the (shift, sum)
+// engines. unit_fn(P, gcur, parity, rb, t0, t1, s, wscale) computes the (shift, sum)
 // state of the 128 rows of row block rb over column tiles [t0, t1) into
 // cs.rm / cs.rl and returns false on a device-side timeout. Units are dealt
 // round-robin (one problem) or from an atomic queue (several problems, in
@@ -174,7 +174,7 @@ __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned
     const float wscale = sweep_wscale(P, sp.mult);
     const float s = 2.0f * P.inv_scale * wscale;
 
-    if (!unit_fn(P, gcur, rb, t0, t1, s, wscale)) return false;
+    if (!unit_fn(P, gcur, parity, rb, t0, t1, s, wscale)) return false;
 
     bool do_final = true;
     if (S > 1) {

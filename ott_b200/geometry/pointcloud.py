@@ -84,7 +84,7 @@ class PointCloud(geometry.Geometry):
     return n == m
 
   # -- cost statistics (geometry.py:113-135 via pointcloud.py:170-186) -----
-  def _cost_stats(self, inv_scale: float) -> Tuple[float, float]:
+  def _cost_stats(self, inv_scale: float, second: bool) -> Tuple[float, float]:
     lib = _lib.load()
     n, m = self.shape
     d = self.dim
@@ -94,7 +94,7 @@ class PointCloud(geometry.Geometry):
     ws = torch.empty(ws_bytes, dtype=torch.uint8, device=self.x.device)
     out = torch.empty(2, dtype=torch.float64, device=self.x.device)
     st = lib.ottb_cost_stats(self.x.data_ptr(), self.y.data_ptr(), n, m, d,
-                             ctypes.c_float(inv_scale), out.data_ptr(),
+                             ctypes.c_float(inv_scale), 1 if second else 0, out.data_ptr(),
                              ws.data_ptr(), ws_bytes, _arrays.stream_handle())
     _lib.check(st, "ottb_cost_stats")
     mean, msq = out.tolist()
@@ -108,23 +108,23 @@ class PointCloud(geometry.Geometry):
       return 1.0 / float(sc)
     if sc == "mean":
       if self._stats_unscaled is None:
-        self._stats_unscaled = self._cost_stats(1.0)
+        self._stats_unscaled = self._cost_stats(1.0, second=False)
       return 1.0 / self._stats_unscaled[0]
     raise NotImplementedError(f"scale_cost={sc!r} is not on this path")
 
-  def _scaled_stats(self) -> Tuple[float, float]:
-    if self._stats is None:
-      self._stats = self._cost_stats(self.inv_scale_cost)
+  def _scaled_stats(self, second: bool) -> Tuple[float, float]:
+    if self._stats is None or (second and self._stats[1] != self._stats[1]):
+      self._stats = self._cost_stats(self.inv_scale_cost, second)
     return self._stats
 
   @property
   def mean_cost_matrix(self) -> float:
-    return self._scaled_stats()[0]
+    return self._scaled_stats(second=False)[0]
 
   @property
   def std_cost_matrix(self) -> float:
     """``sqrt(relu(mean(C^2) - mean(C)^2))`` (geometry.py:120-135)."""
-    mean, msq = self._scaled_stats()
+    mean, msq = self._scaled_stats(second=True)
     return max(msq - mean * mean, 0.0) ** 0.5
 
   def __repr__(self) -> str:

@@ -52,5 +52,5 @@ def test_invalid_arguments_rejected_without_device():
   assert lib.ottb_sinkhorn_workspace_size(None, 0, 2, ctypes.byref(cfg)) == 0
   st = lib.ottb_sinkhorn_pointcloud(None, 1, 2, ctypes.byref(cfg), None, None, 0, None)
   assert st == _lib.OTTB_ERR_INVALID
-  assert lib.ottb_cost_stats(None, None, 0, 0, 2, ctypes.c_float(1.0), None, None, 0,
+  assert lib.ottb_cost_stats(None, None, 0, 0, 2, ctypes.c_float(1.0), 1, None, None, 0,
                              None) == _lib.OTTB_ERR_INVALID
