@@ -82,6 +82,9 @@ typedef struct ottb_solver_cfg {
   int32_t timeout_ms;       /* device wait limit, 0 = default (60 s)        */
   int32_t phantom_arrivals; /* extra grid-barrier arrivals to wait for; 0 in
                                normal use, > 0 only to exercise the timeout */
+  int32_t init_f_from_g;    /* 1: before the loop, f = the f-update of the
+                               initial g (the initializer predicted g; the
+                               first g-update would otherwise discard it)  */
 } ottb_solver_cfg;
 
 /* Per-problem scalar results, written to device memory. */
@@ -143,6 +146,62 @@ int32_t ottb_cost_stats(const float* x, const float* y, int64_t n, int64_t m,
                         int32_t d, float inv_scale_cost, int32_t second,
                         double* out, void* workspace, size_t workspace_bytes,
                         void* stream);
+
+/* ---------------------------------------------------------------------
+ * Learned initializer network (replaces the meta model of
+ * ott/initializers/neural/meta_initializer.py:36-213: flax Dense layers
+ * applied to concat(a, b) in _compute_f :192-207, trained with optax Adam in
+ * update :101-135). Dense layers y = x W^T + b, tanh-GELU between layers,
+ * linear last layer; bf16 operands on tcgen05 tensor cores with FP32
+ * accumulation and FP32 master weights. Every width and the batch must be a
+ * multiple of 128. All pointers are device pointers owned by the caller.
+ * --------------------------------------------------------------------- */
+#define OTTB_MLP_MAX_LAYERS 8
+
+typedef struct ottb_mlp_layer {
+  int32_t in;        /* input width                                      */
+  int32_t out;       /* output width                                     */
+  float* w;          /* [out, in] FP32 master weights                    */
+  void* w_bf16;      /* [out, in] bf16 copy (GEMM operand)               */
+  void* wt_bf16;     /* [in, out] bf16 transposed copy                   */
+  float* b;          /* [out] bias                                       */
+  float* w_m;        /* Adam first / second moments of w and b           */
+  float* w_v;
+  float* b_m;
+  float* b_v;
+  float* w_grad;     /* [out, in] written by ottb_mlp_gradients          */
+  float* b_grad;     /* [out]                                            */
+} ottb_mlp_layer;
+
+typedef struct ottb_mlp {
+  int32_t num_layers;
+  ottb_mlp_layer layers[OTTB_MLP_MAX_LAYERS];
+} ottb_mlp;
+
+/* Workspace bytes for activations and gradients of one batch. */
+size_t ottb_mlp_workspace_size(const ottb_mlp* net, int32_t batch);
+
+/* y[batch, out] = net(x[batch, in]). *status (device int) receives
+ * OTTB_ERR_TIMEOUT if a device wait gave up. */
+int32_t ottb_mlp_forward(const ottb_mlp* net, const float* x, int32_t batch,
+                         float* y, int32_t* status, void* workspace,
+                         size_t workspace_bytes, void* stream);
+
+/* Gradients of the batch-mean centred squared error
+ * (1/m) sum_j ((y_j - mean(y)) - (t_j - mean(t)))^2 into every layer's
+ * w_grad / b_grad; loss_per[batch] receives each sample's loss. */
+int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x,
+                           const float* target, int32_t batch, float* loss_per,
+                           int32_t* status, void* workspace,
+                           size_t workspace_bytes, void* stream);
+
+/* One Adam step (bias-corrected, step >= 1) on every layer from its
+ * gradients; refreshes the bf16 copies. */
+int32_t ottb_mlp_adam(const ottb_mlp* net, float lr, float beta1, float beta2,
+                      float eps, int32_t step, void* stream);
+
+/* Refreshes the bf16 copies (w_bf16, wt_bf16) from the FP32 weights. */
+int32_t ottb_mlp_sync_bf16(const ottb_mlp* net, void* stream);
 
 /* Human-readable text of a status code. */
 const char* ottb_status_string(int32_t status);

@@ -31,6 +31,12 @@ EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_pointcloud",
     "ottb_cost_stats_workspace_size",
     "ottb_cost_stats",
+    "ottb_sinkhorn_pointcloud_noalloc",
+    "ottb_mlp_workspace_size",
+    "ottb_mlp_forward",
+    "ottb_mlp_gradients",
+    "ottb_mlp_adam",
+    "ottb_mlp_sync_bf16",
     "ottb_status_string",
     "ottb_version",
 )
@@ -67,6 +73,7 @@ class OttbSolverCfg(ctypes.Structure):
       ("mask_init", ctypes.c_int32),
       ("timeout_ms", ctypes.c_int32),
       ("phantom_arrivals", ctypes.c_int32),
+      ("init_f_from_g", ctypes.c_int32),
   ]
 
 
@@ -79,6 +86,19 @@ class OttbResult(ctypes.Structure):
       ("status", ctypes.c_int32),
       ("reserved", ctypes.c_int32),
   ]
+
+
+MLP_MAX_LAYERS = 8
+
+
+class OttbMlpLayer(ctypes.Structure):
+  _fields_ = [("in_", ctypes.c_int32), ("out", ctypes.c_int32)] + [
+      (name, ctypes.c_void_p) for name in
+      ("w", "w_bf16", "wt_bf16", "b", "w_m", "w_v", "b_m", "b_v", "w_grad", "b_grad")]
+
+
+class OttbMlp(ctypes.Structure):
+  _fields_ = [("num_layers", ctypes.c_int32), ("layers", OttbMlpLayer * MLP_MAX_LAYERS)]
 
 
 RESULT_BYTES = ctypes.sizeof(OttbResult)
@@ -118,6 +138,18 @@ def load() -> ctypes.CDLL:
     lib.ottb_cost_stats_workspace_size.restype = sz
     lib.ottb_cost_stats.argtypes = [vp, vp, i64, i64, i32, ctypes.c_float, i32, vp, vp, sz, vp]
     lib.ottb_cost_stats.restype = i32
+    mlp = ctypes.POINTER(OttbMlp)
+    f32 = ctypes.c_float
+    lib.ottb_mlp_workspace_size.argtypes = [mlp, i32]
+    lib.ottb_mlp_workspace_size.restype = sz
+    lib.ottb_mlp_forward.argtypes = [mlp, vp, i32, vp, vp, vp, sz, vp]
+    lib.ottb_mlp_forward.restype = i32
+    lib.ottb_mlp_gradients.argtypes = [mlp, vp, vp, i32, vp, vp, vp, sz, vp]
+    lib.ottb_mlp_gradients.restype = i32
+    lib.ottb_mlp_adam.argtypes = [mlp, f32, f32, f32, f32, i32, vp]
+    lib.ottb_mlp_adam.restype = i32
+    lib.ottb_mlp_sync_bf16.argtypes = [mlp, vp]
+    lib.ottb_mlp_sync_bf16.restype = i32
     lib.ottb_status_string.argtypes = [i32]
     lib.ottb_status_string.restype = ctypes.c_char_p
     lib.ottb_version.argtypes = []

@@ -1,0 +1,272 @@
+// BF16 GEMM on tcgen05 for the learned initializer's MLP:
+//   D[M, N] = A[M, K] * B[N, K]^T  (A and B bf16, K contiguous; FP32 in TMEM)
+// with the epilogues the MLP needs fused in:
+//   kEpiHidden   Z = D + bias (bf16), H = GELU(Z) (bf16, row-major and
+//                transposed)
+//   kEpiOutput   Y = D + bias (fp32)
+//   kEpiBackHid  dZ = D * GELU'(Zprev) (bf16, row-major and transposed)
+//   kEpiWeight   G = D (fp32, weight gradient)
+// One CTA per 128 x 128 tile of D (M, N multiples of 128, K of 64). Warp 0
+// issues TMA loads of 64-wide K slabs of A and B through a 4-stage ring, warp
+// 1 the MMAs (M = N = 128, K = 16) into one TMEM accumulator, warps 2-5 read
+// it back (warp w: TMEM lanes 32*(w%4)..) and run the epilogue. Waits are
+// bounded; on a timeout the CTA sets *err and returns after draining.
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "tc_ptx.cuh"
+
+namespace ottb {
+
+enum GemmEpi : int { kEpiHidden = 0, kEpiOutput = 1, kEpiBackHid = 2, kEpiWeight = 3 };
+
+struct GemmArgs {
+  int M, N, K;
+  int epi;
+  const float* bias;          // [N] (kEpiHidden, kEpiOutput)
+  __nv_bfloat16* out_z;       // [M, N] pre-activation (kEpiHidden)
+  __nv_bfloat16* out_h;       // [M, N] activation or dZ
+  __nv_bfloat16* out_ht;      // [N, M] its transpose
+  const __nv_bfloat16* zprev; // [M, N] pre-activation of the layer below (kEpiBackHid)
+  float* out_f32;             // [M, N] (kEpiOutput, kEpiWeight)
+  int* err;
+  uint64_t timeout_ns;
+};
+
+constexpr int kGemmStages = 4;
+constexpr int kGemmSlabBytes = 128 * 64 * 2;  // one [128][64] bf16 slab, 128-byte swizzle
+
+struct GemmSmem {
+  uint8_t A[kGemmStages][kGemmSlabBytes];
+  uint8_t B[kGemmStages][kGemmSlabBytes];
+  uint64_t full[kGemmStages];
+  uint64_t empty[kGemmStages];
+  uint64_t done;
+  uint32_t tmem_base;
+  int err;
+};
+
+// tanh-form GELU, 0.5 z (1 + tanh(sqrt(2/pi) (z + 0.044715 z^3))), and its
+// derivative.
+__device__ __forceinline__ float gelu_tanh(float z) {
+  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+  return 0.5f * z * (1.0f + tanhf(u));
+}
+__device__ __forceinline__ float gelu_tanh_grad(float z) {
+  const float u = 0.7978845608028654f * (z + 0.044715f * z * z * z);
+  const float t = tanhf(u);
+  const float du = 0.7978845608028654f * (1.0f + 3.0f * 0.044715f * z * z);
+  return 0.5f * (1.0f + t) + 0.5f * z * (1.0f - t * t) * du;
+}
+
+__global__ void __launch_bounds__(192, 1)
+gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA,
+                    const __grid_constant__ CUtensorMap mapB, GemmArgs g) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const uint32_t base = tc::smem_u32(smem_raw);
+  GemmSmem& sm = *reinterpret_cast<GemmSmem*>(smem_raw + ((1024u - (base & 1023u)) & 1023u));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m0 = blockIdx.y * 128, n0 = blockIdx.x * 128;
+  const int ksteps = g.K / 64;
+  constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, 128);
+
+  if (threadIdx.x == 0) {
+    for (int i = 0; i < kGemmStages; ++i) {
+      tc::mbar_init(&sm.full[i], 1);
+      tc::mbar_init(&sm.empty[i], 1);
+    }
+    tc::mbar_init(&sm.done, 1);
+    sm.err = 0;
+    tc::fence_barrier_init();
+  }
+  if (warp == 1) {
+    tc::tmem_alloc(&sm.tmem_base, 128);
+    tc::tmem_relinquish();
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) {
+      for (int k = 0; k < ksteps; ++k) {
+        const int st = k % kGemmStages;
+        if (!tc::mbar_wait(&sm.empty[st], ((k / kGemmStages) & 1) ^ 1, g.timeout_ns)) {
+          ok = false;
+          break;
+        }
+        tc::mbar_arrive_expect_tx(&sm.full[st], 2 * kGemmSlabBytes);
+        tc::tma_load_2d(sm.A[st], &mapA, &sm.full[st], 64 * k, m0);
+        tc::tma_load_2d(sm.B[st], &mapB, &sm.full[st], 64 * k, n0);
+      }
+    }
+    __syncwarp();
+  } else if (warp == 1) {
+    if (lane == 0) {
+      for (int k = 0; k < ksteps; ++k) {
+        const int st = k % kGemmStages;
+        if (!tc::mbar_wait(&sm.full[st], (k / kGemmStages) & 1, g.timeout_ns)) {
+          ok = false;
+          break;
+        }
+        tc::fence_after_sync();
+        const uint32_t a0 = tc::smem_u32(sm.A[st]), b0 = tc::smem_u32(sm.B[st]);
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk)
+          tc::mma_bf16(sm.tmem_base, tc::sw128_kmajor_desc(a0 + 32 * kk),
+                       tc::sw128_kmajor_desc(b0 + 32 * kk), kIdesc, (k | kk) ? 1u : 0u);
+        tc::mma_commit(&sm.empty[st]);
+      }
+      tc::mma_commit(&sm.done);  // also issued after a timeout: drains the MMAs
+    }
+    __syncwarp();
+  } else {
+    // epilogue: row r of the tile, 128 columns in 4 chunks of 32
+    const int q = warp & 3;
+    const int r = 32 * q + lane;
+    const int row = m0 + r;
+    if (!tc::mbar_wait(&sm.done, 0, g.timeout_ns)) ok = false;
+    if (ok) {
+      tc::fence_after_sync();
+      for (int c0 = 0; c0 < 128; c0 += 32) {
+        float v[32];
+        tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + c0, v);
+        tc::tmem_ld_wait();
+        const int col0 = n0 + c0;
+        if (g.epi == kEpiHidden) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float z = v[j] + g.bias[col0 + j];
+            const __nv_bfloat16 zb = __float2bfloat16_rn(z);
+            const __nv_bfloat16 hb = __float2bfloat16_rn(gelu_tanh(__bfloat162float(zb)));
+            g.out_z[(int64_t)row * g.N + col0 + j] = zb;
+            g.out_h[(int64_t)row * g.N + col0 + j] = hb;
+            g.out_ht[(int64_t)(col0 + j) * g.M + row] = hb;
+          }
+        } else if (g.epi == kEpiOutput) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) g.out_f32[(int64_t)row * g.N + col0 + j] = v[j] + g.bias[col0 + j];
+        } else if (g.epi == kEpiBackHid) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            const float z = __bfloat162float(g.zprev[(int64_t)row * g.N + col0 + j]);
+            const __nv_bfloat16 db = __float2bfloat16_rn(v[j] * gelu_tanh_grad(z));
+            g.out_h[(int64_t)row * g.N + col0 + j] = db;
+            g.out_ht[(int64_t)(col0 + j) * g.M + row] = db;
+          }
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) g.out_f32[(int64_t)row * g.N + col0 + j] = v[j];
+        }
+      }
+    }
+  }
+  if (!ok) atomicExch(&sm.err, 1);
+  tc::fence_before_sync();
+  __syncthreads();
+  if (warp == 1) {
+    // after a timeout the MMA thread's final commit may not have landed yet
+    if (sm.err && lane == 0) tc::mbar_wait(&sm.done, 0, 1000000000ull);
+    __syncwarp();
+    tc::fence_after_sync();
+    tc::tmem_dealloc(sm.tmem_base, 128);
+  }
+  if (threadIdx.x == 0 && sm.err) atomicExch(g.err, 1);
+}
+
+// Column sums of a [rows, cols] matrix (bias gradients): out[c] = sum_r in[r, c].
+__global__ void colsum_bf16_kernel(const __nv_bfloat16* in, int rows, int cols, float* out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.f;
+  for (int r = 0; r < rows; ++r) s += __bfloat162float(in[(int64_t)r * cols + c]);
+  out[c] = s;
+}
+__global__ void colsum_f32_kernel(const float* in, int rows, int cols, float* out) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= cols) return;
+  float s = 0.f;
+  for (int r = 0; r < rows; ++r) s += in[(int64_t)r * cols + c];
+  out[c] = s;
+}
+
+// Centred squared error per sample,
+//   loss_b = (1/m) sum_j ((y_j - mean(y)) - (t_j - mean(t)))^2
+// (potentials are defined up to a constant, so only centred values are
+// compared); dY = (2 / (m B)) r, r the centred residual (its mean is zero),
+// as bf16 row-major and transposed for the backward GEMMs. One CTA per
+// sample, blockDim a multiple of 32 up to 1024.
+__device__ __forceinline__ float block_sum_f32(float v, float* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  float tot = 0.f;
+  for (int i = 0; i < (int)(blockDim.x >> 5); ++i) tot += red[i];
+  return tot;
+}
+
+__global__ void centred_mse_kernel(const float* y, const float* t, int batch, int m,
+                                   __nv_bfloat16* dy, __nv_bfloat16* dyt, float* loss_per) {
+  __shared__ float red[32];
+  const int b = blockIdx.x;
+  const float* yb = y + (int64_t)b * m;
+  const float* tb = t + (int64_t)b * m;
+  float s = 0.f;
+  for (int j = threadIdx.x; j < m; j += blockDim.x) s += yb[j] - tb[j];
+  const float shift = block_sum_f32(s, red) / (float)m;  // mean(y) - mean(t)
+  float l = 0.f;
+  const float scale = 2.0f / ((float)m * (float)batch);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const float r = yb[j] - tb[j] - shift;
+    l += r * r;
+    const __nv_bfloat16 g = __float2bfloat16_rn(scale * r);
+    dy[(int64_t)b * m + j] = g;
+    dyt[(int64_t)j * batch + b] = g;
+  }
+  const float tot = block_sum_f32(l, red);
+  if (threadIdx.x == 0) loss_per[b] = tot / (float)m;
+}
+
+// Adam (Kingma & Ba) on FP32 master weights; writes the bf16 copies used by
+// the GEMMs, row-major [rows, cols] and transposed [cols, rows] (wt may be
+// null for biases).
+__global__ void adam_kernel(float* w, float* mom, float* vel, const float* grad, int64_t count,
+                            int cols, float lr, float b1, float b2, float eps, float c1, float c2,
+                            __nv_bfloat16* wb, __nv_bfloat16* wt, int rows) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float gr = grad[i];
+    const float m1 = b1 * mom[i] + (1.f - b1) * gr;
+    const float v1 = b2 * vel[i] + (1.f - b2) * gr * gr;
+    mom[i] = m1;
+    vel[i] = v1;
+    const float upd = lr * (m1 / c1) / (sqrtf(v1 / c2) + eps);
+    const float nw = w[i] - upd;
+    w[i] = nw;
+    if (wb) {
+      const __nv_bfloat16 h = __float2bfloat16_rn(nw);
+      wb[i] = h;
+      if (wt) {
+        const int64_t r = i / cols, c = i % cols;
+        wt[c * rows + r] = h;
+      }
+    }
+  }
+}
+
+// f32 -> bf16 (row-major and optionally transposed) for the network input.
+__global__ void to_bf16_kernel(const float* in, int64_t rows, int cols, __nv_bfloat16* out,
+                               __nv_bfloat16* outt) {
+  const int64_t count = rows * cols;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const __nv_bfloat16 h = __float2bfloat16_rn(in[i]);
+    out[i] = h;
+    if (outt) outt[(i % cols) * rows + i / cols] = h;
+  }
+}
+
+}  // namespace ottb

@@ -256,6 +256,13 @@ __device__ void persistent_main(const KernelArgs& A, SweepFn&& sweep) {
     if (!grid_barrier(A.gl, A.expected_arrivals, A.timeout_ns, status)) return; \
   } while (0)
 
+  if (c.init_f_from_g && scan_end > 0) {
+    // f = update_potential(., g_init, log a, 0, axis=1): the c-transform of
+    // an initializer's g, so that g is not discarded by the first g-update.
+    SweepParams sp{kSweepF, eps_mult(c, 0), 0, 1, 0, 0};
+    OTTB_SWEEP(sp);
+    OTTB_BARRIER();
+  }
   while (true) {
     bool fused = false;
     if (it > 0 && it % inner == 0) {

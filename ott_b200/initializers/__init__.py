@@ -1,1 +1,1 @@
-from ott_b200.initializers import linear  # noqa: F401
+from ott_b200.initializers import linear, neural  # noqa: F401

@@ -1,0 +1,204 @@
+"""Learned Sinkhorn initializer on a fixed support
+(ott/initializers/neural/meta_initializer.py:36-213).
+
+The network maps the measure weights concat(a, b) to a dual potential. The
+reference's meta model predicts f (``init_fu``, :137-158) and trains it on
+the dual objective (:160-190). Here the network predicts g, regressed on the
+centred g of problems solved by the plain kernel. The solver then starts
+with one f-update from that g (its c-transform,
+``ottb_solver_cfg.init_f_from_g``), because a g alone would be discarded by
+the first g-update of the loop. Forward, backward and Adam run in this
+library's tcgen05 bf16 kernels (``ottb_mlp_*``).
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from ott_b200 import _arrays, _lib
+from ott_b200.initializers.linear import initializers
+
+
+class MLP:
+  """Dense layers with tanh-GELU between them, parameters on the device.
+
+  Initialisation follows flax ``nn.Dense`` defaults: weights from a
+  truncated normal with variance 1 / fan_in (lecun normal), zero biases.
+  """
+
+  def __init__(self, dims: Sequence[int], seed: int = 0, device=None):
+    self.dims = list(dims)
+    dev = device or _arrays.device()
+    rng = np.random.default_rng(seed)
+    self.tensors = []
+    self.net = _lib.OttbMlp()
+    self.net.num_layers = len(dims) - 1
+    for l in range(len(dims) - 1):
+      fan_in, fan_out = dims[l], dims[l + 1]
+      std = np.sqrt(1.0 / fan_in) / 0.87962566103423978  # truncated-normal variance fix
+      w0 = np.clip(rng.standard_normal((fan_out, fan_in)), -2, 2) * std
+      t = dict(
+          w=torch.tensor(w0, dtype=torch.float32, device=dev),
+          w_bf16=torch.empty((fan_out, fan_in), dtype=torch.bfloat16, device=dev),
+          wt_bf16=torch.empty((fan_in, fan_out), dtype=torch.bfloat16, device=dev),
+          b=torch.zeros(fan_out, dtype=torch.float32, device=dev),
+          w_m=torch.zeros((fan_out, fan_in), dtype=torch.float32, device=dev),
+          w_v=torch.zeros((fan_out, fan_in), dtype=torch.float32, device=dev),
+          b_m=torch.zeros(fan_out, dtype=torch.float32, device=dev),
+          b_v=torch.zeros(fan_out, dtype=torch.float32, device=dev),
+          w_grad=torch.zeros((fan_out, fan_in), dtype=torch.float32, device=dev),
+          b_grad=torch.zeros(fan_out, dtype=torch.float32, device=dev))
+      self.tensors.append(t)
+      ly = self.net.layers[l]
+      ly.in_, ly.out = fan_in, fan_out
+      for k, v in t.items():
+        setattr(ly, k, v.data_ptr())
+    self.lib = _lib.load()
+    self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+    self.step = 0
+    self._ws = {}
+    _lib.check(self.lib.ottb_mlp_sync_bf16(ctypes.byref(self.net), _arrays.stream_handle()),
+               "ottb_mlp_sync_bf16")
+
+  def _workspace(self, batch: int) -> torch.Tensor:
+    if batch not in self._ws:
+      nbytes = self.lib.ottb_mlp_workspace_size(ctypes.byref(self.net), batch)
+      if nbytes == 0:
+        raise ValueError(f"batch {batch} and widths {self.dims} must be multiples of 128")
+      self._ws[batch] = torch.empty(nbytes, dtype=torch.uint8, device=self.status.device)
+    return self._ws[batch]
+
+  def params_numpy(self):
+    return [(t["w"].double().cpu().numpy(), t["b"].double().cpu().numpy()) for t in self.tensors]
+
+  def forward(self, x: torch.Tensor) -> torch.Tensor:
+    x = x.contiguous().float()
+    batch = x.shape[0]
+    y = torch.empty((batch, self.dims[-1]), dtype=torch.float32, device=x.device)
+    ws = self._workspace(batch)
+    st = self.lib.ottb_mlp_forward(ctypes.byref(self.net), x.data_ptr(), batch, y.data_ptr(),
+                                   self.status.data_ptr(), ws.data_ptr(), ws.numel(),
+                                   _arrays.stream_handle())
+    _lib.check(st, "ottb_mlp_forward")
+    return y
+
+  def gradients(self, x: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
+    x = x.contiguous().float()
+    target = target.contiguous().float()
+    batch = x.shape[0]
+    loss = torch.empty(batch, dtype=torch.float32, device=x.device)
+    ws = self._workspace(batch)
+    st = self.lib.ottb_mlp_gradients(ctypes.byref(self.net), x.data_ptr(), target.data_ptr(),
+                                     batch, loss.data_ptr(), self.status.data_ptr(),
+                                     ws.data_ptr(), ws.numel(), _arrays.stream_handle())
+    _lib.check(st, "ottb_mlp_gradients")
+    return loss
+
+  def adam(self, lr=1e-3, b1=0.9, b2=0.999, eps=1e-8):
+    self.step += 1
+    _lib.check(self.lib.ottb_mlp_adam(ctypes.byref(self.net), lr, b1, b2, eps, self.step,
+                                      _arrays.stream_handle()), "ottb_mlp_adam")
+
+  def check_status(self):
+    st = int(self.status.item())
+    if st != _lib.OTTB_OK:
+      raise _lib.OttbError(st, "ottb_mlp (device)")
+
+
+class MetaInitializer(initializers.SinkhornInitializer):
+  """Meta-OT initializer for problems on one fixed support.
+
+  Args:
+    geom: the fixed geometry (n and m multiples of 128).
+    dims: hidden widths; the network is (n + m) -> dims... -> m.
+    lr: Adam learning rate (the reference's default, 1e-3).
+    seed: initialisation seed.
+  """
+
+  half_step_from_g = True
+
+  def __init__(self, geom, dims: Sequence[int] = (1024, 1024, 1024), lr: float = 1e-3,
+               seed: int = 0):
+    self.geom = geom
+    n, m = geom.shape
+    self.lr = lr
+    self.mlp = MLP([n + m, *dims, m], seed=seed, device=geom.x.device)
+
+  def _inputs(self, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    # concat(a, b) as in _compute_f (:192-207), scaled by the support sizes
+    # so that a uniform measure reads 1: raw weights of a 1024-point support
+    # are ~1e-3, far below the scale the initialisation expects.
+    n, m = self.geom.shape
+    a2 = a if a.ndim == 2 else a[None]
+    b2 = b if b.ndim == 2 else b[None]
+    return torch.cat([a2 * n, b2 * m], dim=1).float()
+
+  def update(self, a: torch.Tensor, b: torch.Tensor, g_target: torch.Tensor) -> float:
+    """One Adam step on a batch (batch a multiple of 128) regressing the
+    centred g of solved problems. Returns the batch-mean loss."""
+    x = self._inputs(a, b)
+    t = g_target.float()
+    loss = self.mlp.gradients(x, t)
+    self.mlp.adam(lr=self.lr)
+    return loss.mean()
+
+  def predict_g(self, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
+    x = self._inputs(a, b)
+    batch = x.shape[0]
+    padded = (batch + 127) // 128 * 128
+    if padded != batch:
+      x = torch.cat([x, torch.zeros((padded - batch, x.shape[1]), device=x.device)], dim=0)
+    return self.mlp.forward(x)[:batch]
+
+  def batch_init(self, probs, **unused):
+    """One network call for a batch of problems: [(None, g_k)]."""
+    a = torch.stack([p.a for p in probs])
+    b = torch.stack([p.b for p in probs])
+    g = self.predict_g(a, b)
+    return [(None, g[k]) for k in range(len(probs))]
+
+  def init_fu(self, ot_prob, lse_mode: bool, rng=None):
+    return None  # derived in the solver from g (init_f_from_g)
+
+  def init_gv(self, ot_prob, lse_mode: bool, rng=None):
+    return self.predict_g(ot_prob.a, ot_prob.b)[0]
+
+
+def fit(meta: MetaInitializer, a: torch.Tensor, b: torch.Tensor, g: torch.Tensor, steps: int,
+        batch_size: int = 512, seed: int = 0, log_every: int = 0):
+  """Adam steps on random minibatches of solved problems (rows of a, b and
+  their solved g). Returns the per-step batch losses (device tensor)."""
+  gen = torch.Generator(device="cpu").manual_seed(seed)
+  num = a.shape[0]
+  losses = []
+  for step in range(steps):
+    idx = torch.randint(0, num, (batch_size,), generator=gen).to(a.device)
+    losses.append(meta.update(a[idx], b[idx], g[idx]))
+    if log_every and (step + 1) % log_every == 0:
+      print(f"step {step + 1}: loss {float(losses[-1]):.3e}", flush=True)
+  return torch.stack(losses)
+
+
+def solve_warm_started(probs, meta: MetaInitializer, budget: Optional[int] = None,
+                       **solver_kwargs):
+  """Solves a batch with the learned warm start; problems that have not
+  converged within ``budget`` iterations are solved again from the default
+  initialisation with the full ``max_iterations`` (the plain solver stays
+  the fallback and the judge of convergence).
+
+  Returns (outputs, fallback_indices).
+  """
+  from ott_b200.solvers.linear import sinkhorn
+  max_it = solver_kwargs.get("max_iterations", 2000)
+  warm_kw = dict(solver_kwargs, max_iterations=budget or max_it)
+  outs = sinkhorn.run_batch(probs, sinkhorn.Sinkhorn(initializer=meta, **warm_kw))
+  conv = torch.tensor([bool(o.converged) for o in outs])
+  redo = [k for k in range(len(probs)) if not conv[k]]
+  if redo:
+    again = sinkhorn.run_batch([probs[k] for k in redo], sinkhorn.Sinkhorn(**solver_kwargs))
+    for k, o in zip(redo, again):
+      outs[k] = o
+  return outs, redo

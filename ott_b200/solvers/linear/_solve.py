@@ -35,5 +35,6 @@ def solve_batch(geoms: Sequence[Any], a: Optional[Sequence[Any]] = None,
   b = [None] * k if b is None else list(b)
   probs = [linear_problem.LinearProblem(g, a=ai, b=bi)
            for g, ai, bi in zip(geoms, a, b)]
+  f_from_g = kwargs.pop("f_from_g", None)
   solver = sinkhorn.Sinkhorn(**kwargs)
-  return sinkhorn.run_batch(probs, solver, init)
+  return sinkhorn.run_batch(probs, solver, init, f_from_g=f_from_g)

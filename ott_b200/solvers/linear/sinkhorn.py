@@ -220,9 +220,17 @@ class Sinkhorn:
 
 def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
               inits: Optional[Sequence[Optional[Tuple[Any, Any]]]] = None,
+              f_from_g: Optional[bool] = None,
               **init_kwargs: Any) -> List[SinkhornOutput]:
   """Solves independent problems of the same dimension in ONE persistent
-  launch (the batched form of ``jax.vmap`` over ``Sinkhorn``)."""
+  launch (the batched form of ``jax.vmap`` over ``Sinkhorn``).
+
+  ``f_from_g``: start with one f-update from the initial g (its
+  c-transform), for initializers that predict g. Defaults to the
+  initializer's ``half_step_from_g`` when no explicit ``inits`` are given.
+  An initializer with a ``batch_init(probs)`` method is called once for the
+  whole batch instead of once per problem.
+  """
   if not probs:
     return []
   lib = _lib.load()
@@ -246,9 +254,15 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
   keep: List[torch.Tensor] = []
   outs = []
   mask_init = False
+  explicit = any(i is not None for i in inits)
+  if f_from_g is None:
+    f_from_g = bool(getattr(solver.initializer, "half_step_from_g", False)) and not explicit
+  batch_init = getattr(solver.initializer, "batch_init", None)
+  if batch_init is not None and not explicit:
+    inits = list(batch_init(probs, **init_kwargs))
+    mask_init = True
   for k, p in enumerate(probs):
     n, m = p.geom.shape
-    a, b = p.a, p.b
     init = inits[k]
     if init is None:
       fi, gi = solver.initializer(p, lse_mode=True, **init_kwargs)
@@ -265,8 +279,8 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
     q = arr[k]
     q.x = p.geom.x.data_ptr()
     q.y = p.geom.y.data_ptr()
-    q.a = a.data_ptr()
-    q.b = b.data_ptr()
+    q.a = p.a.data_ptr()
+    q.b = p.b.data_ptr()
     q.f_init = None if fi is None else fi.data_ptr()
     q.g_init = None if gi is None else gi.data_ptr()
     q.f = f.data_ptr()
@@ -278,6 +292,7 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
     q.inv_scale_cost = float(p.geom.inv_scale_cost)
     outs.append((f, g, errors[:outer]))
   cfg = solver._cfg(mask_init, s0)
+  cfg.init_f_from_g = 1 if f_from_g else 0
   nprob = len(probs)
   ws_bytes = lib.ottb_sinkhorn_workspace_size(arr, nprob, d, ctypes.byref(cfg))
   if ws_bytes == 0:

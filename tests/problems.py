@@ -65,3 +65,31 @@ def batched_uneven_problems(num, d=32, lo=128, hi=16384, seed=0):
     b = rng.dirichlet(np.ones(m)).astype(np.float32)
     out.append((x, y, a, b))
   return out
+
+
+def grid_support(side=32):
+  """side x side grid on [0, 1]^2 (the fixed support of the learned warm
+  start workload), row-major."""
+  t = np.linspace(0.0, 1.0, side)
+  gx, gy = np.meshgrid(t, t, indexing="ij")
+  return np.stack([gx.ravel(), gy.ravel()], axis=1).astype(np.float32)
+
+
+def grid_mixture_weights(num, grid, seed=0, floor=1e-6):
+  """num measures on a fixed grid: each is a mixture of 1-5 isotropic
+  Gaussians (means U[0,1]^2, std U[0.03, 0.2], mixture weights Dirichlet(1))
+  evaluated at the grid points, normalised, plus a floor, renormalised.
+  Returns [num, len(grid)] float32."""
+  rng = np.random.default_rng(seed)
+  out = np.empty((num, len(grid)), np.float64)
+  g = grid.astype(np.float64)
+  for i in range(num):
+    k = int(rng.integers(1, 6))
+    mu = rng.uniform(size=(k, 2))
+    sd = rng.uniform(0.03, 0.2, size=k)
+    pi = rng.dirichlet(np.ones(k))
+    d2 = ((g[:, None, :] - mu[None]) ** 2).sum(-1)
+    dens = (pi / (2 * np.pi * sd * sd) * np.exp(-d2 / (2 * sd * sd))).sum(1)
+    w = dens / dens.sum() + floor
+    out[i] = w / w.sum()
+  return out.astype(np.float32)

@@ -39,8 +39,10 @@ def test_status_strings_and_version():
 def test_struct_layouts_match_header():
   # sizes follow from the C declarations on LP64
   assert ctypes.sizeof(_lib.OttbProblem) == 9 * 8 + 2 * 8 + 2 * 4
-  assert ctypes.sizeof(_lib.OttbSolverCfg) == 11 * 4
+  assert ctypes.sizeof(_lib.OttbSolverCfg) == 12 * 4
   assert ctypes.sizeof(_lib.OttbResult) == 2 * 8 + 4 * 4
+  assert ctypes.sizeof(_lib.OttbMlpLayer) == 2 * 4 + 10 * 8
+  assert ctypes.sizeof(_lib.OttbMlp) == 8 + _lib.MLP_MAX_LAYERS * (2 * 4 + 10 * 8)
 
 
 def test_invalid_arguments_rejected_without_device():
@@ -54,3 +56,21 @@ def test_invalid_arguments_rejected_without_device():
   assert st == _lib.OTTB_ERR_INVALID
   assert lib.ottb_cost_stats(None, None, 0, 0, 2, ctypes.c_float(1.0), 1, None, None, 0,
                              None) == _lib.OTTB_ERR_INVALID
+
+
+def test_mlp_shape_checks_without_device():
+  lib = _lib.load()
+  net = _lib.OttbMlp()
+  net.num_layers = 2
+  net.layers[0].in_, net.layers[0].out = 256, 128
+  net.layers[1].in_, net.layers[1].out = 128, 128
+  ws = lib.ottb_mlp_workspace_size(ctypes.byref(net), 128)
+  # bf16 input (+ transpose), one hidden layer's five bf16 buffers, fp32 output and
+  # its bf16 gradient (+ transpose)
+  assert ws == 2 * (2 * 128 * 256) + 5 * (2 * 128 * 128) + 4 * 128 * 128 + 2 * (2 * 128 * 128)
+  assert lib.ottb_mlp_workspace_size(ctypes.byref(net), 100) == 0  # batch not a multiple of 128
+  net.layers[1].in_ = 256  # widths must chain
+  assert lib.ottb_mlp_workspace_size(ctypes.byref(net), 128) == 0
+  assert lib.ottb_mlp_forward(None, None, 128, None, None, None, 0, None) == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_mlp_adam(ctypes.byref(net), 1e-3, 0.9, 0.999, 1e-8, 0, None) == \
+      _lib.OTTB_ERR_INVALID

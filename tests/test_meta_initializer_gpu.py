@@ -1,0 +1,157 @@
+"""The learned warm start on the GPU: the tcgen05 MLP kernels against the
+float64 network oracle (forward, gradients, Adam), the f half-update from an
+initial g against the Sinkhorn oracle, and a trained network cutting the
+iterations of the plain solver at equal accuracy (the reference's
+tests/initializers/neural/meta_initializer_test.py:62-93 asks the same of its
+MetaInitializer)."""
+import numpy as np
+import pytest
+
+from oracle import mlp_np
+from oracle import sinkhorn_np as oracle
+from tests import problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _mlp(dims, seed):
+  from ott_b200.initializers.neural import meta_initializer
+  return meta_initializer.MLP(dims, seed=seed)
+
+
+def _rel(a, b):
+  return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+def test_mlp_forward_matches_oracle():
+  import torch
+  net = _mlp([256, 384, 256, 128], seed=1)
+  x = np.random.default_rng(0).standard_normal((256, 256)).astype(np.float32)
+  y = net.forward(torch.tensor(x, device="cuda")).cpu().numpy()
+  net.check_status()
+  params = net.params_numpy()
+  y_emul, _ = mlp_np.forward_bf16(params, x)
+  y_exact, _ = mlp_np.forward(params, x.astype(np.float64))
+  # same roundings as the device: only summation order and tanh differ
+  assert _rel(y, y_emul) < 2e-3
+  # against float64 weights and activations: bf16 operand error
+  assert _rel(y, y_exact) < 2e-2
+
+
+def test_mlp_gradients_match_oracle():
+  import torch
+  dims = [256, 256, 128, 128]
+  net = _mlp(dims, seed=2)
+  rng = np.random.default_rng(1)
+  batch = 384
+  x = rng.standard_normal((batch, 256)).astype(np.float32)
+  t = rng.standard_normal((batch, 128)).astype(np.float32)
+  loss = net.gradients(torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda"))
+  loss = loss.cpu().numpy()
+  net.check_status()
+  params = net.params_numpy()
+  bparams = [(mlp_np.bf16(w).astype(np.float64), b) for w, b in params]
+  loss_ref, grads = mlp_np.loss_and_grads(bparams, mlp_np.bf16(x).astype(np.float64),
+                                          t.astype(np.float64))
+  np.testing.assert_allclose(loss, loss_ref, rtol=2e-2)
+  for l, tens in enumerate(net.tensors):
+    gw = tens["w_grad"].cpu().numpy()
+    gb = tens["b_grad"].cpu().numpy()
+    # bf16 activations and bf16 output gradient, FP32 accumulation
+    assert _rel(gw, grads[l][0]) < 3e-2, (l, _rel(gw, grads[l][0]))
+    assert _rel(gb, grads[l][1]) < 3e-2, (l, _rel(gb, grads[l][1]))
+
+
+def test_mlp_adam_step_matches_oracle():
+  import torch
+  net = _mlp([128, 256, 128], seed=3)
+  rng = np.random.default_rng(2)
+  x = torch.tensor(rng.standard_normal((128, 128)).astype(np.float32), device="cuda")
+  t = torch.tensor(rng.standard_normal((128, 128)).astype(np.float32), device="cuda")
+  params = net.params_numpy()
+  state = [[np.zeros_like(w), np.zeros_like(w), np.zeros_like(b), np.zeros_like(b)]
+           for w, b in params]
+  for step in (1, 2, 3):
+    net.gradients(x, t)
+    grads = [(tn["w_grad"].double().cpu().numpy(), tn["b_grad"].double().cpu().numpy())
+             for tn in net.tensors]
+    net.adam(lr=1e-3)
+    params = mlp_np.adam_step(params, grads, state, step, lr=1e-3)
+    got = net.params_numpy()
+    for (w, b), (w_ref, b_ref) in zip(got, params):
+      np.testing.assert_allclose(w, w_ref, rtol=0, atol=1e-6)
+      np.testing.assert_allclose(b, b_ref, rtol=0, atol=1e-6)
+  net.check_status()
+  for tn in net.tensors:  # bf16 copies refreshed from the FP32 weights
+    wb = tn["w_bf16"].float().cpu().numpy()
+    np.testing.assert_array_equal(wb, mlp_np.bf16(tn["w"].cpu().numpy()))
+    np.testing.assert_array_equal(tn["wt_bf16"].float().cpu().numpy(), wb.T)
+
+
+@pytest.mark.parametrize("n,m,d,precision", [(200, 300, 2, "fp32"), (300, 257, 64, "auto")])
+def test_f_from_g_matches_oracle(n, m, d, precision):
+  """init (f, g) = (c-transform of g0, g0): one f-update before the loop."""
+  import torch
+  from ott_b200.solvers import linear
+  from ott_b200.geometry import pointcloud
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + d)
+  rng = np.random.default_rng(7)
+  g0 = (0.3 * rng.standard_normal(m)).astype(np.float32)
+  geom = pointcloud.PointCloud(torch.tensor(x).cuda(), torch.tensor(y).cuda(), epsilon=0.05,
+                               relative_epsilon="mean")
+  out = linear.solve_batch([geom], [torch.tensor(a).cuda()], [torch.tensor(b).cuda()],
+                           init=[(None, torch.tensor(g0).cuda())], f_from_g=True,
+                           precision=precision)[0]
+  xd, yd = x.astype(np.float64), y.astype(np.float64)
+  eps = oracle.resolve_epsilon(xd, yd, 0.05, "mean", 1.0)
+  og = oracle.Geom(xd, yd, float(eps))
+  f0 = og.update_potential(np.zeros(n), g0.astype(np.float64), np.log(a.astype(np.float64)),
+                           0, axis=1)
+  ref = oracle.sinkhorn(og, a, b, init=(f0, g0.astype(np.float64)))
+  from tests import helpers
+  helpers.assert_parity(geom, out, ref)
+
+
+def _grid_batch(geom, A, B):
+  from ott_b200.problems.linear import linear_problem
+  return [linear_problem.LinearProblem(geom, a=A[k], b=B[k]) for k in range(A.shape[0])]
+
+
+def test_trained_warm_start_cuts_iterations():
+  """A 16 x 16 grid (n = m = 256, eps 1e-2), measures as in the 32 x 32
+  learned-warm-start workload; the network is trained for a few hundred Adam
+  steps on 2048 problems solved by the plain kernel, then warm-starts 256
+  held-out problems. Both runs converge to the same threshold; the costs
+  agree to the accuracy the threshold allows."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.initializers.neural import meta_initializer
+  from ott_b200.solvers.linear import sinkhorn
+  grid = problems.grid_support(16)
+  W = problems.grid_mixture_weights(2 * (2048 + 256), grid, seed=11)
+  A = torch.tensor(W[0::2]).cuda()
+  B = torch.tensor(W[1::2]).cuda()
+  geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
+  train = _grid_batch(geom, A[:2048], B[:2048])
+  solved = sinkhorn.run_batch(train, sinkhorn.Sinkhorn())
+  assert all(o.converged for o in solved)
+  G = torch.stack([o.g for o in solved])
+
+  meta = meta_initializer.MetaInitializer(geom, dims=(512, 512), lr=1e-3, seed=0)
+  losses = meta_initializer.fit(meta, A[:2048], B[:2048], G, steps=600, batch_size=256)
+  meta.mlp.check_status()
+  losses = losses.cpu().numpy()
+  assert losses[-50:].mean() < 0.1 * losses[:10].mean(), (losses[:10].mean(), losses[-50:])
+
+  held = _grid_batch(geom, A[2048:], B[2048:])
+  cold = sinkhorn.run_batch(held, sinkhorn.Sinkhorn())
+  warm, redo = meta_initializer.solve_warm_started(held, meta)
+  it_cold = np.array([o.n_iters for o in cold])
+  it_warm = np.array([o.n_iters for o in warm])
+  assert all(o.converged for o in cold) and all(o.converged for o in warm)
+  print(f"iterations: cold {it_cold.mean():.1f}, warm {it_warm.mean():.1f}, "
+        f"fallbacks {len(redo)}, loss {losses[:10].mean():.3e} -> {losses[-50:].mean():.3e}")
+  assert it_warm.mean() < 0.8 * it_cold.mean()
+  c_cold = np.array([o.reg_ot_cost for o in cold])
+  c_warm = np.array([o.reg_ot_cost for o in warm])
+  np.testing.assert_allclose(c_warm, c_cold, rtol=1e-3)
