@@ -50,6 +50,15 @@ def parse_args():
   p.add_argument("--d", type=int, default=64)
   p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
   p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+  p.add_argument("--workload", default="gaussian64",
+                 choices=["gaussian64", "warmstart", "batched", "anneal"],
+                 help="gaussian64: the headline single large solve (default); "
+                      "warmstart: learned warm start on a 32x32 grid; batched: 512 "
+                      "uneven problems in one launch; anneal: epsilon-annealed solves")
+  p.add_argument("--train-pairs", type=int, default=100000)
+  p.add_argument("--test-pairs", type=int, default=10000)
+  p.add_argument("--train-steps", type=int, default=12000)
+  p.add_argument("--problems", type=int, default=512)
   return p.parse_args()
 
 
@@ -395,12 +404,130 @@ def run_ours(args):
   return 0
 
 
+# ---------------------------------------------------------------------------
+# learned warm start on a fixed 32 x 32 grid
+# ---------------------------------------------------------------------------
+def run_warmstart(args):
+  """Trains the learned initializer on problems solved by the plain kernel
+  and times held-out solves from zero init and from the warm start.
+
+  Problems: 32 x 32 grid on [0, 1]^2 (n = m = 1024), sqeuclidean cost,
+  epsilon 1e-2, weights from mixtures of 1-5 Gaussians plus a 1e-6 floor.
+  Network 2048 -> 1024 x 3 -> 1024 (GELU), bf16 operands, FP32 master
+  weights, Adam lr 1e-3 with cosine decay, batch 512, mass-weighted loss on
+  g - eps log b. Held-out timing covers the network call,
+  the warm solve and any fallback solves; the L2 is flushed before each
+  timed chunk.
+  """
+  import torch
+  from tests import problems
+  from ott_b200.geometry import pointcloud
+  from ott_b200.initializers.neural import meta_initializer
+  from ott_b200.solvers.linear import sinkhorn
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  grid = problems.grid_support(32)
+  ntr, nte = args.train_pairs, args.test_pairs
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+  W = problems.grid_mixture_weights(2 * (ntr + nte), grid, seed=0, device="cuda")
+  A, B = W[0::2].contiguous(), W[1::2].contiguous()
+  del W
+  geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
+  chunk = 2048
+  flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
+
+  # 1. training targets: the plain solver's g
+  e0, e1 = ev(), ev()
+  e0.record()
+  G = torch.empty((ntr, 1024), dtype=torch.float32, device="cuda")
+  it_train = []
+  for s in range(0, ntr, chunk):
+    e = min(s + chunk, ntr)
+    out = sinkhorn.run_stacked(geom, A[s:e], B[s:e], sinkhorn.Sinkhorn())
+    G[s:e] = out.g
+    it_train.append(out.n_iters)
+  e1.record()
+  e1.synchronize()
+  gen_s = e0.elapsed_time(e1) * 1e-3
+  it_train = np.concatenate(it_train)
+
+  # 2. training
+  meta = meta_initializer.MetaInitializer(geom, dims=(1024, 1024, 1024), lr=1e-3, seed=0)
+  e0.record()
+  losses = meta_initializer.fit(meta, A[:ntr], B[:ntr], G, steps=args.train_steps,
+                                batch_size=512).cpu().numpy()
+  e1.record()
+  e1.synchronize()
+  train_s = e0.elapsed_time(e1) * 1e-3
+  meta.mlp.check_status()
+  del G
+
+  # 3. held-out: zero init vs warm start (with fallback), same chunks
+  At, Bt = A[ntr:], B[ntr:]
+
+  def cold(a, b):
+    o = sinkhorn.run_stacked(geom, a, b, sinkhorn.Sinkhorn())
+    return o, np.zeros(0, np.int64)
+
+  def warm(a, b):
+    return meta_initializer.solve_warm_started(geom, a, b, meta)
+
+  def timed(fn):
+    fn(At[:chunk], Bt[:chunk])  # warm-up
+    fn(At[:chunk], Bt[:chunk])
+    fn(At[:chunk], Bt[:chunk])
+    ms, its, costs, conv, redo = 0.0, [], [], [], 0
+    for s in range(0, nte, chunk):
+      flush.zero_()
+      e0.record()
+      o, r = fn(At[s:s + chunk], Bt[s:s + chunk])
+      e1.record()
+      e1.synchronize()
+      ms += e0.elapsed_time(e1)
+      n_it, cv, c = o.scalars()
+      its.append(n_it)
+      costs.append(c)
+      conv.append(cv)
+      redo += len(r)
+    return (ms * 1e-3, np.concatenate(its), np.concatenate(costs), np.concatenate(conv),
+            redo)
+
+  clocks = ClockSampler(0)
+  clocks.start()
+  cold_s, it_c, cost_c, conv_c, _ = timed(cold)
+  warm_s, it_w, cost_w, conv_w, redo = timed(warm)
+  clk = clocks.stop()
+  rel = np.abs(cost_w - cost_c) / np.abs(cost_c)
+  line = {
+      "metric": "s to 1e-3 marginal err: learned warm start vs zero init, 32x32 grid",
+      "value": warm_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "workload": "warmstart", "dtype": "f32 solve / bf16 MLP", "data": "synthetic",
+      "config": {"workload": f"{nte} held-out grid problems n=m=1024 d=2 eps=1e-2 thr=1e-3",
+                 "train_pairs": ntr, "train_steps": args.train_steps, "batch": 512,
+                 "net": "2048-1024-1024-1024-1024 GELU, Adam lr 1e-3 cosine",
+                 "l2": "flushed before each timed chunk of 2048 problems"},
+      "zero_init": {"s": cold_s, "mean_iters": float(it_c.mean()),
+                    "converged": int(conv_c.sum())},
+      "warm_start": {"s": warm_s, "mean_iters": float(it_w.mean()),
+                     "converged": int(conv_w.sum()), "fallbacks": int(redo)},
+      "speedup": cold_s / warm_s, "iteration_ratio": float(it_w.mean() / it_c.mean()),
+      "cost_rel_diff": {"max": float(rel.max()), "median": float(np.median(rel))},
+      "training": {"target_solve_s": gen_s, "target_mean_iters": float(it_train.mean()),
+                   "train_s": train_s, "loss_first": float(losses[:20].mean()),
+                   "loss_last": float(losses[-100:].mean())},
+      "clocks": clk,
+  }
+  print(json.dumps(line))
+  return 0
+
+
 def main():
   args = parse_args()
   if args.warmup < 3:
     print("warning: fewer than 3 warm-up steps", file=sys.stderr)
   if args.impl == "reference":
     return run_reference(args)
+  if args.workload == "warmstart":
+    return run_warmstart(args)
   return run_ours(args)
 
 

@@ -187,13 +187,16 @@ int32_t ottb_mlp_forward(const ottb_mlp* net, const float* x, int32_t batch,
                          float* y, int32_t* status, void* workspace,
                          size_t workspace_bytes, void* stream);
 
-/* Gradients of the batch-mean centred squared error
- * (1/m) sum_j ((y_j - mean(y)) - (t_j - mean(t)))^2 into every layer's
- * w_grad / b_grad; loss_per[batch] receives each sample's loss. */
+/* Gradients of the batch mean of the centred squared error
+ *   loss_b = sum_j w_j ((y_j - t_j) - s_b)^2 / sum_j w_j,
+ *   s_b = sum_j w_j (y_j - t_j) / sum_j w_j
+ * into every layer's w_grad / b_grad; weight [batch, out] (> 0) or NULL for
+ * w = 1; loss_per[batch] receives each sample's loss. */
 int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x,
-                           const float* target, int32_t batch, float* loss_per,
-                           int32_t* status, void* workspace,
-                           size_t workspace_bytes, void* stream);
+                           const float* target, const float* weight,
+                           int32_t batch, float* loss_per, int32_t* status,
+                           void* workspace, size_t workspace_bytes,
+                           void* stream);
 
 /* One Adam step (bias-corrected, step >= 1) on every layer from its
  * gradients; refreshes the bf16 copies. */

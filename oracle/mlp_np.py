@@ -31,21 +31,25 @@ def forward(params, x):
   return h, (acts, zs)
 
 
-def loss_and_grads(params, x, t):
-  """Batch-mean of the centred squared error
-  (1/m) sum_j ((y_j - mean(y)) - (t_j - mean(t)))^2 and its gradients (the
-  residual has zero mean, so d loss / d y_j = 2 r_j / (m B))."""
+def loss_and_grads(params, x, t, w=None):
+  """Batch mean of the (optionally weighted) centred squared error
+  sum_j w_j ((y_j - t_j) - s)^2 / sum_j w_j, s the weighted mean of y - t,
+  and its gradients (the residual has zero weighted mean, so
+  d loss / d y_j = 2 w_j r_j / (sum w B))."""
   y, (acts, zs) = forward(params, x)
   B, m = y.shape
-  r = (y - y.mean(axis=1, keepdims=True)) - (t - t.mean(axis=1, keepdims=True))
-  loss_per = (r * r).mean(axis=1)
-  dz = 2.0 * r / (m * B)
+  w = np.ones_like(y) if w is None else np.asarray(w, np.float64)
+  sw = w.sum(axis=1, keepdims=True)
+  diff = y - t
+  r = diff - (w * diff).sum(axis=1, keepdims=True) / sw
+  loss_per = (w * r * r).sum(axis=1) / sw[:, 0]
+  dz = 2.0 * w * r / (sw * B)
   grads = [None] * len(params)
   for l in range(len(params) - 1, -1, -1):
-    w, _ = params[l]
+    w_l, _ = params[l]
     grads[l] = (dz.T @ acts[l], dz.sum(axis=0))
     if l > 0:
-      dz = (dz @ w) * gelu_grad(zs[l - 1])
+      dz = (dz @ w_l) * gelu_grad(zs[l - 1])
   return loss_per, grads
 
 

@@ -103,6 +103,21 @@ class OttbMlp(ctypes.Structure):
 
 RESULT_BYTES = ctypes.sizeof(OttbResult)
 
+_NP_CODES = {ctypes.c_void_p: "<u8", ctypes.c_int64: "<i8", ctypes.c_int32: "<i4",
+             ctypes.c_float: "<f4", ctypes.c_double: "<f8"}
+
+
+def numpy_dtype(struct) -> "np.dtype":
+  """NumPy structured dtype with the layout of a flat ctypes Structure."""
+  import numpy as np
+  names, formats, offsets = [], [], []
+  for name, ctype in struct._fields_:
+    names.append(name)
+    formats.append(_NP_CODES[ctype])
+    offsets.append(getattr(struct, name).offset)
+  return np.dtype({"names": names, "formats": formats, "offsets": offsets,
+                   "itemsize": ctypes.sizeof(struct)})
+
 _lock = threading.Lock()
 _lib: Optional[ctypes.CDLL] = None
 
@@ -144,7 +159,7 @@ def load() -> ctypes.CDLL:
     lib.ottb_mlp_workspace_size.restype = sz
     lib.ottb_mlp_forward.argtypes = [mlp, vp, i32, vp, vp, vp, sz, vp]
     lib.ottb_mlp_forward.restype = i32
-    lib.ottb_mlp_gradients.argtypes = [mlp, vp, vp, i32, vp, vp, vp, sz, vp]
+    lib.ottb_mlp_gradients.argtypes = [mlp, vp, vp, vp, i32, vp, vp, vp, sz, vp]
     lib.ottb_mlp_gradients.restype = i32
     lib.ottb_mlp_adam.argtypes = [mlp, f32, f32, f32, f32, i32, vp]
     lib.ottb_mlp_adam.restype = i32

@@ -192,12 +192,15 @@ __global__ void colsum_f32_kernel(const float* in, int rows, int cols, float* ou
   out[c] = s;
 }
 
-// Centred squared error per sample,
-//   loss_b = (1/m) sum_j ((y_j - mean(y)) - (t_j - mean(t)))^2
-// (potentials are defined up to a constant, so only centred values are
-// compared); dY = (2 / (m B)) r, r the centred residual (its mean is zero),
-// as bf16 row-major and transposed for the backward GEMMs. One CTA per
-// sample, blockDim a multiple of 32 up to 1024.
+// Centred squared error per sample, optionally weighted:
+//   loss_b = sum_j w_j ((y_j - t_j) - s)^2 / sum_j w_j,
+//   s = sum_j w_j (y_j - t_j) / sum_j w_j
+// (potentials are defined up to a constant, so only the best-aligned
+// difference is penalised; w = 1 when weight is null). The residual
+// r = y - t - s has zero weighted mean, so d loss_b / d y_j = 2 w_j r_j /
+// sum w; dY (that over the batch size) goes out as bf16, row-major and
+// transposed, for the backward GEMMs. One CTA per sample, blockDim a
+// multiple of 32 up to 1024.
 __device__ __forceinline__ float block_sum_f32(float v, float* red) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   __syncthreads();
@@ -208,26 +211,34 @@ __device__ __forceinline__ float block_sum_f32(float v, float* red) {
   return tot;
 }
 
-__global__ void centred_mse_kernel(const float* y, const float* t, int batch, int m,
-                                   __nv_bfloat16* dy, __nv_bfloat16* dyt, float* loss_per) {
+__global__ void centred_mse_kernel(const float* y, const float* t, const float* weight,
+                                   int batch, int m, __nv_bfloat16* dy, __nv_bfloat16* dyt,
+                                   float* loss_per) {
   __shared__ float red[32];
   const int b = blockIdx.x;
   const float* yb = y + (int64_t)b * m;
   const float* tb = t + (int64_t)b * m;
-  float s = 0.f;
-  for (int j = threadIdx.x; j < m; j += blockDim.x) s += yb[j] - tb[j];
-  const float shift = block_sum_f32(s, red) / (float)m;  // mean(y) - mean(t)
-  float l = 0.f;
-  const float scale = 2.0f / ((float)m * (float)batch);
+  const float* wb = weight ? weight + (int64_t)b * m : nullptr;
+  float s = 0.f, sw = 0.f;
   for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const float w = wb ? wb[j] : 1.f;
+    s += w * (yb[j] - tb[j]);
+    sw += w;
+  }
+  const float wsum = block_sum_f32(sw, red);
+  const float shift = block_sum_f32(s, red) / wsum;
+  float l = 0.f;
+  const float scale = 2.0f / (wsum * (float)batch);
+  for (int j = threadIdx.x; j < m; j += blockDim.x) {
+    const float w = wb ? wb[j] : 1.f;
     const float r = yb[j] - tb[j] - shift;
-    l += r * r;
-    const __nv_bfloat16 g = __float2bfloat16_rn(scale * r);
+    l += w * r * r;
+    const __nv_bfloat16 g = __float2bfloat16_rn(scale * w * r);
     dy[(int64_t)b * m + j] = g;
     dyt[(int64_t)j * batch + b] = g;
   }
   const float tot = block_sum_f32(l, red);
-  if (threadIdx.x == 0) loss_per[b] = tot / (float)m;
+  if (threadIdx.x == 0) loss_per[b] = tot / wsum;
 }
 
 // Adam (Kingma & Ba) on FP32 master weights; writes the bf16 copies used by

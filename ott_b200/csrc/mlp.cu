@@ -182,8 +182,9 @@ int32_t ottb_mlp_forward(const ottb_mlp* net, const float* x, int32_t batch, flo
 }
 
 int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x, const float* target,
-                           int32_t batch, float* loss_per, int32_t* status, void* workspace,
-                           size_t workspace_bytes, void* stream_ptr) {
+                           const float* weight, int32_t batch, float* loss_per,
+                           int32_t* status, void* workspace, size_t workspace_bytes,
+                           void* stream_ptr) {
   MlpPlan p;
   int st = plan_mlp(net, batch, p);
   if (st != OTTB_OK) return st;
@@ -197,7 +198,8 @@ int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x, const float* tar
   if (st != OTTB_OK) return st;
   const int L = p.L;
   const int out = p.dims[L];
-  centred_mse_kernel<<<batch, 256, 0, stream>>>((const float*)(ws + p.y), target, batch, out,
+  centred_mse_kernel<<<batch, 256, 0, stream>>>((const float*)(ws + p.y), target, weight,
+                                                batch, out,
                                                 (__nv_bfloat16*)(ws + p.dy),
                                                 (__nv_bfloat16*)(ws + p.dyt), loss_per);
   // walk back: dz_l (row-major) and dz_l^T for l = L-1 (the output) .. 0

@@ -13,6 +13,7 @@ library's tcgen05 bf16 kernels (``ottb_mlp_*``).
 from __future__ import annotations
 
 import ctypes
+import math
 from typing import Optional, Sequence
 
 import numpy as np
@@ -85,13 +86,20 @@ class MLP:
     _lib.check(st, "ottb_mlp_forward")
     return y
 
-  def gradients(self, x: torch.Tensor, target: torch.Tensor) -> torch.Tensor:
+  def gradients(self, x: torch.Tensor, target: torch.Tensor,
+                weight: Optional[torch.Tensor] = None) -> torch.Tensor:
+    """Gradients of the centred squared error into the layers' w_grad /
+    b_grad (``weight``: per-entry weights, or None for 1). Returns the
+    per-sample losses."""
     x = x.contiguous().float()
     target = target.contiguous().float()
+    if weight is not None:
+      weight = weight.contiguous().float()
     batch = x.shape[0]
     loss = torch.empty(batch, dtype=torch.float32, device=x.device)
     ws = self._workspace(batch)
     st = self.lib.ottb_mlp_gradients(ctypes.byref(self.net), x.data_ptr(), target.data_ptr(),
+                                     None if weight is None else weight.data_ptr(),
                                      batch, loss.data_ptr(), self.status.data_ptr(),
                                      ws.data_ptr(), ws.numel(), _arrays.stream_handle())
     _lib.check(st, "ottb_mlp_gradients")
@@ -111,20 +119,31 @@ class MLP:
 class MetaInitializer(initializers.SinkhornInitializer):
   """Meta-OT initializer for problems on one fixed support.
 
+  The network output h is read as g = eps log b + h: g_j - eps log b_j is
+  the soft c-transform of f, a smooth function of the support point, while
+  eps log b_j carries the sharp dependence on the weights (b has a 1e-6
+  floor in the grid workload: eps log b spans ~0.14 there). The regression
+  is on centred h (potentials are defined up to a constant), each entry
+  weighted by m b_j + ``mass_floor``: errors of g where b_j is tiny barely
+  move the c-transform f = -eps lse_j((g_j - C_ij) / eps) + eps log a_i
+  that the solver starts from.
+
   Args:
     geom: the fixed geometry (n and m multiples of 128).
     dims: hidden widths; the network is (n + m) -> dims... -> m.
     lr: Adam learning rate (the reference's default, 1e-3).
     seed: initialisation seed.
+    mass_floor: additive floor of the loss weights (None: unweighted).
   """
 
   half_step_from_g = True
 
   def __init__(self, geom, dims: Sequence[int] = (1024, 1024, 1024), lr: float = 1e-3,
-               seed: int = 0):
+               seed: int = 0, mass_floor: Optional[float] = 0.1):
     self.geom = geom
     n, m = geom.shape
     self.lr = lr
+    self.mass_floor = mass_floor
     self.mlp = MLP([n + m, *dims, m], seed=seed, device=geom.x.device)
 
   def _inputs(self, a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
@@ -136,12 +155,20 @@ class MetaInitializer(initializers.SinkhornInitializer):
     b2 = b if b.ndim == 2 else b[None]
     return torch.cat([a2 * n, b2 * m], dim=1).float()
 
-  def update(self, a: torch.Tensor, b: torch.Tensor, g_target: torch.Tensor) -> float:
-    """One Adam step on a batch (batch a multiple of 128) regressing the
-    centred g of solved problems. Returns the batch-mean loss."""
+  def _eps_log(self, b: torch.Tensor) -> torch.Tensor:
+    b2 = (b if b.ndim == 2 else b[None]).float()
+    return float(self.geom.epsilon) * torch.log(b2)
+
+  def update(self, a: torch.Tensor, b: torch.Tensor, g_target: torch.Tensor) -> torch.Tensor:
+    """One Adam step on a batch (batch a multiple of 128) regressing the g
+    of solved problems. Returns the batch-mean loss (device scalar)."""
     x = self._inputs(a, b)
-    t = g_target.float()
-    loss = self.mlp.gradients(x, t)
+    b = b.float()
+    pos = b > 0
+    t = torch.where(pos, g_target.float() - self._eps_log(b), torch.zeros_like(b))
+    m = b.shape[1]
+    w = pos.float() if self.mass_floor is None else pos * (m * b + self.mass_floor)
+    loss = self.mlp.gradients(x, t, w)
     self.mlp.adam(lr=self.lr)
     return loss.mean()
 
@@ -151,7 +178,11 @@ class MetaInitializer(initializers.SinkhornInitializer):
     padded = (batch + 127) // 128 * 128
     if padded != batch:
       x = torch.cat([x, torch.zeros((padded - batch, x.shape[1]), device=x.device)], dim=0)
-    return self.mlp.forward(x)[:batch]
+    return self.mlp.forward(x)[:batch] + self._eps_log(b)
+
+  def stacked_init(self, a: torch.Tensor, b: torch.Tensor):
+    """(None, G) for stacked weights a [K, n], b [K, m]: one network call."""
+    return None, self.predict_g(a, b)
 
   def batch_init(self, probs, **unused):
     """One network call for a batch of problems: [(None, g_k)]."""
@@ -168,37 +199,66 @@ class MetaInitializer(initializers.SinkhornInitializer):
 
 
 def fit(meta: MetaInitializer, a: torch.Tensor, b: torch.Tensor, g: torch.Tensor, steps: int,
-        batch_size: int = 512, seed: int = 0, log_every: int = 0):
+        batch_size: int = 512, seed: int = 0, cosine: bool = True, log_every: int = 0):
   """Adam steps on random minibatches of solved problems (rows of a, b and
-  their solved g). Returns the per-step batch losses (device tensor)."""
+  their solved g), the learning rate decayed from ``meta.lr`` to 0 along a
+  cosine when ``cosine``. Returns the per-step batch losses (device)."""
   gen = torch.Generator(device="cpu").manual_seed(seed)
   num = a.shape[0]
+  lr0 = meta.lr
   losses = []
   for step in range(steps):
+    if cosine:
+      meta.lr = lr0 * 0.5 * (1.0 + math.cos(math.pi * step / steps))
     idx = torch.randint(0, num, (batch_size,), generator=gen).to(a.device)
     losses.append(meta.update(a[idx], b[idx], g[idx]))
     if log_every and (step + 1) % log_every == 0:
       print(f"step {step + 1}: loss {float(losses[-1]):.3e}", flush=True)
+  meta.lr = lr0
   return torch.stack(losses)
 
 
-def solve_warm_started(probs, meta: MetaInitializer, budget: Optional[int] = None,
-                       **solver_kwargs):
-  """Solves a batch with the learned warm start; problems that have not
-  converged within ``budget`` iterations are solved again from the default
-  initialisation with the full ``max_iterations`` (the plain solver stays
-  the fallback and the judge of convergence).
+def solve_warm_started(geom, a: torch.Tensor, b: torch.Tensor, meta: MetaInitializer,
+                       budget: Optional[int] = None, **solver_kwargs):
+  """Solves the stacked problems (a [K, n], b [K, m] on ``geom``) with the
+  learned warm start; problems that have not converged within ``budget``
+  iterations are solved again from the default initialisation with the
+  full ``max_iterations`` (the plain solver stays the fallback and the judge
+  of convergence).
 
-  Returns (outputs, fallback_indices).
+  Returns (output, fallback_indices); the output's rows of the fallback
+  problems hold the fallback solve.
   """
   from ott_b200.solvers.linear import sinkhorn
   max_it = solver_kwargs.get("max_iterations", 2000)
   warm_kw = dict(solver_kwargs, max_iterations=budget or max_it)
-  outs = sinkhorn.run_batch(probs, sinkhorn.Sinkhorn(initializer=meta, **warm_kw))
-  conv = torch.tensor([bool(o.converged) for o in outs])
-  redo = [k for k in range(len(probs)) if not conv[k]]
-  if redo:
-    again = sinkhorn.run_batch([probs[k] for k in redo], sinkhorn.Sinkhorn(**solver_kwargs))
-    for k, o in zip(redo, again):
-      outs[k] = o
-  return outs, redo
+  out = sinkhorn.run_stacked(geom, a, b, sinkhorn.Sinkhorn(initializer=meta, **warm_kw))
+  n_it, conv, cost = out.scalars()
+  redo = np.nonzero(~conv)[0]
+  if redo.size == 0:
+    return out, redo
+  idx = torch.as_tensor(redo, device=a.device)
+  again = sinkhorn.run_stacked(geom, a[idx], b[idx], sinkhorn.Sinkhorn(**solver_kwargs))
+  # merged output: warm rows, fallback rows replaced (iteration counts add up)
+  f, g = out.f.clone(), out.g.clone()
+  f[idx], g[idx] = again.f, again.g
+  return _Merged(out, again, redo, f, g), redo
+
+
+class _Merged:
+  """A warm-started stacked output with its fallback rows replaced."""
+
+  def __init__(self, warm, again, redo, f, g):
+    self.f, self.g = f, g
+    self._warm, self._again, self._redo = warm, again, redo
+
+  def scalars(self):
+    n_it, conv, cost = self._warm.scalars()
+    n2, c2, cost2 = self._again.scalars()
+    n_it = n_it.copy()
+    n_it[self._redo] += n2  # the wasted warm iterations count too
+    conv = conv.copy()
+    conv[self._redo] = c2
+    cost = cost.copy()
+    cost[self._redo] = cost2
+    return n_it, conv, cost

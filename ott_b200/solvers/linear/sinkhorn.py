@@ -333,3 +333,120 @@ def _replay_progress(solver: Sinkhorn, outs: List[SinkhornOutput]) -> None:
     for blk in range(int((errs != -1).sum())):
       it = (blk + 1) * solver.inner_iterations - 1
       solver.progress_fn((it, solver.inner_iterations, solver.max_iterations, o))
+
+
+class StackedSinkhornOutput(NamedTuple):
+  """Output of ``run_stacked``: the leaves of ``jax.vmap(solve)`` over
+  problems that share one geometry, stacked along axis 0.
+
+  ``f`` [K, n], ``g`` [K, m], ``errors`` [K, outer] are device tensors;
+  ``n_iters``, ``converged`` and ``reg_ot_cost`` are host arrays read from
+  the device records once.
+  """
+
+  f: torch.Tensor
+  g: torch.Tensor
+  errors: torch.Tensor
+  records: torch.Tensor  # [K * sizeof(ottb_result)] device bytes
+  geom: Any
+  a: torch.Tensor
+  b: torch.Tensor
+
+  def _host(self):
+    import numpy as np
+    raw = self.records.cpu().numpy()
+    rec = np.frombuffer(raw.tobytes(), dtype=_lib.numpy_dtype(_lib.OttbResult))
+    bad = rec["status"] != _lib.OTTB_OK
+    if bad.any():
+      raise _lib.OttbError(int(rec["status"][bad][0]), "ottb_sinkhorn_pointcloud (device)")
+    return rec
+
+  def scalars(self):
+    """(n_iters, converged, reg_ot_cost) as numpy arrays, one device read."""
+    rec = self._host()
+    return rec["n_iters"].copy(), rec["converged"].astype(bool), rec["reg_ot_cost"].copy()
+
+  @property
+  def n_iters(self):
+    return self.scalars()[0]
+
+  @property
+  def converged(self):
+    return self.scalars()[1]
+
+  @property
+  def reg_ot_cost(self):
+    return self.scalars()[2]
+
+
+def run_stacked(geom, a: torch.Tensor, b: torch.Tensor, solver: Sinkhorn,
+                init: Optional[Tuple[Optional[torch.Tensor], Optional[torch.Tensor]]] = None,
+                f_from_g: Optional[bool] = None) -> StackedSinkhornOutput:
+  """Solves K problems on ONE geometry with weights ``a`` [K, n] and ``b``
+  [K, m] in one persistent launch: ``jax.vmap(lambda a, b:
+  solve(geom, a, b))(a, b)`` of the reference, without per-problem host
+  objects (the problem records are filled as arrays).
+
+  ``init``: stacked (F, G), either may be None. Without it, an initializer
+  with a ``stacked_init(a, b)`` method supplies (F, G) in one call (its
+  ``half_step_from_g`` then defaults ``f_from_g``); otherwise the default
+  initialisation runs on the device.
+  """
+  import numpy as np
+  lib = _lib.load()
+  dev = geom.x.device
+  n, m = geom.shape
+  a = _arrays.as_f32(a, dev).contiguous()
+  b = _arrays.as_f32(b, dev).contiguous()
+  K = a.shape[0]
+  if a.shape != (K, n) or b.shape != (K, m):
+    raise ValueError(f"a must be [K, {n}] and b [K, {m}]")
+  mask_init = False
+  if init is None:
+    fn = getattr(solver.initializer, "stacked_init", None)
+    if fn is not None:
+      init = fn(a, b)
+      mask_init = True
+      if f_from_g is None:
+        f_from_g = bool(getattr(solver.initializer, "half_step_from_g", False))
+    elif not isinstance(solver.initializer, init_lib.DefaultInitializer):
+      raise NotImplementedError("run_stacked needs an initializer with stacked_init")
+  fi, gi = (None, None) if init is None else init
+  fi = None if fi is None else _arrays.as_f32(fi, dev).contiguous()
+  gi = None if gi is None else _arrays.as_f32(gi, dev).contiguous()
+  outer = solver.outer_iterations
+  f = torch.empty((K, n), dtype=torch.float32, device=dev)
+  g = torch.empty((K, m), dtype=torch.float32, device=dev)
+  errors = torch.empty((K, max(outer, 1)), dtype=torch.float32, device=dev)
+  arr = (_lib.OttbProblem * K)()
+  rec = np.frombuffer(arr, dtype=_lib.numpy_dtype(_lib.OttbProblem))
+  ks = np.arange(K, dtype=np.uint64)
+  rec["x"] = geom.x.data_ptr()
+  rec["y"] = geom.y.data_ptr()
+  rec["a"] = a.data_ptr() + ks * (4 * n)
+  rec["b"] = b.data_ptr() + ks * (4 * m)
+  rec["f_init"] = 0 if fi is None else fi.data_ptr() + ks * (4 * n)
+  rec["g_init"] = 0 if gi is None else gi.data_ptr() + ks * (4 * m)
+  rec["f"] = f.data_ptr() + ks * (4 * n)
+  rec["g"] = g.data_ptr() + ks * (4 * m)
+  rec["errors"] = errors.data_ptr() + ks * (4 * errors.shape[1])
+  rec["n"] = n
+  rec["m"] = m
+  rec["epsilon"] = float(geom.epsilon)
+  rec["inv_scale_cost"] = float(geom.inv_scale_cost)
+  cfg = solver._cfg(mask_init or init is None, geom.epsilon_scheduler)
+  cfg.init_f_from_g = 1 if f_from_g else 0
+  ws_bytes = lib.ottb_sinkhorn_workspace_size(arr, K, geom.dim, ctypes.byref(cfg))
+  if ws_bytes == 0:
+    raise NotImplementedError("problem sizes or configuration not supported")
+  ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+  res = torch.empty(K * _lib.RESULT_BYTES, dtype=torch.uint8, device=dev)
+  st = lib.ottb_sinkhorn_pointcloud(arr, K, geom.dim, ctypes.byref(cfg), res.data_ptr(),
+                                    ws.data_ptr(), ws_bytes, _arrays.stream_handle())
+  if st == _lib.OTTB_ERR_UNSUPPORTED:
+    raise NotImplementedError(_lib.status_string(st))
+  _lib.check(st, "ottb_sinkhorn_pointcloud")
+  cur = torch.cuda.current_stream()
+  for t in (ws, a, b) + tuple(t for t in (fi, gi) if t is not None):
+    t.record_stream(cur)
+  return StackedSinkhornOutput(f, g, errors[:, :outer], res, geom, a, b)

@@ -75,21 +75,35 @@ def grid_support(side=32):
   return np.stack([gx.ravel(), gy.ravel()], axis=1).astype(np.float32)
 
 
-def grid_mixture_weights(num, grid, seed=0, floor=1e-6):
+def grid_mixture_weights(num, grid, seed=0, floor=1e-6, chunk=4096, device=None):
   """num measures on a fixed grid: each is a mixture of 1-5 isotropic
   Gaussians (means U[0,1]^2, std U[0.03, 0.2], mixture weights Dirichlet(1))
   evaluated at the grid points, normalised, plus a floor, renormalised.
-  Returns [num, len(grid)] float32."""
+  Returns [num, len(grid)] float32: numpy, or a torch tensor evaluated on
+  ``device`` when one is given (same parameters, float64 evaluation)."""
   rng = np.random.default_rng(seed)
-  out = np.empty((num, len(grid)), np.float64)
-  g = grid.astype(np.float64)
-  for i in range(num):
-    k = int(rng.integers(1, 6))
-    mu = rng.uniform(size=(k, 2))
-    sd = rng.uniform(0.03, 0.2, size=k)
-    pi = rng.dirichlet(np.ones(k))
-    d2 = ((g[:, None, :] - mu[None]) ** 2).sum(-1)
-    dens = (pi / (2 * np.pi * sd * sd) * np.exp(-d2 / (2 * sd * sd))).sum(1)
-    w = dens / dens.sum() + floor
-    out[i] = w / w.sum()
-  return out.astype(np.float32)
+  if device is not None:
+    import torch
+    xp_g = torch.tensor(grid, dtype=torch.float64, device=device)
+    out = torch.empty((num, len(grid)), dtype=torch.float32, device=device)
+    conv = lambda v: torch.as_tensor(v, device=device)
+    xp_exp = torch.exp
+  else:
+    xp_g = grid.astype(np.float64)
+    out = np.empty((num, len(grid)), np.float32)
+    conv = lambda v: v
+    xp_exp = np.exp
+  for s in range(0, num, chunk):
+    c = min(chunk, num - s)
+    k = rng.integers(1, 6, size=c)
+    mu = rng.uniform(size=(c, 5, 2))
+    sd = rng.uniform(0.03, 0.2, size=(c, 5))
+    # Dirichlet(1) over the first k components: normalised exponentials
+    e = rng.exponential(size=(c, 5)) * (np.arange(5)[None] < k[:, None])
+    pi = e / e.sum(1, keepdims=True)
+    mu, var, coef = conv(mu), conv(2 * sd * sd), conv(pi / (2 * np.pi * sd * sd))
+    d2 = ((xp_g[None, :, None, :] - mu[:, None]) ** 2).sum(-1)          # [c, P, 5]
+    dens = (coef[:, None] * xp_exp(-d2 / var[:, None])).sum(-1)
+    w = dens / dens.sum(1, keepdims=True) + floor
+    out[s:s + c] = w / w.sum(1, keepdims=True)
+  return out

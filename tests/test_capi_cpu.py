@@ -45,6 +45,21 @@ def test_struct_layouts_match_header():
   assert ctypes.sizeof(_lib.OttbMlp) == 8 + _lib.MLP_MAX_LAYERS * (2 * 4 + 10 * 8)
 
 
+def test_numpy_record_views_match_ctypes():
+  import numpy as np
+  arr = (_lib.OttbProblem * 3)()
+  rec = np.frombuffer(arr, dtype=_lib.numpy_dtype(_lib.OttbProblem))
+  rec["n"] = [1, 2, 3]
+  rec["b"] = np.arange(3, dtype=np.uint64) * 8 + 64
+  rec["inv_scale_cost"] = 0.25
+  assert [p.n for p in arr] == [1, 2, 3]
+  assert arr[2].b == 80 and arr[1].inv_scale_cost == 0.25
+  res = (_lib.OttbResult * 2)()
+  res[1].n_iters, res[1].reg_ot_cost = 7, 1.5
+  view = np.frombuffer(bytes(res), dtype=_lib.numpy_dtype(_lib.OttbResult))
+  assert view["n_iters"][1] == 7 and view["reg_ot_cost"][1] == 1.5
+
+
 def test_invalid_arguments_rejected_without_device():
   lib = _lib.load()
   cfg = _lib.OttbSolverCfg(threshold=1e-3, norm_error=1, inner_iterations=10,

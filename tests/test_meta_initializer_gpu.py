@@ -38,7 +38,8 @@ def test_mlp_forward_matches_oracle():
   assert _rel(y, y_exact) < 2e-2
 
 
-def test_mlp_gradients_match_oracle():
+@pytest.mark.parametrize("weighted", [False, True])
+def test_mlp_gradients_match_oracle(weighted):
   import torch
   dims = [256, 256, 128, 128]
   net = _mlp(dims, seed=2)
@@ -46,13 +47,15 @@ def test_mlp_gradients_match_oracle():
   batch = 384
   x = rng.standard_normal((batch, 256)).astype(np.float32)
   t = rng.standard_normal((batch, 128)).astype(np.float32)
-  loss = net.gradients(torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda"))
+  w = rng.uniform(0.05, 2.0, size=(batch, 128)).astype(np.float32) if weighted else None
+  loss = net.gradients(torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda"),
+                       None if w is None else torch.tensor(w, device="cuda"))
   loss = loss.cpu().numpy()
   net.check_status()
   params = net.params_numpy()
-  bparams = [(mlp_np.bf16(w).astype(np.float64), b) for w, b in params]
+  bparams = [(mlp_np.bf16(wt).astype(np.float64), b) for wt, b in params]
   loss_ref, grads = mlp_np.loss_and_grads(bparams, mlp_np.bf16(x).astype(np.float64),
-                                          t.astype(np.float64))
+                                          t.astype(np.float64), w)
   np.testing.assert_allclose(loss, loss_ref, rtol=2e-2)
   for l, tens in enumerate(net.tensors):
     gw = tens["w_grad"].cpu().numpy()
@@ -112,46 +115,79 @@ def test_f_from_g_matches_oracle(n, m, d, precision):
   helpers.assert_parity(geom, out, ref)
 
 
-def _grid_batch(geom, A, B):
+def test_run_stacked_matches_run_batch():
+  """The array-filled problem records give the per-problem path's results."""
+  import torch
+  from ott_b200.geometry import pointcloud
   from ott_b200.problems.linear import linear_problem
-  return [linear_problem.LinearProblem(geom, a=A[k], b=B[k]) for k in range(A.shape[0])]
+  from ott_b200.solvers.linear import sinkhorn
+  grid = problems.grid_support(16)
+  W = torch.tensor(problems.grid_mixture_weights(12, grid, seed=5)).cuda()
+  geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
+  A, B = W[0::2], W[1::2]
+  st = sinkhorn.run_stacked(geom, A, B, sinkhorn.Sinkhorn())
+  outs = sinkhorn.run_batch([linear_problem.LinearProblem(geom, A[k], B[k]) for k in range(6)],
+                            sinkhorn.Sinkhorn())
+  n_it, conv, cost = st.scalars()
+  for k, o in enumerate(outs):
+    assert n_it[k] == o.n_iters and conv[k] == o.converged
+    assert cost[k] == o.reg_ot_cost
+    torch.testing.assert_close(st.f[k], o.f, rtol=0, atol=0)
+    torch.testing.assert_close(st.g[k], o.g, rtol=0, atol=0)
 
 
 def test_trained_warm_start_cuts_iterations():
   """A 16 x 16 grid (n = m = 256, eps 1e-2), measures as in the 32 x 32
-  learned-warm-start workload; the network is trained for a few hundred Adam
-  steps on 2048 problems solved by the plain kernel, then warm-starts 256
-  held-out problems. Both runs converge to the same threshold; the costs
-  agree to the accuracy the threshold allows."""
+  learned-warm-start workload; the network is trained for 1500 Adam steps on
+  16384 problems solved by the plain kernel, then warm-starts 256 held-out
+  problems. Both runs converge to the same threshold; the costs agree to the
+  accuracy the threshold allows."""
   import torch
   from ott_b200.geometry import pointcloud
   from ott_b200.initializers.neural import meta_initializer
   from ott_b200.solvers.linear import sinkhorn
   grid = problems.grid_support(16)
-  W = problems.grid_mixture_weights(2 * (2048 + 256), grid, seed=11)
-  A = torch.tensor(W[0::2]).cuda()
-  B = torch.tensor(W[1::2]).cuda()
+  ntr = 16384
+  W = problems.grid_mixture_weights(2 * (ntr + 256), grid, seed=11, device="cuda")
+  A, B = W[0::2].contiguous(), W[1::2].contiguous()
   geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
-  train = _grid_batch(geom, A[:2048], B[:2048])
-  solved = sinkhorn.run_batch(train, sinkhorn.Sinkhorn())
-  assert all(o.converged for o in solved)
-  G = torch.stack([o.g for o in solved])
+  solved = sinkhorn.run_stacked(geom, A[:ntr], B[:ntr], sinkhorn.Sinkhorn())
+  assert solved.converged.all()
 
   meta = meta_initializer.MetaInitializer(geom, dims=(512, 512), lr=1e-3, seed=0)
-  losses = meta_initializer.fit(meta, A[:2048], B[:2048], G, steps=600, batch_size=256)
+  losses = meta_initializer.fit(meta, A[:ntr], B[:ntr], solved.g, steps=1500, batch_size=512)
   meta.mlp.check_status()
   losses = losses.cpu().numpy()
   assert losses[-50:].mean() < 0.1 * losses[:10].mean(), (losses[:10].mean(), losses[-50:])
 
-  held = _grid_batch(geom, A[2048:], B[2048:])
-  cold = sinkhorn.run_batch(held, sinkhorn.Sinkhorn())
-  warm, redo = meta_initializer.solve_warm_started(held, meta)
-  it_cold = np.array([o.n_iters for o in cold])
-  it_warm = np.array([o.n_iters for o in warm])
-  assert all(o.converged for o in cold) and all(o.converged for o in warm)
+  cold = sinkhorn.run_stacked(geom, A[ntr:], B[ntr:], sinkhorn.Sinkhorn())
+  warm, redo = meta_initializer.solve_warm_started(geom, A[ntr:], B[ntr:], meta)
+  it_cold, conv_cold, c_cold = cold.scalars()
+  it_warm, conv_warm, c_warm = warm.scalars()
+  assert conv_cold.all() and conv_warm.all()
   print(f"iterations: cold {it_cold.mean():.1f}, warm {it_warm.mean():.1f}, "
         f"fallbacks {len(redo)}, loss {losses[:10].mean():.3e} -> {losses[-50:].mean():.3e}")
   assert it_warm.mean() < 0.8 * it_cold.mean()
-  c_cold = np.array([o.reg_ot_cost for o in cold])
-  c_warm = np.array([o.reg_ot_cost for o in warm])
   np.testing.assert_allclose(c_warm, c_cold, rtol=1e-3)
+
+
+def test_warm_start_fallback_restores_default_init():
+  """A budget too small for the warm start: every problem falls back to the
+  default initialisation and ends with the plain solver's result."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.initializers.neural import meta_initializer
+  from ott_b200.solvers.linear import sinkhorn
+  grid = problems.grid_support(16)
+  W = torch.tensor(problems.grid_mixture_weights(16, grid, seed=9)).cuda()
+  A, B = W[0::2], W[1::2]
+  geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
+  meta = meta_initializer.MetaInitializer(geom, dims=(256,), seed=1)  # untrained
+  out, redo = meta_initializer.solve_warm_started(geom, A, B, meta, budget=10)
+  plain = sinkhorn.run_stacked(geom, A, B, sinkhorn.Sinkhorn())
+  n_it, conv, cost = out.scalars()
+  n0, c0, cost0 = plain.scalars()
+  assert len(redo) == 8 and conv.all()
+  np.testing.assert_array_equal(n_it, n0 + 10)
+  np.testing.assert_array_equal(cost, cost0)
+  torch.testing.assert_close(out.g, plain.g, rtol=0, atol=0)

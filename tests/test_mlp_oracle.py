@@ -1,6 +1,7 @@
 """The learned initializer's float64 network oracle: hand-written gradients
 against central finite differences, and Adam's bias-corrected first step."""
 import numpy as np
+import pytest
 
 from oracle import mlp_np
 
@@ -10,12 +11,14 @@ def _params(rng, dims):
           for i, o in zip(dims[:-1], dims[1:])]
 
 
-def test_gradients_match_finite_differences():
+@pytest.mark.parametrize("weighted", [False, True])
+def test_gradients_match_finite_differences(weighted):
   rng = np.random.default_rng(0)
   params = _params(rng, [6, 5, 4, 3])
   x = rng.standard_normal((7, 6))
   t = rng.standard_normal((7, 3))
-  loss, grads = mlp_np.loss_and_grads(params, x, t)
+  lw = rng.uniform(0.1, 2.0, size=(7, 3)) if weighted else None
+  loss, grads = mlp_np.loss_and_grads(params, x, t, lw)
   h = 1e-6
   for l, (w, b) in enumerate(params):
     for arr, g in ((w, grads[l][0]), (b, grads[l][1])):
@@ -24,9 +27,9 @@ def test_gradients_match_finite_differences():
       for k in range(0, flat.size, 3):
         old = flat[k]
         flat[k] = old + h
-        lp = mlp_np.loss_and_grads(params, x, t)[0].mean()
+        lp = mlp_np.loss_and_grads(params, x, t, lw)[0].mean()
         flat[k] = old - h
-        lm = mlp_np.loss_and_grads(params, x, t)[0].mean()
+        lm = mlp_np.loss_and_grads(params, x, t, lw)[0].mean()
         flat[k] = old
         np.testing.assert_allclose(gflat[k], (lp - lm) / (2 * h), rtol=1e-5, atol=1e-9)
 
