@@ -59,6 +59,8 @@ def parse_args():
   p.add_argument("--test-pairs", type=int, default=10000)
   p.add_argument("--train-steps", type=int, default=12000)
   p.add_argument("--problems", type=int, default=512)
+  p.add_argument("--pairs", type=int, default=8)
+  p.add_argument("--stages", type=int, default=10)
   return p.parse_args()
 
 
@@ -520,6 +522,164 @@ def run_warmstart(args):
   return 0
 
 
+# ---------------------------------------------------------------------------
+# batched uneven problems in one persistent launch
+# ---------------------------------------------------------------------------
+def run_batched(args):
+  """512 independent problems, n_k and m_k log-uniform in [128, 16384],
+  d = 32, 4-component Gaussian-mixture clouds, Dirichlet(1) weights,
+  epsilon_k = 0.05 * mean(C_k), threshold 1e-3: one launch for all of them
+  (chosen precision and FP32), and one launch per problem for comparison.
+  Inputs (~440 MB) exceed the L2."""
+  import torch
+  from tests import problems
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers.linear import sinkhorn
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  data = problems.batched_uneven_problems(args.problems, d=32, seed=0)
+  probs = []
+  for x, y, a, b in data:
+    geom = pointcloud.PointCloud(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(),
+                                 epsilon=0.05, relative_epsilon="mean")
+    probs.append(linear_problem.LinearProblem(geom, torch.from_numpy(a).cuda(),
+                                              torch.from_numpy(b).cuda()))
+  for p in probs:
+    _ = p.geom.epsilon  # resolve the relative epsilons before timing
+  entries_per_it = 2.0 * sum(p.geom.shape[0] * p.geom.shape[1] for p in probs)
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+
+  def timed(fn, steps, warm):
+    for _ in range(warm):
+      fn()
+    torch.cuda.synchronize()
+    ms, outs = 0.0, None
+    for _ in range(steps):
+      e0, e1 = ev(), ev()
+      e0.record()
+      outs = fn()
+      e1.record()
+      e1.synchronize()
+      ms += e0.elapsed_time(e1)
+    return ms / steps * 1e-3, outs
+
+  def batch(precision):
+    return lambda: sinkhorn.run_batch(probs, sinkhorn.Sinkhorn(precision=precision))
+
+  def one_by_one(precision):
+    solver = sinkhorn.Sinkhorn(precision=precision)
+    return lambda: [solver(p) for p in probs]
+
+  clocks = ClockSampler(0)
+  clocks.start()
+  t_b, o_b = timed(batch("auto"), args.steps, args.warmup)
+  clk = clocks.stop()
+  t_f, o_f = timed(batch("fp32"), 1, 1)
+  t_s, o_s = timed(one_by_one("auto"), 1, 1)
+  it_b = np.array([o.n_iters for o in o_b])
+  it_f = np.array([o.n_iters for o in o_f])
+  conv = np.array([o.converged for o in o_b])
+  c_b = np.array([o.reg_ot_cost for o in o_b])
+  c_f = np.array([o.reg_ot_cost for o in o_f])
+  entries = sum(2.0 * p.geom.shape[0] * p.geom.shape[1] * o.n_iters
+                for p, o in zip(probs, o_b))
+  peaks = measure_pipe_peaks(torch)
+  ach = entries / t_b / 1e9
+  roof = {"bound": "mufu_ex2", "achieved": ach, "peak": peaks["ex2_per_s"] / 1e9,
+          "unit": "Gex2/s", "frac": ach / (peaks["ex2_per_s"] / 1e9),
+          "peak_source": "measured in bench.py (MUFU ex2 probe kernel)"}
+  if clk and clk.get("sm_mhz"):
+    at = 16 * torch.cuda.get_device_properties(0).multi_processor_count * clk["sm_mhz"] * 1e-3
+    roof["peak_at_sampled_clock"] = at
+    roof["frac_at_sampled_clock"] = ach / at
+  sizes = np.array([p.geom.shape for p in probs])
+  line = {
+      "metric": "s to 1e-3 marginal err, 512 uneven problems in one launch",
+      "value": t_b, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "workload": "batched", "dtype": "bf16x3/f32", "data": "synthetic",
+      "steps": args.steps, "warmup": args.warmup,
+      "config": {"workload": f"{args.problems} problems n,m log-uniform [128,16384] d=32 "
+                             "GMM clouds, Dirichlet(1) weights, eps=0.05*mean(C_k), thr=1e-3",
+                 "total_entries_per_iteration": entries_per_it,
+                 "n_range": [int(sizes[:, 0].min()), int(sizes[:, 0].max())],
+                 "l2": "inputs ~440 MB > L2"},
+      "converged": int(conv.sum()), "mean_iters": float(it_b.mean()),
+      "max_iters": int(it_b.max()), "entries_per_s": entries / t_b,
+      "plain_fp32_batched": {"s": t_f, "mean_iters": float(it_f.mean())},
+      "one_launch_per_problem": {"s": t_s},
+      "speedup_vs_plain_fp32": t_f / t_b, "speedup_vs_per_problem": t_s / t_b,
+      "cost_rel_diff_vs_fp32": float(np.max(np.abs(c_b - c_f) / np.abs(c_f))),
+      "iters_equal_fp32": int((it_b == it_f).sum()),
+      "roofline": roof, "clocks": clk,
+  }
+  print(json.dumps(line))
+  return 0
+
+
+# ---------------------------------------------------------------------------
+# epsilon-annealed solves
+# ---------------------------------------------------------------------------
+def run_anneal(args):
+  """``--pairs`` pairs of 8-component Gaussian mixtures in R^128 (means
+  N(0, I), std U[0.2, 1]), n = m = ``--n``, uniform weights; epsilon annealed
+  geometrically from 1 to 1e-3 * mean(C) over ``--stages`` stages, threshold
+  1e-3 per stage, every pair in one launch per stage, each stage warm-started
+  from the previous one; FP32 redoes any stage the chosen form does not
+  converge. The plain FP32 chain on pair 0 is the judge."""
+  import torch
+  from tests import problems
+  from ott_b200.solvers.linear import annealing
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  d = 128
+  pairs = [problems.gmm8_pair(args.n, args.n, d, seed=s) for s in range(args.pairs)]
+  xs = [torch.from_numpy(p[0]).cuda() for p in pairs]
+  ys = [torch.from_numpy(p[1]).cuda() for p in pairs]
+  del pairs
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+
+  def timed(fn):
+    e0, e1 = ev(), ev()
+    e0.record()
+    out = fn()
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) * 1e-3, out
+
+  run = lambda xs_, ys_, prec, fb: annealing.solve_annealed(
+      xs_, ys_, stages=args.stages, start=1.0, final=1e-3, precision=prec,
+      fallback_precision=fb)
+  # warm-up on a reduced copy (compiles nothing; loads modules, sizes caches)
+  run([x[:4096] for x in xs[:1]], [y[:4096] for y in ys[:1]], "auto", "fp32")
+  clocks = ClockSampler(0)
+  clocks.start()
+  t_c, out = timed(lambda: run(xs, ys, "auto", "fp32"))
+  clk = clocks.stop()
+  it = out.stage_iters
+  entries = float((2.0 * args.n * args.n * it).sum())
+  line = {
+      "metric": "s to 1e-3 marginal err per stage, epsilon annealed 1 -> 1e-3 mean(C)",
+      "value": t_c, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "workload": "anneal", "dtype": "bf16x3/f32", "data": "synthetic",
+      "config": {"workload": f"{args.pairs} pairs GMM8 n=m={args.n} d={d}, "
+                             f"{args.stages} geometric stages 1 -> 1e-3 mean(C), thr 1e-3",
+                 "l2": f"inputs {2 * args.pairs * args.n * d * 4 / 2**20:.0f} MiB"},
+      "stage_iters_mean": it.mean(axis=1).tolist(), "total_iters": int(it.sum()),
+      "entries_per_s": entries / t_c, "fallbacks": out.fallbacks,
+      "converged": int(sum(o.converged for o in out.outputs)),
+      "clocks": clk,
+  }
+  if not args.no_plain:
+    t_p, plain = timed(lambda: run(xs[:1], ys[:1], "fp32", None))
+    c0, c1 = out.outputs[0].reg_ot_cost, plain.outputs[0].reg_ot_cost
+    line["plain_fp32_pair0"] = {
+        "s": t_p, "stage_iters": plain.stage_iters[:, 0].tolist(),
+        "chosen_stage_iters": it[:, 0].tolist(),
+        "reg_ot_cost_rel_diff": abs(c0 - c1) / abs(c1),
+        "speedup_per_pair": t_p / (t_c / args.pairs)}
+  print(json.dumps(line))
+  return 0
+
+
 def main():
   args = parse_args()
   if args.warmup < 3:
@@ -528,6 +688,10 @@ def main():
     return run_reference(args)
   if args.workload == "warmstart":
     return run_warmstart(args)
+  if args.workload == "batched":
+    return run_batched(args)
+  if args.workload == "anneal":
+    return run_anneal(args)
   return run_ours(args)
 
 

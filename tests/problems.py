@@ -107,3 +107,19 @@ def grid_mixture_weights(num, grid, seed=0, floor=1e-6, chunk=4096, device=None)
     w = dens / dens.sum(1, keepdims=True) + floor
     out[s:s + c] = w / w.sum(1, keepdims=True)
   return out
+
+
+def gmm8_pair(n, m, d=128, seed=0):
+  """Two independent 8-component Gaussian mixtures in R^d (means N(0, I),
+  per-component std U[0.2, 1], equal component probabilities), uniform
+  weights: the epsilon-annealing workload's clouds."""
+  rng = np.random.default_rng(seed)
+
+  def cloud(size):
+    means = rng.standard_normal((8, d))
+    std = rng.uniform(0.2, 1.0, size=8)
+    comp = rng.integers(0, 8, size=size)
+    return (means[comp] + std[comp, None] * rng.standard_normal((size, d))).astype(np.float32)
+
+  x, y = cloud(n), cloud(m)
+  return x, y, np.full(n, 1.0 / n, np.float32), np.full(m, 1.0 / m, np.float32)
