@@ -277,12 +277,15 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     ProbPlan& pp = plan.probs[t];
     pp.n = q.n;
     pp.m = q.m;
-    pp.n_pad = round_up(q.n, kBM);
-    pp.m_pad = round_up(q.m, kBM);
-    pp.rb_f = (int)(pp.n_pad / kBM);
-    pp.rb_g = (int)(pp.m_pad / kBM);
-    pp.split_f = choose_split(pp.rb_f, (int)(pp.m_pad / kBN), plan.grid, num);
-    pp.split_g = choose_split(pp.rb_g, (int)(pp.n_pad / kBN), plan.grid, num);
+    // Points are padded to whole column tiles (128 columns on the CUDA
+    // cores, 256 on the tensor cores); row blocks of 128 cover the real rows.
+    const int64_t tile_n = plan.tc ? TcCfg<64>::kTileN : kBN;
+    pp.n_pad = round_up(q.n, tile_n);
+    pp.m_pad = round_up(q.m, tile_n);
+    pp.rb_f = (int)((q.n + kBM - 1) / kBM);
+    pp.rb_g = (int)((q.m + kBM - 1) / kBM);
+    pp.split_f = choose_split(pp.rb_f, (int)(pp.m_pad / tile_n), plan.grid, num);
+    pp.split_g = choose_split(pp.rb_g, (int)(pp.n_pad / tile_n), plan.grid, num);
     const size_t fsz = sizeof(float);
     // FP32 engine: transposed [DP][pad] floats; tensor cores: [2][pad][DK] bf16
     const size_t elt = plan.tc ? 2 * 2 : fsz;
@@ -293,8 +296,8 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.off_galt = off; off = align_up(off + fsz * pp.m);
     // Partials are sized for the largest split any grid could choose, so the
     // workspace size does not depend on the device the call runs on.
-    const int64_t smax_f = num > 1 ? 1 : std::min<int64_t>(32, pp.m_pad / kBN);
-    const int64_t smax_g = num > 1 ? 1 : std::min<int64_t>(32, pp.n_pad / kBN);
+    const int64_t smax_f = num > 1 ? 1 : std::min<int64_t>(32, pp.m_pad / tile_n);
+    const int64_t smax_g = num > 1 ? 1 : std::min<int64_t>(32, pp.n_pad / tile_n);
     const int64_t parts = std::max(smax_f * pp.n, smax_g * pp.m);
     const bool split = smax_f > 1 || smax_g > 1;
     pp.off_pm = off; off = align_up(off + (split ? fsz * parts : 0));

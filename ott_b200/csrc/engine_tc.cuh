@@ -3,11 +3,14 @@
 // log-sum-exp as the CUDA-core engine.
 //
 // Points are stored as bf16 pairs v = hi + lo (hi = bf16(v), lo =
-// bf16(v - hi)), rows of DK (64 or 128) elements, hi rows then lo rows. For a
-// 128 x 128 tile the three products hi*hi + hi*lo + lo*hi accumulate into one
-// TMEM tile (3 * DK / 16 MMAs of M = N = 128, K = 16); lo*lo (~2^-16
-// relative) is dropped. One more K = 16 MMA adds the column shift: A's
-// extension block holds ones in its first 3 K columns, B's holds
+// bf16(v - hi)), rows of DK (64 or 128) elements, hi rows then lo rows. A
+// tile is 128 rows of A by 256 columns of B: the three products hi*hi +
+// hi*lo + lo*hi accumulate into one TMEM tile (3 * DK / 16 MMAs of M = 128,
+// N = 256, K = 16); lo*lo (~2^-16 relative) is dropped. N = 256 because an
+// N = 128 MMA takes ~84 cycles on B200 where an N = 256 one takes 128 (the
+// full rate; measured with back-to-back MMAs, A in shared or tensor memory
+// alike). One more K = 16 MMA adds the column shift: A's extension block
+// holds ones in its first 3 K columns, B's holds
 // w'_c = (pot_c - inv |B_c|^2) / (2 inv) as 3 bf16 terms (~24 bits), so the
 // accumulator is acc = <a_r, b_c> + w'_c and the exponent is s * acc,
 // s = 2 inv log2(e) / eps. The epilogue needs no per-column data, and w' is
@@ -16,13 +19,15 @@
 // producer loads by TMA with the B tile.
 //
 // Warp roles in the 576-thread CTA:
-//   warp 0      producer (lane 0): A tile once per unit; B tiles and their
-//               column-shift rows through a ring of kStages shared-memory
-//               stages (TMA, no multicast).
-//   warp 1      TMEM owner and MMA issuer (lane 0): two 128-column
-//               accumulators, so MMAs of tile t+1 overlap the epilogue of t.
+//   warp 0      producer (lane 0): A tile once per unit; B tiles, one 64-wide
+//               K chunk (hi and lo) per shared-memory stage, and their
+//               column-shift rows with the last chunk, through a ring of
+//               kStages stages (TMA, no multicast).
+//   warp 1      TMEM owner and MMA issuer (lane 0): two 256-column
+//               accumulators (all of TMEM), so MMAs of tile t+1 overlap the
+//               epilogue of t.
 //   warps 2-17  epilogue: warp w reads TMEM lanes 32*(w%4).. (its rows) and
-//               the 32-column group (w-2)/4 of each tile and keeps a running
+//               the 64-column group (w-2)/4 of each tile and keeps a running
 //               (max, sum) of 2^(s * acc) per row.
 // Every wait is bounded; a timeout marks the CTA and unwinds.
 #pragma once
@@ -36,33 +41,39 @@ namespace ottb {
 
 template <int DK>
 struct TcCfg {
-  static constexpr int kChunks = DK / 64;                 // 128-byte swizzle atoms along K
-  static constexpr int kBlockBytes = 128 * 64 * 2;        // one [128][64] bf16 block
-  static constexpr int kOperandBytes = 2 * kChunks * kBlockBytes;  // hi + lo
-  static constexpr int kStages = DK <= 64 ? 4 : 2;
+  static constexpr int kChunks = DK / 64;           // 64-wide K chunks (128-byte swizzle atoms)
+  static constexpr int kTileN = 256;                // columns of B per tile (MMA N)
+  static constexpr int kABlockBytes = 128 * 64 * 2;    // one [128][64] bf16 block
+  static constexpr int kBBlockBytes = kTileN * 64 * 2; // one [256][64] bf16 block
+  static constexpr int kABytes = 2 * kChunks * kABlockBytes;  // hi + lo, every chunk
+  static constexpr int kStageBytes = 2 * kBBlockBytes;        // hi + lo of one chunk
+  static constexpr int kStages = 2;
   static constexpr int kTmemBufs = 2;
-  static constexpr int kTmemCols = 256;
+  static constexpr int kTmemCols = 512;
   static constexpr int kColGroups = 4;    // epilogue warps per TMEM lane quarter
+  static constexpr int kColsPerWarp = kTileN / kColGroups;
   static constexpr int kEpiWarps = 4 * kColGroups;
   static constexpr int kThreads = 64 + 32 * kEpiWarps;
-  static constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, 128);
-  // extension block: 128 rows x 16 bf16, K-major without swizzle: K half 0
+  static constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, kTileN);
+  // extension blocks: R rows x 16 bf16, K-major without swizzle: K half 0
   // (elements 0-7) of all rows first, rows 16 B apart (8-row groups 128 B
-  // apart), then K half 1 (all zeros) 2048 B on
-  static constexpr int kExtBytes = 128 * 16 * 2;
-  static constexpr int kExtHalfBytes = 128 * 16;
-  static constexpr uint32_t kExtLbo = 2048;
+  // apart), then K half 1 (all zeros) 16 * R bytes on
+  static constexpr int kAExtBytes = 128 * 16 * 2;
+  static constexpr uint32_t kAExtLbo = 128 * 16;
+  static constexpr int kBExtBytes = kTileN * 16 * 2;
+  static constexpr int kBExtHalfBytes = kTileN * 16;  // the TMA-loaded K half
+  static constexpr uint32_t kBExtLbo = kTileN * 16;
   static constexpr uint32_t kExtSbo = 128;
 };
 
 template <int DK>
 struct TcSmem {
   // operand tiles first: the struct is placed at a 1024-byte boundary
-  uint8_t A[TcCfg<DK>::kOperandBytes];
-  uint8_t B[TcCfg<DK>::kStages][TcCfg<DK>::kOperandBytes];
-  // K = 16 extension blocks, no swizzle: [16 row groups][2 K halves][8 rows][8]
-  uint8_t Aext[TcCfg<DK>::kExtBytes];
-  uint8_t Bext[TcCfg<DK>::kStages][TcCfg<DK>::kExtBytes];
+  uint8_t A[TcCfg<DK>::kABytes];
+  uint8_t B[TcCfg<DK>::kStages][TcCfg<DK>::kStageBytes];
+  // K = 16 extension blocks, no swizzle: [row groups][2 K halves][8 rows][8]
+  uint8_t Aext[TcCfg<DK>::kAExtBytes];
+  uint8_t Bext[TcCfg<DK>::kStages][TcCfg<DK>::kBExtBytes];
   float part_m[TcCfg<DK>::kColGroups][kBM];
   float part_l[TcCfg<DK>::kColGroups][kBM];
   float rm[kBM];
@@ -82,9 +93,10 @@ struct TcSmem {
 };
 
 // Pipeline positions, one copy per thread, advanced identically by every
-// role over the same sequence of tiles and units.
+// role over the same sequence of tiles, K chunks and units.
 struct TcPipe {
   uint32_t tile;   // tiles processed so far (all units, all sweeps)
+  uint32_t chunk;  // ring stages consumed so far (kChunks per tile)
   uint32_t unit;   // units processed so far
   uint32_t last_full_stage;  // producer: most recent stage issued
   uint32_t last_full_parity;
@@ -94,7 +106,8 @@ struct TcPipe {
 // Tensor maps of a problem, stored in global memory: the point sets
 // [2 * pad][DK] bf16 (hi rows, then lo rows; box 64 x 128, 128-byte swizzle)
 // and their column-shift rows [pad][8] and [2 * pad][8] bf16 (box 8 x 128,
-// no swizzle).
+// no swizzle). pad is a multiple of 256, so a B tile never crosses from the
+// hi rows into the lo rows.
 struct TcMaps {
   CUtensorMap x;
   CUtensorMap y;
@@ -102,48 +115,62 @@ struct TcMaps {
   CUtensorMap exty;
 };
 
+// A tile: 128 rows, every K chunk, hi and lo ([part][chunk] blocks).
 template <int DK>
-__device__ __forceinline__ void tc_load_operand(uint8_t* dst, const CUtensorMap* map,
-                                                uint64_t* bar, int32_t row, int32_t pad) {
+__device__ __forceinline__ void tc_load_a(uint8_t* dst, const CUtensorMap* map, uint64_t* bar,
+                                          int32_t row, int32_t pad) {
   constexpr int C = TcCfg<DK>::kChunks;
 #pragma unroll
   for (int part = 0; part < 2; ++part)
 #pragma unroll
     for (int c = 0; c < C; ++c)
-      tc::tma_load_2d(dst + (part * C + c) * TcCfg<DK>::kBlockBytes, map, bar, 64 * c,
+      tc::tma_load_2d(dst + (part * C + c) * TcCfg<DK>::kABlockBytes, map, bar, 64 * c,
                       row + part * pad);
 }
 
-// Issues the 3 * DK / 16 MMAs of one tile into the TMEM accumulator d_tmem.
+// One ring stage: K chunk c of 256 B rows from row, hi and lo ([part] blocks
+// of 256 rows, each loaded as two 128-row boxes).
 template <int DK>
-__device__ __forceinline__ void tc_issue_tile(uint32_t d_tmem, const uint8_t* A, const uint8_t* B) {
+__device__ __forceinline__ void tc_load_b_chunk(uint8_t* dst, const CUtensorMap* map,
+                                                uint64_t* bar, int c, int32_t row, int32_t pad) {
+#pragma unroll
+  for (int part = 0; part < 2; ++part)
+#pragma unroll
+    for (int h = 0; h < 2; ++h)
+      tc::tma_load_2d(dst + part * TcCfg<DK>::kBBlockBytes + h * TcCfg<DK>::kABlockBytes, map,
+                      bar, 64 * c, row + 128 * h + part * pad);
+}
+
+// Issues the 3 * 4 MMAs of K chunk c of one tile into the TMEM accumulator
+// d_tmem (first = the tile's first MMA, which overwrites the accumulator).
+template <int DK>
+__device__ __forceinline__ void tc_issue_chunk(uint32_t d_tmem, const uint8_t* A,
+                                               const uint8_t* Bst, int c, bool first) {
   constexpr int C = TcCfg<DK>::kChunks;
-  constexpr int BB = TcCfg<DK>::kBlockBytes;
-  const uint32_t a0 = tc::smem_u32(A), b0 = tc::smem_u32(B);
+  const uint32_t a0 = tc::smem_u32(A), b0 = tc::smem_u32(Bst);
   // (A part, B part): hi*hi, hi*lo, lo*hi
   const int pa[3] = {0, 0, 1};
   const int pb[3] = {0, 1, 0};
-  uint32_t acc = 0;
+  uint32_t acc = first ? 0u : 1u;
 #pragma unroll
   for (int prod = 0; prod < 3; ++prod)
 #pragma unroll
-    for (int c = 0; c < C; ++c)
-#pragma unroll
-      for (int kk = 0; kk < 4; ++kk) {
-        const uint64_t ad = tc::sw128_kmajor_desc(a0 + (pa[prod] * C + c) * BB + kk * 32);
-        const uint64_t bd = tc::sw128_kmajor_desc(b0 + (pb[prod] * C + c) * BB + kk * 32);
-        tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, acc);
-        acc = 1;
-      }
+    for (int kk = 0; kk < 4; ++kk) {
+      const uint64_t ad =
+          tc::sw128_kmajor_desc(a0 + (pa[prod] * C + c) * TcCfg<DK>::kABlockBytes + kk * 32);
+      const uint64_t bd = tc::sw128_kmajor_desc(b0 + pb[prod] * TcCfg<DK>::kBBlockBytes + kk * 32);
+      tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, acc);
+      acc = 1;
+    }
 }
 
 // The column-shift MMA: D += Aext * Bext^T over K = 16.
 template <int DK>
 __device__ __forceinline__ void tc_issue_ext(uint32_t d_tmem, const uint8_t* Aext,
                                              const uint8_t* Bext) {
-  const uint64_t ad = tc::plain_kmajor_desc(tc::smem_u32(Aext), TcCfg<DK>::kExtLbo,
+  const uint64_t ad = tc::plain_kmajor_desc(tc::smem_u32(Aext), TcCfg<DK>::kAExtLbo,
                                             TcCfg<DK>::kExtSbo);
-  const uint64_t bd = tc::plain_kmajor_desc(tc::smem_u32(Bext), TcCfg<DK>::kExtLbo,
+  const uint64_t bd = tc::plain_kmajor_desc(tc::smem_u32(Bext), TcCfg<DK>::kBExtLbo,
                                             TcCfg<DK>::kExtSbo);
   tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, 1);
 }
@@ -158,20 +185,22 @@ struct TcOperands {
   int64_t rows, cols;
 };
 
-// One work unit: rows row0..row0+127 of A against B tiles [t0, t1).
-// Leaves the per-row base-2 LSE state in sm.rm / sm.rl. Returns false if a
-// wait timed out.
+// One work unit: rows row0..row0+127 of A against B tiles [t0, t1) of 256
+// columns. Leaves the per-row base-2 LSE state in sm.rm / sm.rl. Returns
+// false if a wait timed out.
 //
-// Per ring stage st the producer fills B's hi/lo tiles and the first K half
-// of B's extension block (TMA); full[st] completes on those bytes,
-// empty[st] on the MMA commit.
+// Per ring stage st the producer fills one K chunk of B's hi/lo tiles (and,
+// with the last chunk, the first K half of B's extension block) by TMA;
+// full[st] completes on those bytes, empty[st] on the MMA commit.
 template <int DK>
 __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
                         int t0, int t1, float s, uint64_t timeout_ns) {
   constexpr int NS = TcCfg<DK>::kStages;
   constexpr int NB = TcCfg<DK>::kTmemBufs;
+  constexpr int C = TcCfg<DK>::kChunks;
   constexpr int CG = TcCfg<DK>::kColGroups;
-  constexpr int CW = kBN / CG;  // columns per epilogue warp per tile
+  constexpr int CW = TcCfg<DK>::kColsPerWarp;  // columns per epilogue warp per tile
+  constexpr int TN = TcCfg<DK>::kTileN;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int ntiles = t1 - t0;
@@ -182,21 +211,28 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
       // A tile: wait until the previous unit's MMAs released it.
       if (!tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns)) ok = false;
       if (ok) {
-        tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK>::kOperandBytes);
-        tc_load_operand<DK>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
+        tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK>::kABytes);
+        tc_load_a<DK>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
       }
       for (int i = 0; ok && i < ntiles; ++i) {
-        const uint32_t g = pp.tile + i;
-        const uint32_t st = g % NS;
-        if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
-        const int32_t brow = (t0 + i) * kBN;
-        tc::mbar_arrive_expect_tx(&sm.full[st],
-                                  TcCfg<DK>::kOperandBytes + TcCfg<DK>::kExtHalfBytes);
-        tc_load_operand<DK>(sm.B[st], op.mapB, &sm.full[st], brow, op.padB);
-        tc::tma_load_2d(sm.Bext[st], op.mapBext, &sm.full[st], 0, op.extRow0 + brow);
-        pp.last_full_stage = st;
-        pp.last_full_parity = (g / NS) & 1;
-        pp.issued = 1;
+        const int32_t brow = (t0 + i) * TN;
+        for (int c = 0; c < C; ++c) {
+          const uint32_t g = pp.chunk + i * C + c;
+          const uint32_t st = g % NS;
+          if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
+          const bool last = c == C - 1;
+          tc::mbar_arrive_expect_tx(&sm.full[st], TcCfg<DK>::kStageBytes +
+                                                      (last ? TcCfg<DK>::kBExtHalfBytes : 0));
+          tc_load_b_chunk<DK>(sm.B[st], op.mapB, &sm.full[st], c, brow, op.padB);
+          if (last) {
+            tc::tma_load_2d(sm.Bext[st], op.mapBext, &sm.full[st], 0, op.extRow0 + brow);
+            tc::tma_load_2d(sm.Bext[st] + 128 * 16, op.mapBext, &sm.full[st], 0,
+                            op.extRow0 + brow + 128);
+          }
+          pp.last_full_stage = st;
+          pp.last_full_parity = (g / NS) & 1;
+          pp.issued = 1;
+        }
       }
     }
     __syncwarp();
@@ -204,16 +240,20 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
     if (lane == 0) {
       if (!tc::mbar_wait(&sm.a_full, pp.unit & 1, timeout_ns)) ok = false;
       for (int i = 0; ok && i < ntiles; ++i) {
-        const uint32_t g = pp.tile + i;
-        const uint32_t st = g % NS;
-        const uint32_t b = g % NB;
-        if (!tc::mbar_wait(&sm.full[st], (g / NS) & 1, timeout_ns)) { ok = false; break; }
-        if (!tc::mbar_wait(&sm.tempty[b], ((g / NB) & 1) ^ 1, timeout_ns)) { ok = false; break; }
-        tc::fence_after_sync();
-        const uint32_t d = sm.tmem_base + b * 128;
-        tc_issue_tile<DK>(d, sm.A, sm.B[st]);
-        tc_issue_ext<DK>(d, sm.Aext, sm.Bext[st]);
-        tc::mma_commit(&sm.empty[st]);
+        const uint32_t gt = pp.tile + i;
+        const uint32_t b = gt % NB;
+        if (!tc::mbar_wait(&sm.tempty[b], ((gt / NB) & 1) ^ 1, timeout_ns)) { ok = false; break; }
+        const uint32_t d = sm.tmem_base + b * TN;
+        for (int c = 0; c < C; ++c) {
+          const uint32_t g = pp.chunk + i * C + c;
+          const uint32_t st = g % NS;
+          if (!tc::mbar_wait(&sm.full[st], (g / NS) & 1, timeout_ns)) { ok = false; break; }
+          tc::fence_after_sync();
+          tc_issue_chunk<DK>(d, sm.A, sm.B[st], c, c == 0);
+          if (c == C - 1) tc_issue_ext<DK>(d, sm.Aext, sm.Bext[st]);
+          tc::mma_commit(&sm.empty[st]);
+        }
+        if (!ok) break;
         tc::mma_commit(&sm.tfull[b]);
       }
       if (ok) tc::mma_commit(&sm.a_empty);
@@ -221,7 +261,7 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
     __syncwarp();
   } else {
     // epilogue: warp e reads TMEM lane quarter q (its 32 rows) and column
-    // group cg (CW columns) of every tile
+    // group cg (CW columns, two 32-column loads) of every tile
     const int e = warp - 2;
     const int q = warp & 3;
     const int cg = e >> 2;
@@ -235,50 +275,56 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
         break;
       }
       tc::fence_after_sync();
-      float v[CW];
-      tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * 128 + CW * cg, v);
-      tc::tmem_ld_wait();
-      // The accumulator buffer can be refilled once every warp has read it.
-      tc::fence_before_sync();
-      __syncwarp();
-      if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
-      // tree maximum (depth 4) instead of a 31-step dependent chain
-      float t11[11];
-#pragma unroll
-      for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
-      t11[10] = fmaxf(v[30], v[31]);
-      const float u0 = fmax3(t11[0], t11[1], t11[2]);
-      const float u1 = fmax3(t11[3], t11[4], t11[5]);
-      const float u2 = fmax3(t11[6], t11[7], t11[8]);
-      const float amax = fmaxf(fmax3(u0, u1, u2), fmaxf(t11[9], t11[10]));
-      const float cm = amax * s;  // s > 0
-      if (cm > mrun + kTau) {
-        const float sc = ex2_approx(mrun - cm);
-        lrun *= sc;
-        lcmp *= sc;
-        mrun = cm;
-      }
-      const float negm = -mrun;
-      // 8 accumulators; lanes k >= 8 - OTTB_POLY_OF_8_TC of each group of 8
-      // columns use exp2_poly (FMA pipe), the rest ex2.approx (MUFU).
-      float acc8[8];
-#pragma unroll
-      for (int k = 0; k < 8; ++k) acc8[k] = 0.f;
-#pragma unroll
-      for (int j = 0; j < CW; j += 8) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float xk = fmaf(v[j + k], s, negm);
-          acc8[k] += (k >= 8 - OTTB_POLY_OF_8_TC) ? exp2_poly(xk) : ex2_approx(xk);
+#pragma unroll 1
+      for (int h = 0; h < CW / 32; ++h) {
+        float v[32];
+        tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg + 32 * h, v);
+        tc::tmem_ld_wait();
+        if (h == CW / 32 - 1) {
+          // The accumulator buffer can be refilled once every warp has read it.
+          tc::fence_before_sync();
+          __syncwarp();
+          if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
         }
+        // tree maximum (depth 4) instead of a 31-step dependent chain
+        float t11[11];
+#pragma unroll
+        for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
+        t11[10] = fmaxf(v[30], v[31]);
+        const float u0 = fmax3(t11[0], t11[1], t11[2]);
+        const float u1 = fmax3(t11[3], t11[4], t11[5]);
+        const float u2 = fmax3(t11[6], t11[7], t11[8]);
+        const float amax = fmaxf(fmax3(u0, u1, u2), fmaxf(t11[9], t11[10]));
+        const float cm = amax * s;  // s > 0
+        if (cm > mrun + kTau) {
+          const float sc = ex2_approx(mrun - cm);
+          lrun *= sc;
+          lcmp *= sc;
+          mrun = cm;
+        }
+        const float negm = -mrun;
+        // 8 accumulators; lanes k >= 8 - OTTB_POLY_OF_8_TC of each group of 8
+        // columns use exp2_poly (FMA pipe), the rest ex2.approx (MUFU).
+        float acc8[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc8[k] = 0.f;
+#pragma unroll
+        for (int j = 0; j < 32; j += 8) {
+#pragma unroll
+          for (int k = 0; k < 8; ++k) {
+            const float xk = fmaf(v[j + k], s, negm);
+            acc8[k] += (k >= 8 - OTTB_POLY_OF_8_TC) ? exp2_poly(xk) : ex2_approx(xk);
+          }
+        }
+        two_sum_acc(lrun, lcmp, ((acc8[0] + acc8[1]) + (acc8[2] + acc8[3])) +
+                                    ((acc8[4] + acc8[5]) + (acc8[6] + acc8[7])));
       }
-      two_sum_acc(lrun, lcmp, ((acc8[0] + acc8[1]) + (acc8[2] + acc8[3])) +
-                                  ((acc8[4] + acc8[5]) + (acc8[6] + acc8[7])));
     }
     sm.part_m[cg][r] = mrun;
     sm.part_l[cg][r] = lrun + lcmp;
   }
   pp.tile += ntiles;
+  pp.chunk += ntiles * C;
   pp.unit += 1;
   if (!ok) atomicExch(&sm.err, 1);
   __syncthreads();

@@ -29,7 +29,7 @@ sinkhorn_simt_kernel(KernelArgs A) {
       simt_unit<DP>(sm.tiles, op, (int64_t)rb * kBM, t0, t1, s, wscale, sm.rm, sm.rl);
       return true;
     };
-    return sweep_units(A, sp, idx, cs, unit);
+    return sweep_units<kBN>(A, sp, idx, cs, unit);
   };
   persistent_main(A, sweep);
 }

@@ -60,10 +60,10 @@ sinkhorn_tc_kernel(KernelArgs A) {
   // Extension blocks: zero everywhere; A's first 3 K columns are ones.
   {
     uint32_t* a32 = reinterpret_cast<uint32_t*>(sm.Aext);
-    for (int i = threadIdx.x; i < TcCfg<DK>::kExtBytes / 4; i += blockDim.x) a32[i] = 0u;
+    for (int i = threadIdx.x; i < TcCfg<DK>::kAExtBytes / 4; i += blockDim.x) a32[i] = 0u;
     for (int st = 0; st < NS; ++st) {
       uint32_t* b32 = reinterpret_cast<uint32_t*>(sm.Bext[st]);
-      for (int i = threadIdx.x; i < TcCfg<DK>::kExtBytes / 4; i += blockDim.x) b32[i] = 0u;
+      for (int i = threadIdx.x; i < TcCfg<DK>::kBExtBytes / 4; i += blockDim.x) b32[i] = 0u;
     }
     __syncthreads();
     if (threadIdx.x < kBM) {
@@ -77,7 +77,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
   __syncthreads();
   tc::fence_after_sync();
 
-  TcPipe pp{0u, 0u, 0u, 0u, 0};
+  TcPipe pp{0u, 0u, 0u, 0u, 0u, 0};
   const CommonSmem cs{sm.rm, sm.rl, sm.red, &sm.unit, &sm.last};
   auto sweep = [&](const SweepParams& sp, unsigned idx) -> bool {
     auto unit = [&](const ProbDev& P, const float* gcur, int parity, int rb, int t0, int t1,
@@ -85,7 +85,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
       const TcOperands op = make_tc_operands(P, sp.kind, parity);
       return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, A.timeout_ns);
     };
-    return sweep_units(A, sp, idx, cs, unit);
+    return sweep_units<TcCfg<DK>::kTileN>(A, sp, idx, cs, unit);
   };
   persistent_main(A, sweep);
 

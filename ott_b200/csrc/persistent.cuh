@@ -130,13 +130,14 @@ struct CommonSmem {
 };
 
 // One sweep over the units of the scheduled problems, common to both
-// engines. unit_fn(P, gcur, parity, rb, t0, t1, s, wscale) computes the (shift, sum)
+// engines (tiles of TILE_N columns: 128 on the CUDA cores, 256 on the tensor
+// cores). unit_fn(P, gcur, parity, rb, t0, t1, s, wscale) computes the (shift, sum)
 // state of the 128 rows of row block rb over column tiles [t0, t1) into
 // cs.rm / cs.rl and returns false on a device-side timeout. Units are dealt
 // round-robin (one problem) or from an atomic queue (several problems, in
 // decreasing-work order). A row block split over S column ranges is
 // combined by the CTA that finishes its last range.
-template <class UnitFn>
+template <int TILE_N, class UnitFn>
 __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned sweep_idx,
                             const CommonSmem& cs, UnitFn&& unit_fn) {
   const int* ids = sp.final_eval ? A.eval_ids : A.active_ids;
@@ -168,7 +169,7 @@ __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned
     const float* gcur = P.gbuf[parity];
     const int64_t R = sp.kind == kSweepG ? P.m : P.n;
     const int64_t Ccols = sp.kind == kSweepG ? P.n : P.m;
-    const int ntiles = (int)((Ccols + kBN - 1) / kBN);
+    const int ntiles = (int)((Ccols + TILE_N - 1) / TILE_N);
     const int t0 = (int)(((int64_t)ntiles * sidx) / S);
     const int t1 = (int)(((int64_t)ntiles * (sidx + 1)) / S);
     const float wscale = sweep_wscale(P, sp.mult);
