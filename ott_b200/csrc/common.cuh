@@ -116,6 +116,15 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
   return t;
 }
 
+// Coefficients of the degree-5 polynomial p(f) ~ 2^f on [-1/2, 1/2].
+constexpr float kExp2C5 = 1.327647245e-03f;
+constexpr float kExp2C4 = 9.675540961e-03f;
+constexpr float kExp2C3 = 5.550713092e-02f;
+constexpr float kExp2C2 = 2.402212024e-01f;
+constexpr float kExp2C1 = 6.931469440e-01f;
+constexpr float kExp2C0 = 1.000000119e+00f;
+constexpr float kRoundShift = 12582912.0f;  // 1.5 * 2^23
+
 // 2^x on the FMA pipe, to take part of the exponentials off the MUFU pipe.
 // Range reduction x = n + f, n = rint(x), f in [-1/2, 1/2] (exact for
 // |x| < 2^22: adding 1.5 * 2^23 rounds x to an integer in the low mantissa
@@ -126,28 +135,76 @@ __device__ __forceinline__ uint64_t global_timer_ns() {
 // next to the running sum's leading term >= 1); callers keep x <= kTau + 1.
 __device__ __forceinline__ float exp2_poly(float x) {
   x = fmaxf(x, -126.0f);
-  const float t = x + 12582912.0f;  // 1.5 * 2^23
-  const float f = x - (t - 12582912.0f);
-  float p = 1.327647245e-03f;
-  p = fmaf(p, f, 9.675540961e-03f);
-  p = fmaf(p, f, 5.550713092e-02f);
-  p = fmaf(p, f, 2.402212024e-01f);
-  p = fmaf(p, f, 6.931469440e-01f);
-  p = fmaf(p, f, 1.000000119e+00f);
+  const float t = x + kRoundShift;
+  const float f = x - (t - kRoundShift);
+  float p = kExp2C5;
+  p = fmaf(p, f, kExp2C4);
+  p = fmaf(p, f, kExp2C3);
+  p = fmaf(p, f, kExp2C2);
+  p = fmaf(p, f, kExp2C1);
+  p = fmaf(p, f, kExp2C0);
   // t's bits are 0x4B400000 + n; shifted left by 23 they are n << 23.
   return __int_as_float(__float_as_int(p) + (__float_as_int(t) << 23));
 }
 
+// Packed pairs of FP32 values (sm_100 fma/add .f32x2: two lanes of FP32
+// arithmetic per instruction, same IEEE rounding as the scalar forms).
+typedef unsigned long long f32x2;
+__device__ __forceinline__ f32x2 pack2(float a, float b) {
+  f32x2 r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void unpack2(f32x2 r, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(r));
+}
+__device__ __forceinline__ f32x2 fma2(f32x2 a, f32x2 b, f32x2 c) {
+  f32x2 r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+__device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
+// exp2_poly on a pair, the range reduction and the polynomial in packed
+// arithmetic (same operations, same results as two exp2_poly calls).
+__device__ __forceinline__ f32x2 exp2_poly2(f32x2 xp) {
+  float x0, x1;
+  unpack2(xp, x0, x1);
+  const f32x2 x = pack2(fmaxf(x0, -126.0f), fmaxf(x1, -126.0f));
+  const f32x2 t = add2(x, pack2(kRoundShift, kRoundShift));
+  const f32x2 u = add2(t, pack2(-kRoundShift, -kRoundShift));
+  float u0, u1;
+  unpack2(u, u0, u1);
+  const f32x2 f = add2(x, pack2(-u0, -u1));
+  f32x2 p = pack2(kExp2C5, kExp2C5);
+  p = fma2(p, f, pack2(kExp2C4, kExp2C4));
+  p = fma2(p, f, pack2(kExp2C3, kExp2C3));
+  p = fma2(p, f, pack2(kExp2C2, kExp2C2));
+  p = fma2(p, f, pack2(kExp2C1, kExp2C1));
+  p = fma2(p, f, pack2(kExp2C0, kExp2C0));
+  float p0, p1, t0, t1;
+  unpack2(p, p0, p1);
+  unpack2(t, t0, t1);
+  return pack2(__int_as_float(__float_as_int(p0) + (__float_as_int(t0) << 23)),
+               __int_as_float(__float_as_int(p1) + (__float_as_int(t1) << 23)));
+}
+
 // Of every 8 exponentials, this many go to exp2_poly: in the CUDA-core
 // engine at d <= 4, where the MUFU pipe binds (measured at n = m = 32768,
-// d = 2: 2 of 8 is 2 % faster than 0, 3 of 8 slower); and in the tensor-core
-// epilogue, where issue slots bind instead (n = m = 65536, d = 64: 0 of 8
-// fastest, every step to 4 of 8 slower by 4-10 %).
+// d = 2: 2 of 8 is 2 % faster than 0, 3 of 8 slower); and in the
+// tensor-core epilogue, which runs its arithmetic on packed pairs (measured
+// in isolation, 16 warps per SM: 15.4 entries/clk/SM with scalar FP32 and
+// every exponential on the MUFU, 18.9 packed with 2 of 8 on the
+// polynomial, 15.6 with 4 of 8).
 #ifndef OTTB_POLY_OF_8
 #define OTTB_POLY_OF_8 2
 #endif
 #ifndef OTTB_POLY_OF_8_TC
-#define OTTB_POLY_OF_8_TC 0
+#define OTTB_POLY_OF_8_TC 2
 #endif
 
 // Three-input maximum (sm_100 max.f32 with three sources; NaN operands are

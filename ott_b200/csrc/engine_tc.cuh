@@ -303,21 +303,32 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
           mrun = cm;
         }
         const float negm = -mrun;
-        // 8 accumulators; lanes k >= 8 - OTTB_POLY_OF_8_TC of each group of 8
-        // columns use exp2_poly (FMA pipe), the rest ex2.approx (MUFU).
-        float acc8[8];
+        // Packed pairs (v[j + 2k], v[j + 2k + 1]) in 4 accumulator pairs; of
+        // every 8 columns the last OTTB_POLY_OF_8_TC go to exp2_poly2 (FMA
+        // pipe), the rest to ex2.approx (MUFU).
+        const f32x2 s2 = pack2(s, s), m2 = pack2(negm, negm);
+        f32x2 acc[4];
 #pragma unroll
-        for (int k = 0; k < 8; ++k) acc8[k] = 0.f;
+        for (int k = 0; k < 4; ++k) acc[k] = 0ull;
 #pragma unroll
         for (int j = 0; j < 32; j += 8) {
 #pragma unroll
-          for (int k = 0; k < 8; ++k) {
-            const float xk = fmaf(v[j + k], s, negm);
-            acc8[k] += (k >= 8 - OTTB_POLY_OF_8_TC) ? exp2_poly(xk) : ex2_approx(xk);
+          for (int k = 0; k < 4; ++k) {
+            const f32x2 x = fma2(pack2(v[j + 2 * k], v[j + 2 * k + 1]), s2, m2);
+            f32x2 e;
+            if (2 * k >= 8 - OTTB_POLY_OF_8_TC) {
+              e = exp2_poly2(x);
+            } else {
+              float x0, x1;
+              unpack2(x, x0, x1);
+              e = pack2(ex2_approx(x0), ex2_approx(x1));
+            }
+            acc[k] = add2(acc[k], e);
           }
         }
-        two_sum_acc(lrun, lcmp, ((acc8[0] + acc8[1]) + (acc8[2] + acc8[3])) +
-                                    ((acc8[4] + acc8[5]) + (acc8[6] + acc8[7])));
+        float ta, tb;
+        unpack2(add2(add2(acc[0], acc[1]), add2(acc[2], acc[3])), ta, tb);
+        two_sum_acc(lrun, lcmp, ta + tb);
       }
     }
     sm.part_m[cg][r] = mrun;
