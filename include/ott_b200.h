@@ -113,6 +113,47 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems,
                                  ottb_result* results, void* workspace,
                                  size_t workspace_bytes, void* stream);
 
+/* ottb_sinkhorn_pointcloud in two halves, for callers that repeat a solve
+ * on the same buffers (the role jax.jit plays for ott/solvers/linear/
+ * _solve.py:29-64: compile once per shape, then re-run the executable).
+ *
+ * ottb_sinkhorn_prepare: the host half. Plans the call and writes its
+ * header (problem table, tensor maps, work schedule, initial state) into
+ * the workspace with one host-to-device copy on stream.
+ *
+ * ottb_sinkhorn_launch: the device half, called with the same arguments as
+ * the prepare that filled this workspace. Issues stream operations only (a
+ * device-to-device copy that restores the header, memsets and kernel
+ * launches; no host memory and no synchronisation), so it can be captured
+ * into a CUDA graph and replayed. Every launch or replay solves again from
+ * the current contents of the problems' x, y, a, b, f_init and g_init;
+ * sizes, epsilon and buffer addresses are those given to prepare.
+ * ottb_sinkhorn_pointcloud is prepare followed by launch. */
+int32_t ottb_sinkhorn_prepare(const ottb_problem* problems, int32_t num_problems,
+                              int32_t d, const ottb_solver_cfg* cfg, void* workspace,
+                              size_t workspace_bytes, void* stream);
+int32_t ottb_sinkhorn_launch(const ottb_problem* problems, int32_t num_problems,
+                             int32_t d, const ottb_solver_cfg* cfg,
+                             ottb_result* results, void* workspace,
+                             size_t workspace_bytes, void* stream);
+
+/* No counterpart in the reference (XLA picks its own kernel schedules).
+ * Times candidate work schedules of a solve with these shapes and this
+ * configuration and records the fastest in a process-wide cache (guarded by
+ * a mutex) that every later plan with the same shapes on this device uses:
+ * for one problem, the column split of each sweep (the heuristic choice
+ * x1/2, x1, x2) and round-robin or queued dealing of work units; for
+ * several problems, how far the column splits of the problems still
+ * iterating may grow as others converge. Each candidate runs the whole
+ * solve twice (one untimed, one timed with CUDA events), writing the
+ * problems' outputs and results; the call blocks until the trials finish
+ * and refuses a stream under capture (OTTB_ERR_INVALID). Returns at once if
+ * the shape is already tuned, unless force != 0. */
+int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problems,
+                               int32_t d, const ottb_solver_cfg* cfg,
+                               ottb_result* results, void* workspace,
+                               size_t workspace_bytes, void* stream, int32_t force);
+
 /* Fixed device scratch of ottb_sinkhorn_pointcloud_noalloc, per device. */
 #define OTTB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

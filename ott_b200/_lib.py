@@ -29,6 +29,9 @@ PRECISION_BF16_SPLIT3 = 1
 EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_workspace_size",
     "ottb_sinkhorn_pointcloud",
+    "ottb_sinkhorn_prepare",
+    "ottb_sinkhorn_launch",
+    "ottb_sinkhorn_autotune",
     "ottb_cost_stats_workspace_size",
     "ottb_cost_stats",
     "ottb_sinkhorn_pointcloud_noalloc",
@@ -149,6 +152,17 @@ def load() -> ctypes.CDLL:
         ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg),
         vp, vp, sz, vp]
     lib.ottb_sinkhorn_pointcloud.restype = i32
+    lib.ottb_sinkhorn_prepare.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg), vp, sz, vp]
+    lib.ottb_sinkhorn_prepare.restype = i32
+    lib.ottb_sinkhorn_launch.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg),
+        vp, vp, sz, vp]
+    lib.ottb_sinkhorn_launch.restype = i32
+    lib.ottb_sinkhorn_autotune.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg),
+        vp, vp, sz, vp, i32]
+    lib.ottb_sinkhorn_autotune.restype = i32
     lib.ottb_cost_stats_workspace_size.argtypes = [i64, i64, i32]
     lib.ottb_cost_stats_workspace_size.restype = sz
     lib.ottb_cost_stats.argtypes = [vp, vp, i64, i64, i32, ctypes.c_float, i32, vp, vp, sz, vp]

@@ -11,7 +11,9 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <mutex>
+#include <tuple>
 #include <vector>
 
 #include <cuda.h>
@@ -152,10 +154,17 @@ bool encode_ext_map(CUtensorMap* map, void* base, int64_t rows) {
          CUDA_SUCCESS;
 }
 
-// Grid size of the persistent launch: all CTAs co-resident.
+// Grid size of the persistent launch: all CTAs co-resident. Computed once
+// per kernel and device (the attribute and occupancy queries then stay out
+// of later calls, which may be under stream capture).
 int persistent_grid(const KernelChoice& k, int sms) {
   static std::mutex mu;
+  static std::map<std::pair<int, void*>, int> cache;
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
   std::lock_guard<std::mutex> lock(mu);
+  auto it = cache.find({dev, k.fn});
+  if (it != cache.end()) return it->second;
   if (cudaFuncSetAttribute(k.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)k.smem) != cudaSuccess)
     return 0;
@@ -163,8 +172,23 @@ int persistent_grid(const KernelChoice& k, int sms) {
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k.fn, k.threads, k.smem) !=
       cudaSuccess)
     return 0;
+  cache[{dev, k.fn}] = per_sm * sms;
   return per_sm * sms;
 }
+
+// Work schedule knobs of a call: the autotuner's search space.
+//   split_scale  the initial column split of a single problem is the
+//                heuristic choice (choose_split) times split_scale / 4
+//   waves        the kernel grows the splits of the still-active problems
+//                whenever they offer fewer than waves * grid units per sweep
+//                (0: never)
+//   dynamic      work units dealt from an atomic queue (1) or round-robin
+//                (0); calls with several problems always use the queue
+struct Schedule {
+  int split_scale = 4;
+  int waves = 2;
+  int dynamic = 0;
+};
 
 // Column splits of one sweep: enough units to keep every CTA busy with
 // little tail (efficiency = units / (waves * grid)).
@@ -186,9 +210,15 @@ int choose_split(int rb, int ntiles, int grid, int num_problems) {
   return best;
 }
 
+// Largest column split the workspace is sized for: 32 for a single
+// problem, 8 per problem in calls with several (splits there only grow once
+// problems have converged).
+constexpr int kMaxSplitSingle = 32;
+constexpr int kMaxSplitBatch = 8;
+
 struct ProbPlan {
   int64_t n, m, n_pad, m_pad;
-  int rb_f, rb_g, split_f, split_g;
+  int rb_f, rb_g, split_f, split_g, smax_f, smax_g;
   size_t off_xt, off_yt, off_nx, off_ny, off_galt, off_pm, off_pl, off_arr, off_err,
       off_msum, off_extx, off_exty;
 };
@@ -206,13 +236,61 @@ struct Plan {
   bool tc = false;
   int grid = 0;
   KernelChoice kern;
+  Schedule sched;
   size_t off_globals = 0, off_sched = 0, off_probs = 0, off_state = 0, off_ids = 0,
          off_prefix = 0, off_eval_ids = 0, off_eval_prefix = 0, off_ptrs = 0, off_maps = 0;
   size_t header_bytes = 0;
+  size_t off_pristine = 0;  // unmodified copy of the header, restored by every launch
   size_t total = 0;
   std::vector<ProbPlan> probs;
   std::vector<int> order;  // table position -> caller index
 };
+
+// ---------------------------------------------------------------- autotune cache
+// Key of a call's shape: device, engine, padded dimension, grid, number of
+// problems and a hash of the (n, m) list.
+struct TuneKey {
+  int dev, tc, dp, grid, num;
+  uint64_t hash;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, tc, dp, grid, num, hash) < std::tie(o.dev, o.tc, o.dp, o.grid, o.num, o.hash);
+  }
+};
+
+std::mutex g_tune_mu;
+std::map<TuneKey, Schedule>& tune_cache() {
+  static std::map<TuneKey, Schedule> cache;
+  return cache;
+}
+
+TuneKey tune_key(const ottb_problem* probs, int num, const Plan& plan) {
+  TuneKey k;
+  k.dev = -1;
+  cudaGetDevice(&k.dev);
+  k.tc = plan.tc ? 1 : 0;
+  k.dp = plan.dp;
+  k.grid = plan.grid;
+  k.num = num;
+  uint64_t h = 1469598103934665603ull;  // FNV-1a over the sizes
+  for (int i = 0; i < num; ++i) {
+    const uint64_t v[2] = {(uint64_t)probs[i].n, (uint64_t)probs[i].m};
+    for (uint64_t x : v)
+      for (int b = 0; b < 8; ++b) {
+        h ^= (x >> (8 * b)) & 0xffu;
+        h *= 1099511628211ull;
+      }
+  }
+  k.hash = h;
+  return k;
+}
+
+bool tuned_schedule(const TuneKey& key, Schedule* out) {
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  auto it = tune_cache().find(key);
+  if (it == tune_cache().end()) return false;
+  *out = it->second;
+  return true;
+}
 
 int validate_cfg(const ottb_solver_cfg* cfg) {
   if (!cfg) return OTTB_ERR_INVALID;
@@ -223,8 +301,11 @@ int validate_cfg(const ottb_solver_cfg* cfg) {
   return OTTB_OK;
 }
 
+// The work plan of a call. sched_override (or else the autotune cache, or
+// else the defaults) sets the schedule knobs; the workspace layout does not
+// depend on them.
 int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* cfg,
-              bool need_grid, Plan& plan) {
+              bool need_grid, Plan& plan, const Schedule* sched_override = nullptr) {
   if (!probs || num < 1 || d < 1) return OTTB_ERR_INVALID;
   int st = validate_cfg(cfg);
   if (st != OTTB_OK) return st;
@@ -259,6 +340,13 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
   std::stable_sort(plan.order.begin(), plan.order.end(), [&](int a, int b) {
     return (double)probs[a].n * probs[a].m > (double)probs[b].n * probs[b].m;
   });
+  if (sched_override) {
+    plan.sched = *sched_override;
+  } else if (need_grid) {
+    Schedule t;
+    if (tuned_schedule(tune_key(probs, num, plan), &t)) plan.sched = t;
+  }
+  if (num > 1) plan.sched.dynamic = 1;
   size_t off = 0;
   plan.off_globals = off; off = align_up(off + sizeof(Globals));
   plan.off_sched = off; off = align_up(off + sizeof(Sched));
@@ -284,8 +372,14 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.m_pad = round_up(q.m, tile_n);
     pp.rb_f = (int)((q.n + kBM - 1) / kBM);
     pp.rb_g = (int)((q.m + kBM - 1) / kBM);
-    pp.split_f = choose_split(pp.rb_f, (int)(pp.m_pad / tile_n), plan.grid, num);
-    pp.split_g = choose_split(pp.rb_g, (int)(pp.n_pad / tile_n), plan.grid, num);
+    const int cap = num > 1 ? kMaxSplitBatch : kMaxSplitSingle;
+    pp.smax_f = (int)std::max<int64_t>(1, std::min<int64_t>(cap, pp.m_pad / tile_n));
+    pp.smax_g = (int)std::max<int64_t>(1, std::min<int64_t>(cap, pp.n_pad / tile_n));
+    auto scaled = [&](int s0, int smax) {
+      return std::max(1, std::min(smax, (s0 * plan.sched.split_scale + 2) / 4));
+    };
+    pp.split_f = scaled(choose_split(pp.rb_f, (int)(pp.m_pad / tile_n), plan.grid, num), pp.smax_f);
+    pp.split_g = scaled(choose_split(pp.rb_g, (int)(pp.n_pad / tile_n), plan.grid, num), pp.smax_g);
     const size_t fsz = sizeof(float);
     // FP32 engine: transposed [DP][pad] floats; tensor cores: [2][pad][DK] bf16
     const size_t elt = plan.tc ? 2 * 2 : fsz;
@@ -294,12 +388,10 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.off_nx = off; off = align_up(off + fsz * pp.n_pad);
     pp.off_ny = off; off = align_up(off + fsz * pp.m_pad);
     pp.off_galt = off; off = align_up(off + fsz * pp.m);
-    // Partials are sized for the largest split any grid could choose, so the
-    // workspace size does not depend on the device the call runs on.
-    const int64_t smax_f = num > 1 ? 1 : std::min<int64_t>(32, pp.m_pad / tile_n);
-    const int64_t smax_g = num > 1 ? 1 : std::min<int64_t>(32, pp.n_pad / tile_n);
-    const int64_t parts = std::max(smax_f * pp.n, smax_g * pp.m);
-    const bool split = smax_f > 1 || smax_g > 1;
+    // Partials of split sweeps, sized for the largest split (smax_f for the
+    // f-sweep over n rows, smax_g for the g-sweep over m rows).
+    const int64_t parts = std::max((int64_t)pp.smax_f * pp.n, (int64_t)pp.smax_g * pp.m);
+    const bool split = pp.smax_f > 1 || pp.smax_g > 1;
     pp.off_pm = off; off = align_up(off + (split ? fsz * parts : 0));
     pp.off_pl = off; off = align_up(off + (split ? fsz * parts : 0));
     pp.off_arr = off; off = align_up(off + sizeof(int) * std::max(pp.rb_f, pp.rb_g));
@@ -309,63 +401,32 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.off_extx = off; off = align_up(off + (plan.tc ? 16 * pp.n_pad : 0));
     pp.off_exty = off; off = align_up(off + (plan.tc ? 16 * 2 * pp.m_pad : 0));
   }
+  plan.off_pristine = off; off = align_up(off + plan.header_bytes);
   plan.total = off;
   return OTTB_OK;
 }
 
 inline int cuda_status(cudaError_t e) { return e == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA; }
 
-}  // namespace
-
-extern "C" {
-
-const char* ottb_version(void) { return "0.1.0"; }
-
-const char* ottb_status_string(int32_t status) {
-  switch (status) {
-    case OTTB_OK: return "ok";
-    case OTTB_ERR_INVALID: return "invalid argument";
-    case OTTB_ERR_UNSUPPORTED: return "unsupported configuration";
-    case OTTB_ERR_CUDA: return "CUDA runtime error";
-    case OTTB_ERR_TIMEOUT: return "device wait timed out";
-    case OTTB_ERR_WORKSPACE: return "workspace missing or too small";
-    case OTTB_ERR_NO_DEVICE: return "no sm_100 device";
-    default: return "unknown status";
-  }
-}
-
-size_t ottb_sinkhorn_workspace_size(const ottb_problem* problems, int32_t num_problems,
-                                    int32_t d, const ottb_solver_cfg* cfg) {
-  Plan plan;
-  // The split choice depends on the grid; size for the largest grid this
-  // device can run so the plan at solve time always fits.
-  if (make_plan(problems, num_problems, d, cfg, true, plan) != OTTB_OK) {
-    if (make_plan(problems, num_problems, d, cfg, false, plan) != OTTB_OK) return 0;
-  }
-  return plan.total;
-}
-
-int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_problems,
-                                 int32_t d, const ottb_solver_cfg* cfg,
-                                 ottb_result* results, void* workspace,
-                                 size_t workspace_bytes, void* stream_ptr) {
-  if (!results) return OTTB_ERR_INVALID;
+int check_problems(const ottb_problem* problems, int num_problems) {
   for (int i = 0; i < num_problems && problems; ++i) {
     const ottb_problem& q = problems[i];
     if (!q.x || !q.y || !q.a || !q.b || !q.f || !q.g || !q.errors) return OTTB_ERR_INVALID;
     if (!(q.epsilon > 0.0f) || !std::isfinite(q.epsilon)) return OTTB_ERR_INVALID;
     if (!(q.inv_scale_cost > 0.0f) || !std::isfinite(q.inv_scale_cost)) return OTTB_ERR_INVALID;
   }
-  Plan plan;
-  int st = make_plan(problems, num_problems, d, cfg, true, plan);
-  if (st != OTTB_OK) return st;
-  if (!workspace || workspace_bytes < plan.total) return OTTB_ERR_WORKSPACE;
-  if (((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
-  cudaStream_t stream = (cudaStream_t)stream_ptr;
-  char* ws = (char*)workspace;
-  const int outer = (int)std::ceil((double)cfg->max_iterations / cfg->inner_iterations);
+  return OTTB_OK;
+}
 
-  // Host image of the header: globals, schedule, tables.
+int outer_of(const ottb_solver_cfg* cfg) {
+  return (int)std::ceil((double)cfg->max_iterations / cfg->inner_iterations);
+}
+
+// Writes the call header (tables, tensor maps, schedule, initial state)
+// into the pristine region of the workspace: one host-to-device copy.
+int write_header(const ottb_problem* problems, int num_problems, const ottb_solver_cfg* cfg,
+                 const Plan& plan, char* ws, cudaStream_t stream) {
+  const int outer = outer_of(cfg);
   std::vector<char> host(plan.header_bytes, 0);
   Sched* sched = (Sched*)(host.data() + plan.off_sched);
   ProbDev* pd = (ProbDev*)(host.data() + plan.off_probs);
@@ -415,14 +476,16 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
     P.m_pad = pp.m_pad;
     P.rb_f = pp.rb_f;
     P.rb_g = pp.rb_g;
-    P.split_f = pp.split_f;
-    P.split_g = pp.split_g;
+    P.smax_f = pp.smax_f;
+    P.smax_g = pp.smax_g;
     P.eps_target = q.epsilon;
     P.inv_scale = q.inv_scale_cost;
     P.uid = plan.order[t];
     P.outer = outer;
     pd[t] = P;
     ps[t].active = 1;
+    ps[t].split_f = pp.split_f;
+    ps[t].split_g = pp.split_g;
     ids[t] = t;
     prefix[t] = ug;
     prefix[num_problems + 1 + t] = uf;
@@ -439,9 +502,23 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
   sched->total_units[0] = ug;
   sched->total_units[1] = uf;
   sched->status = OTTB_OK;
+  sched->dynamic_units = plan.sched.dynamic;
+  sched->target_units = plan.sched.waves * plan.grid;
+  // Pageable source: the copy is staged before cudaMemcpyAsync returns.
+  const cudaError_t e = cudaMemcpyAsync(ws + plan.off_pristine, host.data(), plan.header_bytes,
+                                        cudaMemcpyHostToDevice, stream);
+  return e == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
 
+// The device side of a solve: restore the header from its pristine copy,
+// clear the split-arrival counters, then fill errors -> prep points -> init
+// potentials -> persistent loop (cooperative) -> finalize. Stream
+// operations only (a device-to-device copy, memsets, kernel launches).
+int launch_solve(int num_problems, int d, const ottb_solver_cfg* cfg, ottb_result* results,
+                 const Plan& plan, char* ws, cudaStream_t stream) {
   cudaError_t e;
-  e = cudaMemcpyAsync(ws, host.data(), plan.header_bytes, cudaMemcpyHostToDevice, stream);
+  e = cudaMemcpyAsync(ws, ws + plan.off_pristine, plan.header_bytes, cudaMemcpyDeviceToDevice,
+                      stream);
   if (e != cudaSuccess) return OTTB_ERR_CUDA;
   for (int t = 0; t < num_problems; ++t) {
     const ProbPlan& pp = plan.probs[t];
@@ -452,7 +529,7 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
   const float* const* d_ptrs = (const float* const*)(ws + plan.off_ptrs);
   int64_t maxpts = 1;
   for (const ProbPlan& pp : plan.probs) maxpts = std::max(maxpts, pp.n_pad + 2 * pp.m_pad);
-
+  const int outer = outer_of(cfg);
   {
     dim3 grid(std::max(1, (outer + 255) / 256), num_problems);
     fill_errors_kernel<<<grid, 256, 0, stream>>>(d_probs);
@@ -486,19 +563,180 @@ int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_probl
   ka.eval_ids = (int*)(ws + plan.off_eval_ids);
   ka.eval_prefix = (int*)(ws + plan.off_eval_prefix);
   ka.num_problems = num_problems;
-  ka.dynamic_units = num_problems > 1 ? 1 : 0;
   ka.expected_arrivals = (unsigned)plan.grid + (unsigned)std::max(0, cfg->phantom_arrivals);
   const int tmo = cfg->timeout_ms > 0 ? cfg->timeout_ms : 60000;
   ka.timeout_ns = (uint64_t)tmo * 1000000ull;
   ka.cfg = *cfg;
+  // Cooperative launch (all CTAs co-resident for the grid barrier), through
+  // cudaLaunchKernelEx so that it can be captured into a CUDA graph.
+  cudaLaunchConfig_t lc;
+  std::memset(&lc, 0, sizeof(lc));
+  lc.gridDim = dim3(plan.grid);
+  lc.blockDim = dim3(plan.kern.threads);
+  lc.dynamicSmemBytes = plan.kern.smem;
+  lc.stream = stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeCooperative;
+  attr[0].val.cooperative = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
   void* kargs[] = {&ka};
-  e = cudaLaunchCooperativeKernel(plan.kern.fn, dim3(plan.grid), dim3(plan.kern.threads), kargs,
-                                  plan.kern.smem, stream);
+  e = cudaLaunchKernelExC(&lc, plan.kern.fn, kargs);
   if (e != cudaSuccess) return OTTB_ERR_CUDA;
 
   FinalArgs fa{d_probs, ka.state, ka.sched, results, *cfg};
   finalize_kernel<<<num_problems, 512, 0, stream>>>(fa);
   return cuda_status(cudaGetLastError());
+}
+
+int plan_for_call(const ottb_problem* problems, int32_t num_problems, int32_t d,
+                  const ottb_solver_cfg* cfg, void* workspace, size_t workspace_bytes,
+                  Plan& plan, const Schedule* sched_override = nullptr) {
+  int st = check_problems(problems, num_problems);
+  if (st != OTTB_OK) return st;
+  st = make_plan(problems, num_problems, d, cfg, true, plan, sched_override);
+  if (st != OTTB_OK) return st;
+  if (!workspace || workspace_bytes < plan.total) return OTTB_ERR_WORKSPACE;
+  if (((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  return OTTB_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* ottb_version(void) { return "0.2.0"; }
+
+const char* ottb_status_string(int32_t status) {
+  switch (status) {
+    case OTTB_OK: return "ok";
+    case OTTB_ERR_INVALID: return "invalid argument";
+    case OTTB_ERR_UNSUPPORTED: return "unsupported configuration";
+    case OTTB_ERR_CUDA: return "CUDA runtime error";
+    case OTTB_ERR_TIMEOUT: return "device wait timed out";
+    case OTTB_ERR_WORKSPACE: return "workspace missing or too small";
+    case OTTB_ERR_NO_DEVICE: return "no sm_100 device";
+    default: return "unknown status";
+  }
+}
+
+size_t ottb_sinkhorn_workspace_size(const ottb_problem* problems, int32_t num_problems,
+                                    int32_t d, const ottb_solver_cfg* cfg) {
+  Plan plan;
+  // The layout does not depend on the grid or the schedule; without a
+  // device the plan is made for a 148-SM grid.
+  if (make_plan(problems, num_problems, d, cfg, true, plan) != OTTB_OK) {
+    if (make_plan(problems, num_problems, d, cfg, false, plan) != OTTB_OK) return 0;
+  }
+  return plan.total;
+}
+
+int32_t ottb_sinkhorn_prepare(const ottb_problem* problems, int32_t num_problems, int32_t d,
+                              const ottb_solver_cfg* cfg, void* workspace,
+                              size_t workspace_bytes, void* stream_ptr) {
+  Plan plan;
+  int st = plan_for_call(problems, num_problems, d, cfg, workspace, workspace_bytes, plan);
+  if (st != OTTB_OK) return st;
+  return write_header(problems, num_problems, cfg, plan, (char*)workspace,
+                      (cudaStream_t)stream_ptr);
+}
+
+int32_t ottb_sinkhorn_launch(const ottb_problem* problems, int32_t num_problems, int32_t d,
+                             const ottb_solver_cfg* cfg, ottb_result* results,
+                             void* workspace, size_t workspace_bytes, void* stream_ptr) {
+  if (!results) return OTTB_ERR_INVALID;
+  Plan plan;
+  int st = plan_for_call(problems, num_problems, d, cfg, workspace, workspace_bytes, plan);
+  if (st != OTTB_OK) return st;
+  return launch_solve(num_problems, d, cfg, results, plan, (char*)workspace,
+                      (cudaStream_t)stream_ptr);
+}
+
+int32_t ottb_sinkhorn_pointcloud(const ottb_problem* problems, int32_t num_problems,
+                                 int32_t d, const ottb_solver_cfg* cfg,
+                                 ottb_result* results, void* workspace,
+                                 size_t workspace_bytes, void* stream_ptr) {
+  if (!results) return OTTB_ERR_INVALID;
+  Plan plan;
+  int st = plan_for_call(problems, num_problems, d, cfg, workspace, workspace_bytes, plan);
+  if (st != OTTB_OK) return st;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  st = write_header(problems, num_problems, cfg, plan, (char*)workspace, stream);
+  if (st != OTTB_OK) return st;
+  return launch_solve(num_problems, d, cfg, results, plan, (char*)workspace, stream);
+}
+
+int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problems, int32_t d,
+                               const ottb_solver_cfg* cfg, ottb_result* results,
+                               void* workspace, size_t workspace_bytes, void* stream_ptr,
+                               int32_t force) {
+  if (!results) return OTTB_ERR_INVALID;
+  Plan base;
+  int st = plan_for_call(problems, num_problems, d, cfg, workspace, workspace_bytes, base);
+  if (st != OTTB_OK) return st;
+  const TuneKey key = tune_key(problems, num_problems, base);
+  Schedule cached;
+  if (!force && tuned_schedule(key, &cached)) return OTTB_OK;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) return OTTB_ERR_CUDA;
+  if (cap != cudaStreamCaptureStatusNone) return OTTB_ERR_INVALID;  // trials synchronise
+  // Candidate schedules: initial split of a single problem (x1/2, x1, x2;
+  // round-robin or queued units); for several problems, how far the splits
+  // of the problems still iterating may grow (0, 1, 2, 4 waves of units).
+  std::vector<Schedule> cands;
+  if (num_problems == 1) {
+    for (int scale : {4, 2, 8})
+      for (int dyn : {0, 1}) {
+        Schedule c;
+        c.split_scale = scale;
+        c.dynamic = dyn;
+        cands.push_back(c);
+      }
+  } else {
+    for (int w : {2, 0, 1, 4}) {
+      Schedule c;
+      c.waves = w;
+      c.dynamic = 1;
+      cands.push_back(c);
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    return OTTB_ERR_CUDA;
+  }
+  float best_ms = 0.f;
+  Schedule best = cands[0];
+  for (size_t i = 0; i < cands.size() && st == OTTB_OK; ++i) {
+    Plan plan;
+    st = plan_for_call(problems, num_problems, d, cfg, workspace, workspace_bytes, plan,
+                       &cands[i]);
+    if (st != OTTB_OK) break;
+    st = write_header(problems, num_problems, cfg, plan, (char*)workspace, stream);
+    // one untimed run, then one timed run of the whole solve
+    for (int rep = 0; rep < 2 && st == OTTB_OK; ++rep) {
+      if (rep == 1 && cudaEventRecord(e0, stream) != cudaSuccess) st = OTTB_ERR_CUDA;
+      if (st == OTTB_OK)
+        st = launch_solve(num_problems, d, cfg, results, plan, (char*)workspace, stream);
+      if (rep == 1 && st == OTTB_OK && cudaEventRecord(e1, stream) != cudaSuccess)
+        st = OTTB_ERR_CUDA;
+    }
+    if (st != OTTB_OK) break;
+    if (cudaEventSynchronize(e1) != cudaSuccess) { st = OTTB_ERR_CUDA; break; }
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, e0, e1) != cudaSuccess) { st = OTTB_ERR_CUDA; break; }
+    if (i == 0 || ms < best_ms) {
+      best_ms = ms;
+      best = cands[i];
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (st != OTTB_OK) return st;
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_cache()[key] = best;
+  return OTTB_OK;
 }
 
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {

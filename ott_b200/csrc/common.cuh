@@ -61,7 +61,7 @@ struct ProbDev {
   double* msum_part;   // [rb_g]
   int64_t n, m, n_pad, m_pad;
   int rb_f, rb_g;      // row blocks of the f- and g-sweeps
-  int split_f, split_g;
+  int smax_f, smax_g;  // largest column split the workspace partials hold
   float eps_target;
   float inv_scale;
   int uid;             // index of the problem in the caller's array
@@ -84,6 +84,8 @@ struct ProbState {
   int final_parity;  // g buffer holding the final g once stopped
   int msum_valid;    // msum holds the final state's marginal sum
   int stop_it;       // iteration count at stop
+  int split_f;       // column split of this problem's f- and g-sweeps (set
+  int split_g;       // by the host, grown at schedule rebuilds)
   double msum;
 };
 
@@ -95,6 +97,8 @@ struct Sched {
   int eval_units;
   int commits;          // g commits so far (parity of active problems)
   int status;           // OTTB_OK or OTTB_ERR_TIMEOUT
+  int dynamic_units;    // 1: units dealt from an atomic queue, 0: round-robin
+  int target_units;     // units per sweep the schedule rebuild aims for
 };
 
 struct Globals {

@@ -26,7 +26,6 @@ struct KernelArgs {
   int* eval_ids;     // [P]
   int* eval_prefix;  // [P + 1]
   int num_problems;
-  int dynamic_units;
   unsigned expected_arrivals;
   uint64_t timeout_ns;
   ottb_solver_cfg cfg;

@@ -18,21 +18,50 @@ __device__ __forceinline__ int find_problem(const int* prefix, int count, int u)
   return lo;
 }
 
-__device__ __forceinline__ int units_of(const ProbDev& P, int kind) {
-  return kind == kSweepG ? P.rb_g * P.split_g : P.rb_f * P.split_f;
+__device__ __forceinline__ int split_of(const ProbState& S, int kind) {
+  return kind == kSweepG ? __ldcg(&S.split_g) : __ldcg(&S.split_f);
 }
 
-// CTA 0 only: rebuild the active list and unit prefix sums.
+__device__ __forceinline__ int units_of(const ProbDev& P, const ProbState& S, int kind) {
+  return kind == kSweepG ? P.rb_g * split_of(S, kSweepG) : P.rb_f * split_of(S, kSweepF);
+}
+
+// CTA 0 only: rebuild the active list and unit prefix sums. When the
+// active problems (fewer as problems converge) no longer offer
+// sched->target_units units per sweep, their column splits grow, each up to the
+// largest split its workspace partials hold, so the remaining problems
+// still spread over the whole grid. Splits never shrink.
 __device__ void rebuild_schedule(const KernelArgs& A) {
   if (threadIdx.x == 0) {
-    int na = 0, ug = 0, uf = 0;
+    int ug = 0, uf = 0, rg = 0, rf = 0;
+    for (int p = 0; p < A.num_problems; ++p) {
+      if (!A.state[p].active) continue;
+      ug += units_of(A.probs[p], A.state[p], kSweepG);
+      uf += units_of(A.probs[p], A.state[p], kSweepF);
+      rg += A.probs[p].rb_g;
+      rf += A.probs[p].rb_f;
+    }
+    const int tgt = A.sched->target_units;
+    if (rg > 0 && (ug < tgt || uf < tgt)) {
+      const int kg = (tgt + rg - 1) / rg, kf = (tgt + rf - 1) / rf;
+      for (int p = 0; p < A.num_problems; ++p) {
+        ProbState& S = A.state[p];
+        if (!S.active) continue;
+        const ProbDev& P = A.probs[p];
+        S.split_g = max(S.split_g, min(kg, P.smax_g));
+        S.split_f = max(S.split_f, min(kf, P.smax_f));
+      }
+    }
+    int na = 0;
+    ug = 0;
+    uf = 0;
     for (int p = 0; p < A.num_problems; ++p) {
       if (!A.state[p].active) continue;
       A.active_ids[na] = p;
       A.prefix[na] = ug;
       A.prefix[A.num_problems + 1 + na] = uf;
-      ug += units_of(A.probs[p], kSweepG);
-      uf += units_of(A.probs[p], kSweepF);
+      ug += units_of(A.probs[p], A.state[p], kSweepG);
+      uf += units_of(A.probs[p], A.state[p], kSweepF);
       ++na;
     }
     A.prefix[na] = ug;
@@ -45,7 +74,7 @@ __device__ void rebuild_schedule(const KernelArgs& A) {
       if (A.state[p].active || A.state[p].msum_valid) continue;
       A.eval_ids[ne] = p;
       A.eval_prefix[ne] = ue;
-      ue += units_of(A.probs[p], kSweepG);
+      ue += units_of(A.probs[p], A.state[p], kSweepG);
       ++ne;
     }
     A.eval_prefix[ne] = ue;
@@ -150,8 +179,9 @@ __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned
   unsigned* ctr = &A.gl->unit_ctr[sweep_idx % 3];
   if (blockIdx.x == 0 && threadIdx.x == 0) A.gl->unit_ctr[(sweep_idx + 1) % 3] = 0u;
 
+  const bool dynamic = ld_sched(&A.sched->dynamic_units) != 0;
   int u = blockIdx.x;
-  if (A.dynamic_units) {
+  if (dynamic) {
     if (threadIdx.x == 0) *cs.unit = (int)atomicAdd(ctr, 1u);
     __syncthreads();
     u = *cs.unit;
@@ -162,7 +192,7 @@ __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned
     const int p = __ldcg(ids + q);
     const ProbDev& P = A.probs[p];
     const int local = u - __ldcg(pre + q);
-    const int S = sp.kind == kSweepG ? P.split_g : P.split_f;
+    const int S = split_of(A.state[p], sp.kind);
     const int rb = local / S;
     const int sidx = local % S;
     const int parity = sp.final_eval ? __ldcg(&A.state[p].final_parity) : sp.parity;
@@ -215,7 +245,7 @@ __device__ bool sweep_units(const KernelArgs& A, const SweepParams& sp, unsigned
     if (do_final) finalize_rows(P, sp, parity, rb, cs.rm, cs.rl, A.cfg.norm_error, cs.red);
     __syncthreads();
 
-    if (A.dynamic_units) {
+    if (dynamic) {
       if (threadIdx.x == 0) *cs.unit = (int)atomicAdd(ctr, 1u);
       __syncthreads();
       u = *cs.unit;

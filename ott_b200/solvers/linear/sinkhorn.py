@@ -25,7 +25,7 @@ from ott_b200.geometry import epsilon_scheduler as eps_scheduler
 from ott_b200.initializers.linear import initializers as init_lib
 from ott_b200.problems.linear import linear_problem
 
-__all__ = ["Sinkhorn", "SinkhornOutput", "run_batch"]
+__all__ = ["Sinkhorn", "SinkhornGraph", "SinkhornOutput", "run_batch"]
 
 _PRECISIONS = {
     "auto": _lib.PRECISION_AUTO,
@@ -143,6 +143,10 @@ class Sinkhorn:
   CUDA cores; ``"bf16_split3"`` tcgen05 tensor-core products of bf16 hi/lo
   splits (hi*hi + hi*lo + lo*hi, FP32 accumulation); ``"auto"`` (default)
   uses the tensor cores for d >= 32 and FP32 below.
+
+  ``autotune=True``: before the first solve of each shape, time the
+  candidate work schedules (``ottb_sinkhorn_autotune``) and use the fastest
+  for every later solve of that shape in this process.
   """
 
   def __init__(
@@ -163,6 +167,7 @@ class Sinkhorn:
       progress_fn: Optional[Any] = None,
       precision: str = "auto",
       timeout_ms: int = 0,
+      autotune: bool = False,
   ):
     if not lse_mode:
       raise NotImplementedError("kernel mode (lse_mode=False) is not on this path")
@@ -191,6 +196,7 @@ class Sinkhorn:
     self.progress_fn = progress_fn
     self.precision = precision
     self.timeout_ms = timeout_ms
+    self.autotune = autotune
     self._phantom_arrivals = 0
 
   @property
@@ -218,6 +224,128 @@ class Sinkhorn:
     return run_batch([ot_prob], self, [init], **kwargs)[0]
 
 
+class _Call:
+  """Problem records, configuration and device buffers of one C-ABI call
+  over a batch of problems (initial potentials from ``inits`` or the
+  solver's initializer, computed here, outside any graph)."""
+
+  def __init__(self, probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
+               inits: Optional[Sequence[Optional[Tuple[Any, Any]]]],
+               f_from_g: Optional[bool], init_kwargs: dict):
+    self.lib = _lib.load()
+    self.probs = list(probs)
+    self.solver = solver
+    inits = list(inits) if inits is not None else [None] * len(probs)
+    d = probs[0].geom.dim
+    dev = probs[0].geom.x.device
+    scheds = []
+    for p in probs:
+      if not p.is_balanced:
+        raise NotImplementedError("unbalanced problems (tau < 1) are not on this path")
+      if p.geom.dim != d:
+        raise ValueError("all problems of one batch must have the same dimension")
+      scheds.append(p.geom.epsilon_scheduler)
+    s0 = scheds[0]
+    for sch in scheds:
+      if (sch.init, sch.decay) != (s0.init, s0.decay):
+        raise ValueError("all problems of one batch must share the epsilon schedule")
+    outer = solver.outer_iterations
+    arr = (_lib.OttbProblem * len(probs))()
+    keep: List[torch.Tensor] = []
+    outs = []
+    mask_init = False
+    explicit = any(i is not None for i in inits)
+    if f_from_g is None:
+      f_from_g = bool(getattr(solver.initializer, "half_step_from_g", False)) and not explicit
+    batch_init = getattr(solver.initializer, "batch_init", None)
+    if batch_init is not None and not explicit:
+      inits = list(batch_init(probs, **init_kwargs))
+      mask_init = True
+    for k, p in enumerate(probs):
+      n, m = p.geom.shape
+      init = inits[k]
+      if init is None:
+        fi, gi = solver.initializer(p, lse_mode=True, **init_kwargs)
+        if fi is not None or gi is not None:
+          mask_init = True
+      else:
+        fi, gi = init
+      fi = None if fi is None else _arrays.as_f32(fi, dev)
+      gi = None if gi is None else _arrays.as_f32(gi, dev)
+      f = torch.empty(n, dtype=torch.float32, device=dev)
+      g = torch.empty(m, dtype=torch.float32, device=dev)
+      errors = torch.empty(max(outer, 1), dtype=torch.float32, device=dev)
+      keep += [t for t in (fi, gi) if t is not None]
+      q = arr[k]
+      q.x = p.geom.x.data_ptr()
+      q.y = p.geom.y.data_ptr()
+      q.a = p.a.data_ptr()
+      q.b = p.b.data_ptr()
+      q.f_init = None if fi is None else fi.data_ptr()
+      q.g_init = None if gi is None else gi.data_ptr()
+      q.f = f.data_ptr()
+      q.g = g.data_ptr()
+      q.errors = errors.data_ptr()
+      q.n = n
+      q.m = m
+      q.epsilon = float(p.geom.epsilon)
+      q.inv_scale_cost = float(p.geom.inv_scale_cost)
+      outs.append((f, g, errors[:outer]))
+    cfg = solver._cfg(mask_init, s0)
+    cfg.init_f_from_g = 1 if f_from_g else 0
+    self.arr, self.cfg, self.d, self.nprob = arr, cfg, d, len(probs)
+    self.keep, self.bufs = keep, outs
+    self.ws_bytes = self.lib.ottb_sinkhorn_workspace_size(arr, self.nprob, d, ctypes.byref(cfg))
+    if self.ws_bytes == 0:
+      raise NotImplementedError("problem sizes or configuration not supported")
+    self.ws = torch.empty(self.ws_bytes, dtype=torch.uint8, device=dev)
+    self.res = torch.empty(self.nprob * _lib.RESULT_BYTES, dtype=torch.uint8, device=dev)
+
+  def _check(self, st: int, what: str) -> None:
+    if st == _lib.OTTB_ERR_UNSUPPORTED:
+      raise NotImplementedError(_lib.status_string(st))
+    _lib.check(st, what)
+
+  def autotune(self, stream: int, force: bool = False) -> None:
+    st = self.lib.ottb_sinkhorn_autotune(self.arr, self.nprob, self.d, ctypes.byref(self.cfg),
+                                         self.res.data_ptr(), self.ws.data_ptr(),
+                                         self.ws_bytes, stream, 1 if force else 0)
+    self._check(st, "ottb_sinkhorn_autotune")
+
+  def solve(self, stream: int) -> None:
+    st = self.lib.ottb_sinkhorn_pointcloud(self.arr, self.nprob, self.d, ctypes.byref(self.cfg),
+                                           self.res.data_ptr(), self.ws.data_ptr(),
+                                           self.ws_bytes, stream)
+    self._check(st, "ottb_sinkhorn_pointcloud")
+
+  def prepare(self, stream: int) -> None:
+    st = self.lib.ottb_sinkhorn_prepare(self.arr, self.nprob, self.d, ctypes.byref(self.cfg),
+                                        self.ws.data_ptr(), self.ws_bytes, stream)
+    self._check(st, "ottb_sinkhorn_prepare")
+
+  def launch(self, stream: int) -> None:
+    st = self.lib.ottb_sinkhorn_launch(self.arr, self.nprob, self.d, ctypes.byref(self.cfg),
+                                       self.res.data_ptr(), self.ws.data_ptr(),
+                                       self.ws_bytes, stream)
+    self._check(st, "ottb_sinkhorn_launch")
+
+  def outputs(self) -> List[SinkhornOutput]:
+    results = _Results(self.res, self.nprob)
+    out = []
+    for k, p in enumerate(self.probs):
+      f, g, errors = self.bufs[k]
+      out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
+                                ot_prob=p, threshold=self.solver.threshold,
+                                inner_iterations=self.solver.inner_iterations))
+    return out
+
+  def keep_alive(self, stream: torch.cuda.Stream) -> None:
+    """The workspace and initial potentials must outlive the kernels."""
+    self.ws.record_stream(stream)
+    for t in self.keep:
+      t.record_stream(stream)
+
+
 def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
               inits: Optional[Sequence[Optional[Tuple[Any, Any]]]] = None,
               f_from_g: Optional[bool] = None,
@@ -233,91 +361,64 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
   """
   if not probs:
     return []
-  lib = _lib.load()
-  inits = list(inits) if inits is not None else [None] * len(probs)
-  d = probs[0].geom.dim
-  dev = probs[0].geom.x.device
-  scheds = []
-  for p in probs:
-    if not p.is_balanced:
-      raise NotImplementedError("unbalanced problems (tau < 1) are not on this path")
-    if p.geom.dim != d:
-      raise ValueError("all problems of one batch must have the same dimension")
-    scheds.append(p.geom.epsilon_scheduler)
-  s0 = scheds[0]
-  for s in scheds:
-    if (s.init, s.decay) != (s0.init, s0.decay):
-      raise ValueError("all problems of one batch must share the epsilon schedule")
-
-  outer = solver.outer_iterations
-  arr = (_lib.OttbProblem * len(probs))()
-  keep: List[torch.Tensor] = []
-  outs = []
-  mask_init = False
-  explicit = any(i is not None for i in inits)
-  if f_from_g is None:
-    f_from_g = bool(getattr(solver.initializer, "half_step_from_g", False)) and not explicit
-  batch_init = getattr(solver.initializer, "batch_init", None)
-  if batch_init is not None and not explicit:
-    inits = list(batch_init(probs, **init_kwargs))
-    mask_init = True
-  for k, p in enumerate(probs):
-    n, m = p.geom.shape
-    init = inits[k]
-    if init is None:
-      fi, gi = solver.initializer(p, lse_mode=True, **init_kwargs)
-      if fi is not None or gi is not None:
-        mask_init = True
-    else:
-      fi, gi = init
-    fi = None if fi is None else _arrays.as_f32(fi, dev)
-    gi = None if gi is None else _arrays.as_f32(gi, dev)
-    f = torch.empty(n, dtype=torch.float32, device=dev)
-    g = torch.empty(m, dtype=torch.float32, device=dev)
-    errors = torch.empty(max(outer, 1), dtype=torch.float32, device=dev)
-    keep += [t for t in (fi, gi) if t is not None]
-    q = arr[k]
-    q.x = p.geom.x.data_ptr()
-    q.y = p.geom.y.data_ptr()
-    q.a = p.a.data_ptr()
-    q.b = p.b.data_ptr()
-    q.f_init = None if fi is None else fi.data_ptr()
-    q.g_init = None if gi is None else gi.data_ptr()
-    q.f = f.data_ptr()
-    q.g = g.data_ptr()
-    q.errors = errors.data_ptr()
-    q.n = n
-    q.m = m
-    q.epsilon = float(p.geom.epsilon)
-    q.inv_scale_cost = float(p.geom.inv_scale_cost)
-    outs.append((f, g, errors[:outer]))
-  cfg = solver._cfg(mask_init, s0)
-  cfg.init_f_from_g = 1 if f_from_g else 0
-  nprob = len(probs)
-  ws_bytes = lib.ottb_sinkhorn_workspace_size(arr, nprob, d, ctypes.byref(cfg))
-  if ws_bytes == 0:
-    raise NotImplementedError("problem sizes or configuration not supported")
-  ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
-  res = torch.empty(nprob * _lib.RESULT_BYTES, dtype=torch.uint8, device=dev)
-  st = lib.ottb_sinkhorn_pointcloud(arr, nprob, d, ctypes.byref(cfg), res.data_ptr(),
-                                    ws.data_ptr(), ws_bytes, _arrays.stream_handle())
-  if st == _lib.OTTB_ERR_UNSUPPORTED:
-    raise NotImplementedError(_lib.status_string(st))
-  _lib.check(st, "ottb_sinkhorn_pointcloud")
-  results = _Results(res, nprob)
-  out = []
-  for k, p in enumerate(probs):
-    f, g, errors = outs[k]
-    out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
-                              ot_prob=p, threshold=solver.threshold,
-                              inner_iterations=solver.inner_iterations))
-  # The workspace must outlive the kernels: record it on the stream.
-  ws.record_stream(torch.cuda.current_stream())
-  for t in keep:
-    t.record_stream(torch.cuda.current_stream())
+  call = _Call(probs, solver, inits, f_from_g, init_kwargs)
+  stream = _arrays.stream_handle()
+  if solver.autotune:
+    call.autotune(stream)
+  call.solve(stream)
+  out = call.outputs()
+  call.keep_alive(torch.cuda.current_stream())
   if solver.progress_fn is not None:
     _replay_progress(solver, out)
   return out
+
+
+class SinkhornGraph:
+  """A batch of solves captured in a CUDA graph, for repeating them cheaply.
+
+  Construction computes the initial potentials (initializer or ``inits``,
+  outside the graph), writes the call header once
+  (``ottb_sinkhorn_prepare``), runs the solve once, and captures the device
+  half of the call (``ottb_sinkhorn_launch``: header restore, point
+  preparation, initial potentials, the persistent loop, finalisation) into
+  a ``torch.cuda.CUDAGraph``. ``replay()`` runs the whole solve again on
+  the current contents of the problems' tensors (``x``, ``y``, ``a``, ``b``
+  and the initial potentials), e.g. after copying new data into them in
+  place; sizes, epsilon, the configuration and the tensors themselves are
+  fixed at capture. This plays the role of calling a ``jax.jit``-compiled
+  ``solve`` again. The potentials of ``replay()``'s outputs live in the
+  graph's buffers and are overwritten by the next replay.
+  """
+
+  def __init__(self, probs: Sequence[linear_problem.LinearProblem],
+               solver: Optional[Sinkhorn] = None,
+               inits: Optional[Sequence[Optional[Tuple[Any, Any]]]] = None,
+               f_from_g: Optional[bool] = None, **init_kwargs: Any):
+    if not probs:
+      raise ValueError("no problems")
+    solver = Sinkhorn() if solver is None else solver
+    self.solver = solver
+    self._call = _Call(probs, solver, inits, f_from_g, init_kwargs)
+    cur = torch.cuda.current_stream()
+    if solver.autotune:
+      self._call.autotune(cur.cuda_stream)
+    self._call.prepare(cur.cuda_stream)
+    self._call.launch(cur.cuda_stream)  # one solve outside the graph
+    torch.cuda.synchronize()
+    self.graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream()
+    side.wait_stream(cur)
+    with torch.cuda.graph(self.graph, stream=side):
+      self._call.launch(torch.cuda.current_stream().cuda_stream)
+    cur.wait_stream(side)
+
+  def replay(self) -> List[SinkhornOutput]:
+    """Runs the captured solve on the current stream; returns its outputs."""
+    self.graph.replay()
+    out = self._call.outputs()
+    if self.solver.progress_fn is not None:
+      _replay_progress(self.solver, out)
+    return out
 
 
 def _replay_progress(solver: Sinkhorn, outs: List[SinkhornOutput]) -> None:
@@ -441,6 +542,12 @@ def run_stacked(geom, a: torch.Tensor, b: torch.Tensor, solver: Sinkhorn,
     raise NotImplementedError("problem sizes or configuration not supported")
   ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
   res = torch.empty(K * _lib.RESULT_BYTES, dtype=torch.uint8, device=dev)
+  if solver.autotune:
+    st = lib.ottb_sinkhorn_autotune(arr, K, geom.dim, ctypes.byref(cfg), res.data_ptr(),
+                                    ws.data_ptr(), ws_bytes, _arrays.stream_handle(), 0)
+    if st == _lib.OTTB_ERR_UNSUPPORTED:
+      raise NotImplementedError(_lib.status_string(st))
+    _lib.check(st, "ottb_sinkhorn_autotune")
   st = lib.ottb_sinkhorn_pointcloud(arr, K, geom.dim, ctypes.byref(cfg), res.data_ptr(),
                                     ws.data_ptr(), ws_bytes, _arrays.stream_handle())
   if st == _lib.OTTB_ERR_UNSUPPORTED:
