@@ -55,6 +55,8 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
   const int tid = threadIdx.x;
   const int tx = tid & 15;
   const int ty = tid >> 4;
+  // dot-product unrolling (registers are capped at 128 by two CTAs per SM)
+  constexpr int kDotUnroll = DP <= 8 ? 2 : 4;
 
   // A tile.
   for (int idx = tid; idx < DP * kBM; idx += blockDim.x) {
@@ -104,7 +106,7 @@ __device__ void simt_unit(SimtSmem<DP>& sm, const SweepOperands& op,
     for (int i = 0; i < 8; ++i)
 #pragma unroll
       for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
-#pragma unroll 4
+#pragma unroll(kDotUnroll)
     for (int k = 0; k < DP; ++k) {
       float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
       float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
