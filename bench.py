@@ -36,6 +36,9 @@ if ROOT not in sys.path:
   sys.path.insert(0, ROOT)
 
 METRIC = "s to 1e-3 marginal err & Sinkhorn iters/s: chosen form vs plain FP32, 1 B200"
+# Sinkhorn iterations to the 1e-3 threshold on the default workload (d = 64),
+# measured on the FP32 CUDA path, by n.
+REF_ITERS = {65536: 30, 16384: 40, 4096: 50}
 L2_BYTES = 126 * 1024 * 1024
 
 
@@ -134,6 +137,9 @@ class ClockSampler:
 # measured pipe peaks (no driver figure exists for these pipes)
 # ---------------------------------------------------------------------------
 def measure_pipe_peaks(torch):
+  """FFMA and MUFU ex2 throughput of this GPU (best of 3 runs each). Called
+  before any solve, while the GPU is cool: under a sustained load the power
+  cap lowers the clock and a probe run then would understate the peak."""
   lib = ctypes.CDLL(os.path.join(ROOT, "ott_b200", "_lib", "libottb200_peaks.so"))
   lib.ottb_peaks_launch.argtypes = [ctypes.c_int] * 3 + [ctypes.c_void_p] * 2
   out = torch.zeros(4096, device="cuda")
@@ -143,12 +149,15 @@ def measure_pipe_peaks(torch):
   for kind, name, iters in ((0, "ffma_per_s", 20000), (1, "ex2_per_s", 4000)):
     lib.ottb_peaks_launch(kind, blocks, iters, out.data_ptr(), stream)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record()
-    lib.ottb_peaks_launch(kind, blocks, iters, out.data_ptr(), stream)
-    e1.record()
-    torch.cuda.synchronize()
-    res[name] = blocks * 256 * iters * 8 / (e0.elapsed_time(e1) * 1e-3)
+    best = 0.0
+    for _ in range(3):
+      e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+      e0.record()
+      lib.ottb_peaks_launch(kind, blocks, iters, out.data_ptr(), stream)
+      e1.record()
+      torch.cuda.synchronize()
+      best = max(best, blocks * 256 * iters * 8 / (e0.elapsed_time(e1) * 1e-3))
+    res[name] = best
   return res
 
 
@@ -204,9 +213,12 @@ def run_reference(args):
   x, y, a, b = workload(args)
   eps = 0.01 * float(sinkhorn_np.mean_cost_matrix(x.astype(np.float64), y.astype(np.float64)))
   rows = 2048 if args.n >= 8192 else args.n
-  # Iteration count of the reference loop on this workload, from the oracle
-  # port on a reduced-size instance of the same distribution.
-  n_iters = int(os.environ.get("OTTB_REF_ITERS", "50"))
+  # Iterations of the reference loop on this workload (a full-size CPU solve
+  # does not fit the time budget): the count of the FP32 CUDA path on the
+  # same seeded data, which equals the float64 oracle's count on every
+  # instance the oracle can solve (n = 4096: 50, parity tests). n = 65536:
+  # 30; n = 16384: 40.
+  n_iters = int(os.environ.get("OTTB_REF_ITERS", str(REF_ITERS.get(args.n, 30))))
   for _ in range(args.warmup):
     cpu_sample(x, y, a, b, eps, rows)
   samples = []
@@ -266,6 +278,7 @@ def run_ours(args):
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
+  peaks = measure_pipe_peaks(torch)
   x, y, a, b = workload(args)
   xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
   ad, bd = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
@@ -340,7 +353,6 @@ def run_ours(args):
   # roofline of the dominant kernel (the persistent solve kernel)
   entries = 2.0 * args.n * args.n * n_iters      # algorithmic: 2 sweeps/iteration
   t = ms * 1e-3
-  peaks = measure_pipe_peaks(torch)
   mp = load_peaks_json()
   if form == "fp32" and args.d > 8:
     achieved = 2.0 * args.d * entries / t / 1e12
@@ -537,6 +549,7 @@ def run_batched(args):
   from ott_b200.problems.linear import linear_problem
   from ott_b200.solvers.linear import sinkhorn
   torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  peaks = measure_pipe_peaks(torch)
   data = problems.batched_uneven_problems(args.problems, d=32, seed=0)
   probs = []
   for x, y, a, b in data:
@@ -588,7 +601,6 @@ def run_batched(args):
   c_f = np.array([o.reg_ot_cost for o in o_f])
   entries = sum(2.0 * p.geom.shape[0] * p.geom.shape[1] * o.n_iters
                 for p, o in zip(probs, o_b))
-  peaks = measure_pipe_peaks(torch)
   ach = entries / t_b / 1e9
   roof = {"bound": "mufu_ex2", "achieved": ach, "peak": peaks["ex2_per_s"] / 1e9,
           "unit": "Gex2/s", "frac": ach / (peaks["ex2_per_s"] / 1e9),
