@@ -154,6 +154,26 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
                                ottb_result* results, void* workspace,
                                size_t workspace_bytes, void* stream, int32_t force);
 
+/* Transport plan of a point-cloud problem applied to num_vec vectors, from
+ * its dual potentials, without materialising the plan
+ * (geometry/geometry.py:444-486, apply_transport_from_potentials; through
+ * sinkhorn.py:458-469, SinkhornOutput.apply):
+ *   P_ij = exp((f_i + g_j - inv_scale_cost |x_i - y_j|^2) / epsilon),
+ *   axis 1: out[k][i] = sum_j P_ij vec[k][j]   (vec [num_vec][m], out [num_vec][n])
+ *   axis 0: out[k][j] = sum_i P_ij vec[k][i]   (vec [num_vec][n], out [num_vec][m]).
+ * x [n][d], y [m][d], f [n], g [m] (entries may be -inf), vec and out are
+ * device arrays; FP32 with a running row maximum. No workspace. */
+int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
+                             int32_t d, const float* f, const float* g, float epsilon,
+                             float inv_scale_cost, const float* vec, int32_t num_vec,
+                             int32_t axis, float* out, void* stream);
+
+/* The plan itself, out [n][m] row-major (geometry/geometry.py:361-365,
+ * transport_from_potentials; sinkhorn.py:346-349, SinkhornOutput.matrix). */
+int32_t ottb_transport_matrix(const float* x, const float* y, int64_t n, int64_t m,
+                              int32_t d, const float* f, const float* g, float epsilon,
+                              float inv_scale_cost, float* out, void* stream);
+
 /* Fixed device scratch of ottb_sinkhorn_pointcloud_noalloc, per device. */
 #define OTTB_NOALLOC_SCRATCH_BYTES (16u << 20)
 

@@ -411,6 +411,47 @@ def solve(x, y=None, a=None, b=None, *, epsilon=None, relative_epsilon=None,
 
 
 # ---------------------------------------------------------------------------
+# Gradient of reg_ot_cost with the potentials held fixed
+# (sinkhorn.py:329-335 set_cost with use_danskin=True, :779-780 default)
+# ---------------------------------------------------------------------------
+def transport_matrix(f, g, geom: Geom):
+  """geometry.py:361-365: ``exp((f + g - C) / eps)``, dense."""
+  with np.errstate(invalid="ignore", over="ignore"):
+    center = (f[:, None] + g[None, :]) - geom.cost_block()
+    return np.exp(center / geom.epsilon)
+
+
+def reg_ot_cost_grads(f, g, a, b, geom: Geom, scale_cost_mean=False):
+  """d compute_kl_reg_cost(f, g, a, b) / d(x, y, a, b) at fixed f, g.
+
+  ``compute_kl_reg_cost`` (sinkhorn.py:224-277) depends on the points only
+  through ``sum(P)`` with ``P_ij = exp((f_i + g_j - inv C_ij) / eps)``
+  (epsilon carries no gradient: geometry.py:157-163), and on the weights
+  through the explicit ``a (f - eps log a)``, ``b (g - eps log b)`` and
+  ``eps sum(a) sum(b)`` terms. With ``scale_cost="mean"`` the scale
+  ``inv = 1 / mean(C_unscaled)`` (pointcloud.py:348-351) also depends on
+  the points. Zero weights get 0 from their ``where`` term.
+  """
+  x, y = geom.x.astype(np.float64), geom.y.astype(np.float64)
+  n, m = x.shape[0], y.shape[0]
+  inv, eps = geom.inv_scale, geom.epsilon
+  P = transport_matrix(f.astype(np.float64), g.astype(np.float64), geom).astype(np.float64)
+  r, c = P.sum(1), P.sum(0)
+  gx = 2 * inv * (r[:, None] * x - P @ y)
+  gy = 2 * inv * (c[:, None] * y - P.T @ x)
+  if scale_cost_mean:
+    cu = sqeuclidean_all_pairs(x, y)
+    t = np.sum(P * cu)
+    gx = gx - inv * inv * (2.0 / n) * (x - y.mean(0)) * t
+    gy = gy - inv * inv * (2.0 / m) * (y - x.mean(0)) * t
+  a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+  with np.errstate(divide="ignore", invalid="ignore"):
+    ga = np.where(a > 0, f - eps * np.log(a) - eps, 0.0) + eps * b.sum()
+    gb = np.where(b > 0, g - eps * np.log(b) - eps, 0.0) + eps * a.sum()
+  return gx, gy, ga, gb
+
+
+# ---------------------------------------------------------------------------
 # Learned initializer objective (initializers/neural/meta_initializer.py)
 # ---------------------------------------------------------------------------
 def meta_dual_loss(f_pred, a, b, geom: Geom):

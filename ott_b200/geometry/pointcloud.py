@@ -127,6 +127,73 @@ class PointCloud(geometry.Geometry):
     mean, msq = self._scaled_stats(second=True)
     return max(msq - mean * mean, 0.0) ** 0.5
 
+  # -- transport from potentials (geometry.py:361-365, 444-486) ------------
+  def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
+                                      axis: int = 0) -> torch.Tensor:
+    """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
+    forming P (geometry.py:444-486): ``axis=0`` sums over rows
+    (``vec [..., n] -> [..., m]``), ``axis=1`` over columns
+    (``vec [..., m] -> [..., n]``). ``vec`` may be 1-D or a batch."""
+    if axis not in (0, 1):
+      raise ValueError("axis must be 0 or 1")
+    lib = _lib.load()
+    n, m = self.shape
+    dev = self.x.device
+    v = _arrays.as_f32(vec, dev)
+    one = v.ndim == 1
+    v2 = v.reshape(1, -1) if one else v.reshape(-1, v.shape[-1]).contiguous()
+    if v2.shape[1] != (n if axis == 0 else m):
+      raise ValueError(f"vec has length {v2.shape[1]}, expected {n if axis == 0 else m}")
+    fd = _arrays.as_f32(f, dev).detach()
+    gd = _arrays.as_f32(g, dev).detach()
+    out = torch.empty((v2.shape[0], m if axis == 0 else n), dtype=torch.float32, device=dev)
+    st = lib.ottb_apply_transport(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
+                                  fd.data_ptr(), gd.data_ptr(), ctypes.c_float(self.epsilon),
+                                  ctypes.c_float(self.inv_scale_cost), v2.data_ptr(),
+                                  v2.shape[0], axis, out.data_ptr(), _arrays.stream_handle())
+    _lib.check(st, "ottb_apply_transport")
+    return out[0] if one else out.reshape(*v.shape[:-1], out.shape[-1])
+
+  def transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
+    """The plan ``[n, m]`` (geometry.py:361-365)."""
+    lib = _lib.load()
+    n, m = self.shape
+    dev = self.x.device
+    fd = _arrays.as_f32(f, dev).detach()
+    gd = _arrays.as_f32(g, dev).detach()
+    out = torch.empty((n, m), dtype=torch.float32, device=dev)
+    st = lib.ottb_transport_matrix(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
+                                   fd.data_ptr(), gd.data_ptr(), ctypes.c_float(self.epsilon),
+                                   ctypes.c_float(self.inv_scale_cost), out.data_ptr(),
+                                   _arrays.stream_handle())
+    _lib.check(st, "ottb_transport_matrix")
+    return out
+
+  def marginal_from_potentials(self, f: torch.Tensor, g: torch.Tensor,
+                               axis: int = 0) -> torch.Tensor:
+    """geometry.py:326-349: column (``axis=0``) or row (``axis=1``)
+    marginal of the plan."""
+    n, m = self.shape
+    ones = torch.ones(n if axis == 0 else m, dtype=torch.float32, device=self.x.device)
+    return self.apply_transport_from_potentials(f, g, ones, axis=axis)
+
+  # -- divergences (pointcloud.py:226-237, geometry.py:248-254) -------------
+  @classmethod
+  def prepare_divergences(cls, x: Any, y: Any, static_b: bool = False,
+                          **kwargs: Any) -> Tuple["PointCloud", ...]:
+    """The geometries (x, y), (x, x) and, unless ``static_b``, (y, y)."""
+    couples = [(x, y), (x, x)]
+    if not static_b:
+      couples += [(y, y)]
+    return tuple(cls(u, v, **kwargs) for (u, v) in couples)
+
+  def copy_epsilon(self, other: geometry.Geometry) -> "PointCloud":
+    """This geometry with ``other``'s epsilon schedule."""
+    new = PointCloud(self.x, self.y, batch_size=self._batch_size, scale_cost=self._scale_cost,
+                     epsilon=other.epsilon_scheduler,
+                     relative_epsilon=other._relative_epsilon)
+    return new
+
   def __repr__(self) -> str:
     n, m = self.shape
     return f"PointCloud(n={n}, m={m}, d={self.dim}, epsilon={self._epsilon_init})"

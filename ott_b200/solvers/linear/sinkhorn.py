@@ -134,6 +134,80 @@ class SinkhornOutput(NamedTuple):
     """Sum of the transport matrix of the final state (column marginal sum)."""
     return float(self._res().marginal_sum)
 
+  @property
+  def matrix(self) -> torch.Tensor:
+    """The transport plan ``[n, m]`` (sinkhorn.py:442-448)."""
+    return self.geom.transport_from_potentials(self.f, self.g)
+
+  def apply(self, inputs: Any, axis: int = 0) -> torch.Tensor:
+    """The plan applied to ``inputs`` (sinkhorn.py:455-469); ``axis=0``
+    maps ``[..., n]`` to ``[..., m]``, ``axis=1`` the transpose."""
+    return self.geom.apply_transport_from_potentials(self.f, self.g, inputs, axis=axis)
+
+  def marginal(self, axis: int) -> torch.Tensor:
+    """sinkhorn.py:471-472."""
+    return self.geom.marginal_from_potentials(self.f, self.g, axis=axis)
+
+  def reg_ot_cost_grads(self) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor,
+                                       torch.Tensor]:
+    """Gradient of ``reg_ot_cost`` w.r.t. ``(x, y, a, b)`` with the
+    potentials held fixed: the reference's default (``use_danskin=True``,
+    sinkhorn.py:329-335, 779-780, which stops gradients through f and g in
+    ``compute_kl_reg_cost``, :224-277). With ``P`` the plan,
+    ``inv = inv_scale_cost`` and ``r = P 1``, ``c = P^T 1``:
+
+      d/dx_i = 2 inv (r_i x_i - (P y)_i) + d(inv)/dx_i <P, C_unscaled>
+      d/dy_j = 2 inv (c_j y_j - (P^T x)_j) + d(inv)/dy_j <P, C_unscaled>
+      d/da_i = [a_i > 0] (f_i - eps log a_i - eps) + eps sum(b)
+      d/db_j = [b_j > 0] (g_j - eps log b_j - eps) + eps sum(a)
+
+    where ``d(inv)/dx_i = -inv^2 (2/n)(x_i - mean(y))`` for
+    ``scale_cost="mean"`` (pointcloud.py:348-351, differentiable there) and
+    0 for a fixed scale; epsilon is a constant (geometry.py:157-163 stop
+    gradients through a relative epsilon). The plan is applied twice to
+    ``d + 1`` vectors (``ottb_apply_transport``), never formed. At a zero
+    weight the reference's ``jnp.where`` gives NaN gradients; here that
+    term is 0.
+    """
+    geom = self.geom
+    eps = float(geom.epsilon)
+    inv = float(geom.inv_scale_cost)
+    x, y = geom.x.detach(), geom.y.detach()
+    n, m = geom.shape
+    ones_n = torch.ones((1, n), dtype=torch.float32, device=x.device)
+    ones_m = torch.ones((1, m), dtype=torch.float32, device=x.device)
+    ry = self.apply(torch.cat([ones_m, y.t()], 0), axis=1).double()  # [1 + d, n]
+    cx = self.apply(torch.cat([ones_n, x.t()], 0), axis=0).double()  # [1 + d, m]
+    xd, yd = x.double(), y.double()
+    r, py = ry[0], ry[1:].t()
+    c, ptx = cx[0], cx[1:].t()
+    gx = 2.0 * inv * (r[:, None] * xd - py)
+    gy = 2.0 * inv * (c[:, None] * yd - ptx)
+    if geom._scale_cost == "mean":
+      tcost = ((r * (xd * xd).sum(1)).sum() + (c * (yd * yd).sum(1)).sum()
+               - 2.0 * (xd * py).sum())
+      gx = gx - inv * inv * (2.0 / n) * (xd - yd.mean(0)) * tcost
+      gy = gy - inv * inv * (2.0 / m) * (yd - xd.mean(0)) * tcost
+    a, b = self.a.detach().double(), self.b.detach().double()
+    f, g = self.f.detach().double(), self.g.detach().double()
+    zero = torch.zeros((), dtype=torch.float64, device=x.device)
+    la = torch.log(torch.where(a > 0, a, torch.ones_like(a)))
+    lb = torch.log(torch.where(b > 0, b, torch.ones_like(b)))
+    ga = torch.where(a > 0, f - eps * la - eps, zero) + eps * b.sum()
+    gb = torch.where(b > 0, g - eps * lb - eps, zero) + eps * a.sum()
+    return gx, gy, ga, gb
+
+  @property
+  def primal_cost(self) -> float:
+    """``<P, C>`` (sinkhorn.py:346-349 through :395-417), from one
+    application of the plan to ``[1, |y|^2, y]``."""
+    geom = self.geom
+    x, y = geom.x.double(), geom.y.double()
+    vecs = torch.cat([torch.ones_like(y[:, :1]), (y * y).sum(1, keepdim=True), y], 1)
+    r = self.apply(vecs.t().float(), axis=1).double()  # [d + 2, n]
+    tot = (r[0] * (x * x).sum(1) + r[1] - 2.0 * (r[2:].t() * x).sum(1)).sum()
+    return float(geom.inv_scale_cost * tot)
+
 
 class Sinkhorn:
   """Sinkhorn solver (sinkhorn.py:542-780), same constructor arguments.

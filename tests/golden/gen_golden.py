@@ -1,7 +1,8 @@
 """Generates the golden vectors in this directory from the reference itself.
 
 Runs ott-jax's own source for the Sinkhorn path (``ott.solvers.linear.solve``
-on ``ott.geometry.pointcloud.PointCloud``) over the NumPy stand-in for jax
+on ``ott.geometry.pointcloud.PointCloud``, then ``SinkhornOutput.apply`` on
+seeded vectors) over the NumPy stand-in for jax
 (``oracle/jaxshim.py``, loaded by ``oracle/reference_loader.py``), in float64
 (``jax_enable_x64`` semantics) and in float32, on seeded inputs from
 ``tests/problems.py``. Needs the reference source tree (default
@@ -71,6 +72,14 @@ def run(ref, case, dtype):
   if init == "restart":
     res["f_init"] = np.asarray(out0.f)
     res["g_init"] = np.asarray(out0.g)
+  # the plan applied to seeded signed vectors, both axes
+  # (geometry.py:444-486 through SinkhornOutput.apply, sinkhorn.py:455-469)
+  rng = np.random.default_rng(7)
+  vec0 = rng.standard_normal((3, x.shape[0])).astype(dtype)
+  vec1 = rng.standard_normal((3, y.shape[0])).astype(dtype)
+  res["vec0"], res["vec1"] = vec0, vec1
+  res["apply0"] = np.asarray(out.apply(vec0, axis=0))
+  res["apply1"] = np.asarray(out.apply(vec1, axis=1))
   return (x, y, a, b), res
 
 

@@ -1,0 +1,116 @@
+"""The plan from the potentials on the GPU (ottb_apply_transport,
+ottb_transport_matrix) and the gradient of reg_ot_cost built on it.
+
+Tolerances: applications of the plan within 8 FP32 roundings of the
+largest exponent magnitude |f_i + g_j - C_ij| / eps (at least 1e-5) of the
+largest output (FP32 inputs, exponentials and sums against the reference's
+float64 run: with potentials ~100 eps the inputs' own rounding is ~1e-5
+relative); gradients within 1e-4 relative of the float64 oracle's formula
+evaluated at the same potentials.
+"""
+import numpy as np
+import pytest
+
+from oracle import sinkhorn_np as o
+from tests import golden_cases, helpers, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _geom(x, y, eps, **kw):
+  import torch
+  from ott_b200.geometry import pointcloud
+  return pointcloud.PointCloud(torch.as_tensor(x, dtype=torch.float32).cuda(),
+                               torch.as_tensor(y, dtype=torch.float32).cuda(), epsilon=eps, **kw)
+
+
+@pytest.mark.parametrize("name", golden_cases.names())
+def test_apply_matches_reference_golden(name):
+  """The reference's own SinkhornOutput.apply on its own potentials."""
+  import torch
+  data, geom_kw, _, _ = golden_cases.load(name, "f64")
+  geom = _geom(data["x"], data["y"], float(data["epsilon"]),
+               scale_cost=geom_kw.get("scale_cost", 1.0))
+  f = torch.as_tensor(data["f"], dtype=torch.float32).cuda()
+  g = torch.as_tensor(data["g"], dtype=torch.float32).cuda()
+  fin_f, fin_g = data["f"][np.isfinite(data["f"])], data["g"][np.isfinite(data["g"])]
+  cmax = o.sqeuclidean_all_pairs(data["x"], data["y"]).max() * o.inv_scale_cost(
+      data["x"], data["y"], geom_kw.get("scale_cost", 1.0))
+  zmax = (np.abs(fin_f).max() + np.abs(fin_g).max() + cmax) / float(data["epsilon"])
+  rel = max(1e-5, 8 * 2.0 ** -24 * zmax)
+  for axis, key in ((0, "0"), (1, "1")):
+    got = geom.apply_transport_from_potentials(
+        f, g, torch.as_tensor(data["vec" + key], dtype=torch.float32).cuda(), axis=axis)
+    want = data["apply" + key]
+    got = got.cpu().numpy().astype(np.float64)
+    for k in range(want.shape[0]):
+      scale = np.max(np.abs(want[k]))
+      np.testing.assert_allclose(got[k], want[k], rtol=0, atol=rel * scale)
+
+
+@pytest.mark.parametrize("n,m,d", [(200, 300, 3), (1000, 700, 64), (129, 257, 100)])
+def test_matrix_marginals_and_primal_cost(n, m, d):
+  from ott_b200.solvers import linear
+  import torch
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + d)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon))
+  p_ref = o.transport_matrix(f, g, og)
+  p = out.matrix.cpu().numpy().astype(np.float64)
+  np.testing.assert_allclose(p, p_ref, rtol=2e-4, atol=1e-6 * p_ref.max())
+  np.testing.assert_allclose(out.marginal(0).cpu().numpy(), p_ref.sum(0), rtol=1e-4)
+  np.testing.assert_allclose(out.marginal(1).cpu().numpy(), p_ref.sum(1), rtol=1e-4)
+  cost = np.sum(p_ref * o.sqeuclidean_all_pairs(og.x, og.y))
+  np.testing.assert_allclose(out.primal_cost, cost, rtol=1e-4)
+  # batched application: [k, n] -> [k, m]
+  v = torch.randn(5, n, device="cuda")
+  got = out.apply(v, axis=0).cpu().numpy()
+  np.testing.assert_allclose(got, v.cpu().numpy().astype(np.float64) @ p_ref, rtol=0,
+                             atol=2e-5 * np.abs(v.cpu().numpy() @ p_ref).max())
+
+
+@pytest.mark.parametrize("scale_cost,rel", [(1.0, None), ("mean", "mean"), (2.5, "std")])
+def test_reg_ot_cost_gradients_match_oracle(scale_cost, rel):
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(300, 400, 8, seed=2)
+  a[5] = 0.0
+  a /= a.sum()
+  xt = torch.as_tensor(x).cuda().requires_grad_()
+  yt = torch.as_tensor(y).cuda().requires_grad_()
+  at = torch.as_tensor(a).cuda().requires_grad_()
+  bt = torch.as_tensor(b).cuda().requires_grad_()
+  geom = pointcloud.PointCloud(xt, yt, epsilon=0.05, relative_epsilon=rel, scale_cost=scale_cost)
+  cost = linear.reg_ot_cost(geom, at, bt, threshold=1e-6)
+  cost.backward()
+  out = linear.solve(geom, at, bt, threshold=1e-6)
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon),
+              inv_scale=float(geom.inv_scale_cost))
+  gx, gy, ga, gb = o.reg_ot_cost_grads(f, g, a.astype(np.float64), b.astype(np.float64), og,
+                                       scale_cost_mean=scale_cost == "mean")
+  np.testing.assert_allclose(xt.grad.cpu().numpy(), gx, rtol=0, atol=1e-4 * np.abs(gx).max())
+  np.testing.assert_allclose(yt.grad.cpu().numpy(), gy, rtol=0, atol=1e-4 * np.abs(gy).max())
+  np.testing.assert_allclose(at.grad.cpu().numpy(), ga, rtol=0, atol=1e-4 * np.abs(ga).max())
+  np.testing.assert_allclose(bt.grad.cpu().numpy(), gb, rtol=0, atol=1e-4 * np.abs(gb).max())
+  assert abs(float(cost) - out.reg_ot_cost) <= 1e-6 * abs(out.reg_ot_cost)
+
+
+def test_gradient_of_self_transport_sums_both_roles():
+  """PointCloud(x) uses x for rows and columns: autograd adds both."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, _, a, _ = problems.uniform_cloud_problem(150, 150, 4, seed=9)
+  xt = torch.as_tensor(x).cuda().requires_grad_()
+  geom = pointcloud.PointCloud(xt, epsilon=0.1)
+  linear.reg_ot_cost(geom, torch.as_tensor(a).cuda(), torch.as_tensor(a).cuda(),
+                     threshold=1e-6).backward()
+  out = linear.solve(geom, torch.as_tensor(a).cuda(), torch.as_tensor(a).cuda(), threshold=1e-6)
+  gx, gy, _, _ = out.reg_ot_cost_grads()
+  np.testing.assert_allclose(xt.grad.cpu().numpy(), (gx + gy).cpu().numpy(), rtol=1e-5,
+                             atol=1e-7)
