@@ -64,6 +64,14 @@ typedef struct ottb_problem {
   int64_t m;
   float epsilon;        /* target epsilon (already resolved)                */
   float inv_scale_cost; /* cost multiplier, 1 / scale_cost                  */
+  int32_t symmetric;    /* 1: x == y and a == b (same pointers); the update is
+                           sinkhorn.py:836-855 with parallel_dual_updates and
+                           Momentum(start=0, value=0.5) (acceleration.py:
+                           164-172), which keeps f == g: one sweep per
+                           iteration, g <- (fin(g) + T(g)) / 2, the error of
+                           both marginals (sinkhorn.py:168-188), f = g at the
+                           end. 0: the default sequential update.           */
+  int32_t reserved;     /* 0                                                */
 } ottb_problem;
 
 /* Solver configuration shared by every problem of one call

@@ -9,7 +9,8 @@ reference tree:
   geometry/costs.py, geometry/geometry.py, geometry/low_rank.py,
   geometry/pointcloud.py, problems/linear/linear_problem.py,
   initializers/linear/initializers.py, solvers/linear/acceleration.py,
-  solvers/linear/sinkhorn.py, solvers/linear/_solve.py.
+  solvers/linear/sinkhorn.py, solvers/linear/_solve.py, and on request
+  tools/sinkhorn_divergence.py (load_divergence).
 Modules the path imports but never calls for a balanced dense solve
 (regularizers, matrix square roots, implicit differentiation, low-rank and
 semidiscrete solvers, dual potentials, jaxopt) are empty placeholders.
@@ -111,7 +112,18 @@ def load(root: str = DEFAULT_ROOT, x64: bool = True) -> types.SimpleNamespace:
     setattr(sys.modules["ott.solvers.linear"], name,
             sys.modules[f"ott.solvers.linear.{name}"])
   solve_mod = _exec(root, "ott.solvers.linear._solve")
+  sys.modules["ott.solvers.linear"].solve = solve_mod.solve
+  acceleration = sys.modules["ott.solvers.linear.acceleration"]
   return types.SimpleNamespace(utils=utils, costs=costs, geometry=geometry,
                                pointcloud=pointcloud, linear_problem=linear_problem,
                                initializers=initializers, sinkhorn=sinkhorn,
-                               solve=solve_mod.solve)
+                               acceleration=acceleration, solve=solve_mod.solve)
+
+
+def load_divergence(root: str = DEFAULT_ROOT):
+  """tools/sinkhorn_divergence.py from the reference tree, after load():
+  ``segment`` (segmented divergences) is a placeholder, off this path."""
+  _package("ott.tools")
+  _placeholder("ott.geometry.segment")
+  sys.modules["ott.geometry"].segment = sys.modules["ott.geometry.segment"]
+  return _exec(root, "ott.tools.sinkhorn_divergence")

@@ -330,12 +330,15 @@ def default_init(a, b, dtype):
 def sinkhorn(geom: Geom, a=None, b=None, *, threshold=1e-3, norm_error=1,
              inner_iterations=10, min_iterations=0, max_iterations=2000,
              init: Optional[Tuple[np.ndarray, np.ndarray]] = None,
-             progress=None) -> SinkhornResult:
+             progress=None, parallel_dual_updates=False,
+             momentum=1.0) -> SinkhornResult:
   """sinkhorn.py:782-801 (__call__), :1052-1099 (run/iterations).
 
   Loop: math/fixed_point_loop.py:23-93.  One iteration: sinkhorn.py:879-938
-  with the default ``Momentum()`` (weight 1, acceleration.py:161-172) and
-  sequential updates (``parallel_dual_updates=False``, :836-855).
+  (lse_step :803-857) with a constant ``Momentum(start=0, value=momentum)``
+  (acceleration.py:140-142, 164-172; default weight 1) and sequential or
+  parallel updates (``parallel_dual_updates``, :836-855). With parallel
+  updates the error is that of both marginals (solution_error, :127-188).
   """
   dt = geom.dtype
   n, m = geom.shape
@@ -350,19 +353,25 @@ def sinkhorn(geom: Geom, a=None, b=None, *, threshold=1e-3, norm_error=1,
   outer = int(math.ceil(max_iterations / inner_iterations))
   errors = -np.ones((outer,), dt)
 
-  def momentum(old, new):
-    # acceleration.py:168-170 with weight 1
+  w = dt.type(momentum)
+
+  def momentum_step(old, new):
+    # acceleration.py:168-170
     with np.errstate(invalid="ignore"):
       old = np.where(np.isfinite(old), old, 0.0).astype(dt)
-      return ((dt.type(1.0) - dt.type(1.0)) * old + dt.type(1.0) * new).astype(dt)
+      return ((dt.type(1.0) - w) * old + w * new).astype(dt)
 
   def one_iteration(f, g, it, compute_error):
+    old_g = g
     new_g = geom.update_potential(f, g, log_b, it, axis=0)
-    g = momentum(g, new_g)
-    new_f = geom.update_potential(f, g, log_a, it, axis=1)
-    f = momentum(f, new_f)
+    g = momentum_step(g, new_g)
+    new_f = geom.update_potential(f, old_g if parallel_dual_updates else g, log_a, it,
+                                  axis=1)
+    f = momentum_step(f, new_f)
     if it == max_iterations - 1 or (compute_error and it >= min_iterations):
       err = marginal_error(f, g, b, geom, 0, norm_error)
+      if parallel_dual_updates:
+        err = err + marginal_error(f, g, a, geom, 1, norm_error)
     else:
       err = np.inf
     errors[it // inner_iterations] = err
@@ -408,6 +417,29 @@ def solve(x, y=None, a=None, b=None, *, epsilon=None, relative_epsilon=None,
   geom = Geom(x, y, float(eps), inv_scale=float(inv), eps_init=eps_init,
               eps_decay=eps_decay, batch_size=batch_size)
   return sinkhorn(geom, a, b, **kw)
+
+
+def sinkhorn_divergence(x, y, a=None, b=None, *, epsilon=None, relative_epsilon=None,
+                       scale_cost=1.0, symmetric_sinkhorn=True, dtype=np.float64, **kw):
+  """tools/sinkhorn_divergence.py:178-352 on PointClouds: three solves with
+  the (x, y) epsilon shared (share_epsilon, :231-235), the x/x and y/y
+  terms with parallel updates and momentum 1/2 (:318-336) when
+  ``symmetric_sinkhorn``. Returns (divergence, (r_xy, r_xx, r_yy))."""
+  x = np.asarray(x, dtype)
+  y = np.asarray(y, dtype)
+  n, m = x.shape[0], y.shape[0]
+  a = np.full((n,), 1.0 / n, dtype) if a is None else np.asarray(a, dtype)
+  b = np.full((m,), 1.0 / m, dtype) if b is None else np.asarray(b, dtype)
+  inv = inv_scale_cost(x, y, scale_cost)
+  eps = resolve_epsilon(x, y, epsilon, relative_epsilon, inv)
+  sym = dict(parallel_dual_updates=True, momentum=0.5) if symmetric_sinkhorn else {}
+  res = []
+  for (u, v, wu, wv, extra) in ((x, y, a, b, {}), (x, x, a, a, sym), (y, y, b, b, sym)):
+    iv = inv_scale_cost(u, v, scale_cost)
+    res.append(sinkhorn(Geom(u, v, float(eps), inv_scale=float(iv)), wu, wv, **kw, **extra))
+  div = (res[0].reg_ot_cost - 0.5 * (res[1].reg_ot_cost + res[2].reg_ot_cost)
+         + 0.5 * eps * (np.sum(a) - np.sum(b)) ** 2)
+  return div, tuple(res)
 
 
 # ---------------------------------------------------------------------------

@@ -62,6 +62,8 @@ class OttbProblem(ctypes.Structure):
       ("m", ctypes.c_int64),
       ("epsilon", ctypes.c_float),
       ("inv_scale_cost", ctypes.c_float),
+      ("symmetric", ctypes.c_int32),
+      ("reserved", ctypes.c_int32),
   ]
 
 

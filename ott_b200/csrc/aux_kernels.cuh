@@ -149,8 +149,11 @@ __global__ void finalize_kernel(FinalArgs args) {
   double da = 0.0, db = 0.0, sa = 0.0, sb = 0.0;
   for (int64_t i = threadIdx.x; i < P.n; i += blockDim.x) {
     const double a = (double)P.a[i];
+    // a symmetric problem ends with f = g
+    const float fv = P.symmetric ? g[i] : P.f[i];
+    if (P.symmetric) P.f[i] = fv;
     sa += a;
-    if (a > 0.0) da += a * ((double)P.f[i] - eps * log(a));
+    if (a > 0.0) da += a * ((double)fv - eps * log(a));
   }
   for (int64_t j = threadIdx.x; j < P.m; j += blockDim.x) {
     const double b = (double)P.b[j];

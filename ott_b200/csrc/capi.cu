@@ -414,6 +414,8 @@ int check_problems(const ottb_problem* problems, int num_problems) {
     if (!q.x || !q.y || !q.a || !q.b || !q.f || !q.g || !q.errors) return OTTB_ERR_INVALID;
     if (!(q.epsilon > 0.0f) || !std::isfinite(q.epsilon)) return OTTB_ERR_INVALID;
     if (!(q.inv_scale_cost > 0.0f) || !std::isfinite(q.inv_scale_cost)) return OTTB_ERR_INVALID;
+    if (q.symmetric != 0 && (q.symmetric != 1 || q.x != q.y || q.a != q.b || q.n != q.m))
+      return OTTB_ERR_INVALID;
   }
   return OTTB_OK;
 }
@@ -482,6 +484,7 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     P.inv_scale = q.inv_scale_cost;
     P.uid = plan.order[t];
     P.outer = outer;
+    P.symmetric = q.symmetric;
     pd[t] = P;
     ps[t].active = 1;
     ps[t].split_f = pp.split_f;
@@ -490,7 +493,7 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     prefix[t] = ug;
     prefix[num_problems + 1 + t] = uf;
     ug += pp.rb_g * pp.split_g;
-    uf += pp.rb_f * pp.split_f;
+    uf += q.symmetric ? 0 : pp.rb_f * pp.split_f;
     ptrs[2 * t] = q.x;
     ptrs[2 * t + 1] = q.y;
     ptrs[2 * num_problems + 2 * t] = q.f_init;

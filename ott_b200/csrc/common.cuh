@@ -66,6 +66,7 @@ struct ProbDev {
   float inv_scale;
   int uid;             // index of the problem in the caller's array
   int outer;           // length of errors
+  int symmetric;       // x == y, a == b: g-sweeps only, momentum 1/2, f = g
 };
 
 // Operands of one sweep for one problem, resolved from the descriptor.

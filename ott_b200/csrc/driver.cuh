@@ -58,7 +58,7 @@ __device__ __forceinline__ SweepOperands make_operands(const ProbDev& P, int kin
   if (kind == kSweepG) {
     op.At = P.yt; op.a_pad = P.m_pad; op.rows = P.m;
     op.Bt = P.xt; op.b_pad = P.n_pad; op.cols = P.n;
-    op.potB = P.f; op.nb = P.nx;
+    op.potB = P.symmetric ? gcur : P.f; op.nb = P.nx;
   } else {
     op.At = P.xt; op.a_pad = P.n_pad; op.rows = P.n;
     op.Bt = P.yt; op.b_pad = P.m_pad; op.cols = P.m;
@@ -111,7 +111,10 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
     const double mg = (double)marg[r];
     const double logm = log(mg);
     const bool keep = isfinite(old) && isfinite(app);
-    const double newp = eps * logm - (keep ? app : 0.0);
+    double newp = eps * logm - (keep ? app : 0.0);
+    // symmetric problem: Momentum(value=0.5) on the parallel update,
+    // (1 - w) * where(isfinite(old), old, 0) + w * new (acceleration.py:168-170)
+    if (P.symmetric) newp = 0.5 * (isfinite(old) ? old : 0.0) + 0.5 * newp;
     if (sp.write) {
       const float nf = (float)newp;
       outp[r] = nf;

@@ -15,7 +15,10 @@ __device__ __forceinline__ TcOperands make_tc_operands(const ProbDev& P, int kin
   if (kind == kSweepG) {
     op.mapA = &maps->y; op.padA = (int32_t)P.m_pad; op.rows = P.m;
     op.mapB = &maps->x; op.padB = (int32_t)P.n_pad; op.cols = P.n;
-    op.mapBext = &maps->extx; op.extRow0 = 0;
+    // symmetric problem: the columns' potential is the current g, whose
+    // shift rows the g-updates write into y's buffers (y's points are x's)
+    op.mapBext = P.symmetric ? &maps->exty : &maps->extx;
+    op.extRow0 = P.symmetric ? (int32_t)(parity * P.m_pad) : 0;
   } else {
     op.mapA = &maps->x; op.padA = (int32_t)P.n_pad; op.rows = P.n;
     op.mapB = &maps->y; op.padB = (int32_t)P.m_pad; op.cols = P.m;

@@ -22,7 +22,9 @@ __device__ __forceinline__ int split_of(const ProbState& S, int kind) {
   return kind == kSweepG ? __ldcg(&S.split_g) : __ldcg(&S.split_f);
 }
 
+// A symmetric problem has no f-sweep (f = g).
 __device__ __forceinline__ int units_of(const ProbDev& P, const ProbState& S, int kind) {
+  if (kind == kSweepF && P.symmetric) return 0;
   return kind == kSweepG ? P.rb_g * split_of(S, kSweepG) : P.rb_f * split_of(S, kSweepF);
 }
 
@@ -118,6 +120,9 @@ __device__ void block_boundary(const KernelArgs& A, int it, bool need_err,
     if (need_err) {
       reduce_marginals(P, lane, err, msum);
       if (c.norm_error != 1) err = pow(err, 1.0 / (double)c.norm_error);
+      // parallel updates: the error of both marginals (sinkhorn.py:168-188),
+      // equal for a symmetric problem
+      if (P.symmetric) err *= 2.0;
     }
     if (lane == 0) {
       const float errf = (float)err;

@@ -39,7 +39,7 @@ class PointCloud(geometry.Geometry):
     if batch_size is not None:
       assert batch_size > 0, f"`batch_size={batch_size}` must be positive."
     self.x = _arrays.as_f32(x)
-    self.y = self.x if y is None else _arrays.as_f32(y, self.x.device)
+    self.y = self.x if (y is None or y is x) else _arrays.as_f32(y, self.x.device)
     if self.x.ndim != 2 or self.y.ndim != 2 or self.x.shape[1] != self.y.shape[1]:
       raise ValueError(f"x and y must be [n, d] and [m, d], got "
                        f"{tuple(self.x.shape)} and {tuple(self.y.shape)}")

@@ -245,12 +245,20 @@ class Sinkhorn:
   ):
     if not lse_mode:
       raise NotImplementedError("kernel mode (lse_mode=False) is not on this path")
-    if momentum is not None and getattr(momentum, "value", 1.0) != 1.0:
-      raise NotImplementedError("momentum other than weight 1 is not on this path")
+    # Momentum: weight 1 (default), or weight 1/2 from iteration 0 together
+    # with parallel updates (the symmetric update of the reference's
+    # Sinkhorn divergence, run for problems with x = y and a = b).
+    w = 1.0 if momentum is None else float(getattr(momentum, "value", 1.0))
+    start = 0 if momentum is None else int(getattr(momentum, "start", 0))
+    self._symmetric_update = bool(parallel_dual_updates) and w == 0.5 and start == 0
+    if w != 1.0 and not self._symmetric_update:
+      raise NotImplementedError("momentum other than weight 1 is on this path only as "
+                                "Momentum(start=0, value=0.5) with parallel updates")
     if anderson is not None:
       raise NotImplementedError("Anderson acceleration is not on this path")
-    if parallel_dual_updates:
-      raise NotImplementedError("parallel dual updates are not on this path")
+    if parallel_dual_updates and not self._symmetric_update:
+      raise NotImplementedError("parallel dual updates are on this path only with "
+                                "Momentum(start=0, value=0.5) on symmetric problems")
     if recenter_potentials:
       raise NotImplementedError("recentred potentials are not on this path")
     if precision not in _PRECISIONS:
@@ -305,7 +313,8 @@ class _Call:
 
   def __init__(self, probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
                inits: Optional[Sequence[Optional[Tuple[Any, Any]]]],
-               f_from_g: Optional[bool], init_kwargs: dict):
+               f_from_g: Optional[bool], init_kwargs: dict,
+               symmetric: Optional[Sequence[bool]] = None):
     self.lib = _lib.load()
     self.probs = list(probs)
     self.solver = solver
@@ -364,6 +373,14 @@ class _Call:
       q.m = m
       q.epsilon = float(p.geom.epsilon)
       q.inv_scale_cost = float(p.geom.inv_scale_cost)
+      sym = solver._symmetric_update if symmetric is None else bool(symmetric[k])
+      if sym:
+        if not _is_symmetric(p):
+          raise NotImplementedError(
+              "parallel updates with momentum 1/2 need a symmetric problem: the same "
+              "points for x and y and the same weights for a and b")
+        q.symmetric = 1
+        q.b = q.a
       outs.append((f, g, errors[:outer]))
     cfg = solver._cfg(mask_init, s0)
     cfg.init_f_from_g = 1 if f_from_g else 0
@@ -420,12 +437,24 @@ class _Call:
       t.record_stream(stream)
 
 
+def _is_symmetric(p: linear_problem.LinearProblem) -> bool:
+  """x and y the same points (one tensor), a and b equal weights."""
+  x, y, a, b = p.geom.x, p.geom.y, p.a, p.b
+  if x.data_ptr() != y.data_ptr() or x.shape != y.shape:
+    return False
+  return a.data_ptr() == b.data_ptr() or (a.shape == b.shape and bool(torch.equal(a, b)))
+
+
 def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
               inits: Optional[Sequence[Optional[Tuple[Any, Any]]]] = None,
               f_from_g: Optional[bool] = None,
+              symmetric: Optional[Sequence[bool]] = None,
               **init_kwargs: Any) -> List[SinkhornOutput]:
   """Solves independent problems of the same dimension in ONE persistent
   launch (the batched form of ``jax.vmap`` over ``Sinkhorn``).
+
+  ``symmetric`` (one flag per problem; default: the solver's setting) runs
+  a problem with x = y, a = b with the parallel, momentum-1/2 update.
 
   ``f_from_g``: start with one f-update from the initial g (its
   c-transform), for initializers that predict g. Defaults to the
@@ -435,7 +464,7 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
   """
   if not probs:
     return []
-  call = _Call(probs, solver, inits, f_from_g, init_kwargs)
+  call = _Call(probs, solver, inits, f_from_g, init_kwargs, symmetric)
   stream = _arrays.stream_handle()
   if solver.autotune:
     call.autotune(stream)

@@ -83,6 +83,32 @@ def run(ref, case, dtype):
   return (x, y, a, b), res
 
 
+# Sinkhorn divergences (tools/sinkhorn_divergence.py:178-352):
+# name -> (inputs, PointCloud kwargs, sinkhorn_divergence kwargs, weights)
+DIV_CASES = {
+    "div_unif_30x40_d3": ("unif:30:40:3", dict(epsilon=0.1), dict(), True),
+    "div_unif_50x45_d5_relmean": ("unif:50:45:5", dict(epsilon=0.05, relative_epsilon="mean"),
+                                  dict(), True),
+    "div_unif_40x40_d2_nonsym": ("unif:40:40:2", dict(epsilon=0.05), dict(
+        symmetric_sinkhorn=False), True),
+    "div_gauss_64x80_d8_uniform": ("gauss:64:80:8", dict(epsilon=0.05, relative_epsilon="mean"),
+                                   dict(), False),
+}
+
+
+def run_divergence(ref, div_mod, case, dtype):
+  spec, gkw, dkw, weights = DIV_CASES[case]
+  x, y, a, b = [np.asarray(v, dtype) for v in make_inputs(spec)]
+  kw = dict(a=a, b=b) if weights else {}
+  div, out = div_mod.sinkhorn_divergence(ref.pointcloud.PointCloud, x, y, **kw, **dkw, **gkw)
+  res = dict(divergence=np.asarray(div), epsilon=np.asarray(out.geoms[0].epsilon),
+             n_iters=np.asarray(out.n_iters))
+  for k, tag in enumerate(("xy", "xx", "yy")):
+    res[f"f_{tag}"] = np.asarray(out.potentials[k][0])
+    res[f"g_{tag}"] = np.asarray(out.potentials[k][1])
+  return (x, y, a, b), res
+
+
 def main():
   from oracle import reference_loader
   root = sys.argv[1] if len(sys.argv) > 1 else reference_loader.DEFAULT_ROOT
@@ -99,8 +125,17 @@ def main():
       manifest[case] = dict(inputs=spec, geometry={k: str(v) for k, v in gkw.items()},
                             solver=skw, init=init)
       print(tag, case, "n_iters", int(res["n_iters"]), "reg_ot_cost", float(res["reg_ot_cost"]))
+    div_mod = reference_loader.load_divergence(root)
+    for case in DIV_CASES:
+      (x, y, a, b), res = run_divergence(ref, div_mod, case, np.float64 if x64 else np.float32)
+      np.savez_compressed(os.path.join(HERE, f"{case}.{tag}.npz"), x=x, y=y, a=a, b=b, **res)
+      print(tag, case, "n_iters", res["n_iters"].tolist(), "divergence", float(res["divergence"]))
   with open(os.path.join(HERE, "manifest.json"), "w") as fh:
     json.dump(manifest, fh, indent=1, sort_keys=True)
+  div_meta = {c: dict(inputs=s, geometry={k: str(v) for k, v in g.items()}, divergence=d,
+                      weights=w) for c, (s, g, d, w) in DIV_CASES.items()}
+  with open(os.path.join(HERE, "divergence_manifest.json"), "w") as fh:
+    json.dump(div_meta, fh, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

@@ -26,3 +26,18 @@ def load(name, tag="f64"):
     else:
       geom[k] = v
   return data, geom, dict(meta["solver"]), meta["init"]
+
+
+def divergence_names():
+  with open(os.path.join(HERE, "divergence_manifest.json")) as fh:
+    return sorted(json.load(fh))
+
+
+def load_divergence(name, tag="f64"):
+  """Inputs and reference outputs of one Sinkhorn-divergence case, with the
+  PointCloud and sinkhorn_divergence keyword arguments."""
+  with open(os.path.join(HERE, "divergence_manifest.json")) as fh:
+    meta = json.load(fh)[name]
+  data = dict(np.load(os.path.join(HERE, f"{name}.{tag}.npz")))
+  geom = {k: (float(v) if k == "epsilon" else v) for k, v in meta["geometry"].items()}
+  return data, geom, dict(meta["divergence"]), bool(meta["weights"])

@@ -38,7 +38,7 @@ def test_status_strings_and_version():
 
 def test_struct_layouts_match_header():
   # sizes follow from the C declarations on LP64
-  assert ctypes.sizeof(_lib.OttbProblem) == 9 * 8 + 2 * 8 + 2 * 4
+  assert ctypes.sizeof(_lib.OttbProblem) == 9 * 8 + 2 * 8 + 2 * 4 + 2 * 4
   assert ctypes.sizeof(_lib.OttbSolverCfg) == 12 * 4
   assert ctypes.sizeof(_lib.OttbResult) == 2 * 8 + 4 * 4
   assert ctypes.sizeof(_lib.OttbMlpLayer) == 2 * 4 + 10 * 8
