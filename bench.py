@@ -54,10 +54,11 @@ def parse_args():
   p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
   p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
   p.add_argument("--workload", default="gaussian64",
-                 choices=["gaussian64", "warmstart", "batched", "anneal"],
+                 choices=["gaussian64", "warmstart", "batched", "anneal", "divergence"],
                  help="gaussian64: the headline single large solve (default); "
                       "warmstart: learned warm start on a 32x32 grid; batched: 512 "
-                      "uneven problems in one launch; anneal: epsilon-annealed solves")
+                      "uneven problems in one launch; anneal: epsilon-annealed solves; "
+                      "divergence: Sinkhorn divergence and its gradient")
   p.add_argument("--train-pairs", type=int, default=100000)
   p.add_argument("--test-pairs", type=int, default=10000)
   p.add_argument("--train-steps", type=int, default=12000)
@@ -700,6 +701,83 @@ def run_anneal(args):
   return 0
 
 
+# ---------------------------------------------------------------------------
+# Sinkhorn divergence and its gradient
+# ---------------------------------------------------------------------------
+def run_divergence(args):
+  """Sinkhorn divergence of the Gaussian-shift clouds (n = m = ``--n``,
+  d = ``--d``, uniform weights, epsilon = 0.05 * mean(C) of (x, y)): the
+  (x, y), (x, x), (y, y) solves in one launch (symmetric terms with the
+  parallel, momentum-1/2 update), then the gradient w.r.t. x and y (two
+  applications of each plan to d + 1 vectors). Chosen precision and FP32."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.tools import sinkhorn_divergence as sd
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  peaks = measure_pipe_peaks(torch)
+  x, y, _, _ = workload(args)
+  xt = torch.from_numpy(x).cuda().requires_grad_()
+  yt = torch.from_numpy(y).cuda().requires_grad_()
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+  flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
+
+  def step(precision):
+    xt.grad = None
+    yt.grad = None
+    e0, e1, e2 = ev(), ev(), ev()
+    flush.zero_()
+    e0.record()
+    div, out = sd.sinkhorn_divergence(pointcloud.PointCloud, xt, yt, epsilon=0.05,
+                                      relative_epsilon="mean",
+                                      solve_kwargs=dict(precision=precision))
+    e1.record()
+    div.backward()
+    e2.record()
+    e2.synchronize()
+    return e0.elapsed_time(e1), e1.elapsed_time(e2), float(div), out
+
+  for _ in range(args.warmup):
+    step("auto")
+  clocks = ClockSampler(0)
+  clocks.start()
+  fw, bw = [], []
+  for _ in range(args.steps):
+    a, b_, div, out = step("auto")
+    fw.append(a)
+    bw.append(b_)
+  clk = clocks.stop()
+  pf, pb, pdiv, pout = step("fp32")
+  n, d = args.n, args.d
+  iters = list(out.n_iters)
+  fwd_s = statistics.median(fw) * 1e-3
+  bwd_s = statistics.median(bw) * 1e-3
+  # backward: 4 applications of an n x n plan to d + 1 vectors (2 for the
+  # (x, y) term, 1 for each symmetric term, whose plan is symmetric); per
+  # plan entry 2 d flops (cost) + 2 (d + 1) flops (P V) on the FP32 pipe
+  bwd_flops = 4.0 * n * n * (2 * d + 2 * (d + 1))
+  roof = {"bound": "fp32_fma", "kernel": "apply_transport_kernel",
+          "achieved": bwd_flops / bwd_s / 1e12, "peak": 2 * peaks["ffma_per_s"] / 1e12,
+          "unit": "TFLOP/s", "frac": bwd_flops / bwd_s / (2 * peaks["ffma_per_s"]),
+          "peak_source": "measured in bench.py (FFMA probe kernel)"}
+  line = {
+      "metric": "s per Sinkhorn divergence (3 solves to 1e-3 in one launch) and its gradient",
+      "value": fwd_s + bwd_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "workload": "divergence", "dtype": "bf16x3/f32", "data": "synthetic",
+      "steps": args.steps, "warmup": args.warmup,
+      "config": {"workload": f"sinkhorn_divergence n=m={n} d={d} x~N(0,I), "
+                             "y~N(0.5,diag(U[0.5,2])), uniform weights, eps=0.05*mean(C_xy)",
+                 "l2": "flushed before each step (256 MiB write)"},
+      "forward_s": fwd_s, "backward_s": bwd_s, "divergence": div, "n_iters": iters,
+      "plain_fp32": {"forward_s": pf * 1e-3, "backward_s": pb * 1e-3, "divergence": pdiv,
+                     "n_iters": list(pout.n_iters)},
+      "divergence_rel_diff_vs_fp32": abs(div - pdiv) / abs(pdiv),
+      "speedup_forward_vs_plain_fp32": pf * 1e-3 / fwd_s,
+      "roofline_backward": roof, "clocks": clk,
+  }
+  print(json.dumps(line))
+  return 0
+
+
 def main():
   args = parse_args()
   if args.warmup < 3:
@@ -712,6 +790,8 @@ def main():
     return run_batched(args)
   if args.workload == "anneal":
     return run_anneal(args)
+  if args.workload == "divergence":
+    return run_divergence(args)
   return run_ours(args)
 
 

@@ -170,11 +170,18 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
  *   axis 1: out[k][i] = sum_j P_ij vec[k][j]   (vec [num_vec][m], out [num_vec][n])
  *   axis 0: out[k][j] = sum_i P_ij vec[k][i]   (vec [num_vec][n], out [num_vec][m]).
  * x [n][d], y [m][d], f [n], g [m] (entries may be -inf), vec and out are
- * device arrays; FP32 with a running row maximum. No workspace. */
+ * device arrays; FP32 with a running row maximum. The summed-over points
+ * are split across CTAs when the output rows alone would leave SMs idle;
+ * the splits' partial sums then go through the workspace (size from
+ * ottb_apply_transport_workspace_size; 0 bytes, or a smaller workspace,
+ * gives fewer splits). */
+size_t ottb_apply_transport_workspace_size(int64_t n, int64_t m, int32_t d, int32_t num_vec,
+                                           int32_t axis);
 int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
                              int32_t d, const float* f, const float* g, float epsilon,
                              float inv_scale_cost, const float* vec, int32_t num_vec,
-                             int32_t axis, float* out, void* stream);
+                             int32_t axis, float* out, void* workspace,
+                             size_t workspace_bytes, void* stream);
 
 /* The plan itself, out [n][m] row-major (geometry/geometry.py:361-365,
  * transport_from_potentials; sinkhorn.py:346-349, SinkhornOutput.matrix). */

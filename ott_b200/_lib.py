@@ -32,6 +32,7 @@ EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_prepare",
     "ottb_sinkhorn_launch",
     "ottb_sinkhorn_autotune",
+    "ottb_apply_transport_workspace_size",
     "ottb_apply_transport",
     "ottb_transport_matrix",
     "ottb_cost_stats_workspace_size",
@@ -168,8 +169,10 @@ def load() -> ctypes.CDLL:
         vp, vp, sz, vp, i32]
     lib.ottb_sinkhorn_autotune.restype = i32
     f32_ = ctypes.c_float
+    lib.ottb_apply_transport_workspace_size.argtypes = [i64, i64, i32, i32, i32]
+    lib.ottb_apply_transport_workspace_size.restype = sz
     lib.ottb_apply_transport.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, i32,
-                                         i32, vp, vp]
+                                         i32, vp, vp, sz, vp]
     lib.ottb_apply_transport.restype = i32
     lib.ottb_transport_matrix.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, vp]
     lib.ottb_transport_matrix.restype = i32

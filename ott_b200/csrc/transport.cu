@@ -14,8 +14,18 @@
 // threads of a row rescales the running sums when it grows, and the tile's
 // weights 2^(z - max) go through shared memory into O += P V on the same
 // threads. Each tile's contribution is summed apart and added to the
-// running sum once. P is never written to global memory.
+// running sum once. P is never written to global memory. A CTA takes
+// 16 * VT vectors (thread tx owns vectors tx + 16 j, j < VT); the host
+// splits the vectors into the fewest such chunks (every chunk recomputes
+// the cost tile). The P tile is stored as float4 row quads at slots
+// XOR-swizzled by the column, so the quads written by a warp and the quads
+// read back fall in distinct banks. When row blocks x vector chunks give
+// fewer than two waves of CTAs, the B points are split too (blockIdx.z):
+// each split writes its sums with its own row shift to the workspace and
+// combine_splits_kernel merges them.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "../../include/ott_b200.h"
 #include "common.cuh"
@@ -25,22 +35,30 @@ namespace {
 
 constexpr int kTR = 128;   // output rows per CTA
 constexpr int kTC = 128;   // B points per tile
-constexpr int kKT = 64;    // vectors per CTA
 constexpr int kSampleMax = 256;
 
-// Rows of the shared tiles are padded by 4 floats (16-byte reads stay
-// aligned, stores spread over 8 banks instead of 1) where it fits: at
-// DP = 128 the unpadded tiles already take 224 KB.
+// Vectors per thread: up to 5 (80 per CTA), 4 at DP = 128 (shared memory).
 template <int DP>
+constexpr int max_vt() { return DP == 128 ? 4 : 5; }
+
+// Rows of the A and B tiles are padded by 4 floats (16-byte reads stay
+// aligned, stores spread over 8 banks instead of 1) where it fits.
+template <int DP, int VT>
 struct ApplySmem {
   static constexpr int kPad = DP <= 64 ? 4 : 0;
+  static constexpr int kKT = 16 * VT;
   float As[DP][kTR + kPad];   // A tile, transposed, centred
   float Bs[DP][kTC + kPad];   // B tile, transposed, centred
-  float Ps[kTC][kTR + kPad];  // weights of the tile, [column][row]
-  float Vs[kTC][kKT + kPad];  // vectors of the tile, [column][k]
+  float Ps[kTC][kTR];         // weights of the tile, [column][swizzled row quads]
+  float Vs[kTC][kKT + 1];     // vectors of the tile, [column][k]
   float wb[kTC];              // (potB - inv |B|^2) * log2e / eps
   float center[DP];
 };
+
+// Float offset of row quad q (rows 4q .. 4q + 3, q < 32) of column c in Ps.
+__device__ __forceinline__ int pquad(int c, int q) {
+  return c * kTR + (q & 16) * 4 + (((q & 15) ^ ((c >> 2) & 7)) * 4);
+}
 
 struct ApplyArgs {
   const float* A;     // [R][d] output-side points
@@ -53,6 +71,9 @@ struct ApplyArgs {
   int d, K;
   float ws;           // log2(e) / eps
   float inv;          // inverse cost scale
+  int splits;         // column splits (1: write out directly)
+  float* part_o;      // [splits][K][R] sums of each split (splits > 1)
+  float* part_m;      // [splits][R] their row shifts (log2 units)
 };
 
 // Common centre of both point sets: the mean of up to kSampleMax points of
@@ -74,10 +95,11 @@ __device__ void apply_center(const ApplyArgs& p, float* center) {
   }
 }
 
-template <int DP>
+template <int DP, int VT>
 __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  ApplySmem<DP>& sm = *reinterpret_cast<ApplySmem<DP>*>(smem_raw);
+  ApplySmem<DP, VT>& sm = *reinterpret_cast<ApplySmem<DP, VT>*>(smem_raw);
+  constexpr int kKT = ApplySmem<DP, VT>::kKT;
   const int tid = threadIdx.x;
   const int tx = tid & 15;
   const int ty = tid >> 4;
@@ -106,16 +128,18 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
   }
 
   float mrow[8];
-  float o[8][4];
+  float o[8][VT];
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     mrow[i] = kNegSentinel;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) o[i][j] = 0.f;
+    for (int j = 0; j < VT; ++j) o[i][j] = 0.f;
   }
 
-  const int64_t ntiles = (p.C + kTC - 1) / kTC;
-  for (int64_t t = 0; t < ntiles; ++t) {
+  const int64_t ntiles_all = (p.C + kTC - 1) / kTC;
+  const int64_t t_begin = ntiles_all * blockIdx.z / p.splits;
+  const int64_t t_end = ntiles_all * (blockIdx.z + 1) / p.splits;
+  for (int64_t t = t_begin; t < t_end; ++t) {
     const int64_t c0 = t * kTC;
     __syncthreads();  // previous tile's Ps / Vs / Bs consumed
     for (int idx = tid; idx < DP * kTC; idx += blockDim.x) {
@@ -176,55 +200,92 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
       if (mx > mrow[i]) {
         const float sc = ex2_approx(mrow[i] - mx);
 #pragma unroll
-        for (int j = 0; j < 4; ++j) o[i][j] *= sc;
+        for (int j = 0; j < VT; ++j) o[i][j] *= sc;
         mrow[i] = mx;
       }
-      const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
-        sm.Ps[c][r] = ex2_approx(z[i][j] - mrow[i]);
-      }
+      for (int j = 0; j < 8; ++j) z[i][j] = ex2_approx(z[i][j] - mrow[i]);
+    }
+    // P quads: rows ty*4 .. +3 (quad ty) and 64 + ty*4 .. +3 (quad 16 + ty)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
+      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, ty)) =
+          make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
+      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty)) =
+          make_float4(z[4][j], z[5][j], z[6][j], z[7][j]);
     }
     __syncthreads();
     // O[r][k] += sum_c P[r][c] V[c][k]: rows of this thread's micro-tile,
-    // vectors tx * 4 .. tx * 4 + 3
-    float acc[8][4];
+    // vectors tx + 16 j
+    float acc[8][VT];
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) acc[i][j] = 0.f;
+      for (int j = 0; j < VT; ++j) acc[i][j] = 0.f;
 #pragma unroll 4
     for (int c = 0; c < kTC; ++c) {
-      const float4 p0 = *reinterpret_cast<const float4*>(&sm.Ps[c][ty * 4]);
-      const float4 p1 = *reinterpret_cast<const float4*>(&sm.Ps[c][64 + ty * 4]);
-      const float4 v = *reinterpret_cast<const float4*>(&sm.Vs[c][tx * 4]);
+      const float4 p0 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, ty));
+      const float4 p1 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty));
       const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-      const float vv[4] = {v.x, v.y, v.z, v.w};
+      float vv[VT];
+#pragma unroll
+      for (int j = 0; j < VT; ++j) vv[j] = sm.Vs[c][tx + 16 * j];
 #pragma unroll
       for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
+        for (int j = 0; j < VT; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
     }
 #pragma unroll
     for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int j = 0; j < 4; ++j) o[i][j] += acc[i][j];
+      for (int j = 0; j < VT; ++j) o[i][j] += acc[i][j];
   }
 
-  // out = O * 2^max (a row whose weights are all zero gives 0)
+  // out = O * 2^max (a row whose weights are all zero gives 0); with
+  // splits, the sums and shifts of this split
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
     const int64_t gr = row0 + r;
     if (gr >= p.R) continue;
     const bool any = mrow[i] > kNegSentinel;
+    if (p.splits > 1) {
+      const int64_t sp = blockIdx.z;
+      if (tx == 0 && blockIdx.y == 0) p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        const int k = k0 + tx + 16 * j;
+        if (k < p.K) p.part_o[(sp * p.K + k) * p.R + gr] = any ? o[i][j] : 0.f;
+      }
+      continue;
+    }
     const float scale = any ? exp2f(mrow[i]) : 0.f;
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int k = k0 + tx * 4 + j;
+    for (int j = 0; j < VT; ++j) {
+      const int k = k0 + tx + 16 * j;
       if (k < p.K) p.out[(int64_t)k * p.R + gr] = any ? o[i][j] * scale : 0.f;
     }
+  }
+}
+
+// out[k][r] = sum_s part_o[s][k][r] 2^(part_m[s][r] - M) 2^M, M = max_s part_m.
+__global__ void combine_splits_kernel(ApplyArgs p) {
+  const int64_t total = (int64_t)p.K * p.R;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r = idx % p.R;
+    float mx = -INFINITY;
+    for (int sp = 0; sp < p.splits; ++sp) mx = fmaxf(mx, p.part_m[(int64_t)sp * p.R + r]);
+    float acc = 0.f;
+    if (mx > -INFINITY) {
+      for (int sp = 0; sp < p.splits; ++sp) {
+        const float ms = p.part_m[(int64_t)sp * p.R + r];
+        if (ms > -INFINITY) acc += p.part_o[(int64_t)sp * total + idx] * exp2f(ms - mx);
+      }
+      acc *= exp2f(mx);
+    }
+    p.out[idx] = acc;
   }
 }
 
@@ -255,16 +316,67 @@ __global__ void transport_matrix_kernel(const float* x, const float* y, int64_t 
   }
 }
 
-template <int DP>
-int launch_apply(const ApplyArgs& a, cudaStream_t stream) {
-  const size_t smem = sizeof(ApplySmem<DP>);
-  auto k = apply_transport_kernel<DP>;
+template <int DP, int VT>
+int launch_apply_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
+  const size_t smem = sizeof(ApplySmem<DP, VT>);
+  auto k = apply_transport_kernel<DP, VT>;
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return OTTB_ERR_CUDA;
-  dim3 grid((unsigned)((a.R + kTR - 1) / kTR), (unsigned)((a.K + kKT - 1) / kKT));
+  dim3 grid((unsigned)((a.R + kTR - 1) / kTR), (unsigned)chunks, (unsigned)a.splits);
   k<<<grid, 256, smem, stream>>>(a);
+  if (a.splits > 1) {
+    const int64_t total = (int64_t)a.K * a.R;
+    combine_splits_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 4096), 256, 0,
+                            stream>>>(a);
+  }
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+// Vector chunks of a call: the fewest chunks of at most 16 * max_vt
+// vectors.
+int apply_chunks(int d, int K) {
+  const int vm = d > 64 ? 4 : 5;
+  return (K + 16 * vm - 1) / (16 * vm);
+}
+
+// Column splits: enough CTAs for two waves of one CTA per SM, at most one
+// tile of B points per split and at most 16 splits.
+int apply_splits(int64_t R, int64_t C, int d, int K, int sms) {
+  const int64_t units = ((R + kTR - 1) / kTR) * apply_chunks(d, K);
+  const int64_t want = (2 * (int64_t)sms + units - 1) / units;
+  const int64_t tiles = (C + kTC - 1) / kTC;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, tiles), 16));
+}
+
+size_t apply_workspace(int64_t R, int K, int splits) {
+  return splits > 1 ? sizeof(float) * (size_t)splits * ((size_t)K + 1) * (size_t)R : 0;
+}
+
+int device_sms() {
+  int dev = 0, sms = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+    return 148;
+  return sms > 0 ? sms : 148;
+}
+
+// The fewest chunks of at most 16 * max_vt vectors, then the smallest
+// vectors-per-thread count that covers a chunk.
+template <int DP>
+int launch_apply(const ApplyArgs& a, cudaStream_t stream) {
+  constexpr int VM = max_vt<DP>();
+  const int chunks = (a.K + 16 * VM - 1) / (16 * VM);
+  const int per = (a.K + chunks - 1) / chunks;
+  const int vt = (per + 15) / 16;
+  switch (vt) {
+    case 1: return launch_apply_vt<DP, 1>(a, (a.K + 15) / 16, stream);
+    case 2: return launch_apply_vt<DP, 2>(a, (a.K + 31) / 32, stream);
+    case 3: return launch_apply_vt<DP, 3>(a, (a.K + 47) / 48, stream);
+    case 4: return launch_apply_vt<DP, 4>(a, (a.K + 63) / 64, stream);
+    default: return launch_apply_vt<DP, (VM > 4 ? 5 : 4)>(a, (a.K + 16 * VM - 1) / (16 * VM),
+                                                         stream);
+  }
 }
 
 }  // namespace
@@ -272,10 +384,18 @@ int launch_apply(const ApplyArgs& a, cudaStream_t stream) {
 
 using namespace ottb;
 
+extern "C" size_t ottb_apply_transport_workspace_size(int64_t n, int64_t m, int32_t d,
+                                                     int32_t num_vec, int32_t axis) {
+  if (n < 1 || m < 1 || d < 1 || d > 128 || num_vec < 1 || (axis != 0 && axis != 1)) return 0;
+  const int64_t R = axis == 1 ? n : m, C = axis == 1 ? m : n;
+  return apply_workspace(R, num_vec, apply_splits(R, C, d, num_vec, device_sms()));
+}
+
 extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
                                         int32_t d, const float* f, const float* g,
                                         float epsilon, float inv_scale_cost, const float* vec,
                                         int32_t num_vec, int32_t axis, float* out,
+                                        void* workspace, size_t workspace_bytes,
                                         void* stream) {
   if (!x || !y || !f || !g || !vec || !out || n < 1 || m < 1 || d < 1 || num_vec < 1)
     return OTTB_ERR_INVALID;
@@ -295,6 +415,12 @@ extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t 
   a.K = num_vec;
   a.ws = (float)(kLog2eD / (double)epsilon);
   a.inv = inv_scale_cost;
+  // as many column splits as wanted and as the workspace holds
+  a.splits = apply_splits(a.R, a.C, d, num_vec, device_sms());
+  while (a.splits > 1 && (!workspace || apply_workspace(a.R, num_vec, a.splits) > workspace_bytes))
+    --a.splits;
+  a.part_o = (float*)workspace;
+  a.part_m = a.splits > 1 ? a.part_o + (size_t)a.splits * num_vec * a.R : nullptr;
   cudaStream_t s = (cudaStream_t)stream;
   if (d <= 8) return launch_apply<8>(a, s);
   if (d <= 16) return launch_apply<16>(a, s);

@@ -147,10 +147,13 @@ class PointCloud(geometry.Geometry):
     fd = _arrays.as_f32(f, dev).detach()
     gd = _arrays.as_f32(g, dev).detach()
     out = torch.empty((v2.shape[0], m if axis == 0 else n), dtype=torch.float32, device=dev)
+    ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, self.dim, v2.shape[0], axis)
+    ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
     st = lib.ottb_apply_transport(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
                                   fd.data_ptr(), gd.data_ptr(), ctypes.c_float(self.epsilon),
                                   ctypes.c_float(self.inv_scale_cost), v2.data_ptr(),
-                                  v2.shape[0], axis, out.data_ptr(), _arrays.stream_handle())
+                                  v2.shape[0], axis, out.data_ptr(), ws.data_ptr(), ws_bytes,
+                                  _arrays.stream_handle())
     _lib.check(st, "ottb_apply_transport")
     return out[0] if one else out.reshape(*v.shape[:-1], out.shape[-1])
 

@@ -68,6 +68,7 @@ class SinkhornOutput(NamedTuple):
   ot_prob: Optional[linear_problem.LinearProblem] = None
   threshold: Optional[float] = None
   inner_iterations: Optional[int] = None
+  symmetric: bool = False  # solved with the symmetric update (f = g, x = y)
 
   def _res(self) -> _lib.OttbResult:
     results, k = self.reg_ot_cost_
@@ -177,7 +178,9 @@ class SinkhornOutput(NamedTuple):
     ones_n = torch.ones((1, n), dtype=torch.float32, device=x.device)
     ones_m = torch.ones((1, m), dtype=torch.float32, device=x.device)
     ry = self.apply(torch.cat([ones_m, y.t()], 0), axis=1).double()  # [1 + d, n]
-    cx = self.apply(torch.cat([ones_n, x.t()], 0), axis=0).double()  # [1 + d, m]
+    # symmetric solve: f = g and x = y make P symmetric, so the column
+    # application equals the row one
+    cx = ry if self.symmetric else self.apply(torch.cat([ones_n, x.t()], 0), axis=0).double()
     xd, yd = x.double(), y.double()
     r, py = ry[0], ry[1:].t()
     c, ptx = cx[0], cx[1:].t()
@@ -427,7 +430,8 @@ class _Call:
       f, g, errors = self.bufs[k]
       out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
                                 ot_prob=p, threshold=self.solver.threshold,
-                                inner_iterations=self.solver.inner_iterations))
+                                inner_iterations=self.solver.inner_iterations,
+                                symmetric=bool(self.arr[k].symmetric)))
     return out
 
   def keep_alive(self, stream: torch.cuda.Stream) -> None:
