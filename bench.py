@@ -512,6 +512,23 @@ def run_warmstart(args):
   warm_s, it_w, cost_w, conv_w, redo = timed(warm)
   clk = clocks.stop()
   rel = np.abs(cost_w - cost_c) / np.abs(cost_c)
+
+  # plain FP32 kernel, one problem per launch from zero init (the plain
+  # form), on the first `sample` held-out problems, scaled to all of them
+  sample = min(nte, 400)
+  solver1 = sinkhorn.Sinkhorn()
+  from ott_b200.problems.linear import linear_problem
+  probs1 = [linear_problem.LinearProblem(geom, At[k], Bt[k]) for k in range(sample)]
+  for p1 in probs1[:3]:
+    solver1(p1).n_iters
+  torch.cuda.synchronize()
+  flush.zero_()
+  e0.record()
+  outs1 = [solver1(p1) for p1 in probs1]
+  e1.record()
+  e1.synchronize()
+  plain_s = e0.elapsed_time(e1) * 1e-3 * nte / sample
+  plain_it = float(np.mean([o1.n_iters for o1 in outs1]))
   line = {
       "metric": "s to 1e-3 marginal err: learned warm start vs zero init, 32x32 grid",
       "value": warm_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
@@ -525,6 +542,10 @@ def run_warmstart(args):
       "warm_start": {"s": warm_s, "mean_iters": float(it_w.mean()),
                      "converged": int(conv_w.sum()), "fallbacks": int(redo)},
       "speedup": cold_s / warm_s, "iteration_ratio": float(it_w.mean() / it_c.mean()),
+      "plain_fp32_one_launch_per_problem": {
+          "s": plain_s, "mean_iters": plain_it,
+          "sample": f"first {sample} of {nte} held-out problems, time scaled by {nte}/{sample}"},
+      "speedup_vs_plain_fp32": plain_s / warm_s,
       "cost_rel_diff": {"max": float(rel.max()), "median": float(np.median(rel))},
       "training": {"target_solve_s": gen_s, "target_mean_iters": float(it_train.mean()),
                    "train_s": train_s, "loss_first": float(losses[:20].mean()),
