@@ -30,6 +30,15 @@ import numpy as np
 class JArray(np.ndarray):
   """ndarray with jax's functional ``.at[idx].set(v)`` update."""
 
+  def repeat(self, repeats, axis=None, total_repeat_length=None):
+    """jnp.ndarray.repeat: ``total_repeat_length`` fixes the output length
+    (truncated, or padded with the last element)."""
+    out = np.repeat(np.asarray(self), np.asarray(repeats), axis=axis)
+    if total_repeat_length is not None:
+      n = int(total_repeat_length)
+      out = out[:n] if len(out) >= n else np.concatenate([out, np.repeat(out[-1:], n - len(out))])
+    return wrap(out)
+
   @property
   def at(self):
     arr = self
@@ -48,6 +57,9 @@ class JArray(np.ndarray):
             return out
 
           def get(self):
+            # jax clamps out-of-bounds gather indices to the array bounds
+            if isinstance(idx, np.ndarray) and idx.dtype.kind in "iu":
+              return wrap(arr[np.clip(idx, 0, arr.shape[0] - 1)])
             return wrap(arr[idx])
         return _Upd()
     return _Indexer()
@@ -126,6 +138,17 @@ def _make_jnp() -> types.ModuleType:
 # ---------------------------------------------------------------- jax.lax
 def _make_lax() -> types.ModuleType:
   m = types.ModuleType("jax.lax")
+
+  def dynamic_slice(operand, start_indices, slice_sizes):
+    """lax.dynamic_slice: starts clamped so that the slice fits."""
+    a = np.asarray(operand)
+    idx = []
+    for dim, (st, sz) in enumerate(zip(start_indices, slice_sizes)):
+      st = int(min(max(int(st), 0), a.shape[dim] - int(sz)))
+      idx.append(slice(st, st + int(sz)))
+    return wrap(a[tuple(idx)])
+
+  m.dynamic_slice = dynamic_slice
 
   def while_loop(cond_fun, body_fun, init_val):
     val = init_val
@@ -272,6 +295,17 @@ def install(x64: bool = True) -> types.ModuleType:
   batching = types.ModuleType("jax.interpreters.batching")
   batching.is_vmappable = lambda x: False
   interpreters.batching = batching
+  ops = types.ModuleType("jax.ops")
+
+  def segment_sum(data, segment_ids, num_segments=None, indices_are_sorted=False, **k):
+    data, ids = np.asarray(data), np.asarray(segment_ids)
+    n = int(num_segments) if num_segments is not None else int(ids.max()) + 1
+    out = np.zeros((n,) + data.shape[1:], dtype=data.dtype)
+    ok = (ids >= 0) & (ids < n)
+    np.add.at(out, ids[ok], data[ok])
+    return wrap(out)
+
+  ops.segment_sum = segment_sum
   nn = types.ModuleType("jax.nn")
   nn.relu = lambda x: wrap(np.maximum(x, 0))
   config = types.SimpleNamespace(update=lambda *a, **k: None)
@@ -284,6 +318,7 @@ def install(x64: bool = True) -> types.ModuleType:
   jax.debug = debug
   jax.interpreters = interpreters
   jax.nn = nn
+  jax.ops = ops
   jax.config = config
   jax.Array = np.ndarray
   jax.vmap = vmap
@@ -296,6 +331,7 @@ def install(x64: bool = True) -> types.ModuleType:
                     "jax.scipy.special": special, "jax.tree_util": tree_util,
                     "jax.tree": tree, "jax.random": random, "jax.debug": debug,
                     "jax.interpreters": interpreters,
-                    "jax.interpreters.batching": batching, "jax.nn": nn}.items():
+                    "jax.interpreters.batching": batching, "jax.nn": nn,
+                    "jax.ops": ops}.items():
     sys.modules[name] = mod
   return jax

@@ -10,7 +10,8 @@ reference tree:
   geometry/pointcloud.py, problems/linear/linear_problem.py,
   initializers/linear/initializers.py, solvers/linear/acceleration.py,
   solvers/linear/sinkhorn.py, solvers/linear/_solve.py, and on request
-  tools/sinkhorn_divergence.py (load_divergence).
+  geometry/segment.py, tools/sinkhorn_divergence.py and
+  tools/segment_sinkhorn.py (load_tools).
 Modules the path imports but never calls for a balanced dense solve
 (regularizers, matrix square roots, implicit differentiation, low-rank and
 semidiscrete solvers, dual potentials, jaxopt) are empty placeholders.
@@ -120,10 +121,12 @@ def load(root: str = DEFAULT_ROOT, x64: bool = True) -> types.SimpleNamespace:
                                acceleration=acceleration, solve=solve_mod.solve)
 
 
-def load_divergence(root: str = DEFAULT_ROOT):
-  """tools/sinkhorn_divergence.py from the reference tree, after load():
-  ``segment`` (segmented divergences) is a placeholder, off this path."""
+def load_tools(root: str = DEFAULT_ROOT) -> types.SimpleNamespace:
+  """geometry/segment.py, tools/sinkhorn_divergence.py and
+  tools/segment_sinkhorn.py from the reference tree, after load()."""
   _package("ott.tools")
-  _placeholder("ott.geometry.segment")
-  sys.modules["ott.geometry"].segment = sys.modules["ott.geometry.segment"]
-  return _exec(root, "ott.tools.sinkhorn_divergence")
+  segment = _exec(root, "ott.geometry.segment")
+  divergence = _exec(root, "ott.tools.sinkhorn_divergence")
+  segment_sinkhorn = _exec(root, "ott.tools.segment_sinkhorn")
+  return types.SimpleNamespace(segment=segment, sinkhorn_divergence=divergence,
+                               segment_sinkhorn=segment_sinkhorn)

@@ -442,6 +442,46 @@ def sinkhorn_divergence(x, y, a=None, b=None, *, epsilon=None, relative_epsilon=
   return div, tuple(res)
 
 
+def segment_point_cloud(x, a=None, num_segments=None, max_measure_size=None,
+                        segment_ids=None, num_per_segment=None):
+  """geometry/segment.py:23-131: segments padded to ``max_measure_size``
+  with zero points of weight 0; default weights 1 / (segment size)."""
+  num, dim = x.shape
+  if segment_ids is not None:
+    counts = np.bincount(segment_ids, minlength=num_segments)
+  else:
+    counts = np.asarray(num_per_segment)
+    if max_measure_size is None:
+      max_measure_size = int(counts.max())
+    num_segments = len(counts)
+    segment_ids = np.repeat(np.arange(num_segments), counts)
+  size = min(int(max_measure_size), num)
+  if a is None:
+    a = (1.0 / counts)[segment_ids]
+  xs = np.zeros((num_segments, size, dim), x.dtype)
+  ws = np.zeros((num_segments, size), x.dtype)
+  for s in range(num_segments):
+    idx = np.flatnonzero(segment_ids == s)[:size]
+    xs[s, :len(idx)] = x[idx]
+    ws[s, :len(idx)] = a[idx]
+  return xs, ws
+
+
+def segment_sinkhorn(x, y, num_segments=None, max_measure_size=None, segment_ids_x=None,
+                     segment_ids_y=None, num_per_segment_x=None, num_per_segment_y=None,
+                     weights_x=None, weights_y=None, sinkhorn_kwargs=None,
+                     dtype=np.float64, **geom_kw):
+  """tools/segment_sinkhorn.py:24-138: one padded solve per segment."""
+  x, y = np.asarray(x, dtype), np.asarray(y, dtype)
+  sx, wx = segment_point_cloud(x, None if weights_x is None else np.asarray(weights_x, dtype),
+                               num_segments, max_measure_size, segment_ids_x, num_per_segment_x)
+  sy, wy = segment_point_cloud(y, None if weights_y is None else np.asarray(weights_y, dtype),
+                               num_segments, max_measure_size, segment_ids_y, num_per_segment_y)
+  kw = dict(sinkhorn_kwargs or {})
+  return np.array([solve(sx[s], sy[s], wx[s], wy[s], dtype=dtype, **geom_kw, **kw).reg_ot_cost
+                   for s in range(sx.shape[0])])
+
+
 # ---------------------------------------------------------------------------
 # Gradient of reg_ot_cost with the potentials held fixed
 # (sinkhorn.py:329-335 set_cost with use_danskin=True, :779-780 default)

@@ -1,3 +1,3 @@
-from ott_b200.tools import sinkhorn_divergence  # noqa: F401
+from ott_b200.tools import segment_sinkhorn, sinkhorn_divergence  # noqa: F401
 
-__all__ = ["sinkhorn_divergence"]
+__all__ = ["segment_sinkhorn", "sinkhorn_divergence"]

@@ -109,6 +109,39 @@ def run_divergence(ref, div_mod, case, dtype):
   return (x, y, a, b), res
 
 
+# Segmented solves (tools/segment_sinkhorn.py:24-138):
+# name -> (x size, y size, d, keyword arguments)
+SEG_CASES = {
+    "seg_contig_relmean": (208, 183, 3, dict(num_per_segment_x=(40, 7, 100, 61),
+                                             num_per_segment_y=(30, 80, 12, 61),
+                                             epsilon=0.1, relative_epsilon="mean")),
+    "seg_ids_weights_max60": (150, 170, 4, dict(num_segments=5, max_measure_size=60,
+                                                epsilon=0.05)),
+}
+
+
+def run_segment(tools, case, dtype):
+  nx, ny, d, kw = SEG_CASES[case]
+  rng = np.random.default_rng(nx + ny + d)
+  x = rng.uniform(size=(nx, d)).astype(dtype)
+  y = rng.uniform(size=(ny, d)).astype(dtype)
+  kw = dict(kw)
+  extra = {}
+  if "num_segments" in kw:
+    ns = kw["num_segments"]
+    ids_x = rng.integers(0, ns, size=nx)
+    ids_y = rng.integers(0, ns, size=ny)
+    wx = rng.uniform(0.5, 1.5, size=nx)
+    wy = rng.uniform(0.5, 1.5, size=ny)
+    for s in range(ns):
+      wx[ids_x == s] /= wx[ids_x == s].sum()
+      wy[ids_y == s] /= wy[ids_y == s].sum()
+    extra = dict(segment_ids_x=ids_x, segment_ids_y=ids_y, weights_x=wx.astype(dtype),
+                 weights_y=wy.astype(dtype))
+  out = tools.segment_sinkhorn.segment_sinkhorn(x, y, **kw, **extra)
+  return x, y, extra, np.asarray(out)
+
+
 def main():
   from oracle import reference_loader
   root = sys.argv[1] if len(sys.argv) > 1 else reference_loader.DEFAULT_ROOT
@@ -125,17 +158,28 @@ def main():
       manifest[case] = dict(inputs=spec, geometry={k: str(v) for k, v in gkw.items()},
                             solver=skw, init=init)
       print(tag, case, "n_iters", int(res["n_iters"]), "reg_ot_cost", float(res["reg_ot_cost"]))
-    div_mod = reference_loader.load_divergence(root)
+    tools = reference_loader.load_tools(root)
+    div_mod = tools.sinkhorn_divergence
     for case in DIV_CASES:
       (x, y, a, b), res = run_divergence(ref, div_mod, case, np.float64 if x64 else np.float32)
       np.savez_compressed(os.path.join(HERE, f"{case}.{tag}.npz"), x=x, y=y, a=a, b=b, **res)
       print(tag, case, "n_iters", res["n_iters"].tolist(), "divergence", float(res["divergence"]))
+    for case in SEG_CASES:
+      x, y, extra, costs = run_segment(tools, case, np.float64 if x64 else np.float32)
+      np.savez_compressed(os.path.join(HERE, f"{case}.{tag}.npz"), x=x, y=y, costs=costs,
+                          **extra)
+      print(tag, case, "costs", costs.tolist())
   with open(os.path.join(HERE, "manifest.json"), "w") as fh:
     json.dump(manifest, fh, indent=1, sort_keys=True)
   div_meta = {c: dict(inputs=s, geometry={k: str(v) for k, v in g.items()}, divergence=d,
                       weights=w) for c, (s, g, d, w) in DIV_CASES.items()}
   with open(os.path.join(HERE, "divergence_manifest.json"), "w") as fh:
     json.dump(div_meta, fh, indent=1, sort_keys=True)
+  seg_meta = {c: dict(sizes=[nx, ny, d], kwargs={k: (list(v) if isinstance(v, tuple) else v)
+                                                 for k, v in kw.items()})
+              for c, (nx, ny, d, kw) in SEG_CASES.items()}
+  with open(os.path.join(HERE, "segment_manifest.json"), "w") as fh:
+    json.dump(seg_meta, fh, indent=1, sort_keys=True)
 
 
 if __name__ == "__main__":

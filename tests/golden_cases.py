@@ -41,3 +41,21 @@ def load_divergence(name, tag="f64"):
   data = dict(np.load(os.path.join(HERE, f"{name}.{tag}.npz")))
   geom = {k: (float(v) if k == "epsilon" else v) for k, v in meta["geometry"].items()}
   return data, geom, dict(meta["divergence"]), bool(meta["weights"])
+
+
+def segment_names():
+  with open(os.path.join(HERE, "segment_manifest.json")) as fh:
+    return sorted(json.load(fh))
+
+
+def load_segment(name, tag="f64"):
+  """Inputs, segment_sinkhorn keyword arguments and the reference's costs
+  of one segmented case."""
+  with open(os.path.join(HERE, "segment_manifest.json")) as fh:
+    meta = json.load(fh)[name]
+  data = dict(np.load(os.path.join(HERE, f"{name}.{tag}.npz")))
+  kw = dict(meta["kwargs"])
+  for k in ("segment_ids_x", "segment_ids_y", "weights_x", "weights_y"):
+    if k in data:
+      kw[k] = data[k]
+  return data, kw
