@@ -121,6 +121,17 @@ def load(root: str = DEFAULT_ROOT, x64: bool = True) -> types.SimpleNamespace:
                                acceleration=acceleration, solve=solve_mod.solve)
 
 
+def load_implicit(linear_solver, root: str = DEFAULT_ROOT) -> types.ModuleType:
+  """solvers/linear/implicit_differentiation.py from the reference tree,
+  after load(). Its default linear solver (``lineax_implicit.solve_lineax``:
+  lineax is not installed) is replaced by ``linear_solver``, called with the
+  same ``(lin, b, lin_t, symmetric, **kwargs)`` arguments."""
+  _placeholder("ott.solvers.linear.lineax_implicit", solve_lineax=linear_solver)
+  sys.modules["ott.solvers.linear"].lineax_implicit = sys.modules[
+      "ott.solvers.linear.lineax_implicit"]
+  return _exec(root, "ott.solvers.linear.implicit_differentiation")
+
+
 def load_tools(root: str = DEFAULT_ROOT) -> types.SimpleNamespace:
   """geometry/segment.py, tools/sinkhorn_divergence.py and
   tools/segment_sinkhorn.py from the reference tree, after load()."""

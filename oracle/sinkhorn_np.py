@@ -524,6 +524,105 @@ def reg_ot_cost_grads(f, g, a, b, geom: Geom, scale_cost_mean=False):
 
 
 # ---------------------------------------------------------------------------
+# Implicit differentiation of the potentials
+# (solvers/linear/implicit_differentiation.py, default ImplicitDiff():
+# precondition h = eps log, balanced problem, lineax NormalCG)
+# ---------------------------------------------------------------------------
+def first_order_conditions(f, g, a, b, geom: Geom):
+  """implicit_differentiation.py:235-273 (tau = 1: grad_of_marginal_fit is
+  the weight itself, unbalanced_functions.py:30-50):
+  ``[a > 0](eps log(P 1) - eps log a)`` and ``[b > 0](eps log(P^T 1) -
+  eps log b)``."""
+  eps = geom.epsilon
+  P = transport_matrix(f, g, geom)
+  ma, mb = P.sum(1), P.sum(0)
+  with np.errstate(divide="ignore", invalid="ignore"):
+    ra = np.where(a > 0, eps * np.log(ma) - eps * np.log(a), 0.0)
+    rb = np.where(b > 0, eps * np.log(mb) - eps * np.log(b), 0.0)
+  return np.concatenate([ra, rb])
+
+
+def _lstsq_min_norm(mat, rhs):
+  """The least-squares solution of least norm: the limit of CG on the
+  normal equations started from zero (lineax NormalCG,
+  lineax_implicit.py:49-101), which ImplicitDiff uses by default."""
+  return np.linalg.lstsq(mat, rhs, rcond=None)[0]
+
+
+def implicit_solve(gr_f, gr_g, f, g, a, b, geom: Geom):
+  """implicit_differentiation.py:80-233 with ``h = eps log``, dense.
+
+  ``-(J^-1)^T gr`` for the Jacobian J of the first-order conditions in
+  (f, g): the Schur complement of the larger side's diagonal block is
+  solved (size m if n > m, else n). Points of zero weight are left out of
+  the system and get 0 (the reference's ``eps / 0`` makes them NaN).
+  """
+  n, m = geom.shape
+  eps = geom.epsilon
+  sa, sb = np.asarray(a) > 0, np.asarray(b) > 0
+  P = transport_matrix(f, g, geom)[np.ix_(sa, sb)]
+  gf, gg = np.asarray(gr_f, np.float64)[sa], np.asarray(gr_g, np.float64)[sb]
+  ma, mb = P.sum(1), P.sum(0)
+  hp = lambda v: eps / v  # derivative of eps * log
+  vjp_fg = lambda z: P @ (z * hp(mb)) / eps
+  vjp_gf = lambda z: P.T @ (z * hp(ma)) / eps
+  diag_a = ma * hp(ma) / eps
+  diag_b = mb * hp(mb) / eps
+  if n > m:
+    schur = np.diag(diag_b) - P.T @ np.diag(hp(ma) / eps / diag_a) @ P @ np.diag(hp(mb) / eps)
+    res = gg - vjp_gf(gf / diag_a)
+    sch = _lstsq_min_norm(schur, res)
+    lf, lg = (gf - vjp_fg(sch)) / diag_a, sch
+  else:
+    schur = np.diag(diag_a) - P @ np.diag(hp(mb) / eps / diag_b) @ P.T @ np.diag(hp(ma) / eps)
+    res = gf - vjp_fg(gg / diag_b)
+    sch = _lstsq_min_norm(schur, res)
+    lf, lg = sch, (gg - vjp_gf(sch)) / diag_b
+  out_f, out_g = np.zeros(n), np.zeros(m)
+  out_f[sa], out_g[sb] = -lf, -lg
+  return np.concatenate([out_f, out_g])
+
+
+def implicit_pullback(lam, f, g, a, b, geom: Geom, scale_cost_mean=False):
+  """``lam^T d(first_order_conditions)/d(x, y, a, b)`` at fixed f, g
+  (implicit_differentiation.py:275-287, the ``jax.vjp`` there), closed
+  form: with ``ma = P 1``, ``mb = P^T 1`` and the plan's
+  ``dP_ij / dC_ij = -P_ij / eps``, the cost cotangent is
+  ``G_ij = -P_ij (lam_a,i [a_i>0] / ma_i + lam_b,j [b_j>0] / mb_j)``;
+  ``C = inv C_unscaled`` carries it to the points (and to ``inv`` for
+  ``scale_cost="mean"``, pointcloud.py:348-351); ``d/da_i = -eps lam_a,i /
+  a_i`` on ``a > 0``. Epsilon is a constant (geometry.py:157-163)."""
+  n, m = geom.shape
+  eps, inv = geom.epsilon, geom.inv_scale
+  x, y = geom.x.astype(np.float64), geom.y.astype(np.float64)
+  a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+  la, lb = np.asarray(lam[:n], np.float64), np.asarray(lam[n:], np.float64)
+  P = transport_matrix(f, g, geom).astype(np.float64)
+  ma, mb = P.sum(1), P.sum(0)
+  with np.errstate(divide="ignore", invalid="ignore"):
+    ua = np.where(a > 0, la / ma, 0.0)
+    vb = np.where(b > 0, lb / mb, 0.0)
+    ga = np.where(a > 0, -eps * la / a, 0.0)
+    gb = np.where(b > 0, -eps * lb / b, 0.0)
+  G = -P * (ua[:, None] + vb[None, :])
+  gx = 2 * inv * (G.sum(1)[:, None] * x - G @ y)
+  gy = 2 * inv * (G.sum(0)[:, None] * y - G.T @ x)
+  if scale_cost_mean:
+    t = np.sum(G * sqeuclidean_all_pairs(x, y))
+    gx = gx - inv * inv * (2.0 / n) * (x - y.mean(0)) * t
+    gy = gy - inv * inv * (2.0 / m) * (y - x.mean(0)) * t
+  return gx, gy, ga, gb
+
+
+def implicit_grads(gr_f, gr_g, f, g, a, b, geom: Geom, scale_cost_mean=False):
+  """Gradient w.r.t. (x, y, a, b) of ``<gr_f, f*> + <gr_g, g*>`` through
+  the optimal potentials (sinkhorn.py:1112-1136: the custom VJP of the
+  Sinkhorn loop)."""
+  lam = implicit_solve(gr_f, gr_g, f, g, a, b, geom)
+  return implicit_pullback(lam, f, g, a, b, geom, scale_cost_mean)
+
+
+# ---------------------------------------------------------------------------
 # Learned initializer objective (initializers/neural/meta_initializer.py)
 # ---------------------------------------------------------------------------
 def meta_dual_loss(f_pred, a, b, geom: Geom):

@@ -128,25 +128,18 @@ class PointCloud(geometry.Geometry):
     return max(msq - mean * mean, 0.0) ** 0.5
 
   # -- transport from potentials (geometry.py:361-365, 444-486) ------------
-  def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
-                                      axis: int = 0) -> torch.Tensor:
-    """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
-    forming P (geometry.py:444-486): ``axis=0`` sums over rows
-    (``vec [..., n] -> [..., m]``), ``axis=1`` over columns
-    (``vec [..., m] -> [..., n]``). ``vec`` may be 1-D or a batch."""
-    if axis not in (0, 1):
-      raise ValueError("axis must be 0 or 1")
+  def _apply_raw(self, f: torch.Tensor, g: torch.Tensor, v2: torch.Tensor,
+                 axis: int) -> torch.Tensor:
+    """``ottb_apply_transport`` on ``v2 [k, n or m]`` (FP32, no autograd)."""
     lib = _lib.load()
     n, m = self.shape
     dev = self.x.device
-    v = _arrays.as_f32(vec, dev)
-    one = v.ndim == 1
-    v2 = v.reshape(1, -1) if one else v.reshape(-1, v.shape[-1]).contiguous()
-    if v2.shape[1] != (n if axis == 0 else m):
-      raise ValueError(f"vec has length {v2.shape[1]}, expected {n if axis == 0 else m}")
+    v2 = _arrays.as_f32(v2, dev).detach().contiguous()
     fd = _arrays.as_f32(f, dev).detach()
     gd = _arrays.as_f32(g, dev).detach()
     out = torch.empty((v2.shape[0], m if axis == 0 else n), dtype=torch.float32, device=dev)
+    if v2.shape[0] == 0:
+      return out
     ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, self.dim, v2.shape[0], axis)
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
     st = lib.ottb_apply_transport(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
@@ -155,10 +148,43 @@ class PointCloud(geometry.Geometry):
                                   v2.shape[0], axis, out.data_ptr(), ws.data_ptr(), ws_bytes,
                                   _arrays.stream_handle())
     _lib.check(st, "ottb_apply_transport")
+    return out
+
+  def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
+                                      axis: int = 0) -> torch.Tensor:
+    """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
+    forming P (geometry.py:444-486): ``axis=0`` sums over rows
+    (``vec [..., n] -> [..., m]``), ``axis=1`` over columns
+    (``vec [..., m] -> [..., n]``). ``vec`` may be 1-D or a batch.
+    Differentiable w.r.t. the points, ``f``, ``g`` and ``vec``."""
+    if axis not in (0, 1):
+      raise ValueError("axis must be 0 or 1")
+    n, m = self.shape
+    dev = self.x.device
+    v = _arrays.as_f32(vec, dev)
+    one = v.ndim == 1
+    v2 = v.reshape(1, -1) if one else v.reshape(-1, v.shape[-1])
+    if v2.shape[1] != (n if axis == 0 else m):
+      raise ValueError(f"vec has length {v2.shape[1]}, expected {n if axis == 0 else m}")
+    f = _arrays.as_f32(f, dev)
+    g = _arrays.as_f32(g, dev)
+    if _needs_grad(self.x, self.y, f, g, v2):
+      out = _ApplyTransport.apply(self.x, self.y, f, g, v2, self, axis)
+    else:
+      out = self._apply_raw(f, g, v2, axis)
     return out[0] if one else out.reshape(*v.shape[:-1], out.shape[-1])
 
   def transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
-    """The plan ``[n, m]`` (geometry.py:361-365)."""
+    """The plan ``[n, m]`` (geometry.py:361-365); differentiable w.r.t. the
+    points, ``f`` and ``g``."""
+    dev = self.x.device
+    f = _arrays.as_f32(f, dev)
+    g = _arrays.as_f32(g, dev)
+    if _needs_grad(self.x, self.y, f, g):
+      return _TransportMatrix.apply(self.x, self.y, f, g, self)
+    return self._matrix_raw(f, g)
+
+  def _matrix_raw(self, f: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
     lib = _lib.load()
     n, m = self.shape
     dev = self.x.device
@@ -171,6 +197,70 @@ class PointCloud(geometry.Geometry):
                                    _arrays.stream_handle())
     _lib.check(st, "ottb_transport_matrix")
     return out
+
+  def _points_vjp(self, rows: torch.Tensor, gy_rows: torch.Tensor, cols: torch.Tensor,
+                  gx_cols: torch.Tensor, gc: Optional[torch.Tensor]
+                  ) -> Tuple[torch.Tensor, torch.Tensor]:
+    """Gradient w.r.t. the points of a cost cotangent ``G`` (``dL/dC``,
+    ``C_ij = inv |x_i - y_j|^2``) given through ``rows = G 1``,
+    ``gy_rows = G y``, ``cols = G^T 1``, ``gx_cols = G^T x`` and, for
+    ``scale_cost="mean"``, ``gc = <G, |x_i - y_j|^2>`` (the cotangent of
+    ``inv = 1 / mean(C_unscaled)``, pointcloud.py:348-351, whose gradient
+    is ``-inv^2 (2/n)(x_i - mean(y))``; a float scale is a constant)."""
+    x, y = self.x.detach().double(), self.y.detach().double()
+    n, m = self.shape
+    inv = float(self.inv_scale_cost)
+    gx = 2.0 * inv * (rows[:, None] * x - gy_rows)
+    gy = 2.0 * inv * (cols[:, None] * y - gx_cols)
+    if self._scale_cost == "mean" and gc is not None:
+      gx = gx - inv * inv * (2.0 / n) * (x - y.mean(0)) * gc
+      gy = gy - inv * inv * (2.0 / m) * (y - x.mean(0)) * gc
+    return gx, gy
+
+  def _plan_vjp(self, f: torch.Tensor, g: torch.Tensor, alpha: torch.Tensor,
+                beta: torch.Tensor, points: bool = True):
+    """Backward of the plan for a cotangent of the low-rank form
+    ``dL/dP = sum_t alpha_t beta_t^T`` (``alpha [T, n]``, ``beta [T, m]``),
+    without forming P. Returns ``(gx, gy, u, w)`` in float64: ``u = P
+    beta_t`` ``[T, n]``, ``w = P^T alpha_t`` ``[T, m]`` (so ``dL/df = sum_t
+    alpha_t u_t / eps`` and ``dL/dg = sum_t beta_t w_t / eps``) and the
+    gradient w.r.t. the points (None unless ``points``) through
+    ``dP_ij/dC_ij = -P_ij / eps``. Two applications of the plan: to
+    ``[beta_t, beta_t y, beta_t |y|^2]`` and to ``[alpha_t, alpha_t x]``."""
+    eps = float(self.epsilon)
+    n, m = self.shape
+    d = self.dim
+    T = alpha.shape[0]
+    alpha, beta = alpha.double(), beta.double()
+    if not points:
+      u = self._apply_raw(f, g, beta, 1).double()
+      w = self._apply_raw(f, g, alpha, 0).double()
+      return None, None, u, w
+    x, y = self.x.detach().double(), self.y.detach().double()
+    mean = self._scale_cost == "mean"
+    parts = [beta[:, None, :], beta[:, None, :] * y.t()[None]]
+    if mean:
+      parts.append((beta * (y * y).sum(1)[None])[:, None, :])
+    k_r = len(parts) - 1 + d
+    r = self._apply_raw(f, g, torch.cat(parts, 1).reshape(T * k_r, m), 1).double()
+    r = r.reshape(T, k_r, n)
+    u, py = r[:, 0], r[:, 1:1 + d]
+    c = self._apply_raw(f, g, torch.cat([alpha[:, None, :], alpha[:, None, :] * x.t()[None]],
+                                        1).reshape(T * (1 + d), n), 0).double()
+    c = c.reshape(T, 1 + d, m)
+    w, ptx = c[:, 0], c[:, 1:]
+    # G = dL/dC = -(1/eps) sum_t diag(alpha_t) P diag(beta_t)
+    rows = -(alpha * u).sum(0) / eps
+    gy_rows = -(alpha[:, None, :] * py).sum(0).t() / eps
+    cols = -(beta * w).sum(0) / eps
+    gx_cols = -(beta[:, None, :] * ptx).sum(0).t() / eps
+    gc = None
+    if mean:
+      pysq = r[:, 1 + d]
+      xsq = (x * x).sum(1)
+      gc = -(alpha * (xsq[None] * u + pysq - 2.0 * (py * x.t()[None]).sum(1))).sum() / eps
+    gx, gy = self._points_vjp(rows, gy_rows, cols, gx_cols, gc)
+    return gx, gy, u, w
 
   def marginal_from_potentials(self, f: torch.Tensor, g: torch.Tensor,
                                axis: int = 0) -> torch.Tensor:
@@ -200,3 +290,75 @@ class PointCloud(geometry.Geometry):
   def __repr__(self) -> str:
     n, m = self.shape
     return f"PointCloud(n={n}, m={m}, d={self.dim}, epsilon={self._epsilon_init})"
+
+
+def _needs_grad(*ts: torch.Tensor) -> bool:
+  return torch.is_grad_enabled() and any(t.requires_grad for t in ts)
+
+
+def _cast(t: Optional[torch.Tensor], like: torch.Tensor, need: bool):
+  return t.to(like.dtype) if (need and t is not None) else None
+
+
+class _ApplyTransport(torch.autograd.Function):
+  """``vec -> P^T vec`` (axis 0) or ``P vec`` (axis 1) as a function of
+  ``(x, y, f, g, vec)``; its backward is two more applications of the plan
+  (``PointCloud._plan_vjp``)."""
+
+  @staticmethod
+  def forward(ctx, x, y, f, g, v2, geom, axis):  # pylint: disable=arguments-differ
+    out = geom._apply_raw(f, g, v2, axis)
+    ctx.geom, ctx.axis = geom, axis
+    ctx.save_for_backward(f, g, v2)
+    return out
+
+  @staticmethod
+  @torch.autograd.function.once_differentiable
+  def backward(ctx, gout):  # pylint: disable=arguments-differ
+    f, g, v2 = ctx.saved_tensors
+    geom, axis = ctx.geom, ctx.axis
+    need = ctx.needs_input_grad
+    eps = float(geom.epsilon)
+    W, V = gout.double(), v2.double()
+    # axis 0: out_k = P^T v_k, dL/dP = sum_k v_k W_k^T; axis 1: out_k = P v_k
+    alpha, beta = (V, W) if axis == 0 else (W, V)
+    gx, gy, u, w = geom._plan_vjp(f, g, alpha, beta, points=need[0] or need[1])
+    gf = (alpha * u).sum(0) / eps
+    gg = (beta * w).sum(0) / eps
+    gv = u if axis == 0 else w
+    return (_cast(gx, geom.x, need[0]), _cast(gy, geom.y, need[1]), _cast(gf, f, need[2]),
+            _cast(gg, g, need[3]), _cast(gv, v2, need[4]), None, None)
+
+
+class _TransportMatrix(torch.autograd.Function):
+  """The dense plan as a function of ``(x, y, f, g)``; backward with dense
+  products (the plan is formed anyway)."""
+
+  @staticmethod
+  def forward(ctx, x, y, f, g, geom):  # pylint: disable=arguments-differ
+    p = geom._matrix_raw(f, g)
+    ctx.geom = geom
+    ctx.save_for_backward(f, g, p)
+    return p
+
+  @staticmethod
+  @torch.autograd.function.once_differentiable
+  def backward(ctx, gp):  # pylint: disable=arguments-differ
+    f, g, p = ctx.saved_tensors
+    geom = ctx.geom
+    need = ctx.needs_input_grad
+    eps = float(geom.epsilon)
+    e = gp.double() * p.double()
+    gf = e.sum(1) / eps
+    gg = e.sum(0) / eps
+    gx = gy = None
+    if need[0] or need[1]:
+      x, y = geom.x.detach().double(), geom.y.detach().double()
+      G = -e / eps
+      rows, cols = G.sum(1), G.sum(0)
+      gy_rows, gx_cols = G @ y, G.t() @ x
+      gc = ((rows * (x * x).sum(1)).sum() + (cols * (y * y).sum(1)).sum()
+            - 2.0 * (x * gy_rows).sum())
+      gx, gy = geom._points_vjp(rows, gy_rows, cols, gx_cols, gc)
+    return (_cast(gx, geom.x, need[0]), _cast(gy, geom.y, need[1]), _cast(gf, f, need[2]),
+            _cast(gg, g, need[3]), None)

@@ -42,30 +42,17 @@ def solve_batch(geoms: Sequence[Any], a: Optional[Sequence[Any]] = None,
   return sinkhorn.run_batch(probs, solver, init, f_from_g=f_from_g)
 
 
-class _RegOTCost(torch.autograd.Function):
-  """``reg_ot_cost`` of a solved problem as a function of ``(x, y, a, b)``,
-  its backward the gradient with the potentials held fixed."""
-
-  @staticmethod
-  def forward(ctx, x, y, a, b, out):  # pylint: disable=arguments-differ
-    ctx.out = out
-    return torch.tensor(out.reg_ot_cost, dtype=torch.float64, device=x.device)
-
-  @staticmethod
-  def backward(ctx, gout):  # pylint: disable=arguments-differ
-    gx, gy, ga, gb = ctx.out.reg_ot_cost_grads()
-    need = ctx.needs_input_grad
-    cast = lambda t, i: (gout * t).to(torch.float32) if need[i] else None
-    return cast(gx, 0), cast(gy, 1), cast(ga, 2), cast(gb, 3), None
+_RegOTCost = sinkhorn._RegOTCost
 
 
 def reg_ot_cost(geom, a: Optional[Any] = None, b: Optional[Any] = None,
                 **kwargs: Any) -> torch.Tensor:
   """``solve(geom, a, b, **kwargs).reg_ot_cost`` as a differentiable 0-dim
-  tensor: ``jax.grad`` of the reference's ``reg_ot_cost`` with its default
-  ``use_danskin=True`` corresponds to ``torch.autograd`` here (gradients
-  w.r.t. ``geom.x``, ``geom.y``, ``a``, ``b``;
-  ``SinkhornOutput.reg_ot_cost_grads``)."""
+  tensor: ``jax.grad`` of the reference's ``reg_ot_cost`` corresponds to
+  ``torch.autograd`` here (gradients w.r.t. ``geom.x``, ``geom.y``, ``a``,
+  ``b``): with the default ``use_danskin=True`` the potentials are held
+  fixed (``SinkhornOutput.reg_ot_cost_grads``); ``use_danskin=False``
+  also differentiates them implicitly."""
   prob = linear_problem.LinearProblem(geom, a=a, b=b)
   out = sinkhorn.Sinkhorn(**kwargs)(prob)
-  return _RegOTCost.apply(geom.x, geom.y, prob.a, prob.b, out)
+  return sinkhorn._reg_ot_cost_tensor(out)

@@ -1,0 +1,305 @@
+"""Implicit differentiation of the Sinkhorn potentials
+(ott/solvers/linear/implicit_differentiation.py).
+
+At the solution the first-order conditions
+``F(f, g; C, a, b) = [h(P 1) - h(a), h(P^T 1) - h(b)] = 0`` hold (with the
+preconditioner ``h = eps log`` by default, :235-273). The backward of the
+potentials applies ``-(dF/d(f, g))^-T`` to their cotangent (:80-233) and
+pulls the result back through ``F``'s dependence on the inputs (:275-287).
+Every product with the plan is one ``ottb_apply_transport`` launch; the plan
+is never formed.
+
+Default solver (``solver=None``, ``precondition_fun=None``): the Schur
+complement of the reference's block system on the smaller side,
+``S = I - R D_l^-1 R^T D_s^-1`` (``R`` the plan or its transpose, ``D`` the
+marginals of the two sides), is solved by conjugate gradients on its
+symmetric form ``D_s^-1/2 S D_s^1/2 = I - K K^T``. The reference runs lineax
+``NormalCG`` on ``S`` itself (lineax_implicit.py:49-101), whose limit from
+zero is the least-squares solution of least norm; ``S`` is singular
+(``S ma = 0`` and ``1^T S = 0`` for the small side's marginal ``ma``), so
+here the right-hand side is projected onto ``range(S) = 1^perp`` and the
+solution onto ``ma^perp``, which is that same solution, with the condition
+number of ``S`` instead of its square. A user ``solver`` or
+``precondition_fun`` runs the reference's generic form instead.
+
+Zero-weight points are left out of the system (their gradients are 0; the
+reference's ``eps / 0`` makes them NaN).
+"""
+from __future__ import annotations
+
+import dataclasses
+from typing import Any, Callable, Dict, Optional, Tuple
+
+import torch
+
+__all__ = ["ImplicitDiff", "solve_jax_cg", "solve_normal_cg"]
+
+LinOp = Callable[[torch.Tensor], torch.Tensor]
+
+
+def _cg(op: LinOp, rhs: torch.Tensor, stop: Callable[[torch.Tensor], bool],
+        max_steps: int, stall: int = 0) -> torch.Tensor:
+  """Conjugate gradients from zero for a symmetric positive semi-definite
+  ``op``; ``stop(residual)`` ends it. ``stall > 0`` also ends it after
+  that many steps without a new smallest residual (the FP32 plan
+  applications put a floor under the residual)."""
+  x = torch.zeros_like(rhs)
+  r = rhs.clone()
+  if stop(r):
+    return x
+  p = r.clone()
+  rr = torch.dot(r, r)
+  best, since, best_x = float("inf"), 0, x
+  for _ in range(max_steps):
+    ap = op(p)
+    pap = torch.dot(p, ap)
+    if float(pap) <= 0.0:
+      break
+    alpha = rr / pap
+    x = x + alpha * p
+    r = r - alpha * ap
+    if stop(r):
+      return x
+    rn = float(torch.linalg.vector_norm(r))
+    if rn < best:
+      best, since, best_x = rn, 0, x
+    else:
+      since += 1
+      if stall and since >= stall:
+        return best_x
+    rr_new = torch.dot(r, r)
+    p = r + (rr_new / rr) * p
+    rr = rr_new
+  return x if not stall else best_x
+
+
+def _ridge(op: LinOp, ridge_kernel: float, ridge_identity: float) -> LinOp:
+  if ridge_kernel > 0.0 or ridge_identity > 0.0:
+    return lambda z: op(z) + ridge_kernel * torch.sum(z) + ridge_identity * z
+  return op
+
+
+def solve_jax_cg(lin: LinOp, b: torch.Tensor, lin_t: Optional[LinOp] = None,
+                 symmetric: bool = False, ridge_identity: float = 0.0,
+                 ridge_kernel: float = 0.0, tol: float = 1e-5, atol: float = 0.0,
+                 maxiter: Optional[int] = None, **kwargs: Any) -> torch.Tensor:
+  """implicit_differentiation.py:290-322 with the stopping rule of
+  ``jax.scipy.sparse.linalg.cg`` (``|r| <= max(tol |b|, atol)``, at most
+  ``maxiter = 10 size`` steps): CG on ``lin`` if ``symmetric``, else on
+  ``lin_t(lin(.))``, with the optional ridge terms, against ``b`` as
+  given there."""
+  op = lin if symmetric else (lambda z: lin_t(lin(z)))
+  op = _ridge(op, ridge_kernel, ridge_identity)
+  bound = max(tol * float(torch.linalg.vector_norm(b)), atol)
+  steps = 10 * b.numel() if maxiter is None else int(maxiter)
+  return _cg(op, b, lambda r: float(torch.linalg.vector_norm(r)) <= bound, steps)
+
+
+def solve_normal_cg(lin: LinOp, b: torch.Tensor, lin_t: Optional[LinOp] = None,
+                    symmetric: bool = False, ridge_identity: float = 0.0,
+                    ridge_kernel: float = 0.0, rtol: float = 1e-6, atol: float = 1e-6,
+                    max_steps: Optional[int] = None, **kwargs: Any) -> torch.Tensor:
+  """The reference's default solver (lineax_implicit.py:49-101: lineax
+  ``CG`` if ``symmetric`` else ``NormalCG``, ``rtol = atol = 1e-6``, max
+  norm): CG on ``lin`` against ``b``, or on ``lin_t(lin(.))`` against
+  ``lin_t(b)``. At most ``max_steps`` steps (default ``10 size``; lineax has
+  no bound)."""
+  lin = _ridge(lin, ridge_kernel, ridge_identity)
+  if symmetric:
+    op, rhs = lin, b
+  else:
+    lin_t = _ridge(lin_t, ridge_kernel, ridge_identity)
+    op, rhs = (lambda z: lin_t(lin(z))), lin_t(b)
+  bound = atol + rtol * float(rhs.abs().max())
+  steps = 10 * b.numel() if max_steps is None else int(max_steps)
+  return _cg(op, rhs, lambda r: float(r.abs().max()) <= bound, steps)
+
+
+def _elementwise_derivative(fun: Callable[[torch.Tensor], torch.Tensor],
+                            v: torch.Tensor) -> torch.Tensor:
+  """``vmap(grad(fun))(v)`` for an elementwise scalar function."""
+  with torch.enable_grad():
+    t = v.detach().clone().requires_grad_()
+    (gt,) = torch.autograd.grad(fun(t).sum(), t)
+  return gt.detach()
+
+
+@dataclasses.dataclass
+class ImplicitDiff:
+  """implicit_differentiation.py:34-80, same fields.
+
+  ``solver(lin, b, lin_t, symmetric, **solver_kwargs)`` solves the Schur
+  system; ``None`` picks the symmetric-form CG described in the module
+  docstring (keywords ``rtol`` (1e-6), ``max_steps`` (1000), ``stall``
+  (30)). ``precondition_fun`` replaces ``h = eps log``.
+  """
+
+  solver: Optional[Callable[..., torch.Tensor]] = None
+  solver_kwargs: Optional[Dict[str, Any]] = None
+  symmetric: bool = False
+  precondition_fun: Optional[Callable[[torch.Tensor], torch.Tensor]] = None
+
+  def replace(self, **kwargs: Any) -> "ImplicitDiff":
+    return dataclasses.replace(self, **kwargs)
+
+  # -- plan products ---------------------------------------------------------
+  @staticmethod
+  def _app(geom, f, g):
+    def app(v: torch.Tensor, axis: int) -> torch.Tensor:
+      return geom._apply_raw(f, g, v.reshape(1, -1), axis)[0].double()
+    return app
+
+  def _precond(self, geom) -> Callable[[torch.Tensor], torch.Tensor]:
+    if self.precondition_fun is not None:
+      return self.precondition_fun
+    eps = float(geom.epsilon)
+    return lambda v: eps * torch.log(v)
+
+  def _derivative(self, geom, v: torch.Tensor) -> torch.Tensor:
+    if self.precondition_fun is None:
+      return float(geom.epsilon) / v
+    return _elementwise_derivative(self.precondition_fun, v)
+
+  @staticmethod
+  def _check(ot_prob, lse_mode: bool) -> None:
+    if not lse_mode:
+      raise NotImplementedError("kernel mode (lse_mode=False) is not on this path")
+    if not ot_prob.is_balanced:
+      raise NotImplementedError("unbalanced problems (tau < 1) are not on this path")
+
+  def first_order_conditions(self, prob, f: torch.Tensor, g: torch.Tensor,
+                             lse_mode: bool = True) -> torch.Tensor:
+    """implicit_differentiation.py:235-273: ``[a > 0](h(P 1) - h(a))``,
+    ``[b > 0](h(P^T 1) - h(b))`` (float64, length n + m)."""
+    self._check(prob, lse_mode)
+    geom = prob.geom
+    n, m = geom.shape
+    app = self._app(geom, f, g)
+    dev = f.device
+    ma = app(torch.ones(m, dtype=torch.float64, device=dev), 1)
+    mb = app(torch.ones(n, dtype=torch.float64, device=dev), 0)
+    h = self._precond(geom)
+    a, b = prob.a.detach().double(), prob.b.detach().double()
+    one = lambda v, w: torch.where(w > 0, v, torch.ones_like(v))
+    ra = torch.where(a > 0, h(one(ma, a)) - h(one(a, a)), torch.zeros_like(a))
+    rb = torch.where(b > 0, h(one(mb, b)) - h(one(b, b)), torch.zeros_like(b))
+    return torch.cat([ra, rb])
+
+  # -- the linear solve --------------------------------------------------------
+  def solve(self, gr: Tuple[torch.Tensor, torch.Tensor], ot_prob, f: torch.Tensor,
+            g: torch.Tensor, lse_mode: bool = True) -> torch.Tensor:
+    """implicit_differentiation.py:80-233: ``-(dF/d(f, g))^-T gr`` for the
+    first-order conditions ``F`` (float64, length n + m)."""
+    self._check(ot_prob, lse_mode)
+    geom = ot_prob.geom
+    n, m = geom.shape
+    dev = f.device
+    app = self._app(geom, f, g)
+    gr_f = gr[0].detach().double().reshape(n)
+    gr_g = gr[1].detach().double().reshape(m)
+    sa = ot_prob.a.detach() > 0
+    sb = ot_prob.b.detach() > 0
+    ma = app(torch.ones(m, dtype=torch.float64, device=dev), 1)
+    mb = app(torch.ones(n, dtype=torch.float64, device=dev), 0)
+    sa, sb = sa & (ma > 0), sb & (mb > 0)
+    if self.solver is None and self.precondition_fun is None:
+      lf, lg = self._solve_default(gr_f, gr_g, ma, mb, sa, sb, app, n > m)
+    else:
+      lf, lg = self._solve_generic(geom, gr_f, gr_g, ma, mb, sa, sb, app, n > m)
+    zero = torch.zeros((), dtype=torch.float64, device=dev)
+    return torch.cat([torch.where(sa, -lf, zero), torch.where(sb, -lg, zero)])
+
+  def _solve_default(self, gr_f, gr_g, ma, mb, sa, sb, app, n_gt_m):
+    kw = dict(self.solver_kwargs or {})
+    rtol = float(kw.get("rtol", 1e-6))
+    max_steps = int(kw.get("max_steps", 1000))
+    stall = int(kw.get("stall", 30))
+    zero = torch.zeros((), dtype=torch.float64, device=ma.device)
+    safe_inv = lambda v, s: torch.where(s, 1.0 / torch.where(s, v, torch.ones_like(v)), zero)
+    inv_ma, inv_mb = safe_inv(ma, sa), safe_inv(mb, sb)
+    # small side s (the Schur system's), large side l; R maps l -> s
+    if n_gt_m:
+      gr_s, gr_l, m_s, s_s = gr_g, gr_f, mb, sb
+      inv_s, inv_l = inv_mb, inv_ma
+      r_op, rt_op = (lambda v: app(v, 0)), (lambda v: app(v, 1))
+    else:
+      gr_s, gr_l, m_s, s_s = gr_f, gr_g, ma, sa
+      inv_s, inv_l = inv_ma, inv_mb
+      r_op, rt_op = (lambda v: app(v, 1)), (lambda v: app(v, 0))
+    res = torch.where(s_s, gr_s - r_op(gr_l * inv_l), zero)
+    cnt = s_s.sum().clamp(min=1).double()
+    res = torch.where(s_s, res - res.sum() / cnt, zero)  # onto range(S)
+    c = torch.sqrt(inv_s)
+
+    def sym_op(yv):  # (I - K K^T) y with K = D_s^-1/2 R D_l^-1/2
+      return yv - c * r_op(inv_l * rt_op(c * yv))
+
+    rhs = c * res
+    bound = rtol * float(torch.linalg.vector_norm(rhs))
+    yv = _cg(sym_op, rhs, lambda r: float(torch.linalg.vector_norm(r)) <= bound,
+             max_steps, stall)
+    z = torch.where(s_s, yv / torch.where(s_s, c, torch.ones_like(c)), zero)
+    z = z - (torch.dot(z, m_s) / torch.dot(m_s, m_s)) * m_s  # onto ma^perp
+    other = gr_l - rt_op(z * inv_s)
+    return (other, z) if n_gt_m else (z, other)
+
+  def _solve_generic(self, geom, gr_f, gr_g, ma, mb, sa, sb, app, n_gt_m):
+    """The reference's construction (:156-233) with any solver and
+    preconditioner."""
+    eps = float(geom.epsilon)
+    zero = torch.zeros((), dtype=torch.float64, device=ma.device)
+    one = lambda v, s: torch.where(s, v, torch.ones_like(v))
+    da = torch.where(sa, self._derivative(geom, one(ma, sa)), zero)
+    db = torch.where(sb, self._derivative(geom, one(mb, sb)), zero)
+    symmetric = self.symmetric if self.precondition_fun is not None else False
+    solver = self.solver if self.solver is not None else solve_normal_cg
+    kw = dict(self.solver_kwargs or {})
+    vjp_fg = lambda z: app(z * db, 1) / eps
+    vjp_gf = lambda z: app(z * da, 0) / eps
+    vjp_fgt = lambda z: app(z, 0) * db / eps
+    vjp_gft = lambda z: app(z, 1) * da / eps
+    diag_a = torch.where(sa, ma * da / eps, torch.ones_like(ma))
+    diag_b = torch.where(sb, mb * db / eps, torch.ones_like(mb))
+    if n_gt_m:
+      inv_ff = lambda z: z / diag_a
+      schur = lambda z: z * diag_b - vjp_gf(inv_ff(vjp_fg(z)))
+      schur_t = None if symmetric else (lambda z: z * diag_b - vjp_fgt(inv_ff(vjp_gft(z))))
+      res = gr_g - vjp_gf(inv_ff(gr_f))
+      sch = solver(schur, res, schur_t, symmetric, **kw)
+      return inv_ff(gr_f - vjp_fg(sch)), sch
+    inv_gg = lambda z: z / diag_b
+    schur = lambda z: z * diag_a - vjp_fg(inv_gg(vjp_gf(z)))
+    schur_t = None if symmetric else (lambda z: z * diag_a - vjp_gft(inv_gg(vjp_fgt(z))))
+    res = gr_f - vjp_fg(inv_gg(gr_g))
+    sch = solver(schur, res, schur_t, symmetric, **kw)
+    return sch, inv_gg(gr_g - vjp_gf(sch))
+
+  # -- the pullback ------------------------------------------------------------
+  def gradient(self, prob, f: torch.Tensor, g: torch.Tensor, lse_mode: bool,
+               gr: Tuple[torch.Tensor, torch.Tensor]
+               ) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
+    """implicit_differentiation.py:275-287: the cotangent of the inputs
+    ``(x, y, a, b)`` (float64) for the cotangent ``gr`` of ``(f, g)``:
+    ``lam = solve(gr)`` pulled back through the first-order conditions at
+    fixed ``f, g`` (``d h(P 1)_i / dP_ij = h'(P 1)_i``, ``dP_ij/dC_ij =
+    -P_ij / eps``; ``d/da_i = -lam_i h'(a_i)`` on ``a > 0``)."""
+    lam = self.solve(gr, prob, f, g, lse_mode)
+    geom = prob.geom
+    n, m = geom.shape
+    dev = f.device
+    la, lb = lam[:n], lam[n:]
+    a, b = prob.a.detach().double(), prob.b.detach().double()
+    app = self._app(geom, f, g)
+    ma = app(torch.ones(m, dtype=torch.float64, device=dev), 1)
+    mb = app(torch.ones(n, dtype=torch.float64, device=dev), 0)
+    zero = torch.zeros((), dtype=torch.float64, device=dev)
+    sa, sb = (a > 0) & (ma > 0), (b > 0) & (mb > 0)
+    one = lambda v, s: torch.where(s, v, torch.ones_like(v))
+    alpha1 = torch.where(sa, la * self._derivative(geom, one(ma, sa)), zero)
+    beta2 = torch.where(sb, lb * self._derivative(geom, one(mb, sb)), zero)
+    alpha = torch.stack([alpha1, torch.ones(n, dtype=torch.float64, device=dev)])
+    beta = torch.stack([torch.ones(m, dtype=torch.float64, device=dev), beta2])
+    gx, gy, _, _ = geom._plan_vjp(f, g, alpha, beta, points=True)
+    ga = torch.where(a > 0, -la * self._derivative(geom, one(a, a > 0)), zero)
+    gb = torch.where(b > 0, -lb * self._derivative(geom, one(b, b > 0)), zero)
+    return gx, gy, ga, gb

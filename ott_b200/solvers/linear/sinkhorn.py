@@ -24,6 +24,7 @@ from ott_b200 import _arrays, _lib
 from ott_b200.geometry import epsilon_scheduler as eps_scheduler
 from ott_b200.initializers.linear import initializers as init_lib
 from ott_b200.problems.linear import linear_problem
+from ott_b200.solvers.linear import implicit_differentiation as implicit_lib
 
 __all__ = ["Sinkhorn", "SinkhornGraph", "SinkhornOutput", "run_batch"]
 
@@ -69,6 +70,7 @@ class SinkhornOutput(NamedTuple):
   threshold: Optional[float] = None
   inner_iterations: Optional[int] = None
   symmetric: bool = False  # solved with the symmetric update (f = g, x = y)
+  use_danskin: bool = True  # gradient of reg_ot_cost with f, g held fixed
 
   def _res(self) -> _lib.OttbResult:
     results, k = self.reg_ot_cost_
@@ -83,9 +85,16 @@ class SinkhornOutput(NamedTuple):
     return self.potentials[1]
 
   @property
-  def reg_ot_cost(self) -> float:
-    """sinkhorn.py:224-277 (balanced), FP64 sums on the device."""
-    return self._res().reg_ot_cost
+  def reg_ot_cost(self) -> Any:
+    """sinkhorn.py:224-277 (balanced), FP64 sums on the device: a float, or
+    a differentiable 0-dim float64 tensor when the problem's points or
+    weights require gradients (with ``use_danskin`` the gradient holds the
+    potentials fixed, sinkhorn.py:329-335; otherwise it also flows through
+    the potentials' implicit backward)."""
+    val = self._res().reg_ot_cost
+    if self.ot_prob is None or not _tracks_grad(self.ot_prob):
+      return val
+    return _reg_ot_cost_tensor(self)
 
   @property
   def kl_reg_cost(self) -> float:
@@ -170,6 +179,10 @@ class SinkhornOutput(NamedTuple):
     weight the reference's ``jnp.where`` gives NaN gradients; here that
     term is 0.
     """
+    with torch.no_grad():
+      return self._reg_ot_cost_grads()
+
+  def _reg_ot_cost_grads(self):
     geom = self.geom
     eps = float(geom.epsilon)
     inv = float(geom.inv_scale_cost)
@@ -205,11 +218,88 @@ class SinkhornOutput(NamedTuple):
     """``<P, C>`` (sinkhorn.py:346-349 through :395-417), from one
     application of the plan to ``[1, |y|^2, y]``."""
     geom = self.geom
-    x, y = geom.x.double(), geom.y.double()
-    vecs = torch.cat([torch.ones_like(y[:, :1]), (y * y).sum(1, keepdim=True), y], 1)
-    r = self.apply(vecs.t().float(), axis=1).double()  # [d + 2, n]
-    tot = (r[0] * (x * x).sum(1) + r[1] - 2.0 * (r[2:].t() * x).sum(1)).sum()
+    with torch.no_grad():
+      x, y = geom.x.double(), geom.y.double()
+      vecs = torch.cat([torch.ones_like(y[:, :1]), (y * y).sum(1, keepdim=True), y], 1)
+      r = self.apply(vecs.t().float(), axis=1).double()  # [d + 2, n]
+      tot = (r[0] * (x * x).sum(1) + r[1] - 2.0 * (r[2:].t() * x).sum(1)).sum()
     return float(geom.inv_scale_cost * tot)
+
+
+def _tracks_grad(p: linear_problem.LinearProblem) -> bool:
+  return torch.is_grad_enabled() and any(
+      t.requires_grad for t in (p.geom.x, p.geom.y, p.a, p.b))
+
+
+class _Potentials(torch.autograd.Function):
+  """The solved ``(f, g)`` as a function of ``(x, y, a, b)``; backward by
+  implicit differentiation of the first-order conditions
+  (sinkhorn.py:1102-1136, ``ImplicitDiff.gradient``)."""
+
+  @staticmethod
+  def forward(ctx, x, y, a, b, f, g, prob, implicit_diff):  # pylint: disable=arguments-differ
+    ctx.prob, ctx.implicit_diff = prob, implicit_diff
+    ctx.save_for_backward(f, g)
+    return f.clone(), g.clone()
+
+  @staticmethod
+  @torch.autograd.function.once_differentiable
+  def backward(ctx, gf, gg):  # pylint: disable=arguments-differ
+    if ctx.implicit_diff is None:
+      raise NotImplementedError("gradients through the potentials need implicit_diff "
+                                "(unrolled differentiation is not on this path)")
+    f, g = ctx.saved_tensors
+    gf = torch.zeros_like(f) if gf is None else gf
+    gg = torch.zeros_like(g) if gg is None else gg
+    gx, gy, ga, gb = ctx.implicit_diff.gradient(ctx.prob, f, g, True, (gf, gg))
+    need = ctx.needs_input_grad
+    p = ctx.prob
+    cast = lambda t, like, i: t.to(like.dtype) if need[i] else None
+    return (cast(gx, p.geom.x, 0), cast(gy, p.geom.y, 1), cast(ga, p.a, 2),
+            cast(gb, p.b, 3), None, None, None, None)
+
+
+class _RegOTCost(torch.autograd.Function):
+  """``reg_ot_cost`` of a solved problem as a function of ``(x, y, a, b)``,
+  its backward the gradient with the potentials held fixed
+  (``SinkhornOutput.reg_ot_cost_grads``)."""
+
+  @staticmethod
+  def forward(ctx, x, y, a, b, out):  # pylint: disable=arguments-differ
+    ctx.out = out
+    return torch.tensor(out._res().reg_ot_cost, dtype=torch.float64, device=x.device)
+
+  @staticmethod
+  @torch.autograd.function.once_differentiable
+  def backward(ctx, gout):  # pylint: disable=arguments-differ
+    gx, gy, ga, gb = ctx.out.reg_ot_cost_grads()
+    need = ctx.needs_input_grad
+    cast = lambda t, i: (gout * t).to(torch.float32) if need[i] else None
+    return cast(gx, 0), cast(gy, 1), cast(ga, 2), cast(gb, 3), None
+
+
+def _reg_ot_cost_tensor(out: SinkhornOutput) -> torch.Tensor:
+  """``reg_ot_cost`` as a differentiable tensor: with ``use_danskin`` the
+  fixed-potential gradient; otherwise compute_kl_reg_cost (sinkhorn.py:
+  224-277) written on the differentiable potentials and plan, valued at
+  the device's FP64 result."""
+  p = out.ot_prob
+  if out.use_danskin:
+    return _RegOTCost.apply(p.geom.x, p.geom.y, p.a, p.b, out)
+  geom = p.geom
+  eps = float(geom.epsilon)
+  a, b = p.a.double(), p.b.double()
+  f, g = out.f.double(), out.g.double()
+  zero = torch.zeros((), dtype=torch.float64, device=a.device)
+  fa = torch.where(a > 0, f, zero)
+  gb_ = torch.where(b > 0, g, zero)
+  la = torch.log(torch.where(a > 0, a, torch.ones_like(a)))
+  lb = torch.log(torch.where(b > 0, b, torch.ones_like(b)))
+  mb = geom.marginal_from_potentials(out.f, out.g, axis=0).double()
+  expr = ((a * (fa - eps * la)).sum() + (b * (gb_ - eps * lb)).sum()
+          + eps * (a.sum() * b.sum() - mb.sum()))
+  val = out._res().reg_ot_cost
+  return expr + (val - expr.detach())
 
 
 class Sinkhorn:
@@ -239,7 +329,7 @@ class Sinkhorn:
       parallel_dual_updates: bool = False,
       recenter_potentials: bool = False,
       use_danskin: Optional[bool] = None,
-      implicit_diff: Optional[Any] = "default",
+      implicit_diff: Optional[implicit_lib.ImplicitDiff] = implicit_lib.ImplicitDiff(),
       initializer: Optional[init_lib.SinkhornInitializer] = None,
       progress_fn: Optional[Any] = None,
       precision: str = "auto",
@@ -274,7 +364,8 @@ class Sinkhorn:
     self.max_iterations = max_iterations
     self.parallel_dual_updates = parallel_dual_updates
     self.recenter_potentials = recenter_potentials
-    self.use_danskin = use_danskin
+    # sinkhorn.py:779-780
+    self.use_danskin = (implicit_diff is not None) if use_danskin is None else bool(use_danskin)
     self.implicit_diff = implicit_diff
     self.initializer = (init_lib.DefaultInitializer()
                         if initializer is None else initializer)
@@ -428,10 +519,14 @@ class _Call:
     out = []
     for k, p in enumerate(self.probs):
       f, g, errors = self.bufs[k]
+      if _tracks_grad(p):
+        f, g = _Potentials.apply(p.geom.x, p.geom.y, p.a, p.b, f, g, p,
+                                 self.solver.implicit_diff)
       out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
                                 ot_prob=p, threshold=self.solver.threshold,
                                 inner_iterations=self.solver.inner_iterations,
-                                symmetric=bool(self.arr[k].symmetric)))
+                                symmetric=bool(self.arr[k].symmetric),
+                                use_danskin=self.solver.use_danskin))
     return out
 
   def keep_alive(self, stream: torch.cuda.Stream) -> None:

@@ -142,6 +142,79 @@ def run_segment(tools, case, dtype):
   return x, y, extra, np.asarray(out)
 
 
+# Implicit differentiation of the potentials
+# (solvers/linear/implicit_differentiation.py, default ImplicitDiff()):
+# name -> (n, m, d, PointCloud kwargs with an absolute epsilon, inputs)
+IMP_CASES = {
+    "imp_unif_13x9_d3": (13, 9, 3, dict(epsilon=0.1), "unif"),
+    "imp_unif_8x15_d2_scalemean": (8, 15, 2, dict(epsilon=0.05, scale_cost="mean"), "unif"),
+    "imp_gauss_24x30_d8": (24, 30, 8, dict(epsilon=0.5), "gauss"),
+    "imp_unif_18x18_d4_scale2": (18, 18, 4, dict(epsilon=0.02, scale_cost=2.0), "unif"),
+}
+
+
+def lstsq_solver(lin, b, lin_t=None, symmetric=False, **kwargs):
+  """Stands in for lineax's NormalCG (not installed): the least-squares
+  solution of least norm, its limit from zero, on the materialised
+  operator."""
+  b = np.asarray(b, np.float64)
+  k = b.shape[0]
+  mat = np.stack([np.asarray(lin(np.eye(k)[:, i])) for i in range(k)], 1)
+  return np.linalg.lstsq(mat, b, rcond=None)[0]
+
+
+def run_implicit(ref, imp_mod, case):
+  """The reference's ImplicitDiff.solve on its own converged potentials,
+  then the gradient of ``<lam, first_order_conditions>`` w.r.t. every
+  coordinate of x, y, a and b by central differences of the reference's
+  own first_order_conditions (its ``jax.vjp``, :275-287, needs autodiff).
+  Epsilon is absolute: the reference stops gradients through a relative
+  one (geometry.py:157-163), which finite differences would not."""
+  n, m, d, gkw, kind = IMP_CASES[case]
+  rng = np.random.default_rng(n * m + d)
+  if kind == "unif":
+    x = rng.uniform(size=(n, d))
+    y = rng.uniform(size=(m, d))
+  else:
+    x = rng.standard_normal((n, d))
+    y = 0.5 + rng.standard_normal((m, d)) * rng.uniform(0.5, 1.5, size=d)
+  a = rng.uniform(0.2, 1.2, n)
+  a /= a.sum()
+  b = rng.uniform(0.2, 1.2, m)
+  b /= b.sum()
+  geom = ref.pointcloud.PointCloud(x, y, **gkw)
+  out = ref.solve(geom, a, b, threshold=1e-11, max_iterations=200000)
+  f, g = np.asarray(out.f), np.asarray(out.g)
+  prob = ref.linear_problem.LinearProblem(geom, a, b)
+  gr_f, gr_g = rng.standard_normal(n), rng.standard_normal(m)
+  idiff = imp_mod.ImplicitDiff()
+  lam = np.asarray(idiff.solve((gr_f, gr_g), prob, f, g, True))
+
+  def objective(xx, yy, aa, bb):
+    pr = ref.linear_problem.LinearProblem(ref.pointcloud.PointCloud(xx, yy, **gkw), aa, bb)
+    return float(np.dot(lam, np.asarray(idiff.first_order_conditions(pr, f, g, True))))
+
+  def fd(arr, which):
+    grad = np.zeros_like(arr)
+    flat = grad.reshape(-1)
+    for i in range(arr.size):
+      h = 1e-6 * max(1.0, abs(arr.reshape(-1)[i]))
+      args = {"x": x, "y": y, "a": a, "b": b}
+      up, dn = arr.copy(), arr.copy()
+      up.reshape(-1)[i] += h
+      dn.reshape(-1)[i] -= h
+      args[which] = up
+      fu = objective(args["x"], args["y"], args["a"], args["b"])
+      args[which] = dn
+      fl = objective(args["x"], args["y"], args["a"], args["b"])
+      flat[i] = (fu - fl) / (2 * h)
+    return grad
+
+  res = dict(f=f, g=g, gr_f=gr_f, gr_g=gr_g, lam=lam, n_iters=np.asarray(out.n_iters),
+             gx=fd(x, "x"), gy=fd(y, "y"), ga=fd(a, "a"), gb=fd(b, "b"))
+  return (x, y, a, b), res
+
+
 def main():
   from oracle import reference_loader
   root = sys.argv[1] if len(sys.argv) > 1 else reference_loader.DEFAULT_ROOT
@@ -169,6 +242,16 @@ def main():
       np.savez_compressed(os.path.join(HERE, f"{case}.{tag}.npz"), x=x, y=y, costs=costs,
                           **extra)
       print(tag, case, "costs", costs.tolist())
+  ref = reference_loader.load(root, x64=True)
+  imp_mod = reference_loader.load_implicit(lstsq_solver, root)
+  for case in IMP_CASES:
+    (x, y, a, b), res = run_implicit(ref, imp_mod, case)
+    np.savez_compressed(os.path.join(HERE, f"{case}.f64.npz"), x=x, y=y, a=a, b=b, **res)
+    print("f64", case, "n_iters", int(res["n_iters"]), "|lam|", float(np.abs(res["lam"]).max()))
+  imp_meta = {c: dict(sizes=[n, m, d], geometry={k: v for k, v in g.items()}, inputs=kind)
+              for c, (n, m, d, g, kind) in IMP_CASES.items()}
+  with open(os.path.join(HERE, "implicit_manifest.json"), "w") as fh:
+    json.dump(imp_meta, fh, indent=1, sort_keys=True)
   with open(os.path.join(HERE, "manifest.json"), "w") as fh:
     json.dump(manifest, fh, indent=1, sort_keys=True)
   div_meta = {c: dict(inputs=s, geometry={k: str(v) for k, v in g.items()}, divergence=d,

@@ -59,3 +59,18 @@ def load_segment(name, tag="f64"):
     if k in data:
       kw[k] = data[k]
   return data, kw
+
+
+def implicit_names():
+  with open(os.path.join(HERE, "implicit_manifest.json")) as fh:
+    return sorted(json.load(fh))
+
+
+def load_implicit(name):
+  """Inputs, potentials, cotangents and the reference's implicit-diff
+  results (lam, finite-difference gradients) of one case, with the
+  PointCloud keyword arguments."""
+  with open(os.path.join(HERE, "implicit_manifest.json")) as fh:
+    meta = json.load(fh)[name]
+  data = dict(np.load(os.path.join(HERE, f"{name}.f64.npz")))
+  return data, dict(meta["geometry"])

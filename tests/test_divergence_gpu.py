@@ -51,12 +51,12 @@ def test_divergence_and_gradient_match_oracle(d, precision):
   geom_kw = dict(epsilon=0.05, relative_epsilon="mean")
   div, out, xt, yt = _div(x, y, a, b, geom_kw, {}, precision=precision, grad=True)
   ref, res = o.sinkhorn_divergence(x, y, a, b, **geom_kw)
-  assert abs(float(div) - ref) <= 1e-4 * abs(ref)
+  assert abs(float(div.detach()) - ref) <= 1e-4 * abs(ref)
   tol_pot = (1e-4 if precision == "fp32" else 1e-3) * res[0].epsilon
   for k in range(3):
     assert abs(out.n_iters[k] - res[k].n_iters) <= 10
     if out.n_iters[k] == res[k].n_iters:
-      np.testing.assert_allclose(out.potentials[k][0].cpu().numpy(), res[k].f, atol=tol_pot)
+      np.testing.assert_allclose(out.potentials[k][0].detach().cpu().numpy(), res[k].f, atol=tol_pot)
   div.backward()
   # d div / dx = d reg(x, y)/dx - (d reg(x, x)/dx in both roles) / 2, each
   # with the GPU's potentials held fixed

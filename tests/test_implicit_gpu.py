@@ -1,0 +1,216 @@
+"""Implicit differentiation of the potentials on the GPU: ImplicitDiff, the
+potentials' autograd backward, and differentiable plan applications.
+
+Tolerances (relative to the largest magnitude of the compared quantity):
+- 5e-5 against the reference's own ImplicitDiff results (golden vectors).
+  Float32 inputs and plan applications inside the CG solve give ~1e-6 there.
+- 1e-4 against the float64 oracle at the GPU's potentials, for larger and
+  less well-conditioned systems.
+- 5e-5 for gradients of plan applications against float64 torch autograd
+  on the dense plan.
+"""
+import numpy as np
+import pytest
+
+from oracle import sinkhorn_np as o
+from tests import golden_cases, problems
+
+pytestmark = pytest.mark.gpu
+
+
+def _t(v, grad=False):
+  import torch
+  t = torch.as_tensor(np.asarray(v), dtype=torch.float32).cuda()
+  return t.requires_grad_() if grad else t
+
+
+def _rel(got, want):
+  got = got.detach().cpu().numpy() if hasattr(got, "detach") else np.asarray(got)
+  return float(np.abs(got - want).max() / max(np.abs(want).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name", golden_cases.implicit_names())
+def test_implicit_matches_reference_golden(name):
+  """lam from the reference's ImplicitDiff.solve, gradients from finite
+  differences of its first_order_conditions, at its own potentials."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  data, gkw = golden_cases.load_implicit(name)
+  geom = pointcloud.PointCloud(_t(data["x"]), _t(data["y"]), epsilon=float(gkw["epsilon"]),
+                               scale_cost=gkw.get("scale_cost", 1.0))
+  prob = linear_problem.LinearProblem(geom, _t(data["a"]), _t(data["b"]))
+  f, g = _t(data["f"]), _t(data["g"])
+  gr = (torch.as_tensor(data["gr_f"]).cuda(), torch.as_tensor(data["gr_g"]).cuda())
+  idiff = imp.ImplicitDiff()
+  assert _rel(idiff.solve(gr, prob, f, g), data["lam"]) < 5e-5
+  assert float(idiff.first_order_conditions(prob, f, g).abs().max()) < 1e-5
+  for got, key in zip(idiff.gradient(prob, f, g, True, gr), ("gx", "gy", "ga", "gb")):
+    assert _rel(got, data[key]) < 5e-5, key
+
+
+@pytest.mark.parametrize("n,m,d,eps,scale", [(300, 200, 3, 0.05, 1.0), (257, 400, 16, 0.1, "mean"),
+                                             (640, 640, 64, 0.05, 1.0)])
+def test_autograd_through_potentials_matches_oracle(n, m, d, eps, scale):
+  """torch.autograd of <w, f> + <v, g> (sum w = sum v: independent of the
+  potentials' free constant) through linear.solve."""
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + m)
+  rng = np.random.default_rng(1)
+  w, v = rng.standard_normal(n), rng.standard_normal(m)
+  v += (w.sum() - v.sum()) / m
+  xt, yt, at, bt = _t(x, True), _t(y, True), _t(a, True), _t(b, True)
+  geom = pointcloud.PointCloud(xt, yt, epsilon=eps, relative_epsilon="mean", scale_cost=scale)
+  out = linear.solve(geom, at, bt, threshold=1e-5, max_iterations=5000, precision="fp32")
+  loss = (out.f.double() * _t(w).double()).sum() + (out.g.double() * _t(v).double()).sum()
+  loss.backward()
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon),
+              inv_scale=float(geom.inv_scale_cost))
+  f = out.f.detach().double().cpu().numpy()
+  g = out.g.detach().double().cpu().numpy()
+  want = o.implicit_grads(w, v, f, g, a.astype(np.float64), b.astype(np.float64), og,
+                          scale_cost_mean=scale == "mean")
+  for t, ref, key in zip((xt, yt, at, bt), want, "xyab"):
+    assert _rel(t.grad, ref) < 1e-4, key
+
+
+def test_zero_weight_points_get_zero_gradients():
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(120, 90, 4, seed=4)
+  a[[3, 50]] = 0.0
+  a /= a.sum()
+  xt, at = _t(x, True), _t(a, True)
+  geom = pointcloud.PointCloud(xt, _t(y), epsilon=0.1)
+  out = linear.solve(geom, at, _t(b), threshold=1e-6)
+  w = np.random.default_rng(0).standard_normal(120)
+  w[[3, 50]] = 0.0
+  (out.f.double() * _t(w).double()).sum().backward()
+  gx = xt.grad.cpu().numpy()
+  assert np.isfinite(gx).all() and np.all(gx[[3, 50]] == 0.0)
+  assert np.all(at.grad.cpu().numpy()[[3, 50]] == 0.0)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), 0.1)
+  f = out.f.detach().double().cpu().numpy()
+  g = out.g.detach().double().cpu().numpy()
+  want = o.implicit_grads(w, np.zeros(90), f, g, a.astype(np.float64), b.astype(np.float64), og)
+  assert _rel(xt.grad, want[0]) < 1e-4
+
+
+def test_reg_ot_cost_without_danskin_equals_danskin_at_optimum():
+  """At the optimum the cost is stationary in (f, g): differentiating the
+  potentials too (use_danskin=False) changes the gradient only by the
+  first-order conditions' residual."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(200, 150, 5, seed=6)
+  grads = []
+  for danskin in (True, False):
+    xt, yt, at, bt = _t(x, True), _t(y, True), _t(a, True), _t(b, True)
+    geom = pointcloud.PointCloud(xt, yt, epsilon=0.05, relative_epsilon="mean")
+    cost = linear.reg_ot_cost(geom, at, bt, threshold=1e-6, use_danskin=danskin,
+                              max_iterations=10000)
+    assert isinstance(cost, torch.Tensor)
+    cost.backward()
+    grads.append([t.grad.cpu().numpy().astype(np.float64) for t in (xt, yt, at, bt)])
+  for g0, g1, key in zip(grads[0], grads[1], "xyab"):
+    if key in "ab":  # balanced: the weights' gradients are defined up to a constant
+      g0, g1 = g0 - g0.mean(), g1 - g1.mean()
+    assert _rel(g1, g0) < 1e-3, key
+
+
+def test_output_reg_ot_cost_is_differentiable():
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(100, 80, 3, seed=8)
+  xt = _t(x, True)
+  out = linear.solve(pointcloud.PointCloud(xt, _t(y), epsilon=0.1), _t(a), _t(b))
+  cost = out.reg_ot_cost
+  assert isinstance(cost, torch.Tensor) and cost.requires_grad
+  cost.backward()
+  gx, _, _, _ = out.reg_ot_cost_grads()
+  assert _rel(xt.grad, gx.cpu().numpy()) < 1e-6
+  with torch.no_grad():
+    out2 = linear.solve(pointcloud.PointCloud(_t(x), _t(y), epsilon=0.1), _t(a), _t(b))
+  assert isinstance(out2.reg_ot_cost, float)
+
+
+def test_generic_solver_path_agrees_on_point_gradients():
+  """A user solver (the reference's NormalCG-equivalent) through the
+  reference's generic construction: same point gradients; the weights'
+  gradients agree up to the balanced problem's free constant."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  x, y, a, b = problems.uniform_cloud_problem(150, 110, 4, seed=10)
+  geom = pointcloud.PointCloud(_t(x), _t(y), epsilon=0.1)
+  out = linear.solve(geom, _t(a), _t(b), threshold=1e-7, max_iterations=10000)
+  prob = linear_problem.LinearProblem(geom, _t(a), _t(b))
+  rng = np.random.default_rng(2)
+  gr = (torch.as_tensor(rng.standard_normal(150)).cuda(),
+        torch.as_tensor(rng.standard_normal(110)).cuda())
+  d0 = imp.ImplicitDiff().gradient(prob, out.f, out.g, True, gr)
+  d1 = imp.ImplicitDiff(solver=imp.solve_normal_cg).gradient(prob, out.f, out.g, True, gr)
+  assert _rel(d1[0], d0[0].cpu().numpy()) < 1e-3
+  assert _rel(d1[1], d0[1].cpu().numpy()) < 1e-3
+  for k in (2, 3):
+    u, v = d1[k] - d1[k].mean(), d0[k] - d0[k].mean()
+    assert _rel(u, v.cpu().numpy()) < 1e-3
+
+
+def test_unrolled_differentiation_is_refused():
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x, y, a, b = problems.uniform_cloud_problem(60, 50, 2, seed=12)
+  xt = _t(x, True)
+  out = linear.solve(pointcloud.PointCloud(xt, _t(y), epsilon=0.1), _t(a), _t(b),
+                     implicit_diff=None)
+  with pytest.raises(NotImplementedError):
+    out.f.sum().backward()
+
+
+@pytest.mark.parametrize("axis", [0, 1])
+@pytest.mark.parametrize("scale", [1.0, "mean"])
+def test_apply_and_matrix_gradients_match_dense_autograd(axis, scale):
+  """Gradients of plan applications and of the dense plan w.r.t. the
+  points, the potentials and the vectors against float64 torch autograd on
+  the dense plan."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  n, m, d = 190, 260, 8
+  x, y, _, _ = problems.uniform_cloud_problem(n, m, d, seed=14)
+  rng = np.random.default_rng(3)
+  f0 = 0.05 * rng.standard_normal(n)
+  g0 = 0.05 * rng.standard_normal(m)
+  vec = rng.standard_normal((4, n if axis == 0 else m))
+  xt, yt, ft, gt, vt = (_t(x, True), _t(y, True), _t(f0, True), _t(g0, True), _t(vec, True))
+  geom = pointcloud.PointCloud(xt, yt, epsilon=0.2, scale_cost=scale)
+  outp = geom.apply_transport_from_potentials(ft, gt, vt, axis=axis)
+  wc = torch.randn_like(outp)
+  got = torch.autograd.grad((outp * wc).sum(), (xt, yt, ft, gt, vt))
+  mat = geom.transport_from_potentials(ft, gt)
+  dc = torch.randn_like(mat)
+  got_m = torch.autograd.grad((mat * dc).sum(), (xt, yt, ft, gt))
+
+  def dense(xd, yd, fd, gd):
+    c = ((xd[:, None, :] - yd[None]) ** 2).sum(-1)
+    c = c / c.mean() if scale == "mean" else c
+    return torch.exp((fd[:, None] + gd[None] - c) / 0.2)
+
+  leaves = [torch.as_tensor(np.asarray(v, np.float64)).requires_grad_()
+            for v in (xt.detach().cpu(), yt.detach().cpu(), ft.detach().cpu(),
+                      gt.detach().cpu(), vt.detach().cpu())]
+  p = dense(*leaves[:4])
+  ref_out = leaves[4] @ p if axis == 0 else leaves[4] @ p.t()
+  want = torch.autograd.grad((ref_out * wc.double().cpu()).sum(), leaves)
+  for u, v, key in zip(got, want, ("x", "y", "f", "g", "vec")):
+    assert _rel(u, v.numpy()) < 5e-5, key
+  p = dense(*leaves[:4])
+  want_m = torch.autograd.grad((p * dc.double().cpu()).sum(), leaves[:4])
+  for u, v, key in zip(got_m, want_m, "xyfg"):
+    assert _rel(u, v.numpy()) < 5e-5, key

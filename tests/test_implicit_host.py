@@ -1,0 +1,75 @@
+"""The conjugate-gradient solvers behind ImplicitDiff, on the CPU (plain
+torch tensors): solve_jax_cg (jax.scipy's stopping rule) and
+solve_normal_cg (lineax CG / NormalCG defaults)."""
+import numpy as np
+import torch
+
+from ott_b200.solvers.linear import implicit_differentiation as imp
+
+
+def _spd(k, seed):
+  rng = np.random.default_rng(seed)
+  q = rng.standard_normal((k, k))
+  return torch.as_tensor(q @ q.T + k * np.eye(k))
+
+
+def test_symmetric_cg_solves_spd_system():
+  a = _spd(30, 0)
+  b = torch.as_tensor(np.random.default_rng(1).standard_normal(30))
+  x = imp.solve_normal_cg(lambda z: a @ z, b, None, True, rtol=1e-12, atol=0.0)
+  np.testing.assert_allclose((a @ x).numpy(), b.numpy(), atol=1e-9)
+  x2 = imp.solve_jax_cg(lambda z: a @ z, b, None, True, tol=1e-12)
+  np.testing.assert_allclose(x2.numpy(), x.numpy(), atol=1e-9)
+
+
+def test_normal_cg_least_squares_min_norm():
+  """Non-symmetric, singular: NormalCG's limit is the least-squares
+  solution of least norm."""
+  rng = np.random.default_rng(2)
+  k = 20
+  m = rng.standard_normal((k, k))
+  m[:, -1] = m[:, 0]  # rank k - 1
+  mt = torch.as_tensor(m)
+  b = torch.as_tensor(rng.standard_normal(k))
+  x = imp.solve_normal_cg(lambda z: mt @ z, b, lambda z: mt.T @ z, False,
+                          rtol=1e-13, atol=0.0, max_steps=2000)
+  want = np.linalg.lstsq(m, b.numpy(), rcond=None)[0]
+  np.testing.assert_allclose(x.numpy(), want, atol=1e-7 * np.abs(want).max())
+
+
+def test_jax_cg_normal_operator_and_ridge():
+  """solve_jax_cg on a non-symmetric operator runs CG on lin_t(lin(.))
+  against b as given (implicit_differentiation.py:314-322), ridge terms
+  added to that operator."""
+  rng = np.random.default_rng(3)
+  k = 15
+  m = torch.as_tensor(rng.standard_normal((k, k)) + 4 * np.eye(k))
+  b = torch.as_tensor(rng.standard_normal(k))
+  x = imp.solve_jax_cg(lambda z: m @ z, b, lambda z: m.T @ z, False, ridge_identity=0.5,
+                       ridge_kernel=0.25, tol=1e-13)
+  op = m.T @ m + 0.5 * torch.eye(k, dtype=torch.float64) + 0.25 * torch.ones(k, k,
+                                                                             dtype=torch.float64)
+  np.testing.assert_allclose((op @ x).numpy(), b.numpy(), atol=1e-9)
+
+
+def test_cg_stall_returns_best_iterate():
+  """With a stall limit, CG stops after that many steps without a new
+  smallest residual and returns the best iterate seen."""
+  a = _spd(12, 4)
+  b = torch.as_tensor(np.random.default_rng(5).standard_normal(12))
+  calls = []
+
+  def op(z):
+    calls.append(1)
+    return a @ z
+
+  x = imp._cg(op, b, lambda r: False, max_steps=500, stall=5)
+  assert len(calls) < 500
+  np.testing.assert_allclose((a @ x).numpy(), b.numpy(), atol=1e-8)
+
+
+def test_implicit_diff_fields_and_replace():
+  d = imp.ImplicitDiff()
+  assert d.solver is None and d.precondition_fun is None and d.symmetric is False
+  d2 = d.replace(symmetric=True, solver_kwargs={"rtol": 1e-8})
+  assert d2.symmetric and d2.solver_kwargs == {"rtol": 1e-8} and not d.symmetric

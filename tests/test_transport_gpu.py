@@ -87,8 +87,8 @@ def test_reg_ot_cost_gradients_match_oracle(scale_cost, rel):
   cost = linear.reg_ot_cost(geom, at, bt, threshold=1e-6)
   cost.backward()
   out = linear.solve(geom, at, bt, threshold=1e-6)
-  f = out.f.cpu().numpy().astype(np.float64)
-  g = out.g.cpu().numpy().astype(np.float64)
+  f = out.f.detach().cpu().numpy().astype(np.float64)
+  g = out.g.detach().cpu().numpy().astype(np.float64)
   og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon),
               inv_scale=float(geom.inv_scale_cost))
   gx, gy, ga, gb = o.reg_ot_cost_grads(f, g, a.astype(np.float64), b.astype(np.float64), og,
@@ -97,7 +97,7 @@ def test_reg_ot_cost_gradients_match_oracle(scale_cost, rel):
   np.testing.assert_allclose(yt.grad.cpu().numpy(), gy, rtol=0, atol=1e-4 * np.abs(gy).max())
   np.testing.assert_allclose(at.grad.cpu().numpy(), ga, rtol=0, atol=1e-4 * np.abs(ga).max())
   np.testing.assert_allclose(bt.grad.cpu().numpy(), gb, rtol=0, atol=1e-4 * np.abs(gb).max())
-  assert abs(float(cost) - out.reg_ot_cost) <= 1e-6 * abs(out.reg_ot_cost)
+  assert abs(float(cost.detach()) - out.reg_ot_cost) <= 1e-6 * abs(out.reg_ot_cost)
 
 
 def test_gradient_of_self_transport_sums_both_roles():
