@@ -267,17 +267,14 @@ def run_ours(args):
   from ott_b200.solvers import linear
   from ott_b200.solvers.linear import sinkhorn
 
+  from ott_b200 import distributed as odist
+
   def barrier():
     if world > 1:
       dist.barrier()
     torch.cuda.synchronize()
 
-  def max_over_ranks(v):
-    if world == 1:
-      return v
-    t = torch.tensor([v], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+  max_over_ranks = odist.max_over_ranks
 
   peaks = measure_pipe_peaks(torch)
   x, y, a, b = workload(args)
@@ -566,13 +563,24 @@ def run_batched(args):
   (chosen precision and FP32), and one launch per problem for comparison.
   Inputs (~440 MB) exceed the L2."""
   import torch
+  import torch.distributed as dist
+  from datetime import timedelta
   from tests import problems
+  from ott_b200 import distributed as odist
   from ott_b200.geometry import pointcloud
   from ott_b200.problems.linear import linear_problem
   from ott_b200.solvers.linear import sinkhorn
-  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  rank = int(os.environ.get("RANK", "0"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  torch.cuda.set_device(local)
+  if world > 1:
+    # one process per GPU; each rank solves its own batch (the job is
+    # world x problems independent problems), no data-path collective
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
   peaks = measure_pipe_peaks(torch)
-  data = problems.batched_uneven_problems(args.problems, d=32, seed=0)
+  data = problems.batched_uneven_problems(args.problems, d=32, seed=rank)
   probs = []
   for x, y, a, b in data:
     geom = pointcloud.PointCloud(torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda(),
@@ -584,10 +592,15 @@ def run_batched(args):
   entries_per_it = 2.0 * sum(p.geom.shape[0] * p.geom.shape[1] for p in probs)
   ev = lambda: torch.cuda.Event(enable_timing=True)
 
+  def barrier():
+    if world > 1:
+      dist.barrier()
+    torch.cuda.synchronize()
+
   def timed(fn, steps, warm):
     for _ in range(warm):
       fn()
-    torch.cuda.synchronize()
+    barrier()
     ms, outs = 0.0, None
     for _ in range(steps):
       e0, e1 = ev(), ev()
@@ -596,7 +609,8 @@ def run_batched(args):
       e1.record()
       e1.synchronize()
       ms += e0.elapsed_time(e1)
-    return ms / steps * 1e-3, outs
+    barrier()
+    return odist.max_over_ranks(ms / steps * 1e-3), outs
 
   def batch(precision, autotune=False):
     solver = sinkhorn.Sinkhorn(precision=precision, autotune=autotune)
@@ -632,9 +646,12 @@ def run_batched(args):
     roof["peak_at_sampled_clock"] = at
     roof["frac_at_sampled_clock"] = ach / at
   sizes = np.array([p.geom.shape for p in probs])
+  n_conv = int(odist.sum_over_ranks(float(conv.sum())))
   line = {
       "metric": "s to 1e-3 marginal err, 512 uneven problems in one launch",
-      "value": t_b, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "value": t_b, "unit": "s", "higher_is_better": False, "n_gpus": world,
+      "scaling": "weak", "parallelism": f"{world} rank(s) x {args.problems} problems, "
+                                         "no data-path collective",
       "workload": "batched", "dtype": "bf16x3/f32", "data": "synthetic",
       "steps": args.steps, "warmup": args.warmup,
       "config": {"workload": f"{args.problems} problems n,m log-uniform [128,16384] d=32 "
@@ -644,8 +661,9 @@ def run_batched(args):
                  "total_entries_per_iteration": entries_per_it,
                  "n_range": [int(sizes[:, 0].min()), int(sizes[:, 0].max())],
                  "l2": "inputs ~440 MB > L2"},
-      "converged": int(conv.sum()), "mean_iters": float(it_b.mean()),
-      "max_iters": int(it_b.max()), "entries_per_s": entries / t_b,
+      "converged": n_conv, "mean_iters": float(it_b.mean()),
+      "max_iters": int(it_b.max()),
+      "entries_per_s": odist.sum_over_ranks(entries) / t_b,  # whole job, all ranks
       "direct_call_no_graph": {"s": t_d},
       "plain_fp32_batched": {"s": t_f, "mean_iters": float(it_f.mean())},
       "one_launch_per_problem": {"s": t_s},
@@ -654,7 +672,10 @@ def run_batched(args):
       "iters_equal_fp32": int((it_b == it_f).sum()),
       "roofline": roof, "clocks": clk,
   }
-  print(json.dumps(line))
+  if rank == 0:
+    print(json.dumps(line))
+  if world > 1:
+    dist.destroy_process_group()
   return 0
 
 
