@@ -54,7 +54,8 @@ def parse_args():
   p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
   p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
   p.add_argument("--workload", default="gaussian64",
-                 choices=["gaussian64", "warmstart", "batched", "anneal", "divergence"],
+                 choices=["gaussian64", "warmstart", "batched", "anneal", "divergence",
+                          "implicit"],
                  help="gaussian64: the headline single large solve (default); "
                       "warmstart: learned warm start on a 32x32 grid; batched: 512 "
                       "uneven problems in one launch; anneal: epsilon-annealed solves; "
@@ -820,6 +821,99 @@ def run_divergence(args):
   return 0
 
 
+def run_implicit(args):
+  """Gradient through the potentials of the headline problem (Gaussian-shift
+  clouds, n = m = ``--n``, d = ``--d``, uniform weights, epsilon = 0.01 *
+  mean(C), threshold 1e-3): the solve (chosen precision), then the backward
+  of ``<w, f> + <v, g>`` (sum w = sum v) by implicit differentiation. The
+  backward applies the plan 2 x (CG steps) + 4 times to one vector (the
+  marginals, the right-hand side, the other side's multiplier) and twice to
+  2 (d + 2) and 2 (d + 1) vectors (the pullback to the points)."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+  peaks = measure_pipe_peaks(torch)
+  x, y, _, _ = workload(args)
+  n, d = args.n, args.d
+  xt = torch.from_numpy(x).cuda().requires_grad_()
+  yt = torch.from_numpy(y).cuda().requires_grad_()
+  rng = np.random.default_rng(0)
+  w = torch.from_numpy(rng.standard_normal(n)).cuda()
+  v = torch.from_numpy(rng.standard_normal(n)).cuda()
+  v += (w.sum() - v.sum()) / n
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+  flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
+
+  def step():
+    xt.grad = None
+    yt.grad = None
+    e0, e1, e2 = ev(), ev(), ev()
+    flush.zero_()
+    e0.record()
+    geom = pointcloud.PointCloud(xt, yt, epsilon=0.01, relative_epsilon="mean")
+    out = linear.solve(geom, threshold=1e-3, precision=args.precision)
+    loss = (out.f.double() * w).sum() + (out.g.double() * v).sum()
+    e1.record()
+    loss.backward()
+    e2.record()
+    e2.synchronize()
+    return e0.elapsed_time(e1), e1.elapsed_time(e2), out, geom, dict(imp.last_solve_info)
+
+  for _ in range(args.warmup):
+    step()
+  clocks = ClockSampler(0)
+  clocks.start()
+  fw, bw = [], []
+  for _ in range(args.steps):
+    a_, b_, out, geom, info = step()
+    fw.append(a_)
+    bw.append(b_)
+  clk = clocks.stop()
+  fwd_s = statistics.median(fw) * 1e-3
+  bwd_s = statistics.median(bw) * 1e-3
+  # one single-vector application (the CG steps' launch), timed alone
+  f, g = out.f.detach(), out.g.detach()
+  vec = torch.randn(1, n, device="cuda")
+  for _ in range(3):
+    geom._apply_raw(f, g, vec, 1)
+  e0, e1 = ev(), ev()
+  reps = 20
+  e0.record()
+  for _ in range(reps):
+    geom._apply_raw(f, g, vec, 1)
+  e1.record()
+  e1.synchronize()
+  t_app = e0.elapsed_time(e1) / reps * 1e-3
+  flops_app = float(n) * n * (2 * d + 2)
+  steps = int(info.get("steps", 0))
+  n_app1 = 2 * steps + 4
+  roof = {"bound": "fp32_fma", "kernel": "apply_transport_kernel (one vector)",
+          "achieved": flops_app / t_app / 1e12, "peak": 2 * peaks["ffma_per_s"] / 1e12,
+          "unit": "TFLOP/s", "frac": flops_app / t_app / (2 * peaks["ffma_per_s"]),
+          "work_per_launch": f"{flops_app:.4g} flops (n*m*(2d+2))",
+          "peak_source": "measured in bench.py (FFMA probe kernel)"}
+  line = {
+      "metric": "s per gradient through the Sinkhorn potentials (implicit differentiation)",
+      "value": fwd_s + bwd_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
+      "workload": "implicit", "dtype": "f32 (backward), bf16x3/f32 (solve)",
+      "data": "synthetic", "steps": args.steps, "warmup": args.warmup,
+      "config": {"workload": f"grad of <w,f>+<v,g> through linear.solve, n=m={n} d={d} "
+                             "x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, "
+                             "eps=0.01*mean(C), thr=1e-3",
+                 "l2": "flushed before each step (256 MiB write)"},
+      "forward_s": fwd_s, "backward_s": bwd_s, "n_iters": out.n_iters,
+      "cg_steps": steps, "cg_rel_residual": info.get("rel_residual"),
+      "single_vector_applications": n_app1,
+      "single_vector_application_s": t_app,
+      "backward_share_in_single_vector_applications": n_app1 * t_app / bwd_s,
+      "roofline": roof, "clocks": clk,
+  }
+  print(json.dumps(line))
+  return 0
+
+
 def main():
   args = parse_args()
   if args.warmup < 3:
@@ -834,6 +928,8 @@ def main():
     return run_anneal(args)
   if args.workload == "divergence":
     return run_divergence(args)
+  if args.workload == "implicit":
+    return run_implicit(args)
   return run_ours(args)
 
 

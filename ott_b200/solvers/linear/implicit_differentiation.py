@@ -37,20 +37,27 @@ __all__ = ["ImplicitDiff", "solve_jax_cg", "solve_normal_cg"]
 LinOp = Callable[[torch.Tensor], torch.Tensor]
 
 
+# Steps and final relative residual of the last conjugate-gradient solve in
+# this process (introspection only; nothing reads it back).
+last_solve_info: Dict[str, float] = {}
+
+
 def _cg(op: LinOp, rhs: torch.Tensor, stop: Callable[[torch.Tensor], bool],
         max_steps: int, stall: int = 0) -> torch.Tensor:
   """Conjugate gradients from zero for a symmetric positive semi-definite
   ``op``; ``stop(residual)`` ends it. ``stall > 0`` also ends it after
   that many steps without a new smallest residual (the FP32 plan
   applications put a floor under the residual)."""
+  bnorm = max(float(torch.linalg.vector_norm(rhs)), 1e-300)
   x = torch.zeros_like(rhs)
   r = rhs.clone()
+  last_solve_info.update(steps=0, rel_residual=1.0)
   if stop(r):
     return x
   p = r.clone()
   rr = torch.dot(r, r)
   best, since, best_x = float("inf"), 0, x
-  for _ in range(max_steps):
+  for step in range(1, max_steps + 1):
     ap = op(p)
     pap = torch.dot(p, ap)
     if float(pap) <= 0.0:
@@ -58,14 +65,16 @@ def _cg(op: LinOp, rhs: torch.Tensor, stop: Callable[[torch.Tensor], bool],
     alpha = rr / pap
     x = x + alpha * p
     r = r - alpha * ap
+    rn = float(torch.linalg.vector_norm(r))
+    last_solve_info.update(steps=step, rel_residual=rn / bnorm)
     if stop(r):
       return x
-    rn = float(torch.linalg.vector_norm(r))
     if rn < best:
       best, since, best_x = rn, 0, x
     else:
       since += 1
       if stall and since >= stall:
+        last_solve_info.update(rel_residual=best / bnorm)
         return best_x
     rr_new = torch.dot(r, r)
     p = r + (rr_new / rr) * p
@@ -190,6 +199,10 @@ class ImplicitDiff:
             g: torch.Tensor, lse_mode: bool = True) -> torch.Tensor:
     """implicit_differentiation.py:80-233: ``-(dF/d(f, g))^-T gr`` for the
     first-order conditions ``F`` (float64, length n + m)."""
+    return self._solve(gr, ot_prob, f, g, lse_mode)[0]
+
+  def _solve(self, gr, ot_prob, f, g, lse_mode):
+    """``solve`` and the plan's marginals ``(P 1, P^T 1)`` it used."""
     self._check(ot_prob, lse_mode)
     geom = ot_prob.geom
     n, m = geom.shape
@@ -207,7 +220,7 @@ class ImplicitDiff:
     else:
       lf, lg = self._solve_generic(geom, gr_f, gr_g, ma, mb, sa, sb, app, n > m)
     zero = torch.zeros((), dtype=torch.float64, device=dev)
-    return torch.cat([torch.where(sa, -lf, zero), torch.where(sb, -lg, zero)])
+    return torch.cat([torch.where(sa, -lf, zero), torch.where(sb, -lg, zero)]), ma, mb
 
   def _solve_default(self, gr_f, gr_g, ma, mb, sa, sb, app, n_gt_m):
     kw = dict(self.solver_kwargs or {})
@@ -283,15 +296,12 @@ class ImplicitDiff:
     ``lam = solve(gr)`` pulled back through the first-order conditions at
     fixed ``f, g`` (``d h(P 1)_i / dP_ij = h'(P 1)_i``, ``dP_ij/dC_ij =
     -P_ij / eps``; ``d/da_i = -lam_i h'(a_i)`` on ``a > 0``)."""
-    lam = self.solve(gr, prob, f, g, lse_mode)
+    lam, ma, mb = self._solve(gr, prob, f, g, lse_mode)
     geom = prob.geom
     n, m = geom.shape
     dev = f.device
     la, lb = lam[:n], lam[n:]
     a, b = prob.a.detach().double(), prob.b.detach().double()
-    app = self._app(geom, f, g)
-    ma = app(torch.ones(m, dtype=torch.float64, device=dev), 1)
-    mb = app(torch.ones(n, dtype=torch.float64, device=dev), 0)
     zero = torch.zeros((), dtype=torch.float64, device=dev)
     sa, sb = (a > 0) & (ma > 0), (b > 0) & (mb > 0)
     one = lambda v, s: torch.where(s, v, torch.ones_like(v))
