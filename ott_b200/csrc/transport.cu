@@ -269,6 +269,175 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
   }
 }
 
+// One or two vectors (the conjugate-gradient steps of implicit
+// differentiation apply the plan to one vector at a time): each thread
+// multiplies its 8 x 8 weights by its 8 columns' vector entries in
+// registers, and the 16 threads of a row add their partial sums at the
+// end. No P tile goes through shared memory, so two CTAs share an SM up to
+// d = 64 and one CTA's tile loads overlap the other's arithmetic.
+template <int DP, int KD>
+struct DirectSmem {
+  static constexpr int kPad = DP <= 64 ? 4 : 0;
+  float As[DP][kTR + kPad];   // A tile, transposed, centred
+  float Bs[DP][kTC + kPad];   // B tile, transposed, centred
+  float Vs[KD][kTC];          // vector entries of the tile's B points
+  float wb[kTC];              // (potB - inv |B|^2) * log2e / eps
+  float center[DP];
+};
+
+template <int DP, int KD>
+__global__ void __launch_bounds__(256, (DP <= 64 ? 2 : 1)) apply_direct_kernel(ApplyArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DirectSmem<DP, KD>& sm = *reinterpret_cast<DirectSmem<DP, KD>*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  const int64_t row0 = (int64_t)blockIdx.x * kTR;
+  const float s = 2.f * p.inv * p.ws;
+
+  apply_center<DP>(p, sm.center);
+  __syncthreads();
+  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
+    const int r = idx / DP, k = idx % DP;
+    const int64_t gr = row0 + r;
+    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
+  }
+  __syncthreads();
+  float u[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    float nrm = 0.f;
+    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
+    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
+  }
+
+  float mrow[8];
+  float o[8][KD];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    mrow[i] = kNegSentinel;
+#pragma unroll
+    for (int j = 0; j < KD; ++j) o[i][j] = 0.f;
+  }
+
+  const int64_t ntiles_all = (p.C + kTC - 1) / kTC;
+  const int64_t t_begin = ntiles_all * blockIdx.z / p.splits;
+  const int64_t t_end = ntiles_all * (blockIdx.z + 1) / p.splits;
+  for (int64_t t = t_begin; t < t_end; ++t) {
+    const int64_t c0 = t * kTC;
+    __syncthreads();  // previous tile's Bs / Vs / wb consumed
+    for (int idx = tid; idx < DP * kTC; idx += blockDim.x) {
+      const int c = idx / DP, k = idx % DP;
+      const int64_t gc = c0 + c;
+      sm.Bs[k][c] = (gc < p.C && k < p.d) ? p.B[gc * p.d + k] - sm.center[k] : 0.f;
+    }
+    for (int idx = tid; idx < KD * kTC; idx += blockDim.x) {
+      const int kk = idx / kTC, c = idx % kTC;
+      const int64_t gc = c0 + c;
+      sm.Vs[kk][c] = (gc < p.C && kk < p.K) ? __ldg(p.vec + (int64_t)kk * p.C + gc) : 0.f;
+    }
+    __syncthreads();
+    if (tid < kTC) {
+      const int64_t gc = c0 + tid;
+      float nrm = 0.f;
+      for (int k = 0; k < DP; ++k) nrm = fmaf(sm.Bs[k][tid], sm.Bs[k][tid], nrm);
+      sm.wb[tid] = gc < p.C ? (__ldg(p.potB + gc) - p.inv * nrm) * p.ws : -INFINITY;
+    }
+    __syncthreads();
+
+    float z[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < DP; ++k) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[k][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[k][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
+    }
+    float vv[KD][8];
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk) {
+      const float4 v0 = *reinterpret_cast<const float4*>(&sm.Vs[kk][tx * 4]);
+      const float4 v1 = *reinterpret_cast<const float4*>(&sm.Vs[kk][64 + tx * 4]);
+      vv[kk][0] = v0.x; vv[kk][1] = v0.y; vv[kk][2] = v0.z; vv[kk][3] = v0.w;
+      vv[kk][4] = v1.x; vv[kk][5] = v1.y; vv[kk][6] = v1.z; vv[kk][7] = v1.w;
+    }
+    {
+      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[tx * 4]);
+      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[64 + tx * 4]);
+      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
+                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (mx > mrow[i]) {
+        const float sc = ex2_approx(mrow[i] - mx);
+#pragma unroll
+        for (int kk = 0; kk < KD; ++kk) o[i][kk] *= sc;
+        mrow[i] = mx;
+      }
+      float e[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(z[i][j] - mrow[i]);
+#pragma unroll
+      for (int kk = 0; kk < KD; ++kk) {
+        float part = e[0] * vv[kk][0];
+#pragma unroll
+        for (int j = 1; j < 8; ++j) part = fmaf(e[j], vv[kk][j], part);
+        o[i][kk] += part;
+      }
+    }
+  }
+
+  // the 16 threads of a row hold partial sums with the same shift
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk)
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        o[i][kk] += __shfl_xor_sync(0xffffffffu, o[i][kk], off);
+  if (tx != 0) return;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    if (gr >= p.R) continue;
+    const bool any = mrow[i] > kNegSentinel;
+    if (p.splits > 1) {
+      const int64_t sp = blockIdx.z;
+      p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
+#pragma unroll
+      for (int kk = 0; kk < KD; ++kk)
+        if (kk < p.K) p.part_o[(sp * p.K + kk) * p.R + gr] = any ? o[i][kk] : 0.f;
+      continue;
+    }
+    const float scale = any ? exp2f(mrow[i]) : 0.f;
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk)
+      if (kk < p.K) p.out[(int64_t)kk * p.R + gr] = any ? o[i][kk] * scale : 0.f;
+  }
+}
+
 // out[k][r] = sum_s part_o[s][k][r] 2^(part_m[s][r] - M) 2^M, M = max_s part_m.
 __global__ void combine_splits_kernel(ApplyArgs p) {
   const int64_t total = (int64_t)p.K * p.R;
@@ -333,20 +502,57 @@ int launch_apply_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }
 
+template <int DP, int KD>
+int launch_direct(const ApplyArgs& a, cudaStream_t stream) {
+  const size_t smem = sizeof(DirectSmem<DP, KD>);
+  auto k = apply_direct_kernel<DP, KD>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return OTTB_ERR_CUDA;
+  dim3 grid((unsigned)((a.R + kTR - 1) / kTR), 1u, (unsigned)a.splits);
+  k<<<grid, 256, smem, stream>>>(a);
+  if (a.splits > 1) {
+    const int64_t total = (int64_t)a.K * a.R;
+    combine_splits_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 4096), 256, 0,
+                            stream>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+// Up to this many vectors take the register path (apply_direct_kernel).
+constexpr int kDirectMax = 2;
+
 // Vector chunks of a call: the fewest chunks of at most 16 * max_vt
-// vectors.
+// vectors (one for the register path).
 int apply_chunks(int d, int K) {
+  if (K <= kDirectMax) return 1;
   const int vm = d > 64 ? 4 : 5;
   return (K + 16 * vm - 1) / (16 * vm);
 }
 
-// Column splits: enough CTAs for two waves of one CTA per SM, at most one
-// tile of B points per split and at most 16 splits.
+// Column splits (at most 16, at least one tile of B points each): the count
+// that minimises waves x (tiles per CTA + 1), the launch's time when every
+// CTA slot (two per SM on the register path up to d = 64, else one) runs
+// at the same speed and a CTA's set-up (centre, A tile, norms, output)
+// costs about one tile; more splits only for a 3 % gain. This fills the
+// last wave: n = m = 65536 takes 4 splits (7 waves of 128 tiles) instead
+// of 2 (4 waves of 256), n = m = 8192 takes 4 (one wave of 16 tiles).
 int apply_splits(int64_t R, int64_t C, int d, int K, int sms) {
   const int64_t units = ((R + kTR - 1) / kTR) * apply_chunks(d, K);
-  const int64_t want = (2 * (int64_t)sms + units - 1) / units;
+  const int64_t per_sm = (K <= kDirectMax && d <= 64) ? 2 : 1;
+  const int64_t slots = per_sm * (int64_t)sms;
   const int64_t tiles = (C + kTC - 1) / kTC;
-  return (int)std::max<int64_t>(1, std::min<int64_t>(std::min<int64_t>(want, tiles), 16));
+  const int64_t smax = std::max<int64_t>(1, std::min<int64_t>(tiles, 16));
+  int64_t best = 1, best_t = -1;
+  for (int64_t s = 1; s <= smax; ++s) {
+    const int64_t waves = (units * s + slots - 1) / slots;
+    const int64_t t = waves * ((tiles + s - 1) / s + 1);
+    if (best_t < 0 || 100 * t < 97 * best_t) {
+      best_t = t;
+      best = s;
+    }
+  }
+  return (int)best;
 }
 
 size_t apply_workspace(int64_t R, int K, int splits) {
@@ -365,6 +571,8 @@ int device_sms() {
 // vectors-per-thread count that covers a chunk.
 template <int DP>
 int launch_apply(const ApplyArgs& a, cudaStream_t stream) {
+  if (a.K == 1) return launch_direct<DP, 1>(a, stream);
+  if (a.K == 2) return launch_direct<DP, 2>(a, stream);
   constexpr int VM = max_vt<DP>();
   const int chunks = (a.K + 16 * VM - 1) / (16 * VM);
   const int per = (a.K + chunks - 1) / chunks;

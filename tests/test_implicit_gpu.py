@@ -214,3 +214,48 @@ def test_apply_and_matrix_gradients_match_dense_autograd(axis, scale):
   want_m = torch.autograd.grad((p * dc.double().cpu()).sum(), leaves[:4])
   for u, v, key in zip(got_m, want_m, "xyfg"):
     assert _rel(u, v.numpy()) < 5e-5, key
+
+
+@pytest.mark.parametrize("n,d", [(8192, 64), (16384, 8)])
+def test_solver_converges_at_scale(n, d):
+  """Shapes where conjugate gradients' residual rose for tens of steps
+  (stopping tests on it misfire): MINRES reaches the tolerance with no
+  warning and finite gradients. The residual recomputed with the FP32 plan
+  products stays within 2e-3: their rounding (exponents up to ~500 at
+  d = 8 here) times the system's conditioning sets that floor."""
+  import warnings
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  x, y, _, _ = problems.gaussian_shift_problem(n, n, d, seed=0)
+  xt = torch.from_numpy(x).cuda().requires_grad_()
+  geom = pointcloud.PointCloud(xt, torch.from_numpy(y).cuda(), epsilon=0.01,
+                               relative_epsilon="mean")
+  out = linear.solve(geom, threshold=1e-3)
+  rng = np.random.default_rng(0)
+  w = torch.from_numpy(rng.standard_normal(n)).cuda()
+  v = torch.from_numpy(rng.standard_normal(n)).cuda()
+  v += (w.sum() - v.sum()) / n
+  with warnings.catch_warnings():
+    warnings.simplefilter("error", RuntimeWarning)
+    ((out.f.double() * w).sum() + (out.g.double() * v).sum()).backward()
+  info = imp.last_solve_info
+  assert info["rel_residual"] <= 1e-6 and info["true_rel_residual"] <= 2e-3, info
+  assert torch.isfinite(xt.grad).all()
+
+
+def test_solver_budget_exhaustion_warns():
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  x, y, a, b = problems.uniform_cloud_problem(300, 200, 4, seed=20)
+  geom = pointcloud.PointCloud(_t(x), _t(y), epsilon=0.02)
+  out = linear.solve(geom, _t(a), _t(b), threshold=1e-5)
+  prob = linear_problem.LinearProblem(geom, _t(a), _t(b))
+  gr = (torch.randn(300, dtype=torch.float64, device="cuda"),
+        torch.randn(200, dtype=torch.float64, device="cuda"))
+  with pytest.warns(RuntimeWarning, match="MINRES stopped"):
+    imp.ImplicitDiff(solver_kwargs={"max_steps": 2}).solve(gr, prob, out.f, out.g)

@@ -52,20 +52,39 @@ def test_jax_cg_normal_operator_and_ridge():
   np.testing.assert_allclose((op @ x).numpy(), b.numpy(), atol=1e-9)
 
 
-def test_cg_stall_returns_best_iterate():
-  """With a stall limit, CG stops after that many steps without a new
-  smallest residual and returns the best iterate seen."""
-  a = _spd(12, 4)
-  b = torch.as_tensor(np.random.default_rng(5).standard_normal(12))
-  calls = []
+def test_minres_solves_spd_and_singular_systems():
+  """MINRES: an SPD system to the tolerance; a consistent singular one
+  (null vector removed from the right-hand side) to the solution
+  orthogonal to the null space; the residual estimate never increases."""
+  rng = np.random.default_rng(6)
+  a = _spd(40, 7)
+  b = torch.as_tensor(rng.standard_normal(40))
+  x = imp._minres(lambda z: a @ z, b, 1e-12, 500)
+  np.testing.assert_allclose((a @ x).numpy(), b.numpy(), atol=1e-9)
+  assert imp.last_solve_info["true_rel_residual"] < 1e-10
+  q, _ = np.linalg.qr(rng.standard_normal((30, 30)))
+  lam = np.concatenate([[0.0], rng.uniform(0.01, 1.0, 29)])
+  s = torch.as_tensor(q @ np.diag(lam) @ q.T)
+  rhs = torch.as_tensor(q[:, 1:] @ rng.standard_normal(29))
+  hist = []
 
   def op(z):
-    calls.append(1)
-    return a @ z
+    hist.append(1)
+    return s @ z
 
-  x = imp._cg(op, b, lambda r: False, max_steps=500, stall=5)
-  assert len(calls) < 500
-  np.testing.assert_allclose((a @ x).numpy(), b.numpy(), atol=1e-8)
+  x = imp._minres(op, rhs, 1e-12, 500)
+  want = np.linalg.lstsq(s.numpy(), rhs.numpy(), rcond=1e-10)[0]
+  np.testing.assert_allclose(x.numpy(), want, atol=1e-8 * np.abs(want).max())
+
+
+def test_minres_step_limit_reports_residual():
+  a = _spd(40, 8)
+  b = torch.as_tensor(np.random.default_rng(9).standard_normal(40))
+  x = imp._minres(lambda z: a @ z, b, 1e-14, 3)
+  info = imp.last_solve_info
+  assert info["steps"] == 3 and info["rel_residual"] > 1e-6
+  true = float(torch.linalg.vector_norm(b - a @ x) / torch.linalg.vector_norm(b))
+  assert abs(info["true_rel_residual"] - true) < 1e-12
 
 
 def test_implicit_diff_fields_and_replace():

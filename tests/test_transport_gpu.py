@@ -142,3 +142,28 @@ def test_column_splits_match_single_pass():
     res.append(o.cpu().numpy())
   scale = np.abs(res[0]).max()
   np.testing.assert_allclose(res[1], res[0], rtol=0, atol=1e-5 * scale)
+
+
+@pytest.mark.parametrize("n,m,d,k", [(130, 5000, 3, 1), (1000, 700, 64, 2), (257, 129, 128, 1),
+                                     (5000, 300, 16, 2), (64, 64, 8, 1)])
+def test_one_and_two_vector_applications_match_oracle(n, m, d, k):
+  """The register path for one or two vectors (column splits when the rows
+  alone underfill the GPU) against the float64 plan at the same potentials."""
+  import torch
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + m + d)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon))
+  p_ref = o.transport_matrix(f, g, og)
+  zmax = (np.abs(f).max() + np.abs(g).max() + og.cost_block().max()) / og.epsilon
+  rel = max(1e-5, 8 * 2.0 ** -24 * zmax)
+  rng = np.random.default_rng(k)
+  for axis in (0, 1):
+    vec = rng.standard_normal((k, n if axis == 0 else m))
+    got = out.apply(torch.as_tensor(vec, dtype=torch.float32).cuda(), axis=axis)
+    want = vec @ p_ref if axis == 0 else vec @ p_ref.T
+    for r in range(k):
+      np.testing.assert_allclose(got[r].cpu().numpy(), want[r], rtol=0,
+                                 atol=rel * np.abs(want[r]).max())
