@@ -825,10 +825,11 @@ def run_implicit(args):
   """Gradient through the potentials of the headline problem (Gaussian-shift
   clouds, n = m = ``--n``, d = ``--d``, uniform weights, epsilon = 0.01 *
   mean(C), threshold 1e-3): the solve (chosen precision), then the backward
-  of ``<w, f> + <v, g>`` (sum w = sum v) by implicit differentiation. The
-  backward applies the plan 2 x (CG steps) + 4 times to one vector (the
-  marginals, the right-hand side, the other side's multiplier) and twice to
-  2 (d + 2) and 2 (d + 1) vectors (the pullback to the points)."""
+  of ``<w, f> + <v, g>`` (sum w = sum v) by implicit differentiation. Its
+  MINRES steps apply the plan to one vector twice each; with the chosen
+  precision at d >= 32 each such product is two zero-iteration solves on
+  the tensor-core sweep (``ottb_apply_transport_sweep``). Also reported:
+  the same gradient with the solve and the backward in FP32."""
   import torch
   from ott_b200.geometry import pointcloud
   from ott_b200.solvers import linear
@@ -846,68 +847,94 @@ def run_implicit(args):
   ev = lambda: torch.cuda.Event(enable_timing=True)
   flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
 
-  def step():
+  def step(precision):
     xt.grad = None
     yt.grad = None
     e0, e1, e2 = ev(), ev(), ev()
     flush.zero_()
     e0.record()
     geom = pointcloud.PointCloud(xt, yt, epsilon=0.01, relative_epsilon="mean")
-    out = linear.solve(geom, threshold=1e-3, precision=args.precision)
+    out = linear.solve(geom, threshold=1e-3, precision=precision)
     loss = (out.f.double() * w).sum() + (out.g.double() * v).sum()
     e1.record()
     loss.backward()
     e2.record()
     e2.synchronize()
-    return e0.elapsed_time(e1), e1.elapsed_time(e2), out, geom, dict(imp.last_solve_info)
+    return (e0.elapsed_time(e1), e1.elapsed_time(e2), out, geom, dict(imp.last_solve_info),
+            xt.grad.clone())
 
   for _ in range(args.warmup):
-    step()
+    step(args.precision)
   clocks = ClockSampler(0)
   clocks.start()
   fw, bw = [], []
   for _ in range(args.steps):
-    a_, b_, out, geom, info = step()
+    a_, b_, out, geom, info, grad = step(args.precision)
     fw.append(a_)
     bw.append(b_)
   clk = clocks.stop()
   fwd_s = statistics.median(fw) * 1e-3
   bwd_s = statistics.median(bw) * 1e-3
-  # one single-vector application (the CG steps' launch), timed alone
+  pf, pb, pout, _, pinfo, pgrad = step("fp32")
+  grad_diff = float((grad - pgrad).abs().max() / pgrad.abs().max())
+  # one single-vector product of the backward, timed alone, in both forms
   f, g = out.f.detach(), out.g.detach()
   vec = torch.randn(1, n, device="cuda")
-  for _ in range(3):
-    geom._apply_raw(f, g, vec, 1)
-  e0, e1 = ev(), ev()
-  reps = 20
-  e0.record()
-  for _ in range(reps):
-    geom._apply_raw(f, g, vec, 1)
-  e1.record()
-  e1.synchronize()
-  t_app = e0.elapsed_time(e1) / reps * 1e-3
-  flops_app = float(n) * n * (2 * d + 2)
+
+  def time_app(prec, reps=20):
+    for _ in range(3):
+      geom._apply_raw(f, g, vec, 1, prec)
+    e0, e1 = ev(), ev()
+    e0.record()
+    for _ in range(reps):
+      geom._apply_raw(f, g, vec, 1, prec)
+    e1.record()
+    e1.synchronize()
+    return e0.elapsed_time(e1) / reps * 1e-3
+
+  tc = args.precision == "bf16_split3" or (args.precision == "auto" and d >= 32)
+  t_app = time_app(args.precision)
+  t_app32 = time_app("fp32")
   steps = int(info.get("steps", 0))
   n_app1 = 2 * steps + 4
-  roof = {"bound": "fp32_fma", "kernel": "apply_transport_kernel (one vector)",
-          "achieved": flops_app / t_app / 1e12, "peak": 2 * peaks["ffma_per_s"] / 1e12,
-          "unit": "TFLOP/s", "frac": flops_app / t_app / (2 * peaks["ffma_per_s"]),
-          "work_per_launch": f"{flops_app:.4g} flops (n*m*(2d+2))",
-          "peak_source": "measured in bench.py (FFMA probe kernel)"}
+  if tc:
+    # two sweeps of n x m entries (v+ and v-), one exponential per entry
+    ach = 2.0 * n * n / t_app / 1e9
+    roof = {"bound": "mufu_ex2", "kernel": "sinkhorn persistent sweep (2 zero-iteration "
+                                            "solves per product)",
+            "achieved": ach, "peak": peaks["ex2_per_s"] / 1e9, "unit": "Gex2/s",
+            "frac": ach / (peaks["ex2_per_s"] / 1e9),
+            "work_per_launch": f"{2.0 * n * n:.4g} cost entries (2 sweeps of n*m)",
+            "peak_source": "measured in bench.py (MUFU ex2 probe kernel)"}
+  else:
+    flops_app = float(n) * n * (2 * d + 2)
+    roof = {"bound": "fp32_fma", "kernel": "apply_direct_kernel (one vector)",
+            "achieved": flops_app / t_app / 1e12, "peak": 2 * peaks["ffma_per_s"] / 1e12,
+            "unit": "TFLOP/s", "frac": flops_app / t_app / (2 * peaks["ffma_per_s"]),
+            "work_per_launch": f"{flops_app:.4g} flops (n*m*(2d+2))",
+            "peak_source": "measured in bench.py (FFMA probe kernel)"}
+  flops32 = float(n) * n * (2 * d + 2)
   line = {
       "metric": "s per gradient through the Sinkhorn potentials (implicit differentiation)",
       "value": fwd_s + bwd_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
-      "workload": "implicit", "dtype": "f32 (backward), bf16x3/f32 (solve)",
+      "workload": "implicit", "dtype": "bf16x3/f32" if tc else "f32",
       "data": "synthetic", "steps": args.steps, "warmup": args.warmup,
       "config": {"workload": f"grad of <w,f>+<v,g> through linear.solve, n=m={n} d={d} "
                              "x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, "
                              "eps=0.01*mean(C), thr=1e-3",
                  "l2": "flushed before each step (256 MiB write)"},
       "forward_s": fwd_s, "backward_s": bwd_s, "n_iters": out.n_iters,
-      "cg_steps": steps, "cg_rel_residual": info.get("rel_residual"),
-      "single_vector_applications": n_app1,
-      "single_vector_application_s": t_app,
-      "backward_share_in_single_vector_applications": n_app1 * t_app / bwd_s,
+      "minres_steps": steps, "minres_rel_residual": info.get("rel_residual"),
+      "recomputed_rel_residual": info.get("true_rel_residual"),
+      "single_vector_products": n_app1, "single_vector_product_s": t_app,
+      "backward_share_in_single_vector_products": n_app1 * t_app / bwd_s,
+      "plain_fp32": {"forward_s": pf * 1e-3, "backward_s": pb * 1e-3,
+                     "minres_steps": int(pinfo.get("steps", 0)),
+                     "single_vector_product_s": t_app32,
+                     "single_vector_product_frac_of_ffma_peak":
+                         flops32 / t_app32 / (2 * peaks["ffma_per_s"])},
+      "grad_rel_diff_vs_fp32": grad_diff,
+      "speedup_backward_vs_plain_fp32": pb * 1e-3 / bwd_s,
       "roofline": roof, "clocks": clk,
   }
   print(json.dumps(line))

@@ -183,6 +183,25 @@ int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t 
                              int32_t axis, float* out, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* The same application (geometry/geometry.py:444-486) on the solver's sweep
+ * engine: tcgen05 BF16 split-3 products for d >= 32 under
+ * OTTB_PRECISION_AUTO or _BF16_SPLIT3, FP32 otherwise. Each vector becomes two
+ * zero-iteration solves whose final marginal sweep sums
+ * exp((f_i + eps log(+-v_i) + g_j - C_ij) / eps) over i (axis 0; axis 1 swaps
+ * the point sets); all 2 * num_vec run in one persistent launch and the two
+ * sums are subtracted. Used for the one-vector products of the implicit
+ * backward (implicit_differentiation.py:173-185, app_transport) when the
+ * solve ran on the tensor cores. The workspace (size from
+ * ottb_apply_transport_sweep_workspace_size, 256-byte aligned) is required. */
+size_t ottb_apply_transport_sweep_workspace_size(int64_t n, int64_t m, int32_t d,
+                                                 int32_t num_vec, int32_t axis,
+                                                 int32_t precision);
+int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, int64_t m,
+                                   int32_t d, const float* f, const float* g, float epsilon,
+                                   float inv_scale_cost, const float* vec, int32_t num_vec,
+                                   int32_t axis, int32_t precision, float* out,
+                                   void* workspace, size_t workspace_bytes, void* stream);
+
 /* The plan itself, out [n][m] row-major (geometry/geometry.py:361-365,
  * transport_from_potentials; sinkhorn.py:346-349, SinkhornOutput.matrix). */
 int32_t ottb_transport_matrix(const float* x, const float* y, int64_t n, int64_t m,

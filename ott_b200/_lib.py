@@ -34,6 +34,8 @@ EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_autotune",
     "ottb_apply_transport_workspace_size",
     "ottb_apply_transport",
+    "ottb_apply_transport_sweep_workspace_size",
+    "ottb_apply_transport_sweep",
     "ottb_transport_matrix",
     "ottb_cost_stats_workspace_size",
     "ottb_cost_stats",
@@ -174,6 +176,11 @@ def load() -> ctypes.CDLL:
     lib.ottb_apply_transport.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, i32,
                                          i32, vp, vp, sz, vp]
     lib.ottb_apply_transport.restype = i32
+    lib.ottb_apply_transport_sweep_workspace_size.argtypes = [i64, i64, i32, i32, i32, i32]
+    lib.ottb_apply_transport_sweep_workspace_size.restype = sz
+    lib.ottb_apply_transport_sweep.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp,
+                                               i32, i32, i32, vp, vp, sz, vp]
+    lib.ottb_apply_transport_sweep.restype = i32
     lib.ottb_transport_matrix.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, vp]
     lib.ottb_transport_matrix.restype = i32
     lib.ottb_cost_stats_workspace_size.argtypes = [i64, i64, i32]

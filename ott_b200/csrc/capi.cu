@@ -427,7 +427,8 @@ int outer_of(const ottb_solver_cfg* cfg) {
 // Writes the call header (tables, tensor maps, schedule, initial state)
 // into the pristine region of the workspace: one host-to-device copy.
 int write_header(const ottb_problem* problems, int num_problems, const ottb_solver_cfg* cfg,
-                 const Plan& plan, char* ws, cudaStream_t stream) {
+                 const Plan& plan, char* ws, cudaStream_t stream,
+                 float* const* marg_out = nullptr) {
   const int outer = outer_of(cfg);
   std::vector<char> host(plan.header_bytes, 0);
   Sched* sched = (Sched*)(host.data() + plan.off_sched);
@@ -485,6 +486,7 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     P.uid = plan.order[t];
     P.outer = outer;
     P.symmetric = q.symmetric;
+    P.marg_out = marg_out ? marg_out[plan.order[t]] : nullptr;
     pd[t] = P;
     ps[t].active = 1;
     ps[t].split_f = pp.split_f;
@@ -601,6 +603,119 @@ int plan_for_call(const ottb_problem* problems, int32_t num_problems, int32_t d,
   if (st != OTTB_OK) return st;
   if (!workspace || workspace_bytes < plan.total) return OTTB_ERR_WORKSPACE;
   if (((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  return OTTB_OK;
+}
+
+// ---------------------------------------------------------------------------
+// The plan applied to vectors through the solver's sweep engine.
+//
+// A solve with max_iterations = 0 keeps its initial potentials and runs one
+// evaluation sweep, whose column marginal is
+//   sum_i exp((f'_i + g_j - C_ij) / eps).
+// With f'_i = f_i + eps log v_i that is (P^T v)_j for a vector v >= 0, so a
+// signed vector is two such problems (v+ and v-), and K vectors are 2K
+// problems in one launch. Axis 1 (P v over the columns) swaps the roles of
+// the point sets. The sweep is the solver's: tcgen05 BF16 split-3 for d >= 32
+// under OTTB_PRECISION_AUTO / BF16_SPLIT3, FP32 otherwise.
+// ---------------------------------------------------------------------------
+struct SweepApply {
+  int64_t R = 0;  // points summed over (rows of each problem's x)
+  int64_t C = 0;  // points of the output (each problem's y)
+  int K = 0;
+  ottb_solver_cfg cfg{};
+  Plan plan;
+  size_t off_fp = 0, off_fo = 0, off_go = 0, off_wa = 0, off_wb = 0, off_err = 0,
+         off_marg = 0, off_res = 0, total = 0;
+};
+
+__global__ void sweep_apply_potential_kernel(const float* pot, const float* vec, int64_t R,
+                                             int K, float eps, float* fp) {
+  const int64_t total = (int64_t)2 * K * R;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t q = idx / R, i = idx % R;
+    const int k = (int)(q >> 1);
+    const float v = vec[(int64_t)k * R + i];
+    const float w = (q & 1) ? -v : v;
+    fp[idx] = w > 0.f ? pot[i] + eps * logf(w) : -INFINITY;
+  }
+}
+
+__global__ void fill_kernel(float* p, int64_t n, float v) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    p[i] = v;
+}
+
+__global__ void sweep_apply_diff_kernel(const float* marg, int64_t C, int K, float* out) {
+  const int64_t total = (int64_t)K * C;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx / C, j = idx % C;
+    out[idx] = marg[(2 * k) * C + j] - marg[(2 * k + 1) * C + j];
+  }
+}
+
+// Problem records, configuration and workspace layout; with ws null only
+// the sizes are meaningful.
+int sweep_apply_setup(const float* x, const float* y, int64_t n, int64_t m, int d,
+                      const float* f, const float* g, float eps, float inv, int K, int axis,
+                      int precision, char* ws, bool need_grid, SweepApply& S,
+                      std::vector<ottb_problem>& probs, std::vector<float*>& marg) {
+  S.R = axis == 0 ? n : m;
+  S.C = axis == 0 ? m : n;
+  S.K = K;
+  ottb_solver_cfg& c = S.cfg;
+  std::memset(&c, 0, sizeof(c));
+  c.threshold = 1e-3f;
+  c.norm_error = 1;
+  c.inner_iterations = 1;
+  c.min_iterations = 0;
+  c.max_iterations = 0;
+  c.eps_init = 1.f;
+  c.eps_decay = 1.f;
+  c.precision = precision;
+  const int np = 2 * K;
+  probs.assign(np, ottb_problem{});
+  marg.assign(np, nullptr);
+  for (int q = 0; q < np; ++q) {
+    ottb_problem& P = probs[q];
+    P.x = axis == 0 ? x : y;
+    P.y = axis == 0 ? y : x;
+    P.n = S.R;
+    P.m = S.C;
+    P.epsilon = eps;
+    P.inv_scale_cost = inv;
+  }
+  int st = make_plan(probs.data(), np, d, &c, need_grid, S.plan);
+  if (st != OTTB_OK) return st;
+  size_t off = align_up(S.plan.total);
+  auto take = [&](size_t bytes) {
+    const size_t o = off;
+    off = align_up(off + bytes);
+    return o;
+  };
+  S.off_fp = take(sizeof(float) * np * S.R);
+  S.off_fo = take(sizeof(float) * np * S.R);
+  S.off_go = take(sizeof(float) * np * S.C);
+  S.off_wa = take(sizeof(float) * S.R);
+  S.off_wb = take(sizeof(float) * S.C);
+  S.off_err = take(sizeof(float) * np);
+  S.off_marg = take(sizeof(float) * np * S.C);
+  S.off_res = take(sizeof(ottb_result) * np);
+  S.total = off;
+  if (!ws) return OTTB_OK;
+  for (int q = 0; q < np; ++q) {
+    ottb_problem& P = probs[q];
+    P.a = (const float*)(ws + S.off_wa);
+    P.b = (const float*)(ws + S.off_wb);
+    P.f_init = (const float*)(ws + S.off_fp) + (int64_t)q * S.R;
+    P.g_init = axis == 0 ? g : f;
+    P.f = (float*)(ws + S.off_fo) + (int64_t)q * S.R;
+    P.g = (float*)(ws + S.off_go) + (int64_t)q * S.C;
+    P.errors = (float*)(ws + S.off_err) + q;
+    marg[q] = (float*)(ws + S.off_marg) + (int64_t)q * S.C;
+  }
   return OTTB_OK;
 }
 
@@ -740,6 +855,59 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
   std::lock_guard<std::mutex> lock(g_tune_mu);
   tune_cache()[key] = best;
   return OTTB_OK;
+}
+
+size_t ottb_apply_transport_sweep_workspace_size(int64_t n, int64_t m, int32_t d,
+                                                 int32_t num_vec, int32_t axis,
+                                                 int32_t precision) {
+  if (n < 1 || m < 1 || d < 1 || num_vec < 1 || (axis != 0 && axis != 1)) return 0;
+  SweepApply S;
+  std::vector<ottb_problem> probs;
+  std::vector<float*> marg;
+  if (sweep_apply_setup(nullptr, nullptr, n, m, d, nullptr, nullptr, 1.f, 1.f, num_vec, axis,
+                        precision, nullptr, false, S, probs, marg) != OTTB_OK)
+    return 0;
+  return S.total;
+}
+
+int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, int64_t m,
+                                   int32_t d, const float* f, const float* g, float epsilon,
+                                   float inv_scale_cost, const float* vec, int32_t num_vec,
+                                   int32_t axis, int32_t precision, float* out,
+                                   void* workspace, size_t workspace_bytes, void* stream_ptr) {
+  if (!x || !y || !f || !g || !vec || !out || n < 1 || m < 1 || d < 1 || num_vec < 1)
+    return OTTB_ERR_INVALID;
+  if (axis != 0 && axis != 1) return OTTB_ERR_INVALID;
+  if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
+  if (!workspace || ((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  char* ws = (char*)workspace;
+  SweepApply S;
+  std::vector<ottb_problem> probs;
+  std::vector<float*> marg;
+  int st = sweep_apply_setup(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                             precision, ws, true, S, probs, marg);
+  if (st != OTTB_OK) return st;
+  if (workspace_bytes < S.total) return OTTB_ERR_WORKSPACE;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  const int np = 2 * num_vec;
+  const float* pot = axis == 0 ? f : g;
+  const int64_t fp_n = (int64_t)np * S.R;
+  sweep_apply_potential_kernel<<<(unsigned)std::min<int64_t>((fp_n + 255) / 256, 4096), 256, 0,
+                                 stream>>>(pot, vec, S.R, num_vec, epsilon,
+                                           (float*)(ws + S.off_fp));
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.R + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wa), S.R, 1.f / (float)S.R);
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.C + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wb), S.C, 1.f / (float)S.C);
+  if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+  st = write_header(probs.data(), np, &S.cfg, S.plan, ws, stream, marg.data());
+  if (st != OTTB_OK) return st;
+  st = launch_solve(np, d, &S.cfg, (ottb_result*)(ws + S.off_res), S.plan, ws, stream);
+  if (st != OTTB_OK) return st;
+  const int64_t tot = (int64_t)num_vec * S.C;
+  sweep_apply_diff_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
+                            stream>>>((const float*)(ws + S.off_marg), S.C, num_vec, out);
+  return cuda_status(cudaGetLastError());
 }
 
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {

@@ -67,6 +67,7 @@ struct ProbDev {
   int uid;             // index of the problem in the caller's array
   int outer;           // length of errors
   int symmetric;       // x == y, a == b: g-sweeps only, momentum 1/2, f = g
+  float* marg_out;     // [m] column marginal of the final evaluation sweep, or null
 };
 
 // Operands of one sweep for one problem, resolved from the descriptor.

@@ -131,6 +131,7 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       double dv = fabs(bh - mg);
       err_t = (norm_error == 1) ? dv : pow(dv, (double)norm_error);
       msum_t = bh;
+      if (sp.final_eval && P.marg_out) P.marg_out[r] = (float)bh;
     }
   }
   if (sp.eval) {

@@ -129,8 +129,11 @@ class PointCloud(geometry.Geometry):
 
   # -- transport from potentials (geometry.py:361-365, 444-486) ------------
   def _apply_raw(self, f: torch.Tensor, g: torch.Tensor, v2: torch.Tensor,
-                 axis: int) -> torch.Tensor:
-    """``ottb_apply_transport`` on ``v2 [k, n or m]`` (FP32, no autograd)."""
+                 axis: int, precision: str = "fp32") -> torch.Tensor:
+    """The plan applied to ``v2 [k, n or m]`` (no autograd):
+    ``ottb_apply_transport`` (FP32), or with ``precision`` "auto" (d >= 32)
+    or "bf16_split3" ``ottb_apply_transport_sweep`` on the solver's
+    tensor-core sweep ("sweep_fp32": that entry point on the FP32 sweep)."""
     lib = _lib.load()
     n, m = self.shape
     dev = self.x.device
@@ -139,6 +142,23 @@ class PointCloud(geometry.Geometry):
     gd = _arrays.as_f32(g, dev).detach()
     out = torch.empty((v2.shape[0], m if axis == 0 else n), dtype=torch.float32, device=dev)
     if v2.shape[0] == 0:
+      return out
+    sweep = {"bf16_split3": _lib.PRECISION_BF16_SPLIT3, "sweep_fp32": _lib.PRECISION_FP32}
+    if precision == "auto" and self.dim >= 32:
+      precision = "bf16_split3"
+    if precision in sweep:
+      code = sweep[precision]
+      ws_bytes = lib.ottb_apply_transport_sweep_workspace_size(n, m, self.dim, v2.shape[0],
+                                                               axis, code)
+      if ws_bytes == 0:
+        raise NotImplementedError("problem sizes not supported by the sweep engine")
+      ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+      st = lib.ottb_apply_transport_sweep(
+          self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim, fd.data_ptr(), gd.data_ptr(),
+          ctypes.c_float(self.epsilon), ctypes.c_float(self.inv_scale_cost), v2.data_ptr(),
+          v2.shape[0], axis, code, out.data_ptr(), ws.data_ptr(), ws_bytes,
+          _arrays.stream_handle())
+      _lib.check(st, "ottb_apply_transport_sweep")
       return out
     ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, self.dim, v2.shape[0], axis)
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)

@@ -206,9 +206,9 @@ class ImplicitDiff:
 
   # -- plan products ---------------------------------------------------------
   @staticmethod
-  def _app(geom, f, g):
+  def _app(geom, f, g, precision: str = "fp32"):
     def app(v: torch.Tensor, axis: int) -> torch.Tensor:
-      return geom._apply_raw(f, g, v.reshape(1, -1), axis)[0].double()
+      return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0].double()
     return app
 
   def _precond(self, geom) -> Callable[[torch.Tensor], torch.Tensor]:
@@ -249,18 +249,21 @@ class ImplicitDiff:
 
   # -- the linear solve --------------------------------------------------------
   def solve(self, gr: Tuple[torch.Tensor, torch.Tensor], ot_prob, f: torch.Tensor,
-            g: torch.Tensor, lse_mode: bool = True) -> torch.Tensor:
+            g: torch.Tensor, lse_mode: bool = True, precision: str = "fp32") -> torch.Tensor:
     """implicit_differentiation.py:80-233: ``-(dF/d(f, g))^-T gr`` for the
-    first-order conditions ``F`` (float64, length n + m)."""
-    return self._solve(gr, ot_prob, f, g, lse_mode)[0]
+    first-order conditions ``F`` (float64, length n + m). ``precision`` of
+    the one-vector plan products: "fp32", or "auto" / "bf16_split3" for the
+    solver's tensor-core sweep at d >= 32 (what the potentials' backward
+    uses after a tensor-core solve)."""
+    return self._solve(gr, ot_prob, f, g, lse_mode, precision)[0]
 
-  def _solve(self, gr, ot_prob, f, g, lse_mode):
+  def _solve(self, gr, ot_prob, f, g, lse_mode, precision="fp32"):
     """``solve`` and the plan's marginals ``(P 1, P^T 1)`` it used."""
     self._check(ot_prob, lse_mode)
     geom = ot_prob.geom
     n, m = geom.shape
     dev = f.device
-    app = self._app(geom, f, g)
+    app = self._app(geom, f, g, precision)
     gr_f = gr[0].detach().double().reshape(n)
     gr_g = gr[1].detach().double().reshape(m)
     sa = ot_prob.a.detach() > 0
@@ -352,14 +355,14 @@ class ImplicitDiff:
 
   # -- the pullback ------------------------------------------------------------
   def gradient(self, prob, f: torch.Tensor, g: torch.Tensor, lse_mode: bool,
-               gr: Tuple[torch.Tensor, torch.Tensor]
+               gr: Tuple[torch.Tensor, torch.Tensor], precision: str = "fp32"
                ) -> Tuple[torch.Tensor, torch.Tensor, torch.Tensor, torch.Tensor]:
     """implicit_differentiation.py:275-287: the cotangent of the inputs
     ``(x, y, a, b)`` (float64) for the cotangent ``gr`` of ``(f, g)``:
     ``lam = solve(gr)`` pulled back through the first-order conditions at
     fixed ``f, g`` (``d h(P 1)_i / dP_ij = h'(P 1)_i``, ``dP_ij/dC_ij =
     -P_ij / eps``; ``d/da_i = -lam_i h'(a_i)`` on ``a > 0``)."""
-    lam, ma, mb = self._solve(gr, prob, f, g, lse_mode)
+    lam, ma, mb = self._solve(gr, prob, f, g, lse_mode, precision)
     geom = prob.geom
     n, m = geom.shape
     dev = f.device

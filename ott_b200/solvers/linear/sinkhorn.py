@@ -237,8 +237,8 @@ class _Potentials(torch.autograd.Function):
   (sinkhorn.py:1102-1136, ``ImplicitDiff.gradient``)."""
 
   @staticmethod
-  def forward(ctx, x, y, a, b, f, g, prob, implicit_diff):  # pylint: disable=arguments-differ
-    ctx.prob, ctx.implicit_diff = prob, implicit_diff
+  def forward(ctx, x, y, a, b, f, g, prob, implicit_diff, precision):  # pylint: disable=arguments-differ
+    ctx.prob, ctx.implicit_diff, ctx.precision = prob, implicit_diff, precision
     ctx.save_for_backward(f, g)
     return f.clone(), g.clone()
 
@@ -251,12 +251,13 @@ class _Potentials(torch.autograd.Function):
     f, g = ctx.saved_tensors
     gf = torch.zeros_like(f) if gf is None else gf
     gg = torch.zeros_like(g) if gg is None else gg
-    gx, gy, ga, gb = ctx.implicit_diff.gradient(ctx.prob, f, g, True, (gf, gg))
+    gx, gy, ga, gb = ctx.implicit_diff.gradient(ctx.prob, f, g, True, (gf, gg),
+                                                precision=ctx.precision)
     need = ctx.needs_input_grad
     p = ctx.prob
     cast = lambda t, like, i: t.to(like.dtype) if need[i] else None
     return (cast(gx, p.geom.x, 0), cast(gy, p.geom.y, 1), cast(ga, p.a, 2),
-            cast(gb, p.b, 3), None, None, None, None)
+            cast(gb, p.b, 3), None, None, None, None, None)
 
 
 class _RegOTCost(torch.autograd.Function):
@@ -521,7 +522,7 @@ class _Call:
       f, g, errors = self.bufs[k]
       if _tracks_grad(p):
         f, g = _Potentials.apply(p.geom.x, p.geom.y, p.a, p.b, f, g, p,
-                                 self.solver.implicit_diff)
+                                 self.solver.implicit_diff, self.solver.precision)
       out.append(SinkhornOutput((f, g), errors=errors, reg_ot_cost_=(results, k),
                                 ot_prob=p, threshold=self.solver.threshold,
                                 inner_iterations=self.solver.inner_iterations,

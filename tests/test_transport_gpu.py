@@ -167,3 +167,40 @@ def test_one_and_two_vector_applications_match_oracle(n, m, d, k):
     for r in range(k):
       np.testing.assert_allclose(got[r].cpu().numpy(), want[r], rtol=0,
                                  atol=rel * np.abs(want[r]).max())
+
+
+@pytest.mark.parametrize("n,m,d,precision", [(700, 900, 8, "fp32"), (1000, 600, 64, "fp32"),
+                                             (1000, 600, 64, "bf16_split3"),
+                                             (513, 1500, 40, "bf16_split3"),
+                                             (300, 257, 128, "bf16_split3")])
+def test_sweep_engine_application_matches_oracle(n, m, d, precision):
+  """ottb_apply_transport_sweep (two zero-iteration solves per vector on
+  the solver's sweep) against the float64 plan. FP32: the golden
+  tolerance. BF16 split-3: its products drop the lo*lo term and the
+  inputs' bits below 2^-16, an exponent error up to
+  2^-15 * 2 inv |x_i| |y_j| / eps after centring, relative to the sum of
+  |P| |v|."""
+  import torch
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=n + d)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon))
+  p_ref = o.transport_matrix(f, g, og)
+  if precision == "fp32":
+    zmax = (np.abs(f).max() + np.abs(g).max() + og.cost_block().max()) / og.epsilon
+    rel = max(1e-5, 8 * 2.0 ** -24 * zmax)
+  else:
+    c = 0.5 * (x.mean(0) + y.mean(0))
+    r = np.linalg.norm(x - c, axis=1).max() * np.linalg.norm(y - c, axis=1).max()
+    rel = 2.0 ** -15 * 2 * r / og.epsilon + 1e-5
+  rng = np.random.default_rng(d)
+  for axis in (0, 1):
+    vec = rng.standard_normal((2, n if axis == 0 else m))
+    got = geom._apply_raw(out.f, out.g, torch.as_tensor(vec, dtype=torch.float32).cuda(),
+                          axis, precision if precision != "fp32" else "sweep_fp32")
+    want = vec @ p_ref if axis == 0 else vec @ p_ref.T
+    scale = np.abs(vec) @ p_ref if axis == 0 else np.abs(vec) @ p_ref.T
+    err = np.abs(got.cpu().numpy() - want)
+    assert np.all(err <= rel * scale.max(axis=1, keepdims=True)), (err.max(), rel)
