@@ -71,6 +71,20 @@ def test_invalid_arguments_rejected_without_device():
   assert st == _lib.OTTB_ERR_INVALID
   assert lib.ottb_cost_stats(None, None, 0, 0, 2, ctypes.c_float(1.0), 1, None, None, 0,
                              None) == _lib.OTTB_ERR_INVALID
+  one = ctypes.c_float(1.0)
+  assert lib.ottb_apply_transport(None, None, 10, 10, 2, None, None, one, one, None, 1, 0, None,
+                                  None, 0, None) == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_apply_transport_sweep(None, None, 10, 10, 2, None, None, one, one, None, 1,
+                                        0, 1, None, None, 0, None) == _lib.OTTB_ERR_INVALID
+  # workspace sizes: zero for invalid shapes or axes, d > 128 unsupported
+  assert lib.ottb_apply_transport_sweep_workspace_size(0, 20, 64, 1, 0, 1) == 0
+  assert lib.ottb_apply_transport_sweep_workspace_size(10, 20, 64, 1, 2, 1) == 0
+  assert lib.ottb_apply_transport_sweep_workspace_size(10, 20, 200, 1, 0, 0) == 0
+  ws_tc = lib.ottb_apply_transport_sweep_workspace_size(1000, 2000, 64, 1, 0, 1)
+  assert ws_tc > 0 and ws_tc % 256 == 0
+  # two zero-iteration problems per vector: more vectors, more workspace
+  assert lib.ottb_apply_transport_sweep_workspace_size(1000, 2000, 64, 3, 0, 1) > ws_tc
+  assert lib.ottb_apply_transport_workspace_size(1000, 2000, 64, 1, 3) == 0
 
 
 def test_mlp_shape_checks_without_device():

@@ -259,3 +259,30 @@ def test_solver_budget_exhaustion_warns():
         torch.randn(200, dtype=torch.float64, device="cuda"))
   with pytest.warns(RuntimeWarning, match="MINRES stopped"):
     imp.ImplicitDiff(solver_kwargs={"max_steps": 2}).solve(gr, prob, out.f, out.g)
+
+
+def test_preconditioner_does_not_change_the_gradient():
+  """The implicit derivative of the potentials does not depend on the
+  preconditioner h of the first-order conditions: h = identity with the
+  symmetric CG route of the reference's generic construction
+  (implicit_differentiation.py:162-170, 193-232) gives the default
+  (h = eps log) point gradients."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  x, y, a, b = problems.uniform_cloud_problem(160, 120, 3, seed=22)
+  geom = pointcloud.PointCloud(_t(x), _t(y), epsilon=0.1)
+  out = linear.solve(geom, _t(a), _t(b), threshold=1e-7, max_iterations=10000)
+  prob = linear_problem.LinearProblem(geom, _t(a), _t(b))
+  rng = np.random.default_rng(4)
+  gf, gg = rng.standard_normal(160), rng.standard_normal(120)
+  gg += (gf.sum() - gg.sum()) / 120
+  gr = (torch.as_tensor(gf).cuda(), torch.as_tensor(gg).cuda())
+  d0 = imp.ImplicitDiff().gradient(prob, out.f, out.g, True, gr)
+  ident = imp.ImplicitDiff(precondition_fun=lambda v: v, symmetric=True,
+                           solver=imp.solve_jax_cg, solver_kwargs={"tol": 1e-10})
+  d1 = ident.gradient(prob, out.f, out.g, True, gr)
+  assert _rel(d1[0], d0[0].cpu().numpy()) < 1e-3
+  assert _rel(d1[1], d0[1].cpu().numpy()) < 1e-3
