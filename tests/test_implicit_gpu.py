@@ -286,3 +286,50 @@ def test_preconditioner_does_not_change_the_gradient():
   d1 = ident.gradient(prob, out.f, out.g, True, gr)
   assert _rel(d1[0], d0[0].cpu().numpy()) < 1e-3
   assert _rel(d1[1], d0[1].cpu().numpy()) < 1e-3
+
+
+@pytest.mark.parametrize("arg", ["a", "x"])
+@pytest.mark.parametrize("axis", [0, 1])
+def test_apply_transport_jacobian_matches_finite_differences(arg, axis):
+  """The reference's test of the same name (tests/solvers/linear/
+  sinkhorn_diff_test.py:352-455, balanced, lse mode): the derivative of
+  ``out.apply(vec, axis)`` through the solve, in a direction of the weights
+  (mass-preserving) or of the points, against central differences of
+  float64 oracle solves. The reference allows 1e-2 absolute and 1e-1
+  relative; here 1e-3 of the derivative's magnitude."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  n, m, d, eps = 27, 13, 4, 0.01
+  rng = np.random.default_rng(7 + axis + 2 * (arg == "x"))
+  x = rng.uniform(size=(n, d)) / d
+  y = rng.uniform(size=(m, d)) / d
+  a = rng.uniform(size=n) + 0.2
+  a /= a.sum()
+  b = rng.uniform(size=m) + 0.2
+  b /= b.sum()
+  vec = rng.uniform(size=m if axis else n) - 0.5
+  cot = rng.standard_normal(n if axis else m)
+  delta = rng.uniform(size=n) if arg == "a" else rng.uniform(size=(n, d))
+  if arg == "a":
+    delta -= delta.mean()
+  xt, at = _t(x, arg == "x"), _t(a, arg == "a")
+  geom = pointcloud.PointCloud(xt, _t(y), epsilon=eps)
+  out = linear.solve(geom, at, _t(b), threshold=1e-6, max_iterations=20000)
+  app = out.apply(_t(vec), axis=axis)
+  (app.double() * torch.as_tensor(cot).cuda()).sum().backward()
+  grad = (at if arg == "a" else xt).grad.double().cpu().numpy()
+  got = float((grad * delta).sum())
+
+  def applied(a_, x_):
+    og = o.Geom(x_, y, eps)
+    r = o.sinkhorn(og, a_, b, threshold=1e-12, max_iterations=200000)
+    p = o.transport_matrix(r.f, r.g, og)
+    return float(cot @ (vec @ p if axis == 0 else p @ vec))
+
+  h = 1e-5
+  if arg == "a":
+    fd = (applied(a + h * delta, x) - applied(a - h * delta, x)) / (2 * h)
+  else:
+    fd = (applied(a, x + h * delta) - applied(a, x - h * delta)) / (2 * h)
+  assert abs(got - fd) <= 1e-3 * float(np.abs(grad * delta).sum()), (got, fd)
