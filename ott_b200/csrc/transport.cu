@@ -74,6 +74,13 @@ struct ApplyArgs {
   int splits;         // column splits (1: write out directly)
   float* part_o;      // [splits][K][R] sums of each split (splits > 1)
   float* part_m;      // [splits][R] their row shifts (log2 units)
+  // operands prepared once per call for the pipelined kernel (null: the
+  // tiles are transposed from A, B, vec inside the kernel)
+  float* cen;         // [DP] common centre
+  float* bt;          // [DP][c_pad] B transposed, centred, zero-padded
+  float* wbv;         // [c_pad] (potB - inv |B - centre|^2) * ws, -inf padding
+  float* vt;          // [c_pad][k_pad] vectors transposed, zero-padded
+  int64_t c_pad, k_pad;
 };
 
 // Common centre of both point sets: the mean of up to kSampleMax points of
@@ -244,6 +251,259 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
 
   // out = O * 2^max (a row whose weights are all zero gives 0); with
   // splits, the sums and shifts of this split
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    if (gr >= p.R) continue;
+    const bool any = mrow[i] > kNegSentinel;
+    if (p.splits > 1) {
+      const int64_t sp = blockIdx.z;
+      if (tx == 0 && blockIdx.y == 0) p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
+#pragma unroll
+      for (int j = 0; j < VT; ++j) {
+        const int k = k0 + tx + 16 * j;
+        if (k < p.K) p.part_o[(sp * p.K + k) * p.R + gr] = any ? o[i][j] : 0.f;
+      }
+      continue;
+    }
+    const float scale = any ? exp2f(mrow[i]) : 0.f;
+#pragma unroll
+    for (int j = 0; j < VT; ++j) {
+      const int k = k0 + tx + 16 * j;
+      if (k < p.K) p.out[(int64_t)k * p.R + gr] = any ? o[i][j] * scale : 0.f;
+    }
+  }
+}
+
+__device__ __forceinline__ void tp_cp_async16(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(gmem));
+}
+__device__ __forceinline__ void tp_cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::);
+}
+template <int N>
+__device__ __forceinline__ void tp_cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N));
+}
+
+// The operands of the pipelined kernel, prepared once per call: the common
+// centre (same sample as apply_center), B transposed and centred with its
+// column terms, and the vectors transposed to [point][vector].
+template <int DP>
+__global__ void apply_prep_center_kernel(ApplyArgs p) {
+  apply_center<DP>(p, p.cen);
+}
+
+__global__ void apply_prep_b_kernel(ApplyArgs p, int dp) {
+  const int64_t total = (int64_t)dp * p.c_pad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx / p.c_pad, c = idx % p.c_pad;
+    p.bt[idx] = (c < p.C && k < p.d) ? p.B[c * p.d + k] - p.cen[k] : 0.f;
+  }
+  for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < p.c_pad;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    float nrm = 0.f;
+    if (c < p.C)
+      for (int k = 0; k < p.d; ++k) {
+        const float t = p.B[c * p.d + k] - p.cen[k];
+        nrm = fmaf(t, t, nrm);
+      }
+    p.wbv[c] = c < p.C ? (__ldg(p.potB + c) - p.inv * nrm) * p.ws : -INFINITY;
+  }
+}
+
+// vt[c][k] = vec[k][c] through 32 x 32 shared tiles (both sides coalesced).
+__global__ void apply_prep_v_kernel(ApplyArgs p) {
+  __shared__ float tile[32][33];
+  const int64_t c0 = (int64_t)blockIdx.x * 32, k0 = (int64_t)blockIdx.y * 32;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t k = k0 + r, c = c0 + tx;
+    tile[r][tx] = (k < p.K && c < p.C) ? p.vec[k * p.C + c] : 0.f;
+  }
+  __syncthreads();
+  for (int r = ty; r < 32; r += 8) {
+    const int64_t c = c0 + r, k = k0 + tx;
+    if (c < p.c_pad && k < p.k_pad) p.vt[c * p.k_pad + k] = tile[tx][r];
+  }
+}
+
+// apply_transport_kernel with its B and vector tiles streamed by cp.async
+// from the prepared operands: the next B tile (double-buffered) and this
+// tile's vectors load while the cost tile is computed, instead of stalling
+// the single 8-warp CTA of the SM on global loads at every tile. d <= 64
+// (the double buffers fit in 227 KB with the P tile).
+template <int DP, int VT>
+struct PipeSmem {
+  static constexpr int kKT = 16 * VT;
+  float As[DP][kTR + 4];
+  float Bs[2][DP][kTC + 4];
+  float wb[2][kTC];
+  float Ps[kTC][kTR];
+  float Vs[kTC][kKT + 4];
+  float center[DP];
+};
+
+template <int DP, int VT>
+__global__ void __launch_bounds__(256, 1) apply_pipelined_kernel(ApplyArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  PipeSmem<DP, VT>& sm = *reinterpret_cast<PipeSmem<DP, VT>*>(smem_raw);
+  constexpr int kKT = PipeSmem<DP, VT>::kKT;
+  const int tid = threadIdx.x;
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  const int64_t row0 = (int64_t)blockIdx.x * kTR;
+  const int k0 = blockIdx.y * kKT;
+  const float s = 2.f * p.inv * p.ws;
+
+  for (int k = tid; k < DP; k += blockDim.x) sm.center[k] = p.cen[k];
+  __syncthreads();
+  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
+    const int r = idx / DP, k = idx % DP;
+    const int64_t gr = row0 + r;
+    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
+  }
+  __syncthreads();
+  float u[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    float nrm = 0.f;
+    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
+    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
+  }
+
+  float mrow[8];
+  float o[8][VT];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    mrow[i] = kNegSentinel;
+#pragma unroll
+    for (int j = 0; j < VT; ++j) o[i][j] = 0.f;
+  }
+
+  // B tile t (DP rows of 128 floats) and its column terms into buffer buf
+  auto issue_b = [&](int64_t t, int buf) {
+    const int64_t c0 = t * kTC;
+    for (int idx = tid; idx < DP * (kTC / 4); idx += blockDim.x) {
+      const int k = idx / (kTC / 4), q = idx % (kTC / 4);
+      tp_cp_async16(&sm.Bs[buf][k][q * 4], p.bt + (int64_t)k * p.c_pad + c0 + q * 4);
+    }
+    if (tid < kTC / 4) tp_cp_async16(&sm.wb[buf][tid * 4], p.wbv + c0 + tid * 4);
+    tp_cp_async_commit();
+  };
+  // this chunk's vectors at tile t's points
+  auto issue_v = [&](int64_t t) {
+    const int64_t c0 = t * kTC;
+    for (int idx = tid; idx < kTC * (kKT / 4); idx += blockDim.x) {
+      const int c = idx / (kKT / 4), q = idx % (kKT / 4);
+      tp_cp_async16(&sm.Vs[c][q * 4], p.vt + (c0 + c) * p.k_pad + k0 + q * 4);
+    }
+    tp_cp_async_commit();
+  };
+
+  const int64_t ntiles_all = (p.C + kTC - 1) / kTC;
+  const int64_t t_begin = ntiles_all * blockIdx.z / p.splits;
+  const int64_t t_end = ntiles_all * (blockIdx.z + 1) / p.splits;
+  if (t_begin < t_end) issue_b(t_begin, 0);
+  for (int64_t t = t_begin; t < t_end; ++t) {
+    const int buf = (int)((t - t_begin) & 1);
+    const bool has_next = t + 1 < t_end;
+    __syncthreads();  // previous tile's Ps, Vs and B buffer consumed
+    // commit order: B(t) (earlier), V(t), B(t + 1)
+    issue_v(t);
+    if (has_next) {
+      issue_b(t + 1, buf ^ 1);
+      tp_cp_async_wait<2>();  // B(t) landed
+    } else {
+      tp_cp_async_wait<1>();
+    }
+    __syncthreads();
+
+    float z[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < DP; ++k) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
+    }
+    {
+      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[buf][tx * 4]);
+      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[buf][64 + tx * 4]);
+      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
+                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (mx > mrow[i]) {
+        const float sc = ex2_approx(mrow[i] - mx);
+#pragma unroll
+        for (int j = 0; j < VT; ++j) o[i][j] *= sc;
+        mrow[i] = mx;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[i][j] = ex2_approx(z[i][j] - mrow[i]);
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
+      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, ty)) =
+          make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
+      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty)) =
+          make_float4(z[4][j], z[5][j], z[6][j], z[7][j]);
+    }
+    if (has_next)
+      tp_cp_async_wait<1>();  // V(t) landed (B(t + 1) may still be in flight)
+    else
+      tp_cp_async_wait<0>();
+    __syncthreads();
+    float acc[8][VT];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < VT; ++j) acc[i][j] = 0.f;
+#pragma unroll 4
+    for (int c = 0; c < kTC; ++c) {
+      const float4 p0 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, ty));
+      const float4 p1 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty));
+      const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+      float vv[VT];
+#pragma unroll
+      for (int j = 0; j < VT; ++j) vv[j] = sm.Vs[c][tx + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < VT; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < VT; ++j) o[i][j] += acc[i][j];
+  }
+
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
@@ -559,6 +819,48 @@ size_t apply_workspace(int64_t R, int K, int splits) {
   return splits > 1 ? sizeof(float) * (size_t)splits * ((size_t)K + 1) * (size_t)R : 0;
 }
 
+// Vectors per thread and vector chunks of the many-vector kernels: the
+// fewest chunks of at most 16 * max_vt vectors, then the smallest
+// vectors-per-thread count that covers a chunk.
+void apply_vt_chunks(int d, int K, int* vt, int* chunks) {
+  const int vm = d > 64 ? 4 : 5;
+  const int c0 = (K + 16 * vm - 1) / (16 * vm);
+  const int per = (K + c0 - 1) / c0;
+  *vt = std::min((per + 15) / 16, vm);
+  *chunks = (K + 16 * *vt - 1) / (16 * *vt);
+}
+
+// Byte offsets of the pipelined kernel's prepared operands, which follow
+// the split partials in the workspace (256-byte aligned).
+struct PrepLayout {
+  size_t cen = 0, bt = 0, wbv = 0, vt = 0, total = 0;
+  int64_t c_pad = 0, k_pad = 0;
+};
+
+inline size_t align256(size_t v) { return (v + 255) / 256 * 256; }
+
+bool pipelined_path(int d, int K) { return d <= 64 && K > 2; }
+
+PrepLayout prep_layout(int64_t C, int d, int K, size_t base) {
+  PrepLayout L;
+  int vt = 1, chunks = 1;
+  apply_vt_chunks(d, K, &vt, &chunks);
+  const int dp = d <= 8 ? 8 : d <= 16 ? 16 : d <= 32 ? 32 : 64;
+  L.c_pad = (C + kTC - 1) / kTC * kTC;
+  L.k_pad = (int64_t)chunks * 16 * vt;
+  size_t off = align256(base);
+  L.cen = off;
+  off = align256(off + sizeof(float) * 64);
+  L.bt = off;
+  off = align256(off + sizeof(float) * (size_t)dp * L.c_pad);
+  L.wbv = off;
+  off = align256(off + sizeof(float) * L.c_pad);
+  L.vt = off;
+  off = align256(off + sizeof(float) * (size_t)L.c_pad * L.k_pad);
+  L.total = off;
+  return L;
+}
+
 int device_sms() {
   int dev = 0, sms = 0;
   if (cudaGetDevice(&dev) != cudaSuccess ||
@@ -567,23 +869,56 @@ int device_sms() {
   return sms > 0 ? sms : 148;
 }
 
-// The fewest chunks of at most 16 * max_vt vectors, then the smallest
-// vectors-per-thread count that covers a chunk.
+template <int DP, int VT>
+int launch_pipelined_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
+  const size_t smem = sizeof(PipeSmem<DP, VT>);
+  auto k = apply_pipelined_kernel<DP, VT>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+      cudaSuccess)
+    return OTTB_ERR_CUDA;
+  apply_prep_center_kernel<DP><<<1, 64, 0, stream>>>(a);
+  {
+    const int64_t tot = (int64_t)DP * a.c_pad;
+    apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
+                          stream>>>(a, DP);
+  }
+  {
+    dim3 grid((unsigned)(a.c_pad / 32), (unsigned)((a.k_pad + 31) / 32));
+    apply_prep_v_kernel<<<grid, 256, 0, stream>>>(a);
+  }
+  dim3 grid((unsigned)((a.R + kTR - 1) / kTR), (unsigned)chunks, (unsigned)a.splits);
+  k<<<grid, 256, smem, stream>>>(a);
+  if (a.splits > 1) {
+    const int64_t total = (int64_t)a.K * a.R;
+    combine_splits_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 4096), 256, 0,
+                            stream>>>(a);
+  }
+  return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
 template <int DP>
 int launch_apply(const ApplyArgs& a, cudaStream_t stream) {
   if (a.K == 1) return launch_direct<DP, 1>(a, stream);
   if (a.K == 2) return launch_direct<DP, 2>(a, stream);
-  constexpr int VM = max_vt<DP>();
-  const int chunks = (a.K + 16 * VM - 1) / (16 * VM);
-  const int per = (a.K + chunks - 1) / chunks;
-  const int vt = (per + 15) / 16;
+  int vt = 1, chunks = 1;
+  apply_vt_chunks(a.d, a.K, &vt, &chunks);
+  if constexpr (DP <= 64) {
+    if (a.bt) {
+      switch (vt) {
+        case 1: return launch_pipelined_vt<DP, 1>(a, chunks, stream);
+        case 2: return launch_pipelined_vt<DP, 2>(a, chunks, stream);
+        case 3: return launch_pipelined_vt<DP, 3>(a, chunks, stream);
+        case 4: return launch_pipelined_vt<DP, 4>(a, chunks, stream);
+        default: return launch_pipelined_vt<DP, 5>(a, chunks, stream);
+      }
+    }
+  }
   switch (vt) {
-    case 1: return launch_apply_vt<DP, 1>(a, (a.K + 15) / 16, stream);
-    case 2: return launch_apply_vt<DP, 2>(a, (a.K + 31) / 32, stream);
-    case 3: return launch_apply_vt<DP, 3>(a, (a.K + 47) / 48, stream);
-    case 4: return launch_apply_vt<DP, 4>(a, (a.K + 63) / 64, stream);
-    default: return launch_apply_vt<DP, (VM > 4 ? 5 : 4)>(a, (a.K + 16 * VM - 1) / (16 * VM),
-                                                         stream);
+    case 1: return launch_apply_vt<DP, 1>(a, chunks, stream);
+    case 2: return launch_apply_vt<DP, 2>(a, chunks, stream);
+    case 3: return launch_apply_vt<DP, 3>(a, chunks, stream);
+    case 4: return launch_apply_vt<DP, 4>(a, chunks, stream);
+    default: return launch_apply_vt<DP, (max_vt<DP>() > 4 ? 5 : 4)>(a, chunks, stream);
   }
 }
 
@@ -596,7 +931,8 @@ extern "C" size_t ottb_apply_transport_workspace_size(int64_t n, int64_t m, int3
                                                      int32_t num_vec, int32_t axis) {
   if (n < 1 || m < 1 || d < 1 || d > 128 || num_vec < 1 || (axis != 0 && axis != 1)) return 0;
   const int64_t R = axis == 1 ? n : m, C = axis == 1 ? m : n;
-  return apply_workspace(R, num_vec, apply_splits(R, C, d, num_vec, device_sms()));
+  const size_t part = apply_workspace(R, num_vec, apply_splits(R, C, d, num_vec, device_sms()));
+  return pipelined_path(d, num_vec) ? prep_layout(C, d, num_vec, part).total : part;
 }
 
 extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
@@ -629,6 +965,21 @@ extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t 
     --a.splits;
   a.part_o = (float*)workspace;
   a.part_m = a.splits > 1 ? a.part_o + (size_t)a.splits * num_vec * a.R : nullptr;
+  a.cen = a.bt = a.wbv = a.vt = nullptr;
+  a.c_pad = a.k_pad = 0;
+  if (pipelined_path(d, num_vec) && workspace) {
+    // the prepared operands after the partials, when the workspace holds them
+    const PrepLayout L = prep_layout(a.C, d, num_vec, apply_workspace(a.R, num_vec, a.splits));
+    if (L.total <= workspace_bytes && ((uintptr_t)workspace) % 256 == 0) {
+      char* w = (char*)workspace;
+      a.cen = (float*)(w + L.cen);
+      a.bt = (float*)(w + L.bt);
+      a.wbv = (float*)(w + L.wbv);
+      a.vt = (float*)(w + L.vt);
+      a.c_pad = L.c_pad;
+      a.k_pad = L.k_pad;
+    }
+  }
   cudaStream_t s = (cudaStream_t)stream;
   if (d <= 8) return launch_apply<8>(a, s);
   if (d <= 16) return launch_apply<16>(a, s);
