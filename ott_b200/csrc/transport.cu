@@ -291,9 +291,26 @@ __device__ __forceinline__ void tp_cp_async_wait() {
 // The operands of the pipelined kernel, prepared once per call: the common
 // centre (same sample as apply_center), B transposed and centred with its
 // column terms, and the vectors transposed to [point][vector].
-template <int DP>
+// One block per dimension (256 threads): the same samples as apply_center,
+// summed by a fixed-order tree (any centre gives the same plan; this one is
+// the sample mean of both sets).
 __global__ void apply_prep_center_kernel(ApplyArgs p) {
-  apply_center<DP>(p, p.cen);
+  __shared__ float sa[256], sb[256];
+  const int k = blockIdx.x, t = threadIdx.x;
+  const int64_t na = p.R < kSampleMax ? p.R : kSampleMax;
+  const int64_t nb = p.C < kSampleMax ? p.C : kSampleMax;
+  const int64_t stra = p.R / na, strb = p.C / nb;
+  sa[t] = (k < p.d && t < na) ? p.A[t * stra * p.d + k] : 0.f;
+  sb[t] = (k < p.d && t < nb) ? p.B[t * strb * p.d + k] : 0.f;
+  __syncthreads();
+  for (int off = 128; off > 0; off >>= 1) {
+    if (t < off) {
+      sa[t] += sa[t + off];
+      sb[t] += sb[t + off];
+    }
+    __syncthreads();
+  }
+  if (t == 0) p.cen[k] = k < p.d ? 0.5f * (sa[0] / (float)na + sb[0] / (float)nb) : 0.f;
 }
 
 __global__ void apply_prep_b_kernel(ApplyArgs p, int dp) {
@@ -876,7 +893,7 @@ int launch_pipelined_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return OTTB_ERR_CUDA;
-  apply_prep_center_kernel<DP><<<1, 64, 0, stream>>>(a);
+  apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
   {
     const int64_t tot = (int64_t)DP * a.c_pad;
     apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
