@@ -204,3 +204,41 @@ def test_sweep_engine_application_matches_oracle(n, m, d, precision):
     scale = np.abs(vec) @ p_ref if axis == 0 else np.abs(vec) @ p_ref.T
     err = np.abs(got.cpu().numpy() - want)
     assert np.all(err <= rel * scale.max(axis=1, keepdims=True)), (err.max(), rel)
+
+
+@pytest.mark.parametrize("precision", ["sweep_fp32", "bf16_split3"])
+def test_sweep_engine_application_edge_cases(precision):
+  """Zero-weight points on both sides (-inf potentials), a vector with zero
+  entries and an all-zero vector, three vectors in one launch (six
+  zero-iteration problems)."""
+  import torch
+  n, m, d = 300, 260, 40
+  x, y, a, b = problems.uniform_cloud_problem(n, m, d, seed=31)
+  a[[0, 7, 150]] = 0.0
+  a /= a.sum()
+  b[[3, 259]] = 0.0
+  b /= b.sum()
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  assert np.isneginf(f[[0, 7, 150]]).all() and np.isneginf(g[[3, 259]]).all()
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), float(geom.epsilon))
+  p_ref = np.nan_to_num(o.transport_matrix(f, g, og))
+  c = 0.5 * (x.mean(0) + y.mean(0))
+  r = np.linalg.norm(x - c, axis=1).max() * np.linalg.norm(y - c, axis=1).max()
+  rel = 2.0 ** -15 * 2 * r / og.epsilon + 1e-5 if precision == "bf16_split3" else 2e-5
+  rng = np.random.default_rng(2)
+  for axis in (0, 1):
+    k = n if axis == 0 else m
+    vec = rng.standard_normal((3, k))
+    vec[0, ::3] = 0.0
+    vec[2] = 0.0
+    got = geom._apply_raw(out.f, out.g, torch.as_tensor(vec, dtype=torch.float32).cuda(),
+                          axis, precision).cpu().numpy()
+    want = vec @ p_ref if axis == 0 else vec @ p_ref.T
+    scale = np.abs(vec) @ p_ref if axis == 0 else np.abs(vec) @ p_ref.T
+    assert np.isfinite(got).all()
+    assert np.all(got[2] == 0.0)
+    for i in range(2):
+      assert np.all(np.abs(got[i] - want[i]) <= rel * scale[i].max() + 1e-30)
