@@ -779,8 +779,196 @@ int launch_apply_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }
 
+// The one or two vectors zero-padded to c_pad columns (16-byte cp.async rows).
+__global__ void apply_prep_vpad_kernel(ApplyArgs p) {
+  const int64_t total = (int64_t)p.K * p.c_pad;
+  for (int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; idx < total;
+       idx += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t k = idx / p.c_pad, c = idx % p.c_pad;
+    p.vt[idx] = c < p.C ? p.vec[k * p.C + c] : 0.f;
+  }
+}
+
+// apply_direct_kernel on the prepared operands: the next B tile, its column
+// terms and vector entries stream in by cp.async (double-buffered) while the
+// current tile is computed.
+template <int DP, int KD>
+struct DirectPipeSmem {
+  float As[DP][kTR + 4];
+  float Bs[2][DP][kTC + 4];
+  float Vs[2][KD][kTC];
+  float wb[2][kTC];
+  float center[DP];
+};
+
+template <int DP, int KD>
+__global__ void __launch_bounds__(256, (DP <= 64 ? 2 : 1))
+apply_direct_pipelined_kernel(ApplyArgs p) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  DirectPipeSmem<DP, KD>& sm = *reinterpret_cast<DirectPipeSmem<DP, KD>*>(smem_raw);
+  const int tid = threadIdx.x;
+  const int tx = tid & 15;
+  const int ty = tid >> 4;
+  const int64_t row0 = (int64_t)blockIdx.x * kTR;
+  const float s = 2.f * p.inv * p.ws;
+
+  for (int k = tid; k < DP; k += blockDim.x) sm.center[k] = p.cen[k];
+  __syncthreads();
+  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
+    const int r = idx / DP, k = idx % DP;
+    const int64_t gr = row0 + r;
+    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
+  }
+  __syncthreads();
+  float u[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    float nrm = 0.f;
+    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
+    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
+  }
+  float mrow[8];
+  float o[8][KD];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    mrow[i] = kNegSentinel;
+#pragma unroll
+    for (int j = 0; j < KD; ++j) o[i][j] = 0.f;
+  }
+
+  auto issue = [&](int64_t t, int buf) {
+    const int64_t c0 = t * kTC;
+    for (int idx = tid; idx < DP * (kTC / 4); idx += blockDim.x) {
+      const int k = idx / (kTC / 4), q = idx % (kTC / 4);
+      tp_cp_async16(&sm.Bs[buf][k][q * 4], p.bt + (int64_t)k * p.c_pad + c0 + q * 4);
+    }
+    if (tid < kTC / 4) tp_cp_async16(&sm.wb[buf][tid * 4], p.wbv + c0 + tid * 4);
+    for (int idx = tid; idx < KD * (kTC / 4); idx += blockDim.x) {
+      const int kk = idx / (kTC / 4), q = idx % (kTC / 4);
+      if (kk < p.K)
+        tp_cp_async16(&sm.Vs[buf][kk][q * 4], p.vt + (int64_t)kk * p.c_pad + c0 + q * 4);
+    }
+    tp_cp_async_commit();
+  };
+
+  const int64_t ntiles_all = (p.C + kTC - 1) / kTC;
+  const int64_t t_begin = ntiles_all * blockIdx.z / p.splits;
+  const int64_t t_end = ntiles_all * (blockIdx.z + 1) / p.splits;
+  if (t_begin < t_end) issue(t_begin, 0);
+  for (int64_t t = t_begin; t < t_end; ++t) {
+    const int buf = (int)((t - t_begin) & 1);
+    __syncthreads();  // the other buffer's previous tile consumed
+    if (t + 1 < t_end) {
+      issue(t + 1, buf ^ 1);
+      tp_cp_async_wait<1>();
+    } else {
+      tp_cp_async_wait<0>();
+    }
+    __syncthreads();
+
+    float z[8][8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < DP; ++k) {
+      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
+      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
+      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][tx * 4]);
+      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][64 + tx * 4]);
+      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
+    }
+    float vv[KD][8];
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk) {
+      const float4 v0 = *reinterpret_cast<const float4*>(&sm.Vs[buf][kk][tx * 4]);
+      const float4 v1 = *reinterpret_cast<const float4*>(&sm.Vs[buf][kk][64 + tx * 4]);
+      const bool on = kk < p.K;
+      vv[kk][0] = on ? v0.x : 0.f; vv[kk][1] = on ? v0.y : 0.f;
+      vv[kk][2] = on ? v0.z : 0.f; vv[kk][3] = on ? v0.w : 0.f;
+      vv[kk][4] = on ? v1.x : 0.f; vv[kk][5] = on ? v1.y : 0.f;
+      vv[kk][6] = on ? v1.z : 0.f; vv[kk][7] = on ? v1.w : 0.f;
+    }
+    {
+      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[buf][tx * 4]);
+      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[buf][64 + tx * 4]);
+      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
+                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+      if (mx > mrow[i]) {
+        const float sc = ex2_approx(mrow[i] - mx);
+#pragma unroll
+        for (int kk = 0; kk < KD; ++kk) o[i][kk] *= sc;
+        mrow[i] = mx;
+      }
+      float e[8];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(z[i][j] - mrow[i]);
+#pragma unroll
+      for (int kk = 0; kk < KD; ++kk) {
+        float part = e[0] * vv[kk][0];
+#pragma unroll
+        for (int j = 1; j < 8; ++j) part = fmaf(e[j], vv[kk][j], part);
+        o[i][kk] += part;
+      }
+    }
+  }
+
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk)
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        o[i][kk] += __shfl_xor_sync(0xffffffffu, o[i][kk], off);
+  if (tx != 0) return;
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+    const int64_t gr = row0 + r;
+    if (gr >= p.R) continue;
+    const bool any = mrow[i] > kNegSentinel;
+    if (p.splits > 1) {
+      const int64_t sp = blockIdx.z;
+      p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
+#pragma unroll
+      for (int kk = 0; kk < KD; ++kk)
+        if (kk < p.K) p.part_o[(sp * p.K + kk) * p.R + gr] = any ? o[i][kk] : 0.f;
+      continue;
+    }
+    const float scale = any ? exp2f(mrow[i]) : 0.f;
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk)
+      if (kk < p.K) p.out[(int64_t)kk * p.R + gr] = any ? o[i][kk] * scale : 0.f;
+  }
+}
+
+template <int DP, int KD>
+int launch_direct_pipelined(const ApplyArgs& a, cudaStream_t stream);
+
 template <int DP, int KD>
 int launch_direct(const ApplyArgs& a, cudaStream_t stream) {
+  if constexpr (DP <= 64) {
+    if (a.bt) return launch_direct_pipelined<DP, KD>(a, stream);
+  }
   const size_t smem = sizeof(DirectSmem<DP, KD>);
   auto k = apply_direct_kernel<DP, KD>;
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
@@ -794,6 +982,32 @@ int launch_direct(const ApplyArgs& a, cudaStream_t stream) {
                             stream>>>(a);
   }
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+template <int DP, int KD>
+int launch_direct_pipelined(const ApplyArgs& a, cudaStream_t stream) {
+  {
+    const size_t smem = sizeof(DirectPipeSmem<DP, KD>);
+    auto k = apply_direct_pipelined_kernel<DP, KD>;
+    if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+      return OTTB_ERR_CUDA;
+    apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
+    const int64_t tot = (int64_t)DP * a.c_pad;
+    apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
+                          stream>>>(a, DP);
+    const int64_t vtot = (int64_t)a.K * a.c_pad;
+    apply_prep_vpad_kernel<<<(unsigned)std::min<int64_t>((vtot + 255) / 256, 4096), 256, 0,
+                             stream>>>(a);
+    dim3 grid((unsigned)((a.R + kTR - 1) / kTR), 1u, (unsigned)a.splits);
+    k<<<grid, 256, smem, stream>>>(a);
+    if (a.splits > 1) {
+      const int64_t total = (int64_t)a.K * a.R;
+      combine_splits_kernel<<<(unsigned)std::min<int64_t>((total + 255) / 256, 4096), 256, 0,
+                              stream>>>(a);
+    }
+    return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+  }
 }
 
 // Up to this many vectors take the register path (apply_direct_kernel).
@@ -856,7 +1070,9 @@ struct PrepLayout {
 
 inline size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
-bool pipelined_path(int d, int K) { return d <= 64 && K > 2; }
+// Prepared operands for d <= 64: every vector count (the one- and two-vector
+// register path included).
+bool pipelined_path(int d, int K) { return d <= 64 && K >= 1; }
 
 PrepLayout prep_layout(int64_t C, int d, int K, size_t base) {
   PrepLayout L;
@@ -864,7 +1080,8 @@ PrepLayout prep_layout(int64_t C, int d, int K, size_t base) {
   apply_vt_chunks(d, K, &vt, &chunks);
   const int dp = d <= 8 ? 8 : d <= 16 ? 16 : d <= 32 ? 32 : 64;
   L.c_pad = (C + kTC - 1) / kTC * kTC;
-  L.k_pad = (int64_t)chunks * 16 * vt;
+  // [c_pad][k_pad] for the many-vector kernel; [K][c_pad] on the register path
+  L.k_pad = K <= 2 ? K : (int64_t)chunks * 16 * vt;
   size_t off = align256(base);
   L.cen = off;
   off = align256(off + sizeof(float) * 64);

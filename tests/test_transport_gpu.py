@@ -116,9 +116,12 @@ def test_gradient_of_self_transport_sums_both_roles():
                              atol=1e-7)
 
 
-def test_column_splits_match_single_pass():
-  """The same application with the B points split across CTAs (workspace)
-  and in one pass (no workspace): equal up to FP32 summation order."""
+@pytest.mark.parametrize("k", [1, 2, 7])
+def test_column_splits_match_single_pass(k):
+  """The same application with the workspace (column splits, and the
+  prepared operands of the pipelined kernels) and without (one pass,
+  operands transposed inside the kernel): equal up to FP32 summation
+  order."""
   import ctypes
   import torch
   from ott_b200 import _lib
@@ -126,17 +129,17 @@ def test_column_splits_match_single_pass():
   x, y, a, b = problems.uniform_cloud_problem(900, 3000, 16, seed=12)
   geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean")
   n, m, d = 900, 3000, 16
-  vec = torch.randn(7, m, device="cuda")
+  vec = torch.randn(k, m, device="cuda")
   res = []
   for use_ws in (False, True):
-    ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, d, 7, 1) if use_ws else 0
+    ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, d, k, 1) if use_ws else 0
     assert (ws_bytes > 0) == use_ws
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device="cuda")
-    o = torch.empty(7, n, device="cuda")
+    o = torch.empty(k, n, device="cuda")
     st = lib.ottb_apply_transport(geom.x.data_ptr(), geom.y.data_ptr(), n, m, d,
                                   out.f.data_ptr(), out.g.data_ptr(),
                                   ctypes.c_float(geom.epsilon), ctypes.c_float(1.0),
-                                  vec.data_ptr(), 7, 1, o.data_ptr(), ws.data_ptr(), ws_bytes,
+                                  vec.data_ptr(), k, 1, o.data_ptr(), ws.data_ptr(), ws_bytes,
                                   torch.cuda.current_stream().cuda_stream)
     assert st == 0
     res.append(o.cpu().numpy())
