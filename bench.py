@@ -689,7 +689,7 @@ def run_anneal(args):
   geometrically from 1 to 1e-3 * mean(C) over ``--stages`` stages, threshold
   1e-3 per stage, every pair in one launch per stage, each stage warm-started
   from the previous one; FP32 redoes any stage the chosen form does not
-  converge. The plain FP32 chain on pair 0 is the judge."""
+  converge. The plain FP32 chain on pair 0 is the accuracy reference."""
   import torch
   from tests import problems
   from ott_b200.solvers.linear import annealing

@@ -11,7 +11,7 @@ order of the reference is kept (centre ``f + g - C``, divide by epsilon,
 max-shifted logsumexp, multiply by epsilon, subtract the finite potential) so
 that the float32 mode reproduces the reference's FP32 rounding behaviour as
 closely as a different backend can, and the float64 mode is the accuracy
-judge (the reference run with ``jax_enable_x64``).
+reference (the reference run with ``jax_enable_x64``).
 
 The arithmetic core of the reference lives in a third-party dependency that is
 absent here: ``jax.scipy.special.logsumexp`` (jax, unpinned ``jax>=0.4.0`` in

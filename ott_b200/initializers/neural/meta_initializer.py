@@ -223,8 +223,8 @@ def solve_warm_started(geom, a: torch.Tensor, b: torch.Tensor, meta: MetaInitial
   """Solves the stacked problems (a [K, n], b [K, m] on ``geom``) with the
   learned warm start; problems that have not converged within ``budget``
   iterations are solved again from the default initialisation with the
-  full ``max_iterations`` (the plain solver stays the fallback and the judge
-  of convergence).
+  full ``max_iterations`` (the plain solver stays the fallback and decides
+  convergence).
 
   Returns (output, fallback_indices); the output's rows of the fallback
   problems hold the fallback solve.
