@@ -202,6 +202,21 @@ int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, in
                                    int32_t axis, int32_t precision, float* out,
                                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* The log-domain kernel application (geometry/geometry.py:259-299,
+ * apply_lse_kernel, vec = None) on the solver's sweep engine: axis 0
+ * out[j] = eps log sum_i exp((pot_i - C_ij) / eps) over x (pot = f, out over
+ * y); axis 1 the same over y (pot = g, out over x). One zero-iteration solve
+ * whose final sweep's log-sum-exp is written out; the per-shard step of a
+ * row-sharded solve, whose column log-sum-exps are combined across ranks.
+ * Workspace from ottb_apply_lse_kernel_workspace_size (256-byte aligned). */
+size_t ottb_apply_lse_kernel_workspace_size(int64_t n, int64_t m, int32_t d, int32_t axis,
+                                            int32_t precision);
+int32_t ottb_apply_lse_kernel(const float* x, const float* y, int64_t n, int64_t m,
+                              int32_t d, const float* pot, float epsilon,
+                              float inv_scale_cost, int32_t axis, int32_t precision,
+                              float* out, void* workspace, size_t workspace_bytes,
+                              void* stream);
+
 /* The plan itself, out [n][m] row-major (geometry/geometry.py:361-365,
  * transport_from_potentials; sinkhorn.py:346-349, SinkhornOutput.matrix). */
 int32_t ottb_transport_matrix(const float* x, const float* y, int64_t n, int64_t m,

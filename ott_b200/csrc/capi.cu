@@ -428,7 +428,7 @@ int outer_of(const ottb_solver_cfg* cfg) {
 // into the pristine region of the workspace: one host-to-device copy.
 int write_header(const ottb_problem* problems, int num_problems, const ottb_solver_cfg* cfg,
                  const Plan& plan, char* ws, cudaStream_t stream,
-                 float* const* marg_out = nullptr) {
+                 float* const* marg_out = nullptr, float* const* lse_out = nullptr) {
   const int outer = outer_of(cfg);
   std::vector<char> host(plan.header_bytes, 0);
   Sched* sched = (Sched*)(host.data() + plan.off_sched);
@@ -487,6 +487,7 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     P.outer = outer;
     P.symmetric = q.symmetric;
     P.marg_out = marg_out ? marg_out[plan.order[t]] : nullptr;
+    P.lse_out = lse_out ? lse_out[plan.order[t]] : nullptr;
     pd[t] = P;
     ps[t].active = 1;
     ps[t].split_f = pp.split_f;
@@ -625,7 +626,7 @@ struct SweepApply {
   ottb_solver_cfg cfg{};
   Plan plan;
   size_t off_fp = 0, off_fo = 0, off_go = 0, off_wa = 0, off_wb = 0, off_err = 0,
-         off_marg = 0, off_res = 0, total = 0;
+         off_marg = 0, off_res = 0, off_gz = 0, total = 0;
 };
 
 __global__ void sweep_apply_potential_kernel(const float* pot, const float* vec, int64_t R,
@@ -703,6 +704,7 @@ int sweep_apply_setup(const float* x, const float* y, int64_t n, int64_t m, int 
   S.off_err = take(sizeof(float) * np);
   S.off_marg = take(sizeof(float) * np * S.C);
   S.off_res = take(sizeof(ottb_result) * np);
+  S.off_gz = take(sizeof(float) * S.C);
   S.total = off;
   if (!ws) return OTTB_OK;
   for (int q = 0; q < np; ++q) {
@@ -908,6 +910,59 @@ int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, in
   sweep_apply_diff_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
                             stream>>>((const float*)(ws + S.off_marg), S.C, num_vec, out);
   return cuda_status(cudaGetLastError());
+}
+
+size_t ottb_apply_lse_kernel_workspace_size(int64_t n, int64_t m, int32_t d, int32_t axis,
+                                            int32_t precision) {
+  if (n < 1 || m < 1 || d < 1 || (axis != 0 && axis != 1)) return 0;
+  SweepApply S;
+  std::vector<ottb_problem> probs;
+  std::vector<float*> marg;
+  // one problem: the layout of a one-vector application holds it
+  if (sweep_apply_setup(nullptr, nullptr, n, m, d, nullptr, nullptr, 1.f, 1.f, 1, axis,
+                        precision, nullptr, false, S, probs, marg) != OTTB_OK)
+    return 0;
+  return S.total;
+}
+
+int32_t ottb_apply_lse_kernel(const float* x, const float* y, int64_t n, int64_t m,
+                              int32_t d, const float* pot, float epsilon,
+                              float inv_scale_cost, int32_t axis, int32_t precision,
+                              float* out, void* workspace, size_t workspace_bytes,
+                              void* stream_ptr) {
+  if (!x || !y || !pot || !out || n < 1 || m < 1 || d < 1) return OTTB_ERR_INVALID;
+  if (axis != 0 && axis != 1) return OTTB_ERR_INVALID;
+  if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
+  if (!workspace || ((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  char* ws = (char*)workspace;
+  SweepApply S;
+  std::vector<ottb_problem> probs;
+  std::vector<float*> marg;
+  int st = sweep_apply_setup(x, y, n, m, d, pot, pot, epsilon, inv_scale_cost, 1, axis,
+                             precision, ws, true, S, probs, marg);
+  if (st != OTTB_OK) return st;
+  if (workspace_bytes < S.total) return OTTB_ERR_WORKSPACE;
+  cudaStream_t stream = (cudaStream_t)stream_ptr;
+  // one zero-iteration problem: row potential pot, column potential 0; the
+  // final sweep's log-sum-exp goes to out
+  probs.resize(1);
+  probs[0].f_init = pot;
+  probs[0].g_init = (const float*)(ws + S.off_gz);
+  if (cudaMemsetAsync(ws + S.off_gz, 0, sizeof(float) * S.C, stream) != cudaSuccess)
+    return OTTB_ERR_CUDA;
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.R + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wa), S.R, 1.f / (float)S.R);
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.C + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wb), S.C, 1.f / (float)S.C);
+  if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+  Plan plan1;
+  st = make_plan(probs.data(), 1, d, &S.cfg, true, plan1);
+  if (st != OTTB_OK) return st;
+  if (plan1.total > S.off_fp) return OTTB_ERR_WORKSPACE;  // the solver region of the layout
+  float* lse[1] = {out};
+  st = write_header(probs.data(), 1, &S.cfg, plan1, ws, stream, nullptr, lse);
+  if (st != OTTB_OK) return st;
+  return launch_solve(1, d, &S.cfg, (ottb_result*)(ws + S.off_res), plan1, ws, stream);
 }
 
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {

@@ -68,6 +68,8 @@ struct ProbDev {
   int outer;           // length of errors
   int symmetric;       // x == y, a == b: g-sweeps only, momentum 1/2, f = g
   float* marg_out;     // [m] column marginal of the final evaluation sweep, or null
+  float* lse_out;      // [m] eps log sum_i exp((f_i + g_j - C_ij) / eps) - g_j of
+                       // that sweep (apply_lse_kernel), or null
 };
 
 // Operands of one sweep for one problem, resolved from the descriptor.

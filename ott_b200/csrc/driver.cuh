@@ -132,6 +132,7 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       err_t = (norm_error == 1) ? dv : pow(dv, (double)norm_error);
       msum_t = bh;
       if (sp.final_eval && P.marg_out) P.marg_out[r] = (float)bh;
+      if (sp.final_eval && P.lse_out) P.lse_out[r] = (float)app;  // eps LSE_i - |y_j|^2 term
     }
   }
   if (sp.eval) {

@@ -282,6 +282,40 @@ class PointCloud(geometry.Geometry):
     gx, gy = self._points_vjp(rows, gy_rows, cols, gx_cols, gc)
     return gx, gy, u, w
 
+  def apply_lse_kernel(self, f: torch.Tensor, g: torch.Tensor, eps: float,
+                       vec: Any = None, axis: int = 0,
+                       precision: str = "fp32") -> Tuple[torch.Tensor, torch.Tensor]:
+    """geometry.py:259-299 with ``vec=None``: ``eps log sum exp((f + g - C)
+    / eps)`` over rows (``axis=0``, one value per column) or columns,
+    minus the finite part of g (axis 0) or f, and the sign 1.
+    ``ottb_apply_lse_kernel`` on the solver's sweep ("auto" / "bf16_split3":
+    tensor cores for d >= 32)."""
+    if vec is not None:
+      raise NotImplementedError("the signed-vector form is apply_transport_from_potentials")
+    if axis not in (0, 1):
+      raise ValueError("axis must be 0 or 1")
+    lib = _lib.load()
+    n, m = self.shape
+    dev = self.x.device
+    pot = _arrays.as_f32(f if axis == 0 else g, dev).detach().contiguous()
+    rem = _arrays.as_f32(g if axis == 0 else f, dev).detach()
+    code = {"auto": _lib.PRECISION_AUTO, "fp32": _lib.PRECISION_FP32,
+            "bf16_split3": _lib.PRECISION_BF16_SPLIT3}[precision]
+    ws_bytes = lib.ottb_apply_lse_kernel_workspace_size(n, m, self.dim, axis, code)
+    if ws_bytes == 0:
+      raise NotImplementedError("problem sizes not supported")
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    out = torch.empty(m if axis == 0 else n, dtype=torch.float32, device=dev)
+    st = lib.ottb_apply_lse_kernel(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
+                                   pot.data_ptr(), ctypes.c_float(eps),
+                                   ctypes.c_float(self.inv_scale_cost), axis, code,
+                                   out.data_ptr(), ws.data_ptr(), ws_bytes,
+                                   _arrays.stream_handle())
+    _lib.check(st, "ottb_apply_lse_kernel")
+    # a -inf potential on the output side makes every entry -inf there
+    out = torch.where(torch.isneginf(rem), torch.full_like(out, -float("inf")), out)
+    return out, torch.ones(1, device=dev)
+
   def marginal_from_potentials(self, f: torch.Tensor, g: torch.Tensor,
                                axis: int = 0) -> torch.Tensor:
     """geometry.py:326-349: column (``axis=0``) or row (``axis=1``)
