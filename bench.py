@@ -55,7 +55,7 @@ def parse_args():
   p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
   p.add_argument("--workload", default="gaussian64",
                  choices=["gaussian64", "warmstart", "batched", "anneal", "divergence",
-                          "implicit"],
+                          "implicit", "sharded"],
                  help="gaussian64: the headline single large solve (default); "
                       "warmstart: learned warm start on a 32x32 grid; batched: 512 "
                       "uneven problems in one launch; anneal: epsilon-annealed solves; "
@@ -941,6 +941,88 @@ def run_implicit(args):
   return 0
 
 
+def run_sharded(args):
+  """The headline problem (n = m = ``--n``, d = ``--d``, epsilon = 0.01 *
+  mean(C), threshold 1e-3) row-sharded over the ranks (strong scaling: the
+  problem is fixed, each rank holds n / N rows of x and all of y): per
+  iteration two log-domain kernel applications per rank
+  (``ottb_apply_lse_kernel``) and one all-gather of the column
+  log-sum-exps. Time to threshold, max over ranks; against the one-launch
+  persistent solve of the same problem on one GPU."""
+  import torch
+  import torch.distributed as dist
+  from datetime import timedelta
+  from ott_b200 import distributed as odist
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import sharded
+  world = int(os.environ.get("WORLD_SIZE", "1"))
+  rank = int(os.environ.get("RANK", "0"))
+  local = int(os.environ.get("LOCAL_RANK", "0"))
+  torch.cuda.set_device(local)
+  if world > 1:
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600),
+                            device_id=torch.device("cuda", local))
+  x, y, a, b = workload(args)
+  lo, hi = odist.shard_bounds([1.0] * args.n, world)[rank]
+  xd = torch.from_numpy(x[lo:hi]).cuda()
+  yd = torch.from_numpy(y).cuda()
+  ad = torch.from_numpy(a[lo:hi]).cuda()
+  bd = torch.from_numpy(b).cuda()
+  ev = lambda: torch.cuda.Event(enable_timing=True)
+
+  def step():
+    out = sharded.solve_sharded(xd, yd, ad, bd, epsilon=0.01, relative_epsilon="mean",
+                                threshold=1e-3, precision=args.precision)
+    return out
+
+  for _ in range(args.warmup):
+    step()
+  if world > 1:
+    dist.barrier()
+  torch.cuda.synchronize()
+  clocks = ClockSampler(local)
+  clocks.start()
+  e0, e1 = ev(), ev()
+  e0.record()
+  for _ in range(args.steps):
+    out = step()
+  e1.record()
+  e1.synchronize()
+  clk = clocks.stop()
+  t = odist.max_over_ranks(e0.elapsed_time(e1) / args.steps * 1e-3)
+  single = None
+  if world == 1:
+    geom = pointcloud.PointCloud(torch.from_numpy(x).cuda(), yd, epsilon=0.01,
+                                 relative_epsilon="mean")
+    for _ in range(2):
+      linear.solve(geom, threshold=1e-3, precision=args.precision).n_iters
+    e0, e1 = ev(), ev()
+    e0.record()
+    ref = linear.solve(geom, threshold=1e-3, precision=args.precision)
+    e1.record()
+    e1.synchronize()
+    single = {"s": e0.elapsed_time(e1) * 1e-3, "n_iters": ref.n_iters,
+              "reg_ot_cost": ref.reg_ot_cost}
+  line = {
+      "metric": "s to 1e-3 marginal err, one problem row-sharded over the ranks",
+      "value": t, "unit": "s", "higher_is_better": False, "n_gpus": world,
+      "scaling": "strong", "workload": "sharded", "data": "synthetic",
+      "steps": args.steps, "warmup": args.warmup,
+      "config": {"workload": f"sinkhorn sqeuclidean n=m={args.n} d={args.d} eps=0.01*mean(C) "
+                             f"thr=1e-3, rows split over {world} rank(s)",
+                 "parallelism": f"row shards x{world}, all-gather of m column LSEs per "
+                                "iteration"},
+      "n_iters": out.n_iters, "reg_ot_cost": out.reg_ot_cost, "converged": out.converged,
+      "one_gpu_persistent_solve": single, "clocks": clk,
+  }
+  if rank == 0:
+    print(json.dumps(line))
+  if world > 1:
+    dist.destroy_process_group()
+  return 0
+
+
 def main():
   args = parse_args()
   if args.warmup < 3:
@@ -957,6 +1039,8 @@ def main():
     return run_divergence(args)
   if args.workload == "implicit":
     return run_implicit(args)
+  if args.workload == "sharded":
+    return run_sharded(args)
   return run_ours(args)
 
 
