@@ -57,6 +57,10 @@ def _gpu_lse(x: torch.Tensor, y: torch.Tensor, eps: float, inv: float,
   """``ottb_apply_lse_kernel`` on this rank's rows and all columns."""
   lib = _lib.load()
   n, m, d = x.shape[0], y.shape[0], x.shape[1]
+  if n == 0:  # a rank without rows (more ranks than rows): nothing to sum
+    return lambda pot, axis: (torch.full((m,), -math.inf, dtype=torch.float64,
+                                         device=x.device) if axis == 0
+                              else torch.empty(0, dtype=torch.float64, device=x.device))
   code = _PREC[precision]
   sizes = [lib.ottb_apply_lse_kernel_workspace_size(n, m, d, ax, code) for ax in (0, 1)]
   if min(sizes) == 0:
