@@ -102,6 +102,209 @@ __device__ void apply_center(const ApplyArgs& p, float* center) {
   }
 }
 
+// ---- pieces shared by the application kernels -----------------------------
+// Rows of this thread's 8 x 8 micro-tile: ty*4 + {0..3}, 64 + ty*4 + {0..3};
+// its columns are tx*4 + {0..3}, 64 + tx*4 + {0..3}.
+__device__ __forceinline__ int tile_row(int ty, int i) {
+  return (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
+}
+
+// The A tile (transposed, centred; rows beyond R are zero points), then the
+// row terms u_r = (potA_r - inv |A_r|^2) * ws of this thread's 8 rows
+// (-inf beyond R).
+template <int DP, int LD>
+__device__ __forceinline__ void load_rows(const ApplyArgs& p, float (*As)[LD],
+                                          const float* center, int64_t row0, int ty,
+                                          float u[8]) {
+  for (int idx = threadIdx.x; idx < DP * kTR; idx += blockDim.x) {
+    const int r = idx / DP, k = idx % DP;
+    const int64_t gr = row0 + r;
+    As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - center[k] : 0.f;
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int r = tile_row(ty, i);
+    const int64_t gr = row0 + r;
+    float nrm = 0.f;
+    for (int k = 0; k < DP; ++k) nrm = fmaf(As[k][r], As[k][r], nrm);
+    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
+  }
+}
+
+// Exponents z = s <A_r, B_c> + wb_c + u_r (log2 units) of the micro-tile:
+// an FFMA chain over the d coordinates, then one rounding for the scale and
+// shift.
+template <int DP, int LDA, int LDB>
+__device__ __forceinline__ void cost_tile(const float (*As)[LDA], const float (*Bs)[LDB],
+                                          const float* wb, float s, const float u[8], int tx,
+                                          int ty, float z[8][8]) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
+#pragma unroll 4
+  for (int k = 0; k < DP; ++k) {
+    const float4 a0 = *reinterpret_cast<const float4*>(&As[k][ty * 4]);
+    const float4 a1 = *reinterpret_cast<const float4*>(&As[k][64 + ty * 4]);
+    const float4 b0 = *reinterpret_cast<const float4*>(&Bs[k][tx * 4]);
+    const float4 b1 = *reinterpret_cast<const float4*>(&Bs[k][64 + tx * 4]);
+    const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+    const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
+  }
+  const float4 w0 = *reinterpret_cast<const float4*>(&wb[tx * 4]);
+  const float4 w1 = *reinterpret_cast<const float4*>(&wb[64 + tx * 4]);
+  const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
+}
+
+// Per row: the tile's maximum over the 16 threads of the row; when it grows
+// the row's NA running sums are rescaled; then z = 2^(z - max).
+template <int NA>
+__device__ __forceinline__ void exp_rows(float z[8][8], float mrow[8], float o[8][NA]) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
+                     fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
+#pragma unroll
+    for (int off = 1; off < 16; off <<= 1)
+      mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+    if (mx > mrow[i]) {
+      const float sc = ex2_approx(mrow[i] - mx);
+#pragma unroll
+      for (int j = 0; j < NA; ++j) o[i][j] *= sc;
+      mrow[i] = mx;
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) z[i][j] = ex2_approx(z[i][j] - mrow[i]);
+  }
+}
+
+// The weights of the micro-tile into the swizzled P tile: rows ty*4 .. +3
+// (quad ty) and 64 + ty*4 .. +3 (quad 16 + ty) of each of its columns.
+__device__ __forceinline__ void store_p_quads(float* Ps, const float z[8][8], int tx, int ty) {
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
+    *reinterpret_cast<float4*>(Ps + pquad(c, ty)) =
+        make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
+    *reinterpret_cast<float4*>(Ps + pquad(c, 16 + ty)) =
+        make_float4(z[4][j], z[5][j], z[6][j], z[7][j]);
+  }
+}
+
+// O[r][k] += sum_c P[r][c] V[c][k] for this thread's 8 rows and vectors
+// tx + 16 j; the tile's contribution is summed apart, then added once.
+template <int VT, int LDV>
+__device__ __forceinline__ void pv_tile(const float* Ps, const float (*Vs)[LDV], int tx, int ty,
+                                        float o[8][VT]) {
+  float acc[8][VT];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < VT; ++j) acc[i][j] = 0.f;
+#pragma unroll 4
+  for (int c = 0; c < kTC; ++c) {
+    const float4 p0 = *reinterpret_cast<const float4*>(Ps + pquad(c, ty));
+    const float4 p1 = *reinterpret_cast<const float4*>(Ps + pquad(c, 16 + ty));
+    const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+    float vv[VT];
+#pragma unroll
+    for (int j = 0; j < VT; ++j) vv[j] = Vs[c][tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < VT; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
+  }
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < VT; ++j) o[i][j] += acc[i][j];
+}
+
+// Row r's sums times 2^max into out (a row whose weights are all zero gives
+// 0), or with column splits this split's sums and shift into the workspace.
+// Vector j of this thread is k0 + tx + 16 j (lane_stride 16), or k0 + j with
+// the lanes of a row already reduced (lane_stride 0, thread tx == 0).
+template <int NV>
+__device__ __forceinline__ void store_rows(const ApplyArgs& p, const float o[8][NV],
+                                           const float mrow[8], int64_t row0, int tx, int ty,
+                                           int k0, int lane_stride) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int64_t gr = row0 + tile_row(ty, i);
+    if (gr >= p.R) continue;
+    const bool any = mrow[i] > kNegSentinel;
+    if (p.splits > 1) {
+      const int64_t sp = blockIdx.z;
+      if (tx == 0 && blockIdx.y == 0) p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
+#pragma unroll
+      for (int j = 0; j < NV; ++j) {
+        const int k = k0 + tx * (lane_stride ? 1 : 0) + (lane_stride ? 16 : 1) * j;
+        if (k < p.K) p.part_o[(sp * p.K + k) * p.R + gr] = any ? o[i][j] : 0.f;
+      }
+      continue;
+    }
+    const float scale = any ? exp2f(mrow[i]) : 0.f;
+#pragma unroll
+    for (int j = 0; j < NV; ++j) {
+      const int k = k0 + tx * (lane_stride ? 1 : 0) + (lane_stride ? 16 : 1) * j;
+      if (k < p.K) p.out[(int64_t)k * p.R + gr] = any ? o[i][j] * scale : 0.f;
+    }
+  }
+}
+
+// The one- or two-vector products of the micro-tile: exponentials as in
+// exp_rows, times the vectors' entries at this thread's 8 columns (the
+// first k_valid vectors; the others are 0), added to the row sums.
+template <int KD>
+__device__ __forceinline__ void direct_tile(float z[8][8], float mrow[8], float o[8][KD],
+                                            const float (*Vs)[kTC], int tx, int k_valid) {
+  float vv[KD][8];
+#pragma unroll
+  for (int kk = 0; kk < KD; ++kk) {
+    const float4 v0 = *reinterpret_cast<const float4*>(&Vs[kk][tx * 4]);
+    const float4 v1 = *reinterpret_cast<const float4*>(&Vs[kk][64 + tx * 4]);
+    const bool on = kk < k_valid;
+    vv[kk][0] = on ? v0.x : 0.f; vv[kk][1] = on ? v0.y : 0.f;
+    vv[kk][2] = on ? v0.z : 0.f; vv[kk][3] = on ? v0.w : 0.f;
+    vv[kk][4] = on ? v1.x : 0.f; vv[kk][5] = on ? v1.y : 0.f;
+    vv[kk][6] = on ? v1.z : 0.f; vv[kk][7] = on ? v1.w : 0.f;
+  }
+  exp_rows<KD>(z, mrow, o);
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk) {
+      float part = z[i][0] * vv[kk][0];
+#pragma unroll
+      for (int j = 1; j < 8; ++j) part = fmaf(z[i][j], vv[kk][j], part);
+      o[i][kk] += part;
+    }
+}
+
+// The 16 threads of a row hold partial sums with the same shift: add them,
+// and thread tx == 0 stores the row.
+template <int KD>
+__device__ __forceinline__ void direct_store(const ApplyArgs& p, float o[8][KD],
+                                             const float mrow[8], int64_t row0, int tx, int ty) {
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int kk = 0; kk < KD; ++kk)
+#pragma unroll
+      for (int off = 1; off < 16; off <<= 1)
+        o[i][kk] += __shfl_xor_sync(0xffffffffu, o[i][kk], off);
+  if (tx == 0) store_rows<KD>(p, o, mrow, row0, 0, ty, 0, 0);
+}
+
 template <int DP, int VT>
 __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -116,24 +319,8 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
 
   apply_center<DP>(p, sm.center);
   __syncthreads();
-  // A tile (rows beyond R are zero points with potential -inf)
-  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
-    const int r = idx / DP, k = idx % DP;
-    const int64_t gr = row0 + r;
-    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
-  }
-  __syncthreads();
-  // row terms u_r = (potA_r - inv |A_r|^2) * ws of this thread's 8 rows
   float u[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    float nrm = 0.f;
-    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
-    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
-  }
-
+  load_rows<DP>(p, sm.As, sm.center, row0, ty, u);
   float mrow[8];
   float o[8][VT];
 #pragma unroll
@@ -167,113 +354,14 @@ __global__ void __launch_bounds__(256, 1) apply_transport_kernel(ApplyArgs p) {
       sm.wb[tid] = gc < p.C ? (__ldg(p.potB + gc) - p.inv * nrm) * p.ws : -INFINITY;
     }
     __syncthreads();
-
-    // exponents of the 8 x 8 micro-tile
     float z[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < DP; ++k) {
-      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[k][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[k][64 + tx * 4]);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
-    }
-    {
-      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[tx * 4]);
-      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[64 + tx * 4]);
-      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
-    }
-    // row maxima over the tile (16 threads share a row), rescale the sums
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
-                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (mx > mrow[i]) {
-        const float sc = ex2_approx(mrow[i] - mx);
-#pragma unroll
-        for (int j = 0; j < VT; ++j) o[i][j] *= sc;
-        mrow[i] = mx;
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = ex2_approx(z[i][j] - mrow[i]);
-    }
-    // P quads: rows ty*4 .. +3 (quad ty) and 64 + ty*4 .. +3 (quad 16 + ty)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
-      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, ty)) =
-          make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
-      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty)) =
-          make_float4(z[4][j], z[5][j], z[6][j], z[7][j]);
-    }
+    cost_tile<DP>(sm.As, sm.Bs, sm.wb, s, u, tx, ty, z);
+    exp_rows<VT>(z, mrow, o);
+    store_p_quads(&sm.Ps[0][0], z, tx, ty);
     __syncthreads();
-    // O[r][k] += sum_c P[r][c] V[c][k]: rows of this thread's micro-tile,
-    // vectors tx + 16 j
-    float acc[8][VT];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < VT; ++j) acc[i][j] = 0.f;
-#pragma unroll 4
-    for (int c = 0; c < kTC; ++c) {
-      const float4 p0 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, ty));
-      const float4 p1 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty));
-      const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-      float vv[VT];
-#pragma unroll
-      for (int j = 0; j < VT; ++j) vv[j] = sm.Vs[c][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < VT; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < VT; ++j) o[i][j] += acc[i][j];
+    pv_tile<VT>(&sm.Ps[0][0], sm.Vs, tx, ty, o);
   }
-
-  // out = O * 2^max (a row whose weights are all zero gives 0); with
-  // splits, the sums and shifts of this split
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    if (gr >= p.R) continue;
-    const bool any = mrow[i] > kNegSentinel;
-    if (p.splits > 1) {
-      const int64_t sp = blockIdx.z;
-      if (tx == 0 && blockIdx.y == 0) p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
-#pragma unroll
-      for (int j = 0; j < VT; ++j) {
-        const int k = k0 + tx + 16 * j;
-        if (k < p.K) p.part_o[(sp * p.K + k) * p.R + gr] = any ? o[i][j] : 0.f;
-      }
-      continue;
-    }
-    const float scale = any ? exp2f(mrow[i]) : 0.f;
-#pragma unroll
-    for (int j = 0; j < VT; ++j) {
-      const int k = k0 + tx + 16 * j;
-      if (k < p.K) p.out[(int64_t)k * p.R + gr] = any ? o[i][j] * scale : 0.f;
-    }
-  }
+  store_rows<VT>(p, o, mrow, row0, tx, ty, k0, 16);
 }
 
 __device__ __forceinline__ void tp_cp_async16(void* smem, const void* gmem) {
@@ -378,22 +466,8 @@ __global__ void __launch_bounds__(256, 1) apply_pipelined_kernel(ApplyArgs p) {
 
   for (int k = tid; k < DP; k += blockDim.x) sm.center[k] = p.cen[k];
   __syncthreads();
-  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
-    const int r = idx / DP, k = idx % DP;
-    const int64_t gr = row0 + r;
-    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
-  }
-  __syncthreads();
   float u[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    float nrm = 0.f;
-    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
-    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
-  }
-
+  load_rows<DP>(p, sm.As, sm.center, row0, ty, u);
   float mrow[8];
   float o[8][VT];
 #pragma unroll
@@ -440,110 +514,18 @@ __global__ void __launch_bounds__(256, 1) apply_pipelined_kernel(ApplyArgs p) {
       tp_cp_async_wait<1>();
     }
     __syncthreads();
-
     float z[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < DP; ++k) {
-      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][64 + tx * 4]);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
-    }
-    {
-      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[buf][tx * 4]);
-      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[buf][64 + tx * 4]);
-      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
-                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (mx > mrow[i]) {
-        const float sc = ex2_approx(mrow[i] - mx);
-#pragma unroll
-        for (int j = 0; j < VT; ++j) o[i][j] *= sc;
-        mrow[i] = mx;
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = ex2_approx(z[i][j] - mrow[i]);
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int c = (j < 4) ? (tx * 4 + j) : (64 + tx * 4 + (j - 4));
-      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, ty)) =
-          make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
-      *reinterpret_cast<float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty)) =
-          make_float4(z[4][j], z[5][j], z[6][j], z[7][j]);
-    }
+    cost_tile<DP>(sm.As, sm.Bs[buf], sm.wb[buf], s, u, tx, ty, z);
+    exp_rows<VT>(z, mrow, o);
+    store_p_quads(&sm.Ps[0][0], z, tx, ty);
     if (has_next)
       tp_cp_async_wait<1>();  // V(t) landed (B(t + 1) may still be in flight)
     else
       tp_cp_async_wait<0>();
     __syncthreads();
-    float acc[8][VT];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < VT; ++j) acc[i][j] = 0.f;
-#pragma unroll 4
-    for (int c = 0; c < kTC; ++c) {
-      const float4 p0 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, ty));
-      const float4 p1 = *reinterpret_cast<const float4*>(&sm.Ps[0][0] + pquad(c, 16 + ty));
-      const float pv[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
-      float vv[VT];
-#pragma unroll
-      for (int j = 0; j < VT; ++j) vv[j] = sm.Vs[c][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < VT; ++j) acc[i][j] = fmaf(pv[i], vv[j], acc[i][j]);
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < VT; ++j) o[i][j] += acc[i][j];
+    pv_tile<VT>(&sm.Ps[0][0], sm.Vs, tx, ty, o);
   }
-
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    if (gr >= p.R) continue;
-    const bool any = mrow[i] > kNegSentinel;
-    if (p.splits > 1) {
-      const int64_t sp = blockIdx.z;
-      if (tx == 0 && blockIdx.y == 0) p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
-#pragma unroll
-      for (int j = 0; j < VT; ++j) {
-        const int k = k0 + tx + 16 * j;
-        if (k < p.K) p.part_o[(sp * p.K + k) * p.R + gr] = any ? o[i][j] : 0.f;
-      }
-      continue;
-    }
-    const float scale = any ? exp2f(mrow[i]) : 0.f;
-#pragma unroll
-    for (int j = 0; j < VT; ++j) {
-      const int k = k0 + tx + 16 * j;
-      if (k < p.K) p.out[(int64_t)k * p.R + gr] = any ? o[i][j] * scale : 0.f;
-    }
-  }
+  store_rows<VT>(p, o, mrow, row0, tx, ty, k0, 16);
 }
 
 // One or two vectors (the conjugate-gradient steps of implicit
@@ -574,22 +556,8 @@ __global__ void __launch_bounds__(256, (DP <= 64 ? 2 : 1)) apply_direct_kernel(A
 
   apply_center<DP>(p, sm.center);
   __syncthreads();
-  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
-    const int r = idx / DP, k = idx % DP;
-    const int64_t gr = row0 + r;
-    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
-  }
-  __syncthreads();
   float u[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    float nrm = 0.f;
-    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
-    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
-  }
-
+  load_rows<DP>(p, sm.As, sm.center, row0, ty, u);
   float mrow[8];
   float o[8][KD];
 #pragma unroll
@@ -623,96 +591,11 @@ __global__ void __launch_bounds__(256, (DP <= 64 ? 2 : 1)) apply_direct_kernel(A
       sm.wb[tid] = gc < p.C ? (__ldg(p.potB + gc) - p.inv * nrm) * p.ws : -INFINITY;
     }
     __syncthreads();
-
     float z[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < DP; ++k) {
-      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[k][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[k][64 + tx * 4]);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
-    }
-    float vv[KD][8];
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk) {
-      const float4 v0 = *reinterpret_cast<const float4*>(&sm.Vs[kk][tx * 4]);
-      const float4 v1 = *reinterpret_cast<const float4*>(&sm.Vs[kk][64 + tx * 4]);
-      vv[kk][0] = v0.x; vv[kk][1] = v0.y; vv[kk][2] = v0.z; vv[kk][3] = v0.w;
-      vv[kk][4] = v1.x; vv[kk][5] = v1.y; vv[kk][6] = v1.z; vv[kk][7] = v1.w;
-    }
-    {
-      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[tx * 4]);
-      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[64 + tx * 4]);
-      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
-                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (mx > mrow[i]) {
-        const float sc = ex2_approx(mrow[i] - mx);
-#pragma unroll
-        for (int kk = 0; kk < KD; ++kk) o[i][kk] *= sc;
-        mrow[i] = mx;
-      }
-      float e[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(z[i][j] - mrow[i]);
-#pragma unroll
-      for (int kk = 0; kk < KD; ++kk) {
-        float part = e[0] * vv[kk][0];
-#pragma unroll
-        for (int j = 1; j < 8; ++j) part = fmaf(e[j], vv[kk][j], part);
-        o[i][kk] += part;
-      }
-    }
+    cost_tile<DP>(sm.As, sm.Bs, sm.wb, s, u, tx, ty, z);
+    direct_tile<KD>(z, mrow, o, sm.Vs, tx, KD);
   }
-
-  // the 16 threads of a row hold partial sums with the same shift
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk)
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        o[i][kk] += __shfl_xor_sync(0xffffffffu, o[i][kk], off);
-  if (tx != 0) return;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    if (gr >= p.R) continue;
-    const bool any = mrow[i] > kNegSentinel;
-    if (p.splits > 1) {
-      const int64_t sp = blockIdx.z;
-      p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
-#pragma unroll
-      for (int kk = 0; kk < KD; ++kk)
-        if (kk < p.K) p.part_o[(sp * p.K + kk) * p.R + gr] = any ? o[i][kk] : 0.f;
-      continue;
-    }
-    const float scale = any ? exp2f(mrow[i]) : 0.f;
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk)
-      if (kk < p.K) p.out[(int64_t)kk * p.R + gr] = any ? o[i][kk] * scale : 0.f;
-  }
+  direct_store<KD>(p, o, mrow, row0, tx, ty);
 }
 
 // out[k][r] = sum_s part_o[s][k][r] 2^(part_m[s][r] - M) 2^M, M = max_s part_m.
@@ -814,21 +697,8 @@ apply_direct_pipelined_kernel(ApplyArgs p) {
 
   for (int k = tid; k < DP; k += blockDim.x) sm.center[k] = p.cen[k];
   __syncthreads();
-  for (int idx = tid; idx < DP * kTR; idx += blockDim.x) {
-    const int r = idx / DP, k = idx % DP;
-    const int64_t gr = row0 + r;
-    sm.As[k][r] = (gr < p.R && k < p.d) ? p.A[gr * p.d + k] - sm.center[k] : 0.f;
-  }
-  __syncthreads();
   float u[8];
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    float nrm = 0.f;
-    for (int k = 0; k < DP; ++k) nrm = fmaf(sm.As[k][r], sm.As[k][r], nrm);
-    u[i] = gr < p.R ? (__ldg(p.potA + gr) - p.inv * nrm) * p.ws : -INFINITY;
-  }
+  load_rows<DP>(p, sm.As, sm.center, row0, ty, u);
   float mrow[8];
   float o[8][KD];
 #pragma unroll
@@ -867,98 +737,11 @@ apply_direct_pipelined_kernel(ApplyArgs p) {
       tp_cp_async_wait<0>();
     }
     __syncthreads();
-
     float z[8][8];
-#pragma unroll
-    for (int i = 0; i < 8; ++i)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[i][j] = 0.f;
-#pragma unroll 4
-    for (int k = 0; k < DP; ++k) {
-      const float4 a0 = *reinterpret_cast<const float4*>(&sm.As[k][ty * 4]);
-      const float4 a1 = *reinterpret_cast<const float4*>(&sm.As[k][64 + ty * 4]);
-      const float4 b0 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][tx * 4]);
-      const float4 b1 = *reinterpret_cast<const float4*>(&sm.Bs[buf][k][64 + tx * 4]);
-      const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(av[i], bv[j], z[i][j]);
-    }
-    float vv[KD][8];
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk) {
-      const float4 v0 = *reinterpret_cast<const float4*>(&sm.Vs[buf][kk][tx * 4]);
-      const float4 v1 = *reinterpret_cast<const float4*>(&sm.Vs[buf][kk][64 + tx * 4]);
-      const bool on = kk < p.K;
-      vv[kk][0] = on ? v0.x : 0.f; vv[kk][1] = on ? v0.y : 0.f;
-      vv[kk][2] = on ? v0.z : 0.f; vv[kk][3] = on ? v0.w : 0.f;
-      vv[kk][4] = on ? v1.x : 0.f; vv[kk][5] = on ? v1.y : 0.f;
-      vv[kk][6] = on ? v1.z : 0.f; vv[kk][7] = on ? v1.w : 0.f;
-    }
-    {
-      const float4 w0 = *reinterpret_cast<const float4*>(&sm.wb[buf][tx * 4]);
-      const float4 w1 = *reinterpret_cast<const float4*>(&sm.wb[buf][64 + tx * 4]);
-      const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) z[i][j] = fmaf(z[i][j], s, wv[j]) + u[i];
-    }
-#pragma unroll
-    for (int i = 0; i < 8; ++i) {
-      float mx = fmaxf(fmax3(z[i][0], z[i][1], z[i][2]),
-                       fmax3(z[i][3], z[i][4], fmax3(z[i][5], z[i][6], z[i][7])));
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, off));
-      if (mx > mrow[i]) {
-        const float sc = ex2_approx(mrow[i] - mx);
-#pragma unroll
-        for (int kk = 0; kk < KD; ++kk) o[i][kk] *= sc;
-        mrow[i] = mx;
-      }
-      float e[8];
-#pragma unroll
-      for (int j = 0; j < 8; ++j) e[j] = ex2_approx(z[i][j] - mrow[i]);
-#pragma unroll
-      for (int kk = 0; kk < KD; ++kk) {
-        float part = e[0] * vv[kk][0];
-#pragma unroll
-        for (int j = 1; j < 8; ++j) part = fmaf(e[j], vv[kk][j], part);
-        o[i][kk] += part;
-      }
-    }
+    cost_tile<DP>(sm.As, sm.Bs[buf], sm.wb[buf], s, u, tx, ty, z);
+    direct_tile<KD>(z, mrow, o, sm.Vs[buf], tx, p.K);
   }
-
-#pragma unroll
-  for (int i = 0; i < 8; ++i)
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk)
-#pragma unroll
-      for (int off = 1; off < 16; off <<= 1)
-        o[i][kk] += __shfl_xor_sync(0xffffffffu, o[i][kk], off);
-  if (tx != 0) return;
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int r = (i < 4) ? (ty * 4 + i) : (64 + ty * 4 + (i - 4));
-    const int64_t gr = row0 + r;
-    if (gr >= p.R) continue;
-    const bool any = mrow[i] > kNegSentinel;
-    if (p.splits > 1) {
-      const int64_t sp = blockIdx.z;
-      p.part_m[sp * p.R + gr] = any ? mrow[i] : -INFINITY;
-#pragma unroll
-      for (int kk = 0; kk < KD; ++kk)
-        if (kk < p.K) p.part_o[(sp * p.K + kk) * p.R + gr] = any ? o[i][kk] : 0.f;
-      continue;
-    }
-    const float scale = any ? exp2f(mrow[i]) : 0.f;
-#pragma unroll
-    for (int kk = 0; kk < KD; ++kk)
-      if (kk < p.K) p.out[(int64_t)kk * p.R + gr] = any ? o[i][kk] * scale : 0.f;
-  }
+  direct_store<KD>(p, o, mrow, row0, tx, ty);
 }
 
 template <int DP, int KD>
