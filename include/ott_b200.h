@@ -173,8 +173,12 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
  * device arrays; FP32 with a running row maximum. The summed-over points
  * are split across CTAs when the output rows alone would leave SMs idle;
  * the splits' partial sums then go through the workspace (size from
- * ottb_apply_transport_workspace_size; 0 bytes, or a smaller workspace,
- * gives fewer splits). */
+ * ottb_apply_transport_workspace_size). For d <= 64 the workspace also
+ * holds the operands prepared once per call for the pipelined kernels (the
+ * summed-over points transposed and centred, their column terms, the
+ * vectors transposed). A smaller workspace, or none, gives fewer splits and
+ * the kernels that transpose their tiles themselves; the results agree up
+ * to FP32 summation order. */
 size_t ottb_apply_transport_workspace_size(int64_t n, int64_t m, int32_t d, int32_t num_vec,
                                            int32_t axis);
 int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
