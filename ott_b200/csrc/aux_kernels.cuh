@@ -26,7 +26,13 @@ struct PrepArgs {
 // every exponent. Deterministic: every CTA computes the same value.
 __device__ void sample_center(const float* x, int64_t n, const float* y, int64_t m,
                               int d, float* center) {
-  for (int k = threadIdx.x; k < d; k += blockDim.x) {
+  // warp w takes coordinates w, w + warps, ...; its lanes sum disjoint
+  // samples (q = lane, lane + 32, ...) and a fixed shuffle tree adds them:
+  // the same value on every call, without a 256-long chain of dependent
+  // loads per coordinate (blockDim.x is a multiple of 32)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  for (int k = warp; k < d; k += warps) {
     double acc[2];
     for (int side = 0; side < 2; ++side) {
       const float* src = side ? y : x;
@@ -34,10 +40,11 @@ __device__ void sample_center(const float* x, int64_t n, const float* y, int64_t
       const int64_t ns = cnt < 256 ? cnt : 256;
       const int64_t stride = cnt / ns;
       double s = 0.0;
-      for (int64_t q = 0; q < ns; ++q) s += (double)src[(q * stride) * d + k];
+      for (int64_t q = lane; q < ns; q += 32) s += (double)src[(q * stride) * d + k];
+      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
       acc[side] = s / (double)ns;
     }
-    center[k] = (float)(0.5 * (acc[0] + acc[1]));
+    if (lane == 0) center[k] = (float)(0.5 * (acc[0] + acc[1]));
   }
   __syncthreads();
 }

@@ -87,18 +87,24 @@ struct ApplyArgs {
 // each, taken at a fixed stride (every CTA computes the same value).
 template <int DP>
 __device__ void apply_center(const ApplyArgs& p, float* center) {
-  for (int k = threadIdx.x; k < DP; k += blockDim.x) {
-    float s = 0.f;
+  // warp w takes coordinates w, w + 8, ...; its lanes sum disjoint samples
+  // and a fixed shuffle tree adds them (256 threads per CTA)
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int warps = blockDim.x >> 5;
+  const int64_t na = p.R < kSampleMax ? p.R : kSampleMax;
+  const int64_t nb = p.C < kSampleMax ? p.C : kSampleMax;
+  const int64_t sa = p.R / na, sb = p.C / nb;
+  for (int k = warp; k < DP; k += warps) {
+    float ma = 0.f, mb = 0.f;
     if (k < p.d) {
-      const int64_t na = p.R < kSampleMax ? p.R : kSampleMax;
-      const int64_t nb = p.C < kSampleMax ? p.C : kSampleMax;
-      const int64_t sa = p.R / na, sb = p.C / nb;
-      float ma = 0.f, mb = 0.f;
-      for (int64_t i = 0; i < na; ++i) ma += p.A[i * sa * p.d + k];
-      for (int64_t i = 0; i < nb; ++i) mb += p.B[i * sb * p.d + k];
-      s = 0.5f * (ma / (float)na + mb / (float)nb);
+      for (int64_t i = lane; i < na; i += 32) ma += p.A[i * sa * p.d + k];
+      for (int64_t i = lane; i < nb; i += 32) mb += p.B[i * sb * p.d + k];
     }
-    center[k] = s;
+    for (int off = 16; off > 0; off >>= 1) {
+      ma += __shfl_xor_sync(0xffffffffu, ma, off);
+      mb += __shfl_xor_sync(0xffffffffu, mb, off);
+    }
+    if (lane == 0) center[k] = k < p.d ? 0.5f * (ma / (float)na + mb / (float)nb) : 0.f;
   }
 }
 
