@@ -123,12 +123,16 @@ class SinkhornOutput(NamedTuple):
     return self.ot_prob.b
 
   @property
-  def dual_cost(self) -> float:
-    """sinkhorn.py:337-343."""
+  def dual_cost(self) -> Any:
+    """sinkhorn.py:337-343; a differentiable 0-dim tensor when the problem's
+    points or weights require gradients (through the potentials' implicit
+    backward), else a float."""
     a, b = self.a.double(), self.b.double()
     f, g = self.f.double(), self.g.double()
     zero = torch.zeros((), dtype=torch.float64, device=a.device)
-    return float(torch.where(a > 0, a * f, zero).sum() + torch.where(b > 0, b * g, zero).sum())
+    # mask before multiplying: a zero weight meets an infinite potential
+    val = ((a * torch.where(a > 0, f, zero)).sum() + (b * torch.where(b > 0, g, zero)).sum())
+    return val if (self.ot_prob is not None and _tracks_grad(self.ot_prob)) else float(val)
 
   @property
   def ent_reg_cost(self) -> float:
@@ -214,16 +218,29 @@ class SinkhornOutput(NamedTuple):
     return gx, gy, ga, gb
 
   @property
-  def primal_cost(self) -> float:
+  def primal_cost(self) -> Any:
     """``<P, C>`` (sinkhorn.py:346-349 through :395-417), from one
-    application of the plan to ``[1, |y|^2, y]``."""
+    application of the plan to ``[1, |y|^2, y]``. A differentiable 0-dim
+    tensor when the problem's points or weights require gradients (the plan
+    through the potentials' implicit backward and its own dependence on the
+    points, the cost and, for ``scale_cost="mean"``, its scale
+    ``1 / mean(C)``), else a float."""
     geom = self.geom
-    with torch.no_grad():
+    diff = self.ot_prob is not None and _tracks_grad(self.ot_prob)
+    with torch.set_grad_enabled(diff):
       x, y = geom.x.double(), geom.y.double()
       vecs = torch.cat([torch.ones_like(y[:, :1]), (y * y).sum(1, keepdim=True), y], 1)
       r = self.apply(vecs.t().float(), axis=1).double()  # [d + 2, n]
       tot = (r[0] * (x * x).sum(1) + r[1] - 2.0 * (r[2:].t() * x).sum(1)).sum()
-    return float(geom.inv_scale_cost * tot)
+      inv = float(geom.inv_scale_cost)
+      if diff and geom._scale_cost == "mean":
+        # 1 / mean(C_unscaled) as a function of the points (pointcloud.py:
+        # 348-351), valued at the device's statistic
+        mc = (x * x).sum(1).mean() + (y * y).sum(1).mean() - 2.0 * torch.dot(x.mean(0), y.mean(0))
+        inv_t = 1.0 / mc
+        inv = inv_t + (inv - inv_t.detach())
+      val = inv * tot
+    return val if diff else float(val)
 
 
 def _tracks_grad(p: linear_problem.LinearProblem) -> bool:

@@ -334,3 +334,47 @@ def test_apply_transport_jacobian_matches_finite_differences(arg, axis):
   else:
     fd = (applied(a, x + h * delta) - applied(a, x - h * delta)) / (2 * h)
   assert abs(got - fd) <= 1e-3 * float(np.abs(grad * delta).sum()), (got, fd)
+
+
+@pytest.mark.parametrize("scale", [1.0, "mean"])
+def test_primal_and_dual_cost_gradients_match_finite_differences(scale):
+  """``out.primal_cost`` and ``out.dual_cost`` are differentiable through
+  the solve (implicit backward of the potentials, the plan's own dependence
+  on the points and, for scale_cost="mean", the scale): their derivatives in
+  a direction of the points against central differences of float64 solves."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  n, m, d, eps = 40, 30, 3, 0.05
+  rng = np.random.default_rng(11)
+  x, y = rng.uniform(size=(n, d)), rng.uniform(size=(m, d))
+  a = rng.uniform(0.2, 1.2, n)
+  a /= a.sum()
+  b = rng.uniform(0.2, 1.2, m)
+  b /= b.sum()
+  delta = rng.standard_normal((n, d))
+  xt = _t(x, True)
+  out = linear.solve(pointcloud.PointCloud(xt, _t(y), epsilon=eps, scale_cost=scale),
+                     _t(a), _t(b), threshold=1e-7, max_iterations=20000, precision="fp32")
+  got = {}
+  for name in ("primal_cost", "dual_cost"):
+    val = getattr(out, name)
+    assert isinstance(val, torch.Tensor) and val.requires_grad
+    (g,) = torch.autograd.grad(val, xt, retain_graph=True)
+    got[name] = (float((g.double().cpu().numpy() * delta).sum()),
+                 float(np.abs(g.double().cpu().numpy() * delta).sum()))
+
+  def costs(xx):
+    inv = o.inv_scale_cost(xx, y, scale)
+    og = o.Geom(xx, y, eps, inv_scale=inv)
+    r = o.sinkhorn(og, a, b, threshold=1e-13, max_iterations=200000)
+    p = o.transport_matrix(r.f, r.g, og)
+    primal = float(np.sum(p * og.cost_block()))
+    dual = float(a @ r.f + b @ r.g)
+    return primal, dual
+
+  h = 1e-5
+  up, dn = costs(x + h * delta), costs(x - h * delta)
+  for k, name in enumerate(("primal_cost", "dual_cost")):
+    fd = (up[k] - dn[k]) / (2 * h)
+    assert abs(got[name][0] - fd) <= 1e-3 * got[name][1], (name, got[name][0], fd)
