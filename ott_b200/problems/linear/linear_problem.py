@@ -24,22 +24,30 @@ class LinearProblem:
       raise ValueError(f"b must have shape ({m},), got {tuple(self._b.shape)}")
     self.tau_a = tau_a
     self.tau_b = tau_b
+    # the uniform defaults, made once; _a / _b stay None so that
+    # is_uniform keeps telling whether weights were passed
+    self._a_uniform: Optional[torch.Tensor] = None
+    self._b_uniform: Optional[torch.Tensor] = None
 
   @property
   def a(self) -> torch.Tensor:
     if self._a is not None:
       return self._a
-    n, _ = self.geom.shape
-    self._a = torch.full((n,), 1.0 / n, dtype=torch.float32, device=self.geom.x.device)
-    return self._a
+    if self._a_uniform is None:
+      n, _ = self.geom.shape
+      self._a_uniform = torch.full((n,), 1.0 / n, dtype=torch.float32,
+                                   device=self.geom.x.device)
+    return self._a_uniform
 
   @property
   def b(self) -> torch.Tensor:
     if self._b is not None:
       return self._b
-    _, m = self.geom.shape
-    self._b = torch.full((m,), 1.0 / m, dtype=torch.float32, device=self.geom.x.device)
-    return self._b
+    if self._b_uniform is None:
+      _, m = self.geom.shape
+      self._b_uniform = torch.full((m,), 1.0 / m, dtype=torch.float32,
+                                   device=self.geom.x.device)
+    return self._b_uniform
 
   @property
   def is_balanced(self) -> bool:

@@ -144,9 +144,86 @@ class SinkhornOutput(NamedTuple):
     return self.reg_ot_cost - self.geom.epsilon * float(entr(self.a) + entr(self.b))
 
   @property
-  def transport_mass(self) -> float:
-    """Sum of the transport matrix of the final state (column marginal sum)."""
+  def transport_mass(self) -> Any:
+    """Sum of the transport matrix (sinkhorn.py:451-454, ``marginal(0).sum()``):
+    the final sweep's FP64 sum, or a differentiable tensor when the problem's
+    points or weights require gradients."""
+    if self.ot_prob is not None and _tracks_grad(self.ot_prob):
+      return self.marginal(0).double().sum()
     return float(self._res().marginal_sum)
+
+  @property
+  def scalings(self) -> Tuple[torch.Tensor, torch.Tensor]:
+    """sinkhorn.py:437-441: ``exp(f / eps), exp(g / eps)``
+    (geometry.py:535-546)."""
+    eps = float(self.geom.epsilon)
+    return torch.exp(self.f / eps), torch.exp(self.g / eps)
+
+  @property
+  def entropy(self) -> Any:
+    """Entropy of the coupling (sinkhorn.py:513-523):
+    ``(primal_cost - <f, P 1> - <g, P^T 1>) / eps`` with non-finite
+    potentials counted as 0."""
+    ma = self.marginal(1).double()
+    mb = self.marginal(0).double()
+    f, g = self.f.double(), self.g.double()
+    zero = torch.zeros((), dtype=torch.float64, device=f.device)
+    sf = torch.where(torch.isfinite(f), f, zero)
+    sg = torch.where(torch.isfinite(g), g, zero)
+    val = (self.primal_cost - torch.dot(sf, ma) - torch.dot(sg, mb)) / float(self.geom.epsilon)
+    return val if (self.ot_prob is not None and _tracks_grad(self.ot_prob)) else float(val)
+
+  @property
+  def normalized_entropy(self) -> Any:
+    """sinkhorn.py:525-530: ``entropy / log(n) - 1`` of an assignment
+    problem (equal sizes, uniform weights, balanced)."""
+    assert self.ot_prob.is_assignment, "Normalized entropy only valid for assignment problem."
+    return self.entropy / math.log(self.geom.shape[0]) - 1.0
+
+  @property
+  def diag(self) -> torch.Tensor:
+    """Diagonal of the plan of a square problem (sinkhorn.py:532-538):
+    ``exp((f_i + g_i - c(x_i, y_i)) / eps)`` with the diagonal cost of
+    pointcloud.py:451-454, which is the cost function's value without
+    ``scale_cost``."""
+    geom = self.geom
+    assert geom.is_square, "Problem must be square for transport matrix to have a diag."
+    x, y = geom.x, geom.y
+    diag = ((x - y) ** 2).sum(1)
+    return torch.exp((-diag + self.f + self.g) / float(geom.epsilon))
+
+  def transport_cost_at_geom(self, other_geom) -> Any:
+    """``<P, C_other>`` for the plan of this solution and the cost of another
+    point cloud of the same sizes (sinkhorn.py:395-417; the squared Euclidean
+    cost is a rank d + 2 product there): one application of the plan to
+    ``[1, |y'|^2, y']``, times ``other_geom``'s scale."""
+    if tuple(other_geom.shape) != tuple(self.geom.shape):
+      raise ValueError("the other geometry must have the same shape")
+    diff = self.ot_prob is not None and _tracks_grad(self.ot_prob)
+    with torch.set_grad_enabled(diff):
+      x, y = other_geom.x.double(), other_geom.y.double()
+      vecs = torch.cat([torch.ones_like(y[:, :1]), (y * y).sum(1, keepdim=True), y], 1)
+      r = self.apply(vecs.t().float(), axis=1).double()  # [d + 2, n]
+      tot = (r[0] * (x * x).sum(1) + r[1] - 2.0 * (r[2:].t() * x).sum(1)).sum()
+      val = float(other_geom.inv_scale_cost) * tot
+    return val if diff else float(val)
+
+  def cost_at_geom(self, other_geom) -> Any:
+    """sinkhorn.py:502-507: ``sum(P * C_other) - eps sum(entr(P))`` with
+    the plan formed (``matrix``); for problems whose n x m plan fits."""
+    p = self.matrix.double()
+    x, y = other_geom.x.double(), other_geom.y.double()
+    c = float(other_geom.inv_scale_cost) * ((x * x).sum(1)[:, None] + (y * y).sum(1)[None, :]
+                                            - 2.0 * x @ y.t())
+    zero = torch.zeros((), dtype=torch.float64, device=p.device)
+    entr = torch.where(p > 0, -p * torch.log(torch.where(p > 0, p, torch.ones_like(p))), zero)
+    val = (p * c).sum() - float(self.geom.epsilon) * entr.sum()
+    return val if (self.ot_prob is not None and _tracks_grad(self.ot_prob)) else float(val)
+
+  def to_dual_potentials(self, epsilon: Optional[float] = None):
+    """sinkhorn.py:509-511 builds potential functions of the
+    ``problems/linear/potentials`` module, which is not on this path."""
+    raise NotImplementedError("dual potential functions are not on this path")
 
   @property
   def matrix(self) -> torch.Tensor:

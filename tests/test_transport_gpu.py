@@ -245,3 +245,45 @@ def test_sweep_engine_application_edge_cases(precision):
     assert np.all(got[2] == 0.0)
     for i in range(2):
       assert np.all(np.abs(got[i] - want[i]) <= rel * scale[i].max() + 1e-30)
+
+
+def test_output_members_match_oracle():
+  """entropy, normalized_entropy, diag, scalings, transport_mass,
+  transport_cost_at_geom and cost_at_geom (sinkhorn.py:395-538) against the
+  float64 plan at the GPU's potentials."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  n, d = 300, 5
+  x, y, _, _ = problems.uniform_cloud_problem(n, n, d, seed=41)
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=0.05, scale_cost=2.0)
+  out = linear.solve(geom, threshold=1e-6, precision="fp32")  # uniform weights: an assignment
+  f = out.f.cpu().numpy().astype(np.float64)
+  g = out.g.cpu().numpy().astype(np.float64)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), 0.05, inv_scale=0.5)
+  p = o.transport_matrix(f, g, og)
+  c = og.cost_block()
+  eps = 0.05
+  ent = (np.sum(p * c) - f @ p.sum(1) - g @ p.sum(0)) / eps
+  assert abs(out.entropy - ent) <= 1e-4 * abs(ent)
+  assert abs(out.normalized_entropy - (ent / np.log(n) - 1.0)) <= 1e-4 * abs(ent / np.log(n))
+  raw_diag = ((x.astype(np.float64) - y) ** 2).sum(1)
+  np.testing.assert_allclose(out.diag.cpu().numpy(), np.exp((-raw_diag + f + g) / eps),
+                             rtol=2e-4)
+  u, v = out.scalings
+  np.testing.assert_allclose(u.cpu().numpy(), np.exp(f / eps), rtol=1e-5)
+  np.testing.assert_allclose(v.cpu().numpy(), np.exp(g / eps), rtol=1e-5)
+  assert abs(out.transport_mass - p.sum()) <= 1e-4 * p.sum()
+  x2, y2, _, _ = problems.uniform_cloud_problem(n, n, d, seed=42)
+  other = pointcloud.PointCloud(torch.as_tensor(x2).cuda(), torch.as_tensor(y2).cuda(),
+                                epsilon=0.05, scale_cost=3.0)
+  c2 = o.sqeuclidean_all_pairs(x2.astype(np.float64), y2.astype(np.float64)) / 3.0
+  want = np.sum(p * c2)
+  assert abs(out.transport_cost_at_geom(other) - want) <= 1e-4 * abs(want)
+  with np.errstate(divide="ignore", invalid="ignore"):
+    entr = np.where(p > 0, -p * np.log(p), 0.0).sum()
+  want = np.sum(p * c2) - eps * entr
+  assert abs(out.cost_at_geom(other) - want) <= 1e-4 * abs(want)
+  with pytest.raises(NotImplementedError):
+    out.to_dual_potentials()
