@@ -316,6 +316,58 @@ class PointCloud(geometry.Geometry):
     out = torch.where(torch.isneginf(rem), torch.full_like(out, -float("inf")), out)
     return out, torch.ones(1, device=dev)
 
+  def update_potential(self, f: torch.Tensor, g: torch.Tensor, log_marginal: Any,
+                       iteration: Optional[int] = None, axis: int = 0,
+                       precision: str = "fp32") -> torch.Tensor:
+    """geometry.py:376-398: one Sinkhorn update, ``eps log_marginal -
+    where(isfinite(lse), lse, 0)`` with ``lse = apply_lse_kernel(f, g, eps,
+    axis)`` at the scheduled epsilon of ``iteration``: the new g for
+    ``axis=0``, the new f for ``axis=1``."""
+    eps = float(self.epsilon_scheduler(iteration))
+    app, _ = self.apply_lse_kernel(f, g, eps, axis=axis, precision=precision)
+    lm = _arrays.as_f32(log_marginal, self.x.device)
+    return eps * lm - torch.where(torch.isfinite(app), app, torch.zeros_like(app))
+
+  @property
+  def cost_matrix(self) -> torch.Tensor:
+    """The scaled cost ``[n, m]`` (geometry.py:95-105; formed, for problems
+    whose n x m matrix fits): ``inv (|x|^2 + |y|^2 - 2 <x, y>)``."""
+    x, y = self.x, self.y
+    c = (x * x).sum(1)[:, None] + (y * y).sum(1)[None, :] - 2.0 * (x @ y.t())
+    return self.inv_scale_cost * c
+
+  @property
+  def kernel_matrix(self) -> torch.Tensor:
+    """geometry.py:137-145: ``exp(-C / eps)``, formed."""
+    return torch.exp(-self.cost_matrix / self.epsilon)
+
+  @property
+  def diag_cost(self) -> torch.Tensor:
+    """pointcloud.py:451-454: the cost function on the pairs (x_i, y_i) of a
+    square problem (without ``scale_cost``, as there)."""
+    assert self.is_square, "Cost matrix must be square to compute diagonal."
+    return ((self.x - self.y) ** 2).sum(1)
+
+  def apply_cost(self, arr: Any, axis: int = 0, fn: Optional[Any] = None,
+                 is_linear: bool = False) -> torch.Tensor:
+    """geometry.py:568-600 for the squared Euclidean cost without ``fn``:
+    ``C^T arr`` (axis 0, arr [n] or [n, p]) or ``C arr`` (axis 1) through the
+    rank d + 2 structure ``C = inv (|x|^2 1^T + 1 |y|^2^T - 2 x y^T)``, in
+    O((n + m) d p) without forming C."""
+    if fn is not None:
+      raise NotImplementedError("an elementwise fn of the cost is not on this path")
+    v = _arrays.as_f32(arr, self.x.device)
+    one = v.ndim == 1
+    v2 = v[:, None] if one else v
+    x, y = self.x, self.y
+    nx, ny = (x * x).sum(1), (y * y).sum(1)
+    if axis == 0:   # C^T v: sum over rows
+      out = ny[:, None] * v2.sum(0)[None, :] + (nx @ v2)[None, :] - 2.0 * (y @ (x.t() @ v2))
+    else:           # C v: sum over columns
+      out = nx[:, None] * v2.sum(0)[None, :] + (ny @ v2)[None, :] - 2.0 * (x @ (y.t() @ v2))
+    out = self.inv_scale_cost * out
+    return out[:, 0] if one else out
+
   def marginal_from_potentials(self, f: torch.Tensor, g: torch.Tensor,
                                axis: int = 0) -> torch.Tensor:
     """geometry.py:326-349: column (``axis=0``) or row (``axis=1``)

@@ -68,3 +68,33 @@ def test_sharded_solve_one_rank_matches_solve(n, m, d, precision):
   np.testing.assert_allclose(out.f.cpu().numpy(), ref.f.cpu().numpy(), rtol=0, atol=tol)
   np.testing.assert_allclose(out.g.cpu().numpy(), ref.g.cpu().numpy(), rtol=0, atol=tol)
   assert abs(out.reg_ot_cost - ref.reg_ot_cost) <= 1e-5 * abs(ref.reg_ot_cost)
+
+
+def test_geometry_methods_match_oracle():
+  """PointCloud.update_potential, cost_matrix, kernel_matrix, diag_cost and
+  apply_cost (geometry.py:95-145, 376-398, 568-600; pointcloud.py:451-454)
+  against float64."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  n, d = 200, 4
+  x, y, a, b = problems.uniform_cloud_problem(n, n, d, seed=51)
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=0.1, scale_cost=2.0)
+  og = o.Geom(x.astype(np.float64), y.astype(np.float64), 0.1, inv_scale=0.5)
+  c = og.cost_block()
+  np.testing.assert_allclose(geom.cost_matrix.cpu().numpy(), c, rtol=1e-5, atol=1e-6)
+  np.testing.assert_allclose(geom.kernel_matrix.cpu().numpy(), np.exp(-c / 0.1), rtol=1e-4)
+  np.testing.assert_allclose(geom.diag_cost.cpu().numpy(),
+                             ((x.astype(np.float64) - y) ** 2).sum(1), rtol=1e-5)
+  v = np.random.default_rng(0).standard_normal((n, 3))
+  for axis in (0, 1):
+    got = geom.apply_cost(torch.as_tensor(v, dtype=torch.float32).cuda(), axis=axis)
+    want = c.T @ v if axis == 0 else c @ v
+    np.testing.assert_allclose(got.cpu().numpy(), want, rtol=0, atol=1e-4 * np.abs(want).max())
+  f = np.zeros(n)
+  g = np.zeros(n)
+  new_g = geom.update_potential(torch.as_tensor(f, dtype=torch.float32).cuda(),
+                                torch.as_tensor(g, dtype=torch.float32).cuda(),
+                                torch.as_tensor(np.log(b), dtype=torch.float32).cuda(), axis=0)
+  want = og.update_potential(f, g, np.log(b.astype(np.float64)), None, axis=0)
+  np.testing.assert_allclose(new_g.cpu().numpy(), want, rtol=0, atol=2e-5 * 0.1)
