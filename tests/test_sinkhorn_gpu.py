@@ -8,6 +8,7 @@ on the threshold). Relations mirror the reference's own tests
 import numpy as np
 import pytest
 
+from oracle import sinkhorn_np as o
 from tests import helpers, problems
 
 pytestmark = pytest.mark.gpu
@@ -171,3 +172,50 @@ def test_device_wait_timeout_reports_status():
   assert e.value.status == _lib.OTTB_ERR_TIMEOUT
   geom2, out2 = helpers.gpu_solve(x, y, a, b, epsilon=0.1)
   assert out2.converged
+
+
+def test_diag_sum_of_self_transport():
+  """The reference's test_diag_sum (tests/solvers/linear/sinkhorn_test.py:
+  56-66): a cloud against itself at epsilon = 0.01 keeps more than 99 % of
+  the mass on the diagonal of the plan, and less than all of it (on a draw
+  whose points are at least 0.3 apart: a closer pair, cost ~ epsilon,
+  shares its mass, in the oracle as here), equal to the oracle's sum."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  x = np.random.default_rng(0).uniform(size=(17, 4)).astype(np.float32)
+  out = linear.solve(pointcloud.PointCloud(torch.as_tensor(x).cuda(), epsilon=0.01))
+  s = float(out.diag.sum())
+  assert 0.99 < s < 1.0
+  x64 = x.astype(np.float64)
+  ref = o.solve(x64, None, epsilon=0.01)
+  want = np.trace(o.transport_matrix(ref.f, ref.g, o.Geom(x64, x64, 0.01)))
+  assert abs(s - want) <= 1e-5
+
+
+def test_low_epsilon_plan_matches_assignment():
+  """The reference's test_SqEucl_matches_hungarian (sinkhorn_test.py:68-90,
+  n = 17, d = 4): at epsilon = 0.01 the plan is within cosine distance 0.2
+  of the optimal assignment's (scipy's linear_sum_assignment on the cost),
+  and that distance equals the oracle plan's."""
+  import torch
+  from scipy.optimize import linear_sum_assignment
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  rng = np.random.default_rng(17)
+  n = 17
+  x = rng.uniform(size=(n, 4)).astype(np.float32)
+  y = rng.uniform(size=(n, 4)).astype(np.float32)
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=0.01)
+  p = linear.solve(geom).matrix.cpu().numpy().astype(np.float64).ravel()
+  rows, cols = linear_sum_assignment(geom.cost_matrix.cpu().numpy())
+  h = np.zeros((n, n))
+  h[rows, cols] = 1.0 / n
+  h = h.ravel()
+  cosd = lambda u, v: 1.0 - u @ v / (np.linalg.norm(u) * np.linalg.norm(v))
+  assert cosd(p, h) < 0.2
+  x64, y64 = x.astype(np.float64), y.astype(np.float64)
+  ref = o.solve(x64, y64, epsilon=0.01)
+  p_ref = o.transport_matrix(ref.f, ref.g, o.Geom(x64, y64, 0.01)).ravel()
+  assert abs(cosd(p, h) - cosd(p_ref, h)) <= 1e-4
