@@ -219,3 +219,42 @@ def test_low_epsilon_plan_matches_assignment():
   ref = o.solve(x64, y64, epsilon=0.01)
   p_ref = o.transport_matrix(ref.f, ref.g, o.Geom(x64, y64, 0.01)).ravel()
   assert abs(cosd(p, h) - cosd(p_ref, h)) <= 1e-4
+
+
+def test_progress_callbacks():
+  """The reference's test_custom_progress_fn and test_progress_fn
+  (sinkhorn_test.py:658-749): called on iterations 9, 19, 29 with
+  decreasing errors and the iteration budget; default_progress_fn prints
+  "foo 7/14" first."""
+  import io
+  import torch
+  from ott_b200 import utils
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import sinkhorn
+  x, y, a, b = problems.ref_test_problem()
+  traced = {"iters": [], "error": [], "total": []}
+
+  def progress_fn(status):
+    iteration, inner, total, state = status
+    errors = state.errors.cpu().numpy().ravel()
+    if (int(iteration) + 1) % int(inner) == 0:
+      traced["iters"].append(int(iteration))
+      traced["error"].append(errors[max((int(iteration) + 1) // int(inner) - 1, 0)])
+      traced["total"].append(int(total))
+
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=1e-3)
+  prob = linear_problem.LinearProblem(geom, torch.as_tensor(a).cuda(), torch.as_tensor(b).cuda())
+  sinkhorn.Sinkhorn(progress_fn=progress_fn, max_iterations=30, inner_iterations=10)(prob)
+  assert traced["iters"] == [9, 19, 29]
+  assert np.all(np.diff(traced["error"]) < 0)
+  assert traced["total"] == [30, 30, 30]
+  stream = io.StringIO()
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=1e-1)
+  linear.solve(geom, progress_fn=utils.default_progress_fn(fmt="foo {iter}/{max_iter}",
+                                                          stream=stream),
+               min_iterations=0, inner_iterations=7, max_iterations=14)
+  assert stream.getvalue().startswith("foo 7/14"), stream.getvalue()
