@@ -7,6 +7,7 @@ the fused kernels, which is the reference's online mode
 from __future__ import annotations
 
 import ctypes
+import functools
 from typing import Any, Optional, Tuple, Union
 
 import torch
@@ -148,8 +149,7 @@ class PointCloud(geometry.Geometry):
       precision = "bf16_split3"
     if precision in sweep:
       code = sweep[precision]
-      ws_bytes = lib.ottb_apply_transport_sweep_workspace_size(n, m, self.dim, v2.shape[0],
-                                                               axis, code)
+      ws_bytes = _sweep_ws_bytes(n, m, self.dim, v2.shape[0], axis, code)
       if ws_bytes == 0:
         raise NotImplementedError("problem sizes not supported by the sweep engine")
       ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
@@ -160,7 +160,7 @@ class PointCloud(geometry.Geometry):
           _arrays.stream_handle())
       _lib.check(st, "ottb_apply_transport_sweep")
       return out
-    ws_bytes = lib.ottb_apply_transport_workspace_size(n, m, self.dim, v2.shape[0], axis)
+    ws_bytes = _apply_ws_bytes(n, m, self.dim, v2.shape[0], axis)
     ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
     st = lib.ottb_apply_transport(self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim,
                                   fd.data_ptr(), gd.data_ptr(), ctypes.c_float(self.epsilon),
@@ -396,6 +396,19 @@ class PointCloud(geometry.Geometry):
   def __repr__(self) -> str:
     n, m = self.shape
     return f"PointCloud(n={n}, m={m}, d={self.dim}, epsilon={self._epsilon_init})"
+
+
+@functools.lru_cache(maxsize=256)
+def _apply_ws_bytes(n: int, m: int, d: int, k: int, axis: int) -> int:
+  """Workspace of ``ottb_apply_transport`` (a function of the shapes and the
+  device's SM count, fixed per process)."""
+  return int(_lib.load().ottb_apply_transport_workspace_size(n, m, d, k, axis))
+
+
+@functools.lru_cache(maxsize=256)
+def _sweep_ws_bytes(n: int, m: int, d: int, k: int, axis: int, code: int) -> int:
+  """Workspace of ``ottb_apply_transport_sweep`` (a function of the shapes)."""
+  return int(_lib.load().ottb_apply_transport_sweep_workspace_size(n, m, d, k, axis, code))
 
 
 def _needs_grad(*ts: torch.Tensor) -> bool:

@@ -106,11 +106,12 @@ def _minres(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
     y = op(v)
     if step >= 2:
       y = y - (beta / oldb) * r1
-    alfa = float(torch.dot(v, y))
-    y = y - (alfa / beta) * r2
+    alfa_t = torch.dot(v, y)
+    y = y - (alfa_t / beta) * r2
     r1, r2 = r2, y
     oldb = beta
-    beta = float(torch.linalg.vector_norm(r2))
+    # one host read per step for both Lanczos scalars
+    alfa, beta = torch.stack([alfa_t, torch.linalg.vector_norm(r2)]).tolist()
     # previous rotation applied to the new column of the tridiagonal matrix
     oldeps = epsln
     delta = cs * dbar + sn * alfa
