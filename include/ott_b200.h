@@ -320,6 +320,27 @@ int32_t ottb_mlp_adam(const ottb_mlp* net, float lr, float beta1, float beta2,
 /* Refreshes the bf16 copies (w_bf16, wt_bf16) from the FP32 weights. */
 int32_t ottb_mlp_sync_bf16(const ottb_mlp* net, void* stream);
 
+/* One MINRES step (Paige and Saunders 1975) after the operator product, for
+ * the symmetric linear system of the implicit backward of the potentials
+ * (implicit_differentiation.py:156-233, solved there by lineax CG /
+ * NormalCG; lineax_implicit.py:49-101). On entry y = op(v); the kernel
+ * finishes the Lanczos step (y -= (beta/oldb) r1 for step >= 2,
+ * alfa = <v, y>, y -= (alfa/beta) r2, beta' = |y|), applies and updates the
+ * Givens rotation, writes the new direction into w_prev
+ * ((v - oldeps w_prev - delta w) / gamma), adds phi times it to x, writes
+ * v_next = y / beta', and stores the residual estimate in history[step].
+ * state[16] (float64, device): beta, oldb, dbar, epsln, phibar, cs, sn,
+ * beta1, rtol, active, steps; the host sets it to beta1, 0, 0, 0, beta1,
+ * -1, 0, beta1, rtol, 1, 0 and history[0] = beta1 before step 1. The stop
+ * test (phibar <= rtol beta1, beta' <= 1e-14 beta1, or phibar above
+ * 0.99 history[step - window]) clears active, after which later calls
+ * return at once. All vectors hold s float64 values on the device;
+ * 1 <= step < history_len. */
+int32_t ottb_minres_step(double* state, int32_t step, int32_t window, const double* v,
+                         double* y, const double* r1, const double* r2, const double* w,
+                         double* w_prev, double* x, double* v_next, double* history,
+                         int64_t history_len, int64_t s, void* stream);
+
 /* Human-readable text of a status code. */
 const char* ottb_status_string(int32_t status);
 

@@ -59,7 +59,8 @@ def build(force: bool = False, verbose: bool = False) -> str:
   deps = sources() + [os.path.join(HERE, "..", "include", "ott_b200.h")]
   if force or not up_to_date(OUT, deps):
     _nvcc_shared([os.path.join(CSRC, "capi.cu"), os.path.join(CSRC, "noalloc.cu"),
-                  os.path.join(CSRC, "mlp.cu"), os.path.join(CSRC, "transport.cu")], OUT,
+                  os.path.join(CSRC, "mlp.cu"), os.path.join(CSRC, "transport.cu"),
+                  os.path.join(CSRC, "krylov.cu")], OUT,
                  verbose)
   peaks = os.path.join(CSRC, "peaks", "peaks.cu")
   if force or not up_to_date(PEAKS_OUT, [peaks]):

@@ -83,7 +83,82 @@ def _minres(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
   Givens rotations, so the residual norm estimate never increases. Stops
   when it falls to ``rtol |rhs|``, after ``max_steps``, or when ``window``
   steps lower it by less than 1 %. Records steps, the estimate and the
-  true relative residual ``|rhs - op(x)| / |rhs|`` (one more product)."""
+  true relative residual ``|rhs - op(x)| / |rhs|`` (one more product).
+  On a CUDA device each step after the product is one ``ottb_minres_step``
+  launch (``_minres_device``); elsewhere the steps run here."""
+  if rhs.is_cuda:
+    return _minres_device(op, rhs, rtol, max_steps, window)
+  return _minres_host(op, rhs, rtol, max_steps, window)
+
+
+# ottb_minres_step's state slots read back by the host
+_ST_PHIBAR, _ST_ACTIVE, _ST_STEPS = 4, 9, 10
+
+
+def _minres_device(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
+                   window: int = 50) -> torch.Tensor:
+  """``_minres_host``'s iteration with its scalars on the device: per step
+  the product ``op(v)`` and one ``ottb_minres_step`` launch, which freezes
+  the iterate once the stop test fires, then an asynchronous copy of the
+  stop flag to pinned memory. After issuing step k the host waits for step
+  k - 1's flag only, so step k keeps the GPU busy meanwhile; the one step
+  issued past the stop is discarded work, not a change of the result."""
+  from ott_b200 import _arrays, _lib
+  lib = _lib.load()
+  rhs = rhs.to(torch.float64).contiguous()
+  s = rhs.numel()
+  beta1 = float(torch.linalg.vector_norm(rhs))
+  x = torch.zeros_like(rhs)
+  last_solve_info.clear()
+  last_solve_info.update(steps=0, rel_residual=1.0, true_rel_residual=1.0)
+  if beta1 == 0.0 or max_steps < 1:
+    if beta1 == 0.0:
+      last_solve_info.update(rel_residual=0.0, true_rel_residual=0.0)
+    return x
+  dev = rhs.device
+  state = torch.tensor([beta1, 0.0, 0.0, 0.0, beta1, -1.0, 0.0, beta1, float(rtol), 1.0, 0.0]
+                       + [0.0] * 5, dtype=torch.float64).to(dev)
+  hist = torch.zeros(max_steps + 1, dtype=torch.float64, device=dev)
+  hist[0] = beta1
+  v = rhs / beta1
+  v_next = torch.empty_like(rhs)
+  r1, r2 = rhs, rhs.clone()
+  w, w_prev = torch.zeros_like(rhs), torch.zeros_like(rhs)
+  stream = _arrays.stream_handle()
+  flags = torch.ones(2, dtype=torch.float64).pin_memory()
+  done = [torch.cuda.Event(), torch.cuda.Event()]
+  for step in range(1, max_steps + 1):
+    y = op(v)
+    if y.dtype != torch.float64 or not y.is_contiguous() or y.numel() != s:
+      y = y.to(torch.float64).contiguous().reshape(s)
+    if y.data_ptr() in (v.data_ptr(), v_next.data_ptr(), r1.data_ptr(), r2.data_ptr(),
+                        w.data_ptr(), w_prev.data_ptr(), x.data_ptr()):
+      y = y.clone()  # the step rewrites y in place
+    st = lib.ottb_minres_step(state.data_ptr(), step, int(window), v.data_ptr(), y.data_ptr(),
+                              r1.data_ptr(), r2.data_ptr(), w.data_ptr(), w_prev.data_ptr(),
+                              x.data_ptr(), v_next.data_ptr(), hist.data_ptr(), hist.numel(),
+                              s, stream)
+    _lib.check(st, "ottb_minres_step")
+    r1, r2 = r2, y
+    w, w_prev = w_prev, w
+    v, v_next = v_next, v
+    flags[step % 2].copy_(state[_ST_ACTIVE], non_blocking=True)
+    done[step % 2].record()
+    if step >= 2:
+      done[(step - 1) % 2].synchronize()
+      if float(flags[(step - 1) % 2]) == 0.0:
+        break
+  steps, phibar = state[[_ST_STEPS, _ST_PHIBAR]].tolist()
+  true_res = float(torch.linalg.vector_norm(rhs - op(x))) / beta1
+  last_solve_info.update(steps=int(steps), rel_residual=phibar / beta1,
+                         true_rel_residual=true_res)
+  return x
+
+
+def _minres_host(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
+                 window: int = 50) -> torch.Tensor:
+  """``_minres`` with every step on the host (one read of the two Lanczos
+  scalars per step)."""
   beta1 = float(torch.linalg.vector_norm(rhs))
   x = torch.zeros_like(rhs)
   last_solve_info.clear()

@@ -85,6 +85,18 @@ def test_invalid_arguments_rejected_without_device():
   # two zero-iteration problems per vector: more vectors, more workspace
   assert lib.ottb_apply_transport_sweep_workspace_size(1000, 2000, 64, 3, 0, 1) > ws_tc
   assert lib.ottb_apply_transport_workspace_size(1000, 2000, 64, 1, 3) == 0
+  # MINRES step: null vectors, step outside [1, history_len), window < 1 or
+  # an empty system are refused before any launch (the pointers below are
+  # never dereferenced)
+  p = [256 * (k + 1) for k in range(10)]
+  def step(*, ptrs=p, step=1, window=50, hist_len=11, s=8):
+    return lib.ottb_minres_step(ptrs[0], step, window, *ptrs[1:], hist_len, s, None)
+  assert step(ptrs=[None] + p[1:]) == _lib.OTTB_ERR_INVALID
+  assert step(ptrs=p[:5] + [None] + p[6:]) == _lib.OTTB_ERR_INVALID
+  assert step(step=0) == _lib.OTTB_ERR_INVALID
+  assert step(step=11) == _lib.OTTB_ERR_INVALID
+  assert step(window=0) == _lib.OTTB_ERR_INVALID
+  assert step(s=0) == _lib.OTTB_ERR_INVALID
 
 
 def test_mlp_shape_checks_without_device():

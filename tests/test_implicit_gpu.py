@@ -378,3 +378,52 @@ def test_primal_and_dual_cost_gradients_match_finite_differences(scale):
   for k, name in enumerate(("primal_cost", "dual_cost")):
     fd = (up[k] - dn[k]) / (2 * h)
     assert abs(got[name][0] - fd) <= 1e-3 * got[name][1], (name, got[name][0], fd)
+
+
+@pytest.mark.parametrize("case", ["spd", "singular", "closes", "indefinite", "step_cap",
+                                  "window", "identity"])
+def test_device_minres_matches_host_minres(case):
+  """``ottb_minres_step`` (scalars on the device, stop flag read every few
+  steps) against the host loop on the same float64 operator: the same step
+  count and iterate to rounding. The indefinite system stops on a boundary
+  of its tolerance, so its step count may differ by one. The inconsistent
+  system's plateau stops it on the 1 % window rule, with a ratio 3e-3 away
+  from 0.99 on either side of the stop step."""
+  import torch
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  gen = torch.Generator().manual_seed(3)
+  n = 300
+  q, _ = torch.linalg.qr(torch.randn(n, n, dtype=torch.float64, generator=gen))
+  ev = torch.linspace(0.01, 2.0, n, dtype=torch.float64)
+  rtol, max_steps, window = 1e-12, 2000, 50
+  if case == "singular":
+    ev[:7] = 0.0
+  elif case == "closes":  # four distinct eigenvalues: the Krylov space closes
+    ev = torch.cat([torch.ones(n - 3), torch.tensor([2.0, 3.0, 0.5])]).double()
+  elif case == "indefinite":
+    ev = torch.linspace(-1.0, 2.0, n, dtype=torch.float64)
+  elif case == "step_cap":
+    rtol, max_steps = 1e-14, 13
+  elif case == "window":  # inconsistent singular system: the estimate levels off
+    ev[:7] = 0.0
+    window = 5
+  a = (q * ev) @ q.T
+  b = torch.randn(n, dtype=torch.float64, generator=gen)
+  if case == "singular":
+    b = a @ b
+  a, b = a.cuda(), b.cuda()
+  op = (lambda z: z) if case == "identity" else (lambda z: a @ z)
+  xh = imp._minres_host(op, b, rtol, max_steps, window)
+  ih = dict(imp.last_solve_info)
+  xd = imp._minres_device(op, b, rtol, max_steps, window)
+  idv = dict(imp.last_solve_info)
+  tol_steps = 1 if case == "indefinite" else 0
+  assert abs(idv["steps"] - ih["steps"]) <= tol_steps, (ih, idv)
+  assert _rel(xd, xh.cpu().numpy()) < 1e-9
+  assert abs(idv["rel_residual"] - ih["rel_residual"]) <= 1e-9 * max(ih["rel_residual"], 1e-3)
+  assert abs(idv["true_rel_residual"] - ih["true_rel_residual"]) < 1e-9
+  if case == "identity":
+    assert idv["steps"] == 1 and _rel(xd, b.cpu().numpy()) < 1e-15
+  # the public dispatch takes the device loop for CUDA tensors
+  xp = imp._minres(op, b, rtol, max_steps, window)
+  assert _rel(xp, xd.cpu().numpy()) < 1e-12
