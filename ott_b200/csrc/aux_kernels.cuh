@@ -26,25 +26,45 @@ struct PrepArgs {
 // every exponent. Deterministic: every CTA computes the same value.
 __device__ void sample_center(const float* x, int64_t n, const float* y, int64_t m,
                               int d, float* center) {
-  // warp w takes coordinates w, w + warps, ...; its lanes sum disjoint
-  // samples (q = lane, lane + 32, ...) and a fixed shuffle tree adds them:
-  // the same value on every call, without a 256-long chain of dependent
-  // loads per coordinate (blockDim.x is a multiple of 32)
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int warps = blockDim.x >> 5;
-  for (int k = warp; k < d; k += warps) {
-    double acc[2];
-    for (int side = 0; side < 2; ++side) {
-      const float* src = side ? y : x;
-      const int64_t cnt = side ? m : n;
-      const int64_t ns = cnt < 256 ? cnt : 256;
-      const int64_t stride = cnt / ns;
+  // thread t sums coordinate k = t % d over the samples q = t / d,
+  // t / d + groups, ... of each side (consecutive threads read consecutive
+  // coordinates of one sample row; 16 loads in flight per thread), then
+  // thread k adds the groups' sums in a fixed order: the same value on
+  // every call. Needs d <= 128 and blockDim.x >= d.
+  __shared__ double part[2][256];
+  const int t = threadIdx.x;
+  const int groups = (blockDim.x < 256 ? blockDim.x : 256) / d;
+  const int k = t % d, grp = t / d;
+  int64_t ns_side[2];
+  for (int side = 0; side < 2; ++side) {
+    const float* src = side ? y : x;
+    const int64_t cnt = side ? m : n;
+    const int64_t ns = cnt < 256 ? cnt : 256;
+    const int64_t stride = cnt / ns;
+    ns_side[side] = ns;
+    if (grp < groups) {
       double s = 0.0;
-      for (int64_t q = lane; q < ns; q += 32) s += (double)src[(q * stride) * d + k];
-      for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
-      acc[side] = s / (double)ns;
+      for (int64_t q0 = grp; q0 < ns; q0 += 16 * (int64_t)groups) {
+        float v[16];
+#pragma unroll
+        for (int u = 0; u < 16; ++u) {
+          const int64_t q = q0 + (int64_t)u * groups;
+          v[u] = q < ns ? src[(q * stride) * d + k] : 0.f;
+        }
+#pragma unroll
+        for (int u = 0; u < 16; ++u) s += (double)v[u];
+      }
+      part[side][t] = s;
     }
-    if (lane == 0) center[k] = (float)(0.5 * (acc[0] + acc[1]));
+  }
+  __syncthreads();
+  if (t < d) {
+    double a0 = 0.0, a1 = 0.0;
+    for (int gi = 0; gi < groups; ++gi) {
+      a0 += part[0][gi * d + t];
+      a1 += part[1][gi * d + t];
+    }
+    center[t] = (float)(0.5 * (a0 / (double)ns_side[0] + a1 / (double)ns_side[1]));
   }
   __syncthreads();
 }
@@ -316,28 +336,25 @@ __global__ void prep_points_tc_kernel(PrepArgs args) {
   float* nrm = const_cast<float*>(side ? P.ny : P.nx);
   const int d = args.d, dk = args.dp;
   sample_center(args.src[2 * p], P.n, args.src[2 * p + 1], P.m, d, center);
-  const __nv_bfloat16 zero = __float2bfloat16_rn(0.f);
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pad;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  // one warp per row: lanes over the coordinates, so the bf16 stores of a
+  // warp are contiguous; the squared norm is a fixed shuffle tree
+  const int lane = threadIdx.x & 31;
+  const int64_t warps = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t i = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; i < pad;
+       i += warps) {
     __nv_bfloat16* hi = dst + i * dk;
     __nv_bfloat16* lo = dst + (pad + i) * dk;
+    const float* row = src + i * d;
     double s = 0.0;
-    int k = 0;
-    if (i < cnt) {
-      const float* row = src + i * d;
-      for (; k < d; ++k) {
-        const float v = row[k] - center[k];
-        s += (double)v * (double)v;
-        const __nv_bfloat16 h = __float2bfloat16_rn(v);
-        hi[k] = h;
-        lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
-      }
+    for (int k = lane; k < dk; k += 32) {
+      const float v = (i < cnt && k < d) ? row[k] - center[k] : 0.f;
+      s += (double)v * (double)v;
+      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      hi[k] = h;
+      lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
     }
-    for (; k < dk; ++k) {
-      hi[k] = zero;
-      lo[k] = zero;
-    }
-    nrm[i] = (float)((double)P.inv_scale * s);
+    for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
+    if (lane == 0) nrm[i] = (float)((double)P.inv_scale * s);
   }
 }
 

@@ -544,7 +544,10 @@ int launch_solve(int num_problems, int d, const ottb_solver_cfg* cfg, ottb_resul
     PrepArgs pa{d_ptrs, d_probs, d, plan.dp};
     int64_t mx = 1;
     for (const ProbPlan& pp : plan.probs) mx = std::max(mx, std::max(pp.n_pad, pp.m_pad));
-    dim3 grid((unsigned)std::min<int64_t>((mx + 255) / 256, 1024), num_problems, 2);
+    // one thread per row (FP32 layout) or one warp per row, 8 rows a warp
+    // (tensor-core layout)
+    const int64_t per_cta = plan.tc ? 64 : 256;
+    dim3 grid((unsigned)std::min<int64_t>((mx + per_cta - 1) / per_cta, 1024), num_problems, 2);
     if (plan.tc)
       prep_points_tc_kernel<<<grid, 256, 0, stream>>>(pa);
     else
