@@ -520,8 +520,11 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
 // clear the split-arrival counters, then fill errors -> prep points -> init
 // potentials -> persistent loop (cooperative) -> finalize. Stream
 // operations only (a device-to-device copy, memsets, kernel launches).
+// finalize = false leaves out finalize_kernel (the result records, the
+// user g copy): for zero-iteration solves whose only output is marg_out or
+// lse_out, written by the persistent kernel itself.
 int launch_solve(int num_problems, int d, const ottb_solver_cfg* cfg, ottb_result* results,
-                 const Plan& plan, char* ws, cudaStream_t stream) {
+                 const Plan& plan, char* ws, cudaStream_t stream, bool finalize = true) {
   cudaError_t e;
   e = cudaMemcpyAsync(ws, ws + plan.off_pristine, plan.header_bytes, cudaMemcpyDeviceToDevice,
                       stream);
@@ -592,6 +595,7 @@ int launch_solve(int num_problems, int d, const ottb_solver_cfg* cfg, ottb_resul
   void* kargs[] = {&ka};
   e = cudaLaunchKernelExC(&lc, plan.kern.fn, kargs);
   if (e != cudaSuccess) return OTTB_ERR_CUDA;
+  if (!finalize) return OTTB_OK;
 
   FinalArgs fa{d_probs, ka.state, ka.sched, results, *cfg};
   finalize_kernel<<<num_problems, 512, 0, stream>>>(fa);
@@ -907,7 +911,7 @@ int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, in
   if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
   st = write_header(probs.data(), np, &S.cfg, S.plan, ws, stream, marg.data());
   if (st != OTTB_OK) return st;
-  st = launch_solve(np, d, &S.cfg, (ottb_result*)(ws + S.off_res), S.plan, ws, stream);
+  st = launch_solve(np, d, &S.cfg, (ottb_result*)(ws + S.off_res), S.plan, ws, stream, false);
   if (st != OTTB_OK) return st;
   const int64_t tot = (int64_t)num_vec * S.C;
   sweep_apply_diff_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
@@ -965,7 +969,7 @@ int32_t ottb_apply_lse_kernel(const float* x, const float* y, int64_t n, int64_t
   float* lse[1] = {out};
   st = write_header(probs.data(), 1, &S.cfg, plan1, ws, stream, nullptr, lse);
   if (st != OTTB_OK) return st;
-  return launch_solve(1, d, &S.cfg, (ottb_result*)(ws + S.off_res), plan1, ws, stream);
+  return launch_solve(1, d, &S.cfg, (ottb_result*)(ws + S.off_res), plan1, ws, stream, false);
 }
 
 size_t ottb_cost_stats_workspace_size(int64_t n, int64_t m, int32_t d) {
