@@ -69,6 +69,14 @@ __device__ void sample_center(const float* x, int64_t n, const float* y, int64_t
   __syncthreads();
 }
 
+// The common centre of problem blockIdx.x's two point sets, into its
+// workspace slot (read by the preparation kernels that follow).
+__global__ void center_kernel(PrepArgs args) {
+  const int p = blockIdx.x;
+  sample_center(args.src[2 * p], args.probs[p].n, args.src[2 * p + 1], args.probs[p].m,
+                args.d, args.probs[p].center);
+}
+
 __global__ void prep_points_kernel(PrepArgs args) {
   __shared__ float center[128];
   const int p = blockIdx.y;
@@ -80,7 +88,8 @@ __global__ void prep_points_kernel(PrepArgs args) {
   float* dst = const_cast<float*>(side ? P.yt : P.xt);
   float* nrm = const_cast<float*>(side ? P.ny : P.nx);
   const int d = args.d, dp = args.dp;
-  sample_center(args.src[2 * p], P.n, args.src[2 * p + 1], P.m, d, center);
+  for (int k = threadIdx.x; k < d; k += blockDim.x) center[k] = P.center[k];
+  __syncthreads();
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < pad;
        i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
@@ -335,7 +344,8 @@ __global__ void prep_points_tc_kernel(PrepArgs args) {
   __nv_bfloat16* dst = (__nv_bfloat16*)(side ? P.yh : P.xh);
   float* nrm = const_cast<float*>(side ? P.ny : P.nx);
   const int d = args.d, dk = args.dp;
-  sample_center(args.src[2 * p], P.n, args.src[2 * p + 1], P.m, d, center);
+  for (int k = threadIdx.x; k < d; k += blockDim.x) center[k] = P.center[k];
+  __syncthreads();
   // one warp per row: lanes over the coordinates, so the bf16 stores of a
   // warp are contiguous; the squared norm is a fixed shuffle tree
   const int lane = threadIdx.x & 31;

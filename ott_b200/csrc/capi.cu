@@ -220,7 +220,7 @@ struct ProbPlan {
   int64_t n, m, n_pad, m_pad;
   int rb_f, rb_g, split_f, split_g, smax_f, smax_g;
   size_t off_xt, off_yt, off_nx, off_ny, off_galt, off_pm, off_pl, off_arr, off_err,
-      off_msum, off_extx, off_exty;
+      off_msum, off_extx, off_exty, off_cen;
 };
 
 // BF16 split-3 on tcgen05 when asked for, and by default where the inner
@@ -400,6 +400,7 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     // tensor-core path: column-shift rows, 16 bytes per point (y: per g buffer)
     pp.off_extx = off; off = align_up(off + (plan.tc ? 16 * pp.n_pad : 0));
     pp.off_exty = off; off = align_up(off + (plan.tc ? 16 * 2 * pp.m_pad : 0));
+    pp.off_cen = off; off = align_up(off + fsz * 128);
   }
   plan.off_pristine = off; off = align_up(off + plan.header_bytes);
   plan.total = off;
@@ -468,6 +469,7 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     }
     P.nx = (const float*)(ws + pp.off_nx);
     P.ny = (const float*)(ws + pp.off_ny);
+    P.center = (float*)(ws + pp.off_cen);
     P.part_m = (float*)(ws + pp.off_pm);
     P.part_l = (float*)(ws + pp.off_pl);
     P.arrive = (int*)(ws + pp.off_arr);
@@ -545,6 +547,8 @@ int launch_solve(int num_problems, int d, const ottb_solver_cfg* cfg, ottb_resul
   }
   {
     PrepArgs pa{d_ptrs, d_probs, d, plan.dp};
+    // the common centre once per problem, then the points
+    center_kernel<<<num_problems, 256, 0, stream>>>(pa);
     int64_t mx = 1;
     for (const ProbPlan& pp : plan.probs) mx = std::max(mx, std::max(pp.n_pad, pp.m_pad));
     // one thread per row (FP32 layout) or one warp per row, 8 rows a warp

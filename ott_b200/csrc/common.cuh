@@ -70,6 +70,7 @@ struct ProbDev {
   float* marg_out;     // [m] column marginal of the final evaluation sweep, or null
   float* lse_out;      // [m] eps log sum_i exp((f_i + g_j - C_ij) / eps) - g_j of
                        // that sweep (apply_lse_kernel), or null
+  float* center;       // [128] workspace: the common centre of the two point sets
 };
 
 // Operands of one sweep for one problem, resolved from the descriptor.
