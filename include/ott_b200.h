@@ -206,6 +206,28 @@ int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, in
                                    int32_t axis, int32_t precision, float* out,
                                    void* workspace, size_t workspace_bytes, void* stream);
 
+/* The same product planned once and run many times (the implicit
+ * backward's MINRES steps apply the plan to a new vector at every step,
+ * with the points and potentials fixed). _plan lays out the workspace
+ * (ottb_apply_transport_sweep_workspace_size bytes), writes the uniform
+ * weights and the problem header into it and binds x, y and the output
+ * side's potential (g for axis 0, f for axis 1; the other may be NULL);
+ * it returns a handle in *product. _run takes the summed side's potential
+ * (f for axis 0, g for axis 1), num_vec vectors and the output, and issues
+ * stream operations only. The workspace must stay allocated and untouched
+ * by anything else, and the bound buffers allocated, until _free; their
+ * contents may change between runs. */
+typedef struct ottb_sweep_product ottb_sweep_product;
+int32_t ottb_apply_transport_sweep_plan(const float* x, const float* y, int64_t n, int64_t m,
+                                        int32_t d, const float* f, const float* g,
+                                        float epsilon, float inv_scale_cost, int32_t num_vec,
+                                        int32_t axis, int32_t precision, void* workspace,
+                                        size_t workspace_bytes, void* stream,
+                                        ottb_sweep_product** product);
+int32_t ottb_apply_transport_sweep_run(const ottb_sweep_product* product, const float* pot,
+                                       const float* vec, float* out, void* stream);
+void ottb_apply_transport_sweep_free(ottb_sweep_product* product);
+
 /* The log-domain kernel application (geometry/geometry.py:259-299,
  * apply_lse_kernel, vec = None) on the solver's sweep engine: axis 0
  * out[j] = eps log sum_i exp((pot_i - C_ij) / eps) over x (pot = f, out over

@@ -37,6 +37,9 @@ EXPORTED_SYMBOLS = (
     "ottb_apply_transport_sweep_workspace_size",
     "ottb_apply_transport_sweep",
     "ottb_apply_lse_kernel_workspace_size",
+    "ottb_apply_transport_sweep_plan",
+    "ottb_apply_transport_sweep_run",
+    "ottb_apply_transport_sweep_free",
     "ottb_apply_lse_kernel",
     "ottb_minres_step",
     "ottb_transport_matrix",
@@ -189,6 +192,14 @@ def load() -> ctypes.CDLL:
     lib.ottb_apply_lse_kernel.argtypes = [vp, vp, i64, i64, i32, vp, f32_, f32_, i32, i32, vp,
                                           vp, sz, vp]
     lib.ottb_apply_lse_kernel.restype = i32
+    lib.ottb_apply_transport_sweep_plan.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_,
+                                                    i32, i32, i32, vp, sz, vp,
+                                                    ctypes.POINTER(ctypes.c_void_p)]
+    lib.ottb_apply_transport_sweep_plan.restype = i32
+    lib.ottb_apply_transport_sweep_run.argtypes = [vp, vp, vp, vp, vp]
+    lib.ottb_apply_transport_sweep_run.restype = i32
+    lib.ottb_apply_transport_sweep_free.argtypes = [vp]
+    lib.ottb_apply_transport_sweep_free.restype = None
     lib.ottb_minres_step.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                      i64, vp]
     lib.ottb_minres_step.restype = i32

@@ -13,6 +13,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <new>
 #include <tuple>
 #include <vector>
 
@@ -732,7 +733,56 @@ int sweep_apply_setup(const float* x, const float* y, int64_t n, int64_t m, int 
   return OTTB_OK;
 }
 
+// The part of a sweep product fixed by its sizes, points, the potential of
+// the output side and the workspace: the layout, the uniform weights and the
+// problem header (whose pristine copy every launch restores).
+int sweep_product_plan(const float* x, const float* y, int64_t n, int64_t m, int32_t d,
+                       const float* f, const float* g, float epsilon, float inv_scale_cost,
+                       int32_t num_vec, int32_t axis, int32_t precision, char* ws,
+                       size_t workspace_bytes, cudaStream_t stream, SweepApply& S) {
+  std::vector<ottb_problem> probs;
+  std::vector<float*> marg;
+  int st = sweep_apply_setup(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                             precision, ws, true, S, probs, marg);
+  if (st != OTTB_OK) return st;
+  if (workspace_bytes < S.total) return OTTB_ERR_WORKSPACE;
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.R + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wa), S.R, 1.f / (float)S.R);
+  fill_kernel<<<(unsigned)std::min<int64_t>((S.C + 255) / 256, 1024), 256, 0, stream>>>(
+      (float*)(ws + S.off_wb), S.C, 1.f / (float)S.C);
+  if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+  return write_header(probs.data(), 2 * num_vec, &S.cfg, S.plan, ws, stream, marg.data());
+}
+
+// One planned product: stream operations only. pot is the summed side's
+// potential (f for axis 0, g for axis 1).
+int sweep_product_run(const SweepApply& S, int32_t d, float epsilon, char* ws,
+                      const float* pot, const float* vec, float* out, cudaStream_t stream) {
+  const int np = 2 * S.K;
+  const int64_t fp_n = (int64_t)np * S.R;
+  sweep_apply_potential_kernel<<<(unsigned)std::min<int64_t>((fp_n + 255) / 256, 4096), 256, 0,
+                                 stream>>>(pot, vec, S.R, S.K, epsilon,
+                                           (float*)(ws + S.off_fp));
+  if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+  const int st =
+      launch_solve(np, d, &S.cfg, (ottb_result*)(ws + S.off_res), S.plan, ws, stream, false);
+  if (st != OTTB_OK) return st;
+  const int64_t tot = (int64_t)S.K * S.C;
+  sweep_apply_diff_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
+                            stream>>>((const float*)(ws + S.off_marg), S.C, S.K, out);
+  return cuda_status(cudaGetLastError());
+}
+
 }  // namespace
+
+// A sweep product planned once (ottb_apply_transport_sweep_plan) and run
+// many times on its workspace.
+struct ottb_sweep_product {
+  SweepApply S;
+  int32_t d = 0;
+  float epsilon = 0.f;
+  char* ws = nullptr;
+};
 
 extern "C" {
 
@@ -894,34 +944,52 @@ int32_t ottb_apply_transport_sweep(const float* x, const float* y, int64_t n, in
   if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
   if (!workspace || ((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
   char* ws = (char*)workspace;
-  SweepApply S;
-  std::vector<ottb_problem> probs;
-  std::vector<float*> marg;
-  int st = sweep_apply_setup(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
-                             precision, ws, true, S, probs, marg);
-  if (st != OTTB_OK) return st;
-  if (workspace_bytes < S.total) return OTTB_ERR_WORKSPACE;
   cudaStream_t stream = (cudaStream_t)stream_ptr;
-  const int np = 2 * num_vec;
-  const float* pot = axis == 0 ? f : g;
-  const int64_t fp_n = (int64_t)np * S.R;
-  sweep_apply_potential_kernel<<<(unsigned)std::min<int64_t>((fp_n + 255) / 256, 4096), 256, 0,
-                                 stream>>>(pot, vec, S.R, num_vec, epsilon,
-                                           (float*)(ws + S.off_fp));
-  fill_kernel<<<(unsigned)std::min<int64_t>((S.R + 255) / 256, 1024), 256, 0, stream>>>(
-      (float*)(ws + S.off_wa), S.R, 1.f / (float)S.R);
-  fill_kernel<<<(unsigned)std::min<int64_t>((S.C + 255) / 256, 1024), 256, 0, stream>>>(
-      (float*)(ws + S.off_wb), S.C, 1.f / (float)S.C);
-  if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
-  st = write_header(probs.data(), np, &S.cfg, S.plan, ws, stream, marg.data());
+  SweepApply S;
+  int st = sweep_product_plan(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                              precision, ws, workspace_bytes, stream, S);
   if (st != OTTB_OK) return st;
-  st = launch_solve(np, d, &S.cfg, (ottb_result*)(ws + S.off_res), S.plan, ws, stream, false);
-  if (st != OTTB_OK) return st;
-  const int64_t tot = (int64_t)num_vec * S.C;
-  sweep_apply_diff_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
-                            stream>>>((const float*)(ws + S.off_marg), S.C, num_vec, out);
-  return cuda_status(cudaGetLastError());
+  return sweep_product_run(S, d, epsilon, ws, axis == 0 ? f : g, vec, out, stream);
 }
+
+int32_t ottb_apply_transport_sweep_plan(const float* x, const float* y, int64_t n, int64_t m,
+                                        int32_t d, const float* f, const float* g,
+                                        float epsilon, float inv_scale_cost, int32_t num_vec,
+                                        int32_t axis, int32_t precision, void* workspace,
+                                        size_t workspace_bytes, void* stream_ptr,
+                                        ottb_sweep_product** product) {
+  if (!product) return OTTB_ERR_INVALID;
+  *product = nullptr;
+  if (axis != 0 && axis != 1) return OTTB_ERR_INVALID;
+  // the output side's potential is bound here; the summed side's comes with each run
+  if (!x || !y || !(axis == 0 ? g : f) || n < 1 || m < 1 || d < 1 || num_vec < 1)
+    return OTTB_ERR_INVALID;
+  if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
+  if (!workspace || ((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
+  ottb_sweep_product* h = new (std::nothrow) ottb_sweep_product;
+  if (!h) return OTTB_ERR_INVALID;
+  const int st = sweep_product_plan(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                                    precision, (char*)workspace, workspace_bytes,
+                                    (cudaStream_t)stream_ptr, h->S);
+  if (st != OTTB_OK) {
+    delete h;
+    return st;
+  }
+  h->d = d;
+  h->epsilon = epsilon;
+  h->ws = (char*)workspace;
+  *product = h;
+  return OTTB_OK;
+}
+
+int32_t ottb_apply_transport_sweep_run(const ottb_sweep_product* product, const float* pot,
+                                       const float* vec, float* out, void* stream_ptr) {
+  if (!product || !pot || !vec || !out) return OTTB_ERR_INVALID;
+  return sweep_product_run(product->S, product->d, product->epsilon, product->ws, pot, vec, out,
+                           (cudaStream_t)stream_ptr);
+}
+
+void ottb_apply_transport_sweep_free(ottb_sweep_product* product) { delete product; }
 
 size_t ottb_apply_lse_kernel_workspace_size(int64_t n, int64_t m, int32_t d, int32_t axis,
                                             int32_t precision) {

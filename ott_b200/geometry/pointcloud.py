@@ -170,6 +170,20 @@ class PointCloud(geometry.Geometry):
     _lib.check(st, "ottb_apply_transport")
     return out
 
+  def _sweep_product(self, f: torch.Tensor, g: torch.Tensor, axis: int, precision: str,
+                     num_vec: int = 1) -> Optional["_SweepProduct"]:
+    """``_apply_raw`` on the sweep route planned once for fixed potentials
+    (``ottb_apply_transport_sweep_plan``): calling the result with
+    ``v2 [num_vec, n or m]`` issues stream operations only. None where
+    ``precision`` does not take the sweep route."""
+    if precision == "auto" and self.dim >= 32:
+      precision = "bf16_split3"
+    code = {"bf16_split3": _lib.PRECISION_BF16_SPLIT3,
+            "sweep_fp32": _lib.PRECISION_FP32}.get(precision)
+    if code is None:
+      return None
+    return _SweepProduct(self, f, g, axis, code, num_vec)
+
   def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
                                       axis: int = 0) -> torch.Tensor:
     """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
@@ -481,3 +495,53 @@ class _TransportMatrix(torch.autograd.Function):
       gx, gy = geom._points_vjp(rows, gy_rows, cols, gx_cols, gc)
     return (_cast(gx, geom.x, need[0]), _cast(gy, geom.y, need[1]), _cast(gf, f, need[2]),
             _cast(gg, g, need[3]), None)
+
+
+class _SweepProduct:
+  """One planned ``ottb_apply_transport_sweep`` product (the plan applied to
+  vectors through zero-iteration solves on the solver's sweep engine). It
+  owns the handle and the workspace and keeps the points and both
+  potentials alive; the handle is freed with the object."""
+
+  def __init__(self, geom: "PointCloud", f: torch.Tensor, g: torch.Tensor, axis: int,
+               code: int, num_vec: int):
+    lib = _lib.load()
+    n, m = geom.shape
+    dev = geom.x.device
+    self._lib = lib
+    self._handle = None
+    self._x, self._y = geom.x, geom.y
+    self._f = _arrays.as_f32(f, dev).detach().contiguous()
+    self._g = _arrays.as_f32(g, dev).detach().contiguous()
+    self._axis, self._num_vec = axis, num_vec
+    self._rows_in, self._rows_out = (n, m) if axis == 0 else (m, n)
+    ws_bytes = _sweep_ws_bytes(n, m, geom.dim, num_vec, axis, code)
+    if ws_bytes == 0:
+      raise NotImplementedError("problem sizes not supported by the sweep engine")
+    self._ws = torch.empty(ws_bytes, dtype=torch.uint8, device=dev)
+    h = ctypes.c_void_p()
+    st = lib.ottb_apply_transport_sweep_plan(
+        geom.x.data_ptr(), geom.y.data_ptr(), n, m, geom.dim, self._f.data_ptr(),
+        self._g.data_ptr(), ctypes.c_float(geom.epsilon), ctypes.c_float(geom.inv_scale_cost),
+        num_vec, axis, code, self._ws.data_ptr(), ws_bytes, _arrays.stream_handle(),
+        ctypes.byref(h))
+    _lib.check(st, "ottb_apply_transport_sweep_plan")
+    self._handle = h.value
+
+  def __call__(self, v2: torch.Tensor) -> torch.Tensor:
+    v2 = _arrays.as_f32(v2, self._ws.device).detach().contiguous()
+    if v2.shape != (self._num_vec, self._rows_in):
+      raise ValueError(f"vectors of shape {tuple(v2.shape)}, planned for "
+                       f"{(self._num_vec, self._rows_in)}")
+    out = torch.empty((self._num_vec, self._rows_out), dtype=torch.float32,
+                      device=self._ws.device)
+    pot = self._f if self._axis == 0 else self._g
+    st = self._lib.ottb_apply_transport_sweep_run(self._handle, pot.data_ptr(), v2.data_ptr(),
+                                                  out.data_ptr(), _arrays.stream_handle())
+    _lib.check(st, "ottb_apply_transport_sweep_run")
+    return out
+
+  def __del__(self):
+    if getattr(self, "_handle", None):
+      self._lib.ottb_apply_transport_sweep_free(self._handle)
+      self._handle = None

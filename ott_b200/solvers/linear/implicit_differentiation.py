@@ -289,12 +289,21 @@ class ImplicitDiff:
 
   @classmethod
   def _app(cls, geom, f, g, precision: str = "fp32"):
+    """The one-vector plan product of the backward. On the sweep route each
+    axis is planned once (``ottb_apply_transport_sweep_plan``) and every
+    product after that is stream operations only."""
     n, m = geom.shape
     if precision == "auto" and n * m < cls._TC_MIN_ENTRIES:
       precision = "fp32"
+    planned: Dict[int, Any] = {}
 
     def app(v: torch.Tensor, axis: int) -> torch.Tensor:
-      return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0].double()
+      if axis not in planned:
+        planned[axis] = geom._sweep_product(f, g, axis, precision)
+      prod = planned[axis]
+      if prod is None:
+        return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0].double()
+      return prod(v.reshape(1, -1))[0].double()
     return app
 
   def _precond(self, geom) -> Callable[[torch.Tensor], torch.Tensor]:

@@ -85,6 +85,26 @@ def test_invalid_arguments_rejected_without_device():
   # two zero-iteration problems per vector: more vectors, more workspace
   assert lib.ottb_apply_transport_sweep_workspace_size(1000, 2000, 64, 3, 0, 1) > ws_tc
   assert lib.ottb_apply_transport_workspace_size(1000, 2000, 64, 1, 3) == 0
+  # planned sweep products: no handle slot, no bound potential of the output
+  # side, a bad axis or an unaligned workspace are refused and leave no
+  # handle; a run without a handle is refused; freeing NULL is a no-op
+  h = ctypes.c_void_p(1234)
+  fake = 4096
+  assert lib.ottb_apply_transport_sweep_plan(fake, fake, 10, 10, 64, fake, fake, one, one, 1, 0,
+                                             1, fake, 1 << 20, None, None) == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_apply_transport_sweep_plan(fake, fake, 10, 10, 64, fake, None, one, one, 1, 0,
+                                             1, fake, 1 << 20, None,
+                                             ctypes.byref(h)) == _lib.OTTB_ERR_INVALID
+  assert h.value is None
+  assert lib.ottb_apply_transport_sweep_plan(fake, fake, 10, 10, 64, None, fake, one, one, 1, 2,
+                                             1, fake, 1 << 20, None,
+                                             ctypes.byref(h)) == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_apply_transport_sweep_plan(fake, fake, 10, 10, 64, None, fake, one, one, 1, 0,
+                                             1, fake + 8, 1 << 20, None,
+                                             ctypes.byref(h)) == _lib.OTTB_ERR_WORKSPACE
+  assert h.value is None
+  assert lib.ottb_apply_transport_sweep_run(None, fake, fake, fake, None) == _lib.OTTB_ERR_INVALID
+  lib.ottb_apply_transport_sweep_free(None)
   # MINRES step: null vectors, step outside [1, history_len), window < 1 or
   # an empty system are refused before any launch (the pointers below are
   # never dereferenced)

@@ -287,3 +287,30 @@ def test_output_members_match_oracle():
   assert abs(out.cost_at_geom(other) - want) <= 1e-4 * abs(want)
   with pytest.raises(NotImplementedError):
     out.to_dual_potentials()
+
+
+@pytest.mark.parametrize("precision", ["sweep_fp32", "bf16_split3"])
+@pytest.mark.parametrize("num_vec", [1, 3])
+def test_planned_sweep_product_equals_one_shot(precision, num_vec):
+  """``ottb_apply_transport_sweep_plan`` / ``_run`` against the one-shot
+  ``ottb_apply_transport_sweep`` on the same inputs: the same kernels, so
+  the same values to 1e-6 of the largest entry, for several vectors run in
+  a row on one plan (nothing carries over from one run to the next), on
+  both axes."""
+  import torch
+  x, y, a, b = problems.uniform_cloud_problem(700, 1100, 48, seed=5)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
+  gen = torch.Generator().manual_seed(num_vec)
+  for axis in (0, 1):
+    prod = geom._sweep_product(out.f, out.g, axis, precision, num_vec=num_vec)
+    rows = 700 if axis == 0 else 1100
+    for _ in range(3):
+      vec = torch.randn(num_vec, rows, generator=gen).cuda()
+      got = prod(vec)
+      want = geom._apply_raw(out.f, out.g, vec, axis, precision)
+      assert float((got - want).abs().max()) <= 1e-6 * float(want.abs().max())
+    with pytest.raises(ValueError):
+      prod(torch.zeros(num_vec + 1, rows, device="cuda"))
+    del prod
+  assert geom._sweep_product(out.f, out.g, 0, "fp32") is None
