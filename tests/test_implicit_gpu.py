@@ -427,3 +427,34 @@ def test_device_minres_matches_host_minres(case):
   # the public dispatch takes the device loop for CUDA tensors
   xp = imp._minres(op, b, rtol, max_steps, window)
   assert _rel(xp, xd.cpu().numpy()) < 1e-12
+
+
+def test_tensor_core_products_give_the_fp32_gradient():
+  """Above 2^25 plan entries at d >= 32 the chosen precision runs the
+  backward's one-vector products as planned zero-iteration solves on the
+  tensor-core sweep (``ottb_apply_transport_sweep_plan`` / ``_run``). At
+  the same potentials and cotangent its input cotangents agree with those
+  of the FP32 products within 5e-3 of each one's largest entry (products
+  within ~1.5e-4 relative, amplified by the system's conditioning)."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.problems.linear import linear_problem
+  from ott_b200.solvers import linear
+  from ott_b200.solvers.linear import implicit_differentiation as imp
+  n, d = 6144, 64
+  assert n * n >= imp.ImplicitDiff._TC_MIN_ENTRIES
+  x, y, _, _ = problems.gaussian_shift_problem(n, n, d, seed=1)
+  geom = pointcloud.PointCloud(_t(x), _t(y), epsilon=0.01, relative_epsilon="mean")
+  out = linear.solve(geom, threshold=1e-5, max_iterations=5000, precision="fp32")
+  assert geom._sweep_product(out.f, out.g, 0, "auto") is not None
+  prob = linear_problem.LinearProblem(geom)
+  gen = torch.Generator().manual_seed(2)
+  gr = (torch.randn(n, dtype=torch.float64, generator=gen).cuda(),
+        torch.randn(n, dtype=torch.float64, generator=gen).cuda())
+  tc = imp.ImplicitDiff().gradient(prob, out.f, out.g, True, gr, precision="auto")
+  tc_steps = imp.last_solve_info["steps"]
+  ref = imp.ImplicitDiff().gradient(prob, out.f, out.g, True, gr, precision="fp32")
+  assert tc_steps > 0
+  for got, want in zip(tc, ref):
+    want = want.detach().cpu().numpy()
+    assert _rel(got, want) < 5e-3, _rel(got, want)
