@@ -9,7 +9,7 @@
 // symmetric form.
 //
 // One CTA of 1024 threads: the vectors have the length of the smaller point
-// set, and a step's 13 vector passes cost microseconds next to the two plan
+// set, and a step's 15 vector passes cost microseconds next to the two plan
 // products of the same step. The two inner products are reduced in a fixed
 // order (a strided per-thread sum, then a shuffle tree), so a step is
 // deterministic.
