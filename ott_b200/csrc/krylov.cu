@@ -3,8 +3,8 @@
 // rotation of the tridiagonal system, the stop test and the updates of the
 // search direction, the iterate and the next Lanczos vector, in one launch.
 // The solver's scalars live in a small device array, so the host issues the
-// products of successive steps back to back and reads the state only every
-// few steps. Used by the implicit backward of the Sinkhorn potentials, whose
+// products of successive steps back to back and reads only the previous
+// step's stop flag while the current step runs. Used by the implicit backward of the Sinkhorn potentials, whose
 // linear system (implicit_differentiation.py:156-233) is solved here in a
 // symmetric form.
 //
