@@ -297,13 +297,18 @@ class ImplicitDiff:
       precision = "fp32"
     planned: Dict[int, Any] = {}
 
-    def app(v: torch.Tensor, axis: int) -> torch.Tensor:
+    def app32(v: torch.Tensor, axis: int) -> torch.Tensor:
+      # FP32 in and out: the products' own precision
       if axis not in planned:
         planned[axis] = geom._sweep_product(f, g, axis, precision)
       prod = planned[axis]
       if prod is None:
-        return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0].double()
-      return prod(v.reshape(1, -1))[0].double()
+        return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0]
+      return prod(v.reshape(1, -1))[0]
+
+    def app(v: torch.Tensor, axis: int) -> torch.Tensor:
+      return app32(v, axis).double()
+    app.f32 = app32
     return app
 
   def _precond(self, geom) -> Callable[[torch.Tensor], torch.Tensor]:
@@ -397,10 +402,25 @@ class ImplicitDiff:
     q = torch.where(s_s, torch.sqrt(torch.where(s_s, m_s, torch.ones_like(m_s))), zero)
     q = q / torch.linalg.vector_norm(q).clamp(min=1e-300)
 
-    def sym_op(yv):
-      # (I - K K^T) y with K = D_s^-1/2 R D_l^-1/2, plus q q^T y: the null
-      # eigenvalue moved to 1 (the solution is orthogonal to q)
-      return yv - c * r_op(inv_l * rt_op(c * yv)) + q * torch.dot(q, yv)
+    a32 = getattr(app, "f32", None)
+    if a32 is None:
+      def sym_op(yv):
+        # (I - K K^T) y with K = D_s^-1/2 R D_l^-1/2, plus q q^T y: the null
+        # eigenvalue moved to 1 (the solution is orthogonal to q)
+        return yv - c * r_op(inv_l * rt_op(c * yv)) + q * torch.dot(q, yv)
+    else:
+      # the same with the products' FP32 inputs written in place (the
+      # scaling computed in float64, rounded once) and the output formed
+      # by two fused multiply-adds: 6 small kernels a step instead of 12
+      r32, rt32 = ((lambda v: a32(v, 0)), (lambda v: a32(v, 1))) if n_gt_m else \
+                  ((lambda v: a32(v, 1)), (lambda v: a32(v, 0)))
+      in_s = torch.empty(c.shape, dtype=torch.float32, device=c.device)
+      in_l = torch.empty(inv_l.shape, dtype=torch.float32, device=c.device)
+
+      def sym_op(yv):
+        t = rt32(torch.mul(c, yv, out=in_s))
+        u = r32(torch.mul(inv_l, t, out=in_l))
+        return torch.addcmul(yv, q, torch.dot(q, yv)).addcmul_(c, u, value=-1.0)
 
     rhs = c * res
     rhs = rhs - q * torch.dot(q, rhs)
