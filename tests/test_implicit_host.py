@@ -1,6 +1,7 @@
-"""The conjugate-gradient solvers behind ImplicitDiff, on the CPU (plain
-torch tensors): solve_jax_cg (jax.scipy's stopping rule) and
-solve_normal_cg (lineax CG / NormalCG defaults)."""
+"""The Krylov solvers behind ImplicitDiff, on the CPU (plain torch
+tensors): solve_jax_cg (jax.scipy's stopping rule), solve_normal_cg
+(lineax CG / NormalCG defaults), the host MINRES loop, and the default
+solve's two forms of its symmetric operator on a dense FP32 plan."""
 import numpy as np
 import torch
 
@@ -92,3 +93,42 @@ def test_implicit_diff_fields_and_replace():
   assert d.solver is None and d.precondition_fun is None and d.symmetric is False
   d2 = d.replace(symmetric=True, solver_kwargs={"rtol": 1e-8})
   assert d2.symmetric and d2.solver_kwargs == {"rtol": 1e-8} and not d.symmetric
+
+
+def _dense_app(p, with_f32):
+  """The backward's plan product on a dense CPU plan, FP32 like the GPU's
+  (optionally with the FP32-in, FP32-out form ``app.f32``)."""
+  p32 = p.to(torch.float32)
+
+  def app32(v, axis):
+    v32 = v.to(torch.float32)
+    return v32 @ p32 if axis == 0 else p32 @ v32
+
+  def app(v, axis):
+    return app32(v, axis).double()
+  if with_f32:
+    app.f32 = app32
+  return app
+
+
+def test_default_solve_operator_forms_agree():
+  """``_solve_default`` with the fused symmetric operator (FP32 inputs
+  written in place, output by two multiply-adds) and with the plain
+  expression: the same solution to rounding, on both side orders, and a
+  recomputed residual at the FP32 products' floor."""
+  rng = np.random.default_rng(7)
+  for n, m in ((40, 25), (25, 40)):
+    p = torch.as_tensor(rng.uniform(0.1, 1.0, (n, m)))
+    p = p / p.sum()
+    ma, mb = p.sum(1), p.sum(0)
+    ones_a, ones_b = torch.ones(n, dtype=torch.bool), torch.ones(m, dtype=torch.bool)
+    gr_f = torch.as_tensor(rng.standard_normal(n))
+    gr_g = torch.as_tensor(rng.standard_normal(m))
+    sols = []
+    for with_f32 in (False, True):
+      lf, lg = imp.ImplicitDiff()._solve_default(gr_f, gr_g, ma, mb, ones_a, ones_b,
+                                                 _dense_app(p, with_f32), n > m)
+      assert imp.last_solve_info["true_rel_residual"] < 1e-5, imp.last_solve_info
+      sols.append(torch.cat([lf, lg]))
+    scale = float(sols[0].abs().max())
+    assert float((sols[0] - sols[1]).abs().max()) <= 1e-8 * scale
