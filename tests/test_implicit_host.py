@@ -132,3 +132,40 @@ def test_default_solve_operator_forms_agree():
       sols.append(torch.cat([lf, lg]))
     scale = float(sols[0].abs().max())
     assert float((sols[0] - sols[1]).abs().max()) <= 1e-8 * scale
+
+
+def test_app_plans_each_axis_once_and_falls_back():
+  """``ImplicitDiff._app``: each axis asks the geometry for a planned
+  product once and reuses it; without one it calls ``_apply_raw``; ``app``
+  is ``app.f32`` in float64. Below 2^25 plan entries the chosen precision
+  becomes FP32."""
+  p = torch.as_tensor(np.random.default_rng(3).uniform(size=(6, 4)))
+
+  class Geom:
+    shape = (6, 4)
+
+    def __init__(self, planned):
+      self.planned, self.asked, self.raw = planned, [], []
+
+    def _sweep_product(self, f, g, axis, precision):
+      self.asked.append((axis, precision))
+      if not self.planned:
+        return None
+      return lambda v2: (v2.float() @ p.float()) if axis == 0 else (v2.float() @ p.float().T)
+
+    def _apply_raw(self, f, g, v2, axis, precision):
+      self.raw.append((axis, precision))
+      return (v2.float() @ p.float()) if axis == 0 else (v2.float() @ p.float().T)
+
+  for planned in (True, False):
+    geom = Geom(planned)
+    app = imp.ImplicitDiff._app(geom, None, None, "auto")
+    v0, v1 = torch.ones(6, dtype=torch.float64), torch.ones(4, dtype=torch.float64)
+    for _ in range(3):
+      a0, a1 = app(v0, 0), app(v1, 1)
+      assert a0.dtype == torch.float64 and a0.shape == (4,) and a1.shape == (6,)
+      assert torch.equal(app.f32(v0, 0).double(), a0)
+    np.testing.assert_allclose(a0.numpy(), p.sum(0).numpy(), rtol=1e-6)
+    np.testing.assert_allclose(a1.numpy(), p.sum(1).numpy(), rtol=1e-6)
+    assert geom.asked == [(0, "fp32"), (1, "fp32")]
+    assert (len(geom.raw) == 0) if planned else (len(geom.raw) == 9)
