@@ -187,6 +187,24 @@ int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t 
                              int32_t axis, float* out, void* workspace,
                              size_t workspace_bytes, void* stream);
 
+/* ottb_apply_transport planned once for fixed points and potentials and
+ * run for many vectors (the implicit backward's one-vector products below
+ * the tensor-core route). _plan takes the workspace
+ * (ottb_apply_transport_workspace_size bytes, 256-byte aligned for the
+ * prepared path) and, where the call takes the prepared path (d <= 64),
+ * writes the common centre, B transposed and the column terms into it
+ * once; _run takes num_vec vectors and the output. x, y, f, g and the
+ * workspace must stay allocated and unchanged until _free. */
+typedef struct ottb_apply_product ottb_apply_product;
+int32_t ottb_apply_transport_plan(const float* x, const float* y, int64_t n, int64_t m,
+                                  int32_t d, const float* f, const float* g, float epsilon,
+                                  float inv_scale_cost, int32_t num_vec, int32_t axis,
+                                  void* workspace, size_t workspace_bytes, void* stream,
+                                  ottb_apply_product** product);
+int32_t ottb_apply_transport_run(const ottb_apply_product* product, const float* vec,
+                                 float* out, void* stream);
+void ottb_apply_transport_free(ottb_apply_product* product);
+
 /* The same application (geometry/geometry.py:444-486) on the solver's sweep
  * engine: tcgen05 BF16 split-3 products for d >= 32 under
  * OTTB_PRECISION_AUTO or _BF16_SPLIT3, FP32 otherwise. Each vector becomes two

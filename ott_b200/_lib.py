@@ -37,6 +37,9 @@ EXPORTED_SYMBOLS = (
     "ottb_apply_transport_sweep_workspace_size",
     "ottb_apply_transport_sweep",
     "ottb_apply_lse_kernel_workspace_size",
+    "ottb_apply_transport_plan",
+    "ottb_apply_transport_run",
+    "ottb_apply_transport_free",
     "ottb_apply_transport_sweep_plan",
     "ottb_apply_transport_sweep_run",
     "ottb_apply_transport_sweep_free",
@@ -192,6 +195,13 @@ def load() -> ctypes.CDLL:
     lib.ottb_apply_lse_kernel.argtypes = [vp, vp, i64, i64, i32, vp, f32_, f32_, i32, i32, vp,
                                           vp, sz, vp]
     lib.ottb_apply_lse_kernel.restype = i32
+    lib.ottb_apply_transport_plan.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, i32,
+                                              i32, vp, sz, vp, ctypes.POINTER(ctypes.c_void_p)]
+    lib.ottb_apply_transport_plan.restype = i32
+    lib.ottb_apply_transport_run.argtypes = [vp, vp, vp, vp]
+    lib.ottb_apply_transport_run.restype = i32
+    lib.ottb_apply_transport_free.argtypes = [vp]
+    lib.ottb_apply_transport_free.restype = None
     lib.ottb_apply_transport_sweep_plan.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_,
                                                     i32, i32, i32, vp, sz, vp,
                                                     ctypes.POINTER(ctypes.c_void_p)]

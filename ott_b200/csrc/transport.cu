@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <new>
 
 #include "../../include/ott_b200.h"
 #include "common.cuh"
@@ -81,6 +82,7 @@ struct ApplyArgs {
   float* wbv;         // [c_pad] (potB - inv |B - centre|^2) * ws, -inf padding
   float* vt;          // [c_pad][k_pad] vectors transposed, zero-padded
   int64_t c_pad, k_pad;
+  int prepared;       // host only: cen, bt and wbv already hold this plan's values
 };
 
 // Common centre of both point sets: the mean of up to kSampleMax points of
@@ -781,10 +783,12 @@ int launch_direct_pipelined(const ApplyArgs& a, cudaStream_t stream) {
     if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
         cudaSuccess)
       return OTTB_ERR_CUDA;
-    apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
-    const int64_t tot = (int64_t)DP * a.c_pad;
-    apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
-                          stream>>>(a, DP);
+    if (!a.prepared) {
+      apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
+      const int64_t tot = (int64_t)DP * a.c_pad;
+      apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
+                            stream>>>(a, DP);
+    }
     const int64_t vtot = (int64_t)a.K * a.c_pad;
     apply_prep_vpad_kernel<<<(unsigned)std::min<int64_t>((vtot + 255) / 256, 4096), 256, 0,
                              stream>>>(a);
@@ -899,8 +903,8 @@ int launch_pipelined_vt(const ApplyArgs& a, int chunks, cudaStream_t stream) {
   if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
       cudaSuccess)
     return OTTB_ERR_CUDA;
-  apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
-  {
+  if (!a.prepared) {
+    apply_prep_center_kernel<<<DP, 256, 0, stream>>>(a);
     const int64_t tot = (int64_t)DP * a.c_pad;
     apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0,
                           stream>>>(a, DP);
@@ -958,26 +962,25 @@ extern "C" size_t ottb_apply_transport_workspace_size(int64_t n, int64_t m, int3
   return pipelined_path(d, num_vec) ? prep_layout(C, d, num_vec, part).total : part;
 }
 
-extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
-                                        int32_t d, const float* f, const float* g,
-                                        float epsilon, float inv_scale_cost, const float* vec,
-                                        int32_t num_vec, int32_t axis, float* out,
-                                        void* workspace, size_t workspace_bytes,
-                                        void* stream) {
-  if (!x || !y || !f || !g || !vec || !out || n < 1 || m < 1 || d < 1 || num_vec < 1)
-    return OTTB_ERR_INVALID;
+namespace {
+
+// The launch arguments of one call (vec and out left to the caller).
+int make_apply_args(const float* x, const float* y, int64_t n, int64_t m, int32_t d,
+                    const float* f, const float* g, float epsilon, float inv_scale_cost,
+                    int32_t num_vec, int32_t axis, void* workspace, size_t workspace_bytes,
+                    ApplyArgs& a) {
+  if (!x || !y || !f || !g || n < 1 || m < 1 || d < 1 || num_vec < 1) return OTTB_ERR_INVALID;
   if (axis != 0 && axis != 1) return OTTB_ERR_INVALID;
   if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
   if (d > 128) return OTTB_ERR_UNSUPPORTED;
-  ApplyArgs a;
   a.A = axis == 1 ? x : y;
   a.B = axis == 1 ? y : x;
   a.potA = axis == 1 ? f : g;
   a.potB = axis == 1 ? g : f;
   a.R = axis == 1 ? n : m;
   a.C = axis == 1 ? m : n;
-  a.vec = vec;
-  a.out = out;
+  a.vec = nullptr;
+  a.out = nullptr;
   a.d = d;
   a.K = num_vec;
   a.ws = (float)(kLog2eD / (double)epsilon);
@@ -990,6 +993,7 @@ extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t 
   a.part_m = a.splits > 1 ? a.part_o + (size_t)a.splits * num_vec * a.R : nullptr;
   a.cen = a.bt = a.wbv = a.vt = nullptr;
   a.c_pad = a.k_pad = 0;
+  a.prepared = 0;
   if (pipelined_path(d, num_vec) && workspace) {
     // the prepared operands after the partials, when the workspace holds them
     const PrepLayout L = prep_layout(a.C, d, num_vec, apply_workspace(a.R, num_vec, a.splits));
@@ -1003,13 +1007,81 @@ extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t 
       a.k_pad = L.k_pad;
     }
   }
-  cudaStream_t s = (cudaStream_t)stream;
-  if (d <= 8) return launch_apply<8>(a, s);
-  if (d <= 16) return launch_apply<16>(a, s);
-  if (d <= 32) return launch_apply<32>(a, s);
-  if (d <= 64) return launch_apply<64>(a, s);
+  return OTTB_OK;
+}
+
+int run_apply(const ApplyArgs& a, cudaStream_t s) {
+  if (a.d <= 8) return launch_apply<8>(a, s);
+  if (a.d <= 16) return launch_apply<16>(a, s);
+  if (a.d <= 32) return launch_apply<32>(a, s);
+  if (a.d <= 64) return launch_apply<64>(a, s);
   return launch_apply<128>(a, s);
 }
+
+}  // namespace
+
+extern "C" int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t m,
+                                        int32_t d, const float* f, const float* g,
+                                        float epsilon, float inv_scale_cost, const float* vec,
+                                        int32_t num_vec, int32_t axis, float* out,
+                                        void* workspace, size_t workspace_bytes,
+                                        void* stream) {
+  if (!vec || !out) return OTTB_ERR_INVALID;
+  ApplyArgs a;
+  const int st = make_apply_args(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                                 workspace, workspace_bytes, a);
+  if (st != OTTB_OK) return st;
+  a.vec = vec;
+  a.out = out;
+  return run_apply(a, (cudaStream_t)stream);
+}
+
+// A product planned once (ottb_apply_transport_plan) and run many times.
+struct ottb_apply_product {
+  ApplyArgs a;
+};
+
+extern "C" int32_t ottb_apply_transport_plan(const float* x, const float* y, int64_t n,
+                                             int64_t m, int32_t d, const float* f,
+                                             const float* g, float epsilon,
+                                             float inv_scale_cost, int32_t num_vec,
+                                             int32_t axis, void* workspace,
+                                             size_t workspace_bytes, void* stream,
+                                             ottb_apply_product** product) {
+  if (!product) return OTTB_ERR_INVALID;
+  *product = nullptr;
+  ApplyArgs a;
+  const int st = make_apply_args(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
+                                 workspace, workspace_bytes, a);
+  if (st != OTTB_OK) return st;
+  if (a.bt) {
+    // the centre, B transposed and the column terms, once (d <= 64 here)
+    const int dp = d <= 8 ? 8 : d <= 16 ? 16 : d <= 32 ? 32 : 64;
+    cudaStream_t s = (cudaStream_t)stream;
+    apply_prep_center_kernel<<<dp, 256, 0, s>>>(a);
+    const int64_t tot = (int64_t)dp * a.c_pad;
+    apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0, s>>>(
+        a, dp);
+    if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+    a.prepared = 1;
+  }
+  ottb_apply_product* h = new (std::nothrow) ottb_apply_product;
+  if (!h) return OTTB_ERR_INVALID;
+  h->a = a;
+  *product = h;
+  return OTTB_OK;
+}
+
+extern "C" int32_t ottb_apply_transport_run(const ottb_apply_product* product,
+                                            const float* vec, float* out, void* stream) {
+  if (!product || !vec || !out) return OTTB_ERR_INVALID;
+  ApplyArgs a = product->a;
+  a.vec = vec;
+  a.out = out;
+  return run_apply(a, (cudaStream_t)stream);
+}
+
+extern "C" void ottb_apply_transport_free(ottb_apply_product* product) { delete product; }
 
 extern "C" int32_t ottb_transport_matrix(const float* x, const float* y, int64_t n, int64_t m,
                                          int32_t d, const float* f, const float* g,

@@ -184,6 +184,12 @@ class PointCloud(geometry.Geometry):
       return None
     return _SweepProduct(self, f, g, axis, code, num_vec)
 
+  def _apply_product(self, f: torch.Tensor, g: torch.Tensor, axis: int,
+                     num_vec: int = 1) -> "_ApplyProduct":
+    """``_apply_raw``'s FP32 product (``ottb_apply_transport``) planned once
+    for fixed potentials (``ottb_apply_transport_plan``)."""
+    return _ApplyProduct(self, f, g, axis, num_vec)
+
   def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
                                       axis: int = 0) -> torch.Tensor:
     """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
@@ -544,4 +550,49 @@ class _SweepProduct:
   def __del__(self):
     if getattr(self, "_handle", None):
       self._lib.ottb_apply_transport_sweep_free(self._handle)
+      self._handle = None
+
+
+class _ApplyProduct:
+  """One planned ``ottb_apply_transport`` product (FP32 on the CUDA cores).
+  It owns the handle and the workspace and keeps the points and both
+  potentials alive and unchanged; the handle is freed with the object."""
+
+  def __init__(self, geom: "PointCloud", f: torch.Tensor, g: torch.Tensor, axis: int,
+               num_vec: int):
+    lib = _lib.load()
+    n, m = geom.shape
+    dev = geom.x.device
+    self._lib = lib
+    self._handle = None
+    self._x, self._y = geom.x, geom.y
+    self._f = _arrays.as_f32(f, dev).detach().contiguous().clone()
+    self._g = _arrays.as_f32(g, dev).detach().contiguous().clone()
+    self._num_vec = num_vec
+    self._rows_in, self._rows_out = (n, m) if axis == 0 else (m, n)
+    ws_bytes = _apply_ws_bytes(n, m, geom.dim, num_vec, axis)
+    self._ws = torch.empty(max(ws_bytes, 1), dtype=torch.uint8, device=dev)
+    h = ctypes.c_void_p()
+    st = lib.ottb_apply_transport_plan(
+        geom.x.data_ptr(), geom.y.data_ptr(), n, m, geom.dim, self._f.data_ptr(),
+        self._g.data_ptr(), ctypes.c_float(geom.epsilon), ctypes.c_float(geom.inv_scale_cost),
+        num_vec, axis, self._ws.data_ptr(), ws_bytes, _arrays.stream_handle(), ctypes.byref(h))
+    _lib.check(st, "ottb_apply_transport_plan")
+    self._handle = h.value
+
+  def __call__(self, v2: torch.Tensor) -> torch.Tensor:
+    v2 = _arrays.as_f32(v2, self._ws.device).detach().contiguous()
+    if v2.shape != (self._num_vec, self._rows_in):
+      raise ValueError(f"vectors of shape {tuple(v2.shape)}, planned for "
+                       f"{(self._num_vec, self._rows_in)}")
+    out = torch.empty((self._num_vec, self._rows_out), dtype=torch.float32,
+                      device=self._ws.device)
+    st = self._lib.ottb_apply_transport_run(self._handle, v2.data_ptr(), out.data_ptr(),
+                                            _arrays.stream_handle())
+    _lib.check(st, "ottb_apply_transport_run")
+    return out
+
+  def __del__(self):
+    if getattr(self, "_handle", None):
+      self._lib.ottb_apply_transport_free(self._handle)
       self._handle = None

@@ -289,9 +289,10 @@ class ImplicitDiff:
 
   @classmethod
   def _app(cls, geom, f, g, precision: str = "fp32"):
-    """The one-vector plan product of the backward. On the sweep route each
-    axis is planned once (``ottb_apply_transport_sweep_plan``) and every
-    product after that is stream operations only."""
+    """The one-vector plan product of the backward, planned once per axis:
+    on the sweep route (``ottb_apply_transport_sweep_plan``) or the FP32
+    one (``ottb_apply_transport_plan``); every product after that is
+    stream operations only."""
     n, m = geom.shape
     if precision == "auto" and n * m < cls._TC_MIN_ENTRIES:
       precision = "fp32"
@@ -300,7 +301,10 @@ class ImplicitDiff:
     def app32(v: torch.Tensor, axis: int) -> torch.Tensor:
       # FP32 in and out: the products' own precision
       if axis not in planned:
-        planned[axis] = geom._sweep_product(f, g, axis, precision)
+        prod = geom._sweep_product(f, g, axis, precision)
+        if prod is None and hasattr(geom, "_apply_product"):
+          prod = geom._apply_product(f, g, axis)
+        planned[axis] = prod
       prod = planned[axis]
       if prod is None:
         return geom._apply_raw(f, g, v.reshape(1, -1), axis, precision)[0]

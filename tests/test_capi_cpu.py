@@ -85,6 +85,22 @@ def test_invalid_arguments_rejected_without_device():
   # two zero-iteration problems per vector: more vectors, more workspace
   assert lib.ottb_apply_transport_sweep_workspace_size(1000, 2000, 64, 3, 0, 1) > ws_tc
   assert lib.ottb_apply_transport_workspace_size(1000, 2000, 64, 1, 3) == 0
+  # planned FP32 products: no handle slot, a missing potential, d > 128 or
+  # no vectors are refused before any launch and leave no handle
+  hp = ctypes.c_void_p(99)
+  assert lib.ottb_apply_transport_plan(4096, 4096, 10, 10, 8, 4096, 4096, one, one, 1, 0, 4096,
+                                       1 << 20, None, None) == _lib.OTTB_ERR_INVALID
+  assert lib.ottb_apply_transport_plan(4096, 4096, 10, 10, 8, 4096, None, one, one, 1, 0, 4096,
+                                       1 << 20, None, ctypes.byref(hp)) == _lib.OTTB_ERR_INVALID
+  assert hp.value is None
+  assert lib.ottb_apply_transport_plan(4096, 4096, 10, 10, 200, 4096, 4096, one, one, 1, 0,
+                                       4096, 1 << 20, None,
+                                       ctypes.byref(hp)) == _lib.OTTB_ERR_UNSUPPORTED
+  assert lib.ottb_apply_transport_plan(4096, 4096, 10, 10, 8, 4096, 4096, one, one, 0, 0, 4096,
+                                       1 << 20, None, ctypes.byref(hp)) == _lib.OTTB_ERR_INVALID
+  assert hp.value is None
+  assert lib.ottb_apply_transport_run(None, 4096, 4096, None) == _lib.OTTB_ERR_INVALID
+  lib.ottb_apply_transport_free(None)
   # planned sweep products: no handle slot, no bound potential of the output
   # side, a bad axis or an unaligned workspace are refused and leave no
   # handle; a run without a handle is refused; freeing NULL is a no-op

@@ -314,3 +314,29 @@ def test_planned_sweep_product_equals_one_shot(precision, num_vec):
       prod(torch.zeros(num_vec + 1, rows, device="cuda"))
     del prod
   assert geom._sweep_product(out.f, out.g, 0, "fp32") is None
+
+
+@pytest.mark.parametrize("d", [48, 100])
+@pytest.mark.parametrize("num_vec", [1, 2, 3])
+def test_planned_fp32_product_equals_one_shot(d, num_vec):
+  """``ottb_apply_transport_plan`` / ``_run`` against the one-shot
+  ``ottb_apply_transport`` (FP32): the centre, B and its column terms
+  prepared once at d <= 64 (nothing to prepare at d = 100), several
+  vectors run in a row on one plan, both axes, within 1e-6 of the largest
+  entry."""
+  import torch
+  x, y, a, b = problems.uniform_cloud_problem(900, 1300, d, seed=d)
+  geom, out = helpers.gpu_solve(x, y, a, b, epsilon=0.05, relative_epsilon="mean",
+                                precision="fp32")
+  gen = torch.Generator().manual_seed(num_vec)
+  for axis in (0, 1):
+    prod = geom._apply_product(out.f, out.g, axis, num_vec=num_vec)
+    rows = 900 if axis == 0 else 1300
+    for _ in range(3):
+      vec = torch.randn(num_vec, rows, generator=gen).cuda()
+      got = prod(vec)
+      want = geom._apply_raw(out.f, out.g, vec, axis, "fp32")
+      assert float((got - want).abs().max()) <= 1e-6 * float(want.abs().max())
+    with pytest.raises(ValueError):
+      prod(torch.zeros(num_vec, rows + 1, device="cuda"))
+    del prod
