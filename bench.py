@@ -897,8 +897,11 @@ def run_implicit(args):
     e1.synchronize()
     return e0.elapsed_time(e1) / reps * 1e-3
 
-  tc = args.precision == "bf16_split3" or (args.precision == "auto" and d >= 32)
-  t_app = time_app(args.precision)
+  # the backward's own route: the sweep under the chosen precision at d >= 32
+  # from 2^25 plan entries, FP32 products below
+  tc = args.precision == "bf16_split3" or (
+      args.precision == "auto" and d >= 32 and n * n >= imp.ImplicitDiff._TC_MIN_ENTRIES)
+  t_app = time_app(args.precision if tc else "fp32")
   t_app32 = time_app("fp32")
   steps = int(info.get("steps", 0))
   n_app1 = 2 * steps + 4
@@ -922,7 +925,9 @@ def run_implicit(args):
   line = {
       "metric": "s per gradient through the Sinkhorn potentials (implicit differentiation)",
       "value": fwd_s + bwd_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
-      "workload": "implicit", "dtype": "bf16x3/f32" if tc else "f32",
+      "workload": "implicit",
+      "dtype": ("bf16x3/f32" if (tc or (args.precision == "auto" and d >= 32)) else "f32"),
+      "backward_products": "tensor-core sweep" if tc else "fp32",
       "data": "synthetic", "steps": args.steps, "warmup": args.warmup,
       "config": {"workload": f"grad of <w,f>+<v,g> through linear.solve, n=m={n} d={d} "
                              "x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, "
