@@ -36,10 +36,8 @@ if ROOT not in sys.path:
   sys.path.insert(0, ROOT)
 
 METRIC = "s to 1e-3 marginal err & Sinkhorn iters/s: chosen form vs plain FP32, 1 B200"
-# Sinkhorn iterations to the 1e-3 threshold on the default workload (d = 64),
-# measured on the FP32 CUDA path, by n.
-REF_ITERS = {65536: 30, 16384: 40, 4096: 50}
 L2_BYTES = 126 * 1024 * 1024
+GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 
 def parse_args():
@@ -49,14 +47,16 @@ def parse_args():
   p.add_argument("--warmup", type=int, default=3)
   p.add_argument("--impl", choices=["ours", "reference"], default="ours")
   p.add_argument("--precision", default="auto", choices=["auto", "fp32", "bf16_split3"])
-  p.add_argument("--n", type=int, default=65536)
-  p.add_argument("--d", type=int, default=64)
+  p.add_argument("--n", type=int, default=None, help="points per side (default: the workload's)")
+  p.add_argument("--d", type=int, default=None, help="dimension (default: the workload's)")
   p.add_argument("--no-plain", action="store_true", help="skip the plain FP32 comparison")
   p.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
   p.add_argument("--workload", default="gaussian64",
-                 choices=["gaussian64", "warmstart", "batched", "anneal", "divergence",
-                          "implicit", "sharded"],
+                 choices=["gaussian64", "uniform2048", "warmstart", "batched", "anneal",
+                          "divergence", "implicit", "sharded"],
                  help="gaussian64: the headline single large solve (default); "
+                      "uniform2048: n=m=2048, d=2 uniform clouds (the reference's "
+                      "CPU-runnable configuration, solved to convergence on the CPU too); "
                       "warmstart: learned warm start on a 32x32 grid; batched: 512 "
                       "uneven problems in one launch; anneal: epsilon-annealed solves; "
                       "divergence: Sinkhorn divergence and its gradient")
@@ -66,23 +66,70 @@ def parse_args():
   p.add_argument("--problems", type=int, default=512)
   p.add_argument("--pairs", type=int, default=8)
   p.add_argument("--stages", type=int, default=10)
-  return p.parse_args()
+  args = p.parse_args()
+  default_n, default_d = {"uniform2048": (2048, 2), "anneal": (16384, 128)}.get(
+      args.workload, (65536, 64))
+  args.n = default_n if args.n is None else args.n
+  args.d = default_d if args.d is None else args.d
+  return args
+
+
+# The single-solve workloads: seeded inputs, epsilon = mult * mean(C), and the
+# committed float64 solution of the same inputs where one exists.
+SOLVE_WORKLOADS = {
+    "gaussian64": dict(mult=0.01, fp64={(65536, 64): "gauss65536_d64"},
+                       data="x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, seed 0"),
+    "uniform2048": dict(mult=0.05, fp64={(2048, 2): "uniform2048_d2"},
+                        data="x,y~U[0,1]^d, a,b=U(0,1)+0.2 normalised, seed 0"),
+}
 
 
 def workload(args):
   from tests import problems
   n = args.n
-  x, y, a, b = problems.gaussian_shift_problem(n, n, args.d, seed=0)
-  return x, y, a, b
+  if args.workload == "uniform2048":
+    return problems.uniform_cloud_problem(n, n, args.d, seed=0)
+  return problems.gaussian_shift_problem(n, n, args.d, seed=0)
+
+
+def fp64_record(args):
+  """The committed float64 solve of this workload's inputs
+  (tests/golden/gen_fp64_workloads.py), or None."""
+  name = SOLVE_WORKLOADS[args.workload]["fp64"].get((args.n, args.d))
+  path = os.path.join(GOLDEN, f"{name}.fp64.npz") if name else None
+  if not path or not os.path.exists(path):
+    return None
+  rec = dict(np.load(path))
+  rec["name"] = name
+  return rec
+
+
+def accuracy_vs_fp64(out, rec):
+  """Errors of a solve against the float64 solution of the same inputs."""
+  if rec is None:
+    return None
+  eps = float(rec["epsilon"])
+  f = out.f.detach().cpu().numpy().astype(np.float64)
+  g = out.g.detach().cpu().numpy().astype(np.float64)
+  ff, gf = np.isfinite(rec["f"]), np.isfinite(rec["g"])
+  return {"reference": f"tests/golden/{rec['name']}.fp64.npz (float64 oracle, same inputs)",
+          "reg_ot_cost_rel": abs(out.reg_ot_cost - float(rec["reg_ot_cost"]))
+                             / abs(float(rec["reg_ot_cost"])),
+          "f_max_abs_over_eps": float(np.max(np.abs(f[ff] - rec["f"][ff]))) / eps,
+          "g_max_abs_over_eps": float(np.max(np.abs(g[gf] - rec["g"][gf]))) / eps,
+          "n_iters": int(out.n_iters), "n_iters_fp64": int(rec["n_iters"])}
 
 
 def config_dict(args, n_iters=None):
+  w = SOLVE_WORKLOADS[args.workload]
+  big = 2 * args.n * args.d * 4 > L2_BYTES
   return {"workload": f"sinkhorn sqeuclidean n=m={args.n} d={args.d} "
-                      f"eps=0.01*mean(C) thr=1e-3 (L1)",
-          "n": args.n, "m": args.n, "d": args.d, "epsilon": "0.01*mean(C)",
+                      f"eps={w['mult']}*mean(C) thr=1e-3 (L1)",
+          "n": args.n, "m": args.n, "d": args.d, "epsilon": f"{w['mult']}*mean(C)",
           "threshold": 1e-3, "max_iterations": 2000, "n_iters": n_iters,
-          "data": "x~N(0,I), y~N(0.5,diag(U[0.5,2])), uniform weights, seed 0",
-          "l2": "flushed between timed steps (256 MiB write); inputs 32 MiB < L2",
+          "data": w["data"],
+          "l2": "flushed between timed steps (256 MiB write); inputs "
+                f"{2 * args.n * args.d * 4 / 2**20:.2f} MiB {'>' if big else '<'} L2",
           "parallelism": f"replicas x{args.gpus}"}
 
 
@@ -181,68 +228,137 @@ def ncu_traffic(name):
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: C port of the oracle on a bounded row sample
+# CPU baselines: the C port of the oracle (tiled, vectorised, OpenMP on every
+# host thread) and the float32 NumPy restatement (BLAS products per block)
 # ---------------------------------------------------------------------------
-def cpu_sample(x, y, a, b, eps, rows, repeats=1):
-  """Times a 10-iteration scan solve of the first `rows` rows of x against
-  all of y. Returns seconds per cost entry (one entry of one LSE sweep)."""
+def reference_sweeps(n_iters, inner=10):
+  """Full n x m sweeps of the reference loop to n_iters iterations: two
+  potential updates per iteration, one error sweep per block of inner
+  iterations, one for reg_ot_cost."""
+  return 2 * n_iters + n_iters // inner + 1
+
+
+def cpu_solves_to_convergence(args):
+  """Whether a CPU step is a whole solve to the threshold (the small
+  configuration) or one full-size iteration (the large ones)."""
+  return args.n <= 8192
+
+
+def cpu_step(args, x, y, a, b, eps, variant="tiled"):
+  """One CPU step. Small workloads: the whole solve to the threshold.
+  Large: one full-size iteration as a 1-iteration solve (inner_iterations
+  1, max_iterations 1: the g- and f-update sweeps, the error sweep and the
+  reg_ot_cost sweep, 4 sweeps over all n x m entries). Returns seconds and
+  the result."""
   from oracle import sinkhorn_c
-  xs = np.ascontiguousarray(x[:rows])
-  as_ = a[:rows] / a[:rows].sum()
-  best = None
-  for _ in range(repeats):
-    t0 = time.perf_counter()
-    sinkhorn_c.solve(xs, y, as_, b, epsilon=eps, min_iterations=10, max_iterations=10)
-    dt = time.perf_counter() - t0
-    best = dt if best is None else min(best, dt)
-  # 20 update sweeps + 1 error sweep (it == max-1) + 1 reg_ot_cost sweep
-  sweeps = 22
-  return best / (sweeps * rows * y.shape[0]), sinkhorn_c.threads()
+  kw = {} if cpu_solves_to_convergence(args) else dict(inner_iterations=1, max_iterations=1)
+  t0 = time.perf_counter()
+  r = sinkhorn_c.solve(x, y, a, b, epsilon=eps, threshold=1e-3, variant=variant, **kw)
+  return time.perf_counter() - t0, r
 
 
-def cpu_time_to_threshold(sec_per_entry, n, m, n_iters, inner=10):
-  """Reference loop cost: 2 sweeps per iteration, 1 error sweep per block,
-  1 reg_ot_cost sweep."""
-  sweeps = 2 * n_iters + n_iters / inner + 1
-  return sec_per_entry * sweeps * n * m
+def cpu_seconds_to_threshold(args, step_s, n_iters):
+  """Seconds to the threshold from one step's time: the step itself when it
+  is a whole solve, else 4 full sweeps scaled to the loop's sweep count."""
+  if cpu_solves_to_convergence(args):
+    return step_s
+  return step_s / 4.0 * reference_sweeps(n_iters)
+
+
+def cpu_iteration_count(args, rec, fallback=None):
+  """Iterations the CPU loop runs to the threshold, for the extrapolation:
+  the float64 solve of the same inputs (its count equals the FP32 GPU
+  engine's on every parity case), else the fallback given."""
+  if rec is not None:
+    return int(rec["n_iters"]), f"float64 solve of the same inputs ({rec['name']})"
+  return (fallback or 30), "GPU FP32 engine's count" if fallback else "assumed (no record)"
+
+
+def cpu_sample_text(args, n_iters, src):
+  if cpu_solves_to_convergence(args):
+    return (f"whole solve to 1e-3 (n=m={args.n}, d={args.d}) per step, tiled C port "
+            "on all host threads")
+  return (f"one full-size iteration per step (g- and f-update sweeps, error sweep, "
+          f"reg_ot_cost sweep: 4 sweeps over all {args.n}x{args.n} entries, d={args.d}), "
+          f"scaled to {reference_sweeps(n_iters)} sweeps = {n_iters} iterations "
+          f"({src}) + error and reg_ot_cost sweeps")
+
+
+def numpy_f32_baseline(args, x, y, a, b, eps):
+  """The oracle in float32: the cost of each 1024-column (or row) block from
+  a BLAS product, the reference's centring and max-shifted log-sum-exp, blocks
+  on all host threads. Small workloads: the whole solve to the threshold;
+  large: a 1-iteration solve of the first 4096 rows against every column,
+  its per-entry time scaled to the full loop."""
+  from oracle import sinkhorn_np
+  workers = os.cpu_count() or 1
+  small = cpu_solves_to_convergence(args)
+  rows = args.n if small else min(args.n, 4096)
+  xs, as_ = x[:rows], a[:rows] / a[:rows].sum()
+  kw = {} if small else dict(inner_iterations=1, max_iterations=1)
+  t0 = time.perf_counter()
+  r = sinkhorn_np.solve(xs, y, as_, b, epsilon=eps, dtype=np.float32, batch_size=1024,
+                        workers=workers, threshold=1e-3, **kw)
+  dt = time.perf_counter() - t0
+  return dt, r, rows, workers
 
 
 def run_reference(args):
+  """The reference arm: the CPU restatement of the reference's loop (the
+  reference itself needs JAX, absent here and on the GPU machine), timed on
+  every host thread. Each step is what ``cpu_step`` describes; ``steps`` and
+  ``ms_per_step`` are the measured steps, ``value`` the seconds to the
+  threshold they give (extrapolated over iterations on the large
+  workloads, and marked so)."""
   rank = int(os.environ.get("RANK", "0"))
   if rank != 0:
     return 0
-  from oracle import sinkhorn_np
+  from oracle import sinkhorn_c, sinkhorn_np
+  if args.workload not in SOLVE_WORKLOADS:
+    print(json.dumps({"impl": "reference", "unavailable":
+                      f"no CPU arm for the {args.workload} workload; the reference arm "
+                      "times the single-solve workloads"}))
+    return 0
   x, y, a, b = workload(args)
-  eps = 0.01 * float(sinkhorn_np.mean_cost_matrix(x.astype(np.float64), y.astype(np.float64)))
-  rows = 2048 if args.n >= 8192 else args.n
-  # Iterations of the reference loop on this workload (a full-size CPU solve
-  # does not fit the time budget): the count of the FP32 CUDA path on the
-  # same seeded data, which equals the float64 oracle's count on every
-  # instance the oracle can solve (n = 4096: 50, parity tests). n = 65536:
-  # 30; n = 16384: 40.
-  n_iters = int(os.environ.get("OTTB_REF_ITERS", str(REF_ITERS.get(args.n, 30))))
+  mult = SOLVE_WORKLOADS[args.workload]["mult"]
+  eps = mult * float(sinkhorn_np.mean_cost_matrix(x.astype(np.float64), y.astype(np.float64)))
+  rec = fp64_record(args)
   for _ in range(args.warmup):
-    cpu_sample(x, y, a, b, eps, rows)
-  samples = []
+    cpu_step(args, x, y, a, b, eps)
+  times, r = [], None
   for _ in range(args.steps):
-    spe, cores = cpu_sample(x, y, a, b, eps, rows)
-    samples.append(spe)
-  spe = statistics.median(samples)
-  val = cpu_time_to_threshold(spe, args.n, args.n, n_iters)
-  iters_per_s = 1.0 / (spe * 2 * args.n * args.n)
+    dt, r = cpu_step(args, x, y, a, b, eps)
+    times.append(dt)
+  step_s = statistics.median(times)
+  small = cpu_solves_to_convergence(args)
+  if small:
+    n_iters, src = r.n_iters, "the CPU solve's own count"
+  else:
+    n_iters, src = cpu_iteration_count(args, rec)
+  val = cpu_seconds_to_threshold(args, step_s, n_iters)
+  sweep_s = step_s / (reference_sweeps(n_iters) if small else 4.0)
+  cores = sinkhorn_c.threads("tiled")
+  sample = cpu_sample_text(args, n_iters, src)
   line = {
       "metric": METRIC, "value": val, "unit": "s", "impl": "reference",
       "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-      "ms_per_step": val * 1e3, "higher_is_better": False, "scaling": "weak",
-      "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+      "ms_per_step": 1e3 * sum(times) / len(times), "higher_is_better": False,
+      "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
       "config": config_dict(args, n_iters),
-      "iters_per_s": iters_per_s, "entries_per_s": 1.0 / spe,
+      "extrapolated": not small, "measured_s_per_step": step_s,
+      "n_iters": n_iters, "n_iters_source": src,
+      "iters_per_s": 1.0 / (2 * sweep_s), "entries_per_s": args.n * args.n / sweep_s,
       "cpu_baseline": {"value": val, "unit": "s", "cores": cores, "kind": "port",
-                       "sample": f"10-iteration scan solve of {rows} of {args.n} rows "
-                                 f"x all {args.n} columns (d={args.d}), per-entry time "
-                                 f"scaled to 2.1 sweeps/iteration x {n_iters} iterations"},
+                       "sample": sample},
       "e2e": {"value": val, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
   }
+  if small:
+    line["converged"] = bool(r.converged)
+    line["reg_ot_cost"] = float(r.reg_ot_cost)
+    if rec is not None:
+      line["n_iters_fp64"] = int(rec["n_iters"])
+      line["reg_ot_cost_rel_vs_fp64"] = abs(r.reg_ot_cost - float(rec["reg_ot_cost"])) / abs(
+          float(rec["reg_ot_cost"]))
   print(json.dumps(line))
   return 0
 
@@ -281,7 +397,8 @@ def run_ours(args):
   x, y, a, b = workload(args)
   xd, yd = torch.from_numpy(x).cuda(), torch.from_numpy(y).cuda()
   ad, bd = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
-  geom = pointcloud.PointCloud(xd, yd, epsilon=0.01, relative_epsilon="mean")
+  mult = SOLVE_WORKLOADS[args.workload]["mult"]
+  geom = pointcloud.PointCloud(xd, yd, epsilon=mult, relative_epsilon="mean")
   eps = geom.epsilon
   prob = linear_problem.LinearProblem(geom, ad, bd)
   flush = torch.empty(2 * L2_BYTES, dtype=torch.uint8, device="cuda")
@@ -315,9 +432,9 @@ def run_ours(args):
   # plain FP32 comparison (the "vs plain FP32" half of the metric)
   plain = None
   if not args.no_plain and form != "fp32":
-    pms, pout = timed_solves(sinkhorn.Sinkhorn(threshold=1e-3, precision="fp32"), 1, 1)
-    plain = {"s_to_threshold": pms * 1e-3, "n_iters": pout.n_iters,
-             "iters_per_s": pout.n_iters / (pms * 1e-3)}
+    pms, plain_out = timed_solves(sinkhorn.Sinkhorn(threshold=1e-3, precision="fp32"), 1, 1)
+    plain = {"s_to_threshold": pms * 1e-3, "n_iters": plain_out.n_iters,
+             "iters_per_s": plain_out.n_iters / (pms * 1e-3)}
 
   # end to end through the public API, host buffers in, results out
   xh = torch.from_numpy(x).pin_memory()
@@ -326,7 +443,7 @@ def run_ours(args):
   bh = torch.from_numpy(b).pin_memory()
 
   def e2e_step():
-    g = pointcloud.PointCloud(xh, yh, epsilon=0.01, relative_epsilon="mean")
+    g = pointcloud.PointCloud(xh, yh, epsilon=mult, relative_epsilon="mean")
     o = linear.solve(g, ah, bh, threshold=1e-3, precision=args.precision)
     f_host, g_host = o.f.cpu(), o.g.cpu()
     err_host = o.errors.cpu()
@@ -390,17 +507,43 @@ def run_ours(args):
     roof["measured_peaks_file"] = {"hbm_gbs": mp.get("hbm_gbs"),
                                    "bf16_tflops": mp.get("bf16_tflops")}
 
-  cpu = None
-  if not args.no_cpu and rank == 0 and world == 1:
-    rows = 2048 if args.n >= 8192 else args.n
-    spe, cores = cpu_sample(x, y, a, b, eps, rows)
-    val = cpu_time_to_threshold(spe, args.n, args.n, n_iters)
-    cpu = {"value": val, "unit": "s", "cores": cores, "kind": "port",
-           "sample": f"10-iteration scan solve of {rows} of {args.n} rows x all "
-                     f"{args.n} columns, per-entry time scaled to 2.1 sweeps/iteration "
-                     f"x {n_iters} iterations"}
+  # accuracy of both forms against the float64 solve of the same inputs
+  rec = fp64_record(args)
+  accuracy = {form: accuracy_vs_fp64(out, rec)}
+  if plain is not None:
+    accuracy["fp32"] = accuracy_vs_fp64(plain_out, rec)
 
-  launches_per_solve = 5  # fill errors, prep, init, persistent loop, finalize
+  cpu = cpu_np = None
+  if not args.no_cpu and rank == 0 and world == 1:
+    from oracle import sinkhorn_c
+    cpu_step(args, x, y, a, b, eps)  # warm-up (library load, page-in)
+    step_s, r = cpu_step(args, x, y, a, b, eps)
+    small = cpu_solves_to_convergence(args)
+    c_iters, src = ((r.n_iters, "the CPU solve's own count") if small
+                    else cpu_iteration_count(args, rec, fallback=n_iters))
+    val = cpu_seconds_to_threshold(args, step_s, c_iters)
+    cpu = {"value": val, "unit": "s", "cores": sinkhorn_c.threads("tiled"), "kind": "port",
+           "extrapolated": not small, "measured_s": step_s,
+           "sample": cpu_sample_text(args, c_iters, src)}
+    if small:
+      cpu.update(n_iters=r.n_iters, converged=bool(r.converged),
+                 reg_ot_cost_rel_vs_gpu=abs(r.reg_ot_cost - out.reg_ot_cost)
+                 / abs(out.reg_ot_cost))
+    np_s, r_np, rows, workers = numpy_f32_baseline(args, x, y, a, b, eps)
+    if small:
+      np_val = np_s
+      np_sample = f"whole solve to 1e-3 in float32 NumPy ({r_np.n_iters} iterations)"
+    else:
+      np_val = np_s / (4.0 * rows * args.n) * reference_sweeps(c_iters) * args.n * args.n
+      np_sample = (f"1-iteration solve (4 sweeps) of the first {rows} of {args.n} rows x all "
+                   f"{args.n} columns, per-entry time scaled to {reference_sweeps(c_iters)} "
+                   "full sweeps")
+    cpu_np = {"value": np_val, "unit": "s", "cores": workers, "kind": "port",
+              "extrapolated": not small, "measured_s": np_s, "sample": np_sample}
+
+  # error log fill, common centre, point preparation, potential init, the
+  # persistent solve, finalize
+  launches_per_solve = 6
   line = {
       "metric": METRIC, "value": ms * 1e-3, "unit": "s", "n_gpus": world,
       "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -409,7 +552,8 @@ def run_ours(args):
       "config": config_dict(args, n_iters), "form": form, "converged": converged,
       "iters_per_s": n_iters / t, "entries_per_s": entries / t,
       "plain_fp32": plain,
-      "roofline": roof, "cpu_baseline": cpu,
+      "roofline": roof, "cpu_baseline": cpu, "cpu_baseline_numpy_f32": cpu_np,
+      "accuracy_vs_fp64": accuracy,
       "e2e": {"value": e2e_ms * 1e-3, "unit": "s", "h2d_bytes_per_step": h2d,
               "d2h_bytes_per_step": d2h},
       "clocks": clk, "gpu_launches": launches_per_solve * args.steps,

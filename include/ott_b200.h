@@ -39,7 +39,8 @@ enum {
   OTTB_ERR_CUDA = 3,        /* a CUDA runtime call failed                  */
   OTTB_ERR_TIMEOUT = 4,     /* a device-side wait hit its time limit       */
   OTTB_ERR_WORKSPACE = 5,   /* workspace missing or too small              */
-  OTTB_ERR_NO_DEVICE = 6    /* no sm_100 device visible                    */
+  OTTB_ERR_NO_DEVICE = 6,   /* no sm_100 device visible                    */
+  OTTB_ERR_HOST_MEMORY = 7  /* a host-side allocation (a plan handle) failed */
 };
 
 /* Arithmetic used for the inner products <x_i, y_j>. */
@@ -278,11 +279,13 @@ int32_t ottb_transport_matrix(const float* x, const float* y, int64_t n, int64_t
  * workspace is a 16 MiB (OTTB_NOALLOC_SCRATCH_BYTES) array compiled into the
  * library, held in every GPU that loads the library until the process exits.
  * Calls whose scratch need (ottb_sinkhorn_workspace_size) exceeds that return
- * OTTB_ERR_WORKSPACE before enqueuing anything. The first call on a device
- * looks up the array's device address; make that first call before any
- * stream capture. All calls share the array: calls whose work overlaps on
- * the GPU race, so order them (one stream). Inputs, outputs and status as for
- * ottb_sinkhorn_pointcloud. */
+ * OTTB_ERR_WORKSPACE before enqueuing anything. A call outside stream capture
+ * looks up the array's device address on the current device; a call under
+ * capture reuses the address of the last uncaptured call on that device, so
+ * make one call on each device before capturing (a first call under capture
+ * returns OTTB_ERR_INVALID). All calls share the array: calls whose work
+ * overlaps on the GPU race, so order them (one stream). Inputs, outputs and
+ * status as for ottb_sinkhorn_pointcloud. */
 int32_t ottb_sinkhorn_pointcloud_noalloc(const ottb_problem* problems,
                                          int32_t num_problems, int32_t d,
                                          const ottb_solver_cfg* cfg,

@@ -25,7 +25,12 @@ import types
 
 from oracle import jaxshim
 
-DEFAULT_ROOT = "/root/reference/src"
+# The reference's source root: $OTT_REFERENCE_SRC, else the ott-jax tree
+# checked out beside this repository (<parent>/reference/src).
+DEFAULT_ROOT = os.environ.get(
+    "OTT_REFERENCE_SRC",
+    os.path.join(os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))),
+                 "reference", "src"))
 
 
 class _Anything:

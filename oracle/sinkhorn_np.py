@@ -166,6 +166,11 @@ class Geom:
   ``batch_size`` follows pointcloud.py:438-448: ``None`` materialises the
   cost (geometry.py:260-299); an integer recomputes it in blocks
   (pointcloud.py:85-103), which is what lets the oracle run large inputs.
+  ``workers`` > 1 evaluates the blocks on that many threads, BLAS limited to
+  one thread per block. Each block is computed as in the serial loop and
+  writes its own output slice, so the results are bit-identical to a serial
+  run with one BLAS thread (a multi-threaded BLAS blocks its products
+  differently, a rounding-level difference).
   """
   x: np.ndarray
   y: np.ndarray
@@ -174,7 +179,21 @@ class Geom:
   eps_init: float = 1.0
   eps_decay: float = 1.0
   batch_size: Optional[int] = None
+  workers: int = 1
   _cost: Optional[np.ndarray] = field(default=None, repr=False)
+
+  def _for_blocks(self, total, bs, fn):
+    starts = range(0, total, bs)
+    if self.workers <= 1 or self.batch_size is None or total <= bs:
+      for s in starts:
+        fn(s)
+      return
+    from concurrent.futures import ThreadPoolExecutor
+
+    import threadpoolctl
+    with threadpoolctl.threadpool_limits(1), \
+        ThreadPoolExecutor(max_workers=self.workers) as ex:
+      list(ex.map(fn, starts))
 
   @property
   def dtype(self):
@@ -209,7 +228,8 @@ class Geom:
     if axis == 0:
       out = np.empty((m,), dt)
       sgn = np.ones((m,), dt)
-      for s in range(0, m, bs):
+
+      def block(s):
         cols = slice(s, min(s + bs, m))
         center = (f[:, None] + g[None, cols]) - self.cost_block(cols=cols)
         r, sg = logsumexp(center / eps, axis=0,
@@ -217,11 +237,13 @@ class Geom:
                           return_sign=True)
         out[cols] = eps * r
         sgn[cols] = sg
+      self._for_blocks(m, bs, block)
       remove = g
     else:
       out = np.empty((n,), dt)
       sgn = np.ones((n,), dt)
-      for s in range(0, n, bs):
+
+      def block(s):
         rows = slice(s, min(s + bs, n))
         center = (f[rows, None] + g[None, :]) - self.cost_block(rows=rows)
         r, sg = logsumexp(center / eps, axis=1,
@@ -229,6 +251,7 @@ class Geom:
                           return_sign=True)
         out[rows] = eps * r
         sgn[rows] = sg
+      self._for_blocks(n, bs, block)
       remove = f
     with np.errstate(invalid="ignore"):
       res = out - np.where(np.isfinite(remove), remove, 0).astype(dt)
@@ -408,14 +431,14 @@ def sinkhorn(geom: Geom, a=None, b=None, *, threshold=1e-3, norm_error=1,
 
 def solve(x, y=None, a=None, b=None, *, epsilon=None, relative_epsilon=None,
           scale_cost=1.0, batch_size=None, eps_init=1.0, eps_decay=1.0,
-          dtype=np.float64, **kw) -> SinkhornResult:
+          dtype=np.float64, workers=1, **kw) -> SinkhornResult:
   """_solve.py:29-64 on ``PointCloud(x, y, epsilon, relative_epsilon)``."""
   x = np.asarray(x, dtype)
   y = x if y is None else np.asarray(y, dtype)
   inv = inv_scale_cost(x, y, scale_cost)
   eps = resolve_epsilon(x, y, epsilon, relative_epsilon, inv)
   geom = Geom(x, y, float(eps), inv_scale=float(inv), eps_init=eps_init,
-              eps_decay=eps_decay, batch_size=batch_size)
+              eps_decay=eps_decay, batch_size=batch_size, workers=workers)
   return sinkhorn(geom, a, b, **kw)
 
 

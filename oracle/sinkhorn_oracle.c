@@ -5,7 +5,9 @@
  *
  * Used only by tests (as a second restatement checked against the NumPy
  * oracle) and by bench.py's CPU-baseline leg and `--impl reference` arm.
- * The ott_b200 package never links or loads it.
+ * The ott_b200 package never links or loads it. Compiled with -DOTTB_TILED,
+ * the kernel application is the tiled, vectorised one of lse_tiled.h (the
+ * timed baseline); the loop around it is the same.
  *
  * Follows, in order:
  *   solvers/linear/sinkhorn.py:803-857  lse_step (g-update, then f-update)
@@ -38,6 +40,20 @@ static inline real cost_ij(const real* xi, const real* yj, real nxi, real nyj, i
   return inv * ((nxi + nyj) + (real)(-2.0) * dot);
 }
 
+#ifdef OTTB_TILED
+#include "lse_tiled.h"
+
+/* The tiled, vectorised row log-sum-exp of lse_tiled.h, with the roles of
+ * the two point sets swapped for axis 0. */
+static void apply_lse(const real* x, const real* y, const real* nx, const real* ny,
+                      int64_t n, int64_t m, int d, real inv, const real* f,
+                      const real* g, real eps, int axis, real* out) {
+  if (axis == 0)
+    lt_row_lse(y, x, ny, nx, m, n, d, inv, g, f, eps, out);
+  else
+    lt_row_lse(x, y, nx, ny, n, m, d, inv, f, g, eps, out);
+}
+#else
 /* out[j] = eps * lse_i((f_i + g_j - C_ij) / eps) - finite(g_j)  (axis 0) or
  * out[i] = eps * lse_j((f_i + g_j - C_ij) / eps) - finite(f_i)  (axis 1). */
 static void apply_lse(const real* x, const real* y, const real* nx, const real* ny,
@@ -69,6 +85,7 @@ static void apply_lse(const real* x, const real* y, const real* nx, const real* 
     free(buf);
   }
 }
+#endif
 
 static void update_potential(const real* x, const real* y, const real* nx, const real* ny,
                              int64_t n, int64_t m, int d, real inv, const real* f,

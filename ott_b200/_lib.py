@@ -21,6 +21,7 @@ OTTB_ERR_CUDA = 3
 OTTB_ERR_TIMEOUT = 4
 OTTB_ERR_WORKSPACE = 5
 OTTB_ERR_NO_DEVICE = 6
+OTTB_ERR_HOST_MEMORY = 7
 
 PRECISION_AUTO = -1
 PRECISION_FP32 = 0

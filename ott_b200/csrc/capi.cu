@@ -797,6 +797,7 @@ const char* ottb_status_string(int32_t status) {
     case OTTB_ERR_TIMEOUT: return "device wait timed out";
     case OTTB_ERR_WORKSPACE: return "workspace missing or too small";
     case OTTB_ERR_NO_DEVICE: return "no sm_100 device";
+    case OTTB_ERR_HOST_MEMORY: return "host memory allocation failed";
     default: return "unknown status";
   }
 }
@@ -967,7 +968,7 @@ int32_t ottb_apply_transport_sweep_plan(const float* x, const float* y, int64_t 
   if (!(epsilon > 0.f) || !(inv_scale_cost > 0.f)) return OTTB_ERR_INVALID;
   if (!workspace || ((uintptr_t)workspace) % kAlign != 0) return OTTB_ERR_WORKSPACE;
   ottb_sweep_product* h = new (std::nothrow) ottb_sweep_product;
-  if (!h) return OTTB_ERR_INVALID;
+  if (!h) return OTTB_ERR_HOST_MEMORY;
   const int st = sweep_product_plan(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
                                     precision, (char*)workspace, workspace_bytes,
                                     (cudaStream_t)stream_ptr, h->S);

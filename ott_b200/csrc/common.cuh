@@ -138,7 +138,7 @@ constexpr float kRoundShift = 12582912.0f;  // 1.5 * 2^23
 // Range reduction x = n + f, n = rint(x), f in [-1/2, 1/2] (exact for
 // |x| < 2^22: adding 1.5 * 2^23 rounds x to an integer in the low mantissa
 // bits); 2^f by a degree-5 polynomial minimising the maximum relative error
-// on [-1/2, 1/2], fitted by exp2_poly_fit.py (Remez exchange; 7.5e-8
+// on [-1/2, 1/2], fitted by tests/exp2_poly_fit.py (Remez exchange; 7.5e-8
 // minimax, 2.3e-7 evaluated in FP32); 2^n by adding n to the exponent
 // field. Inputs below -126 are clamped (the result, < 2^-125, is negligible
 // next to the running sum's leading term >= 1); callers keep x <= kTau + 1.

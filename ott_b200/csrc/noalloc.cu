@@ -29,17 +29,25 @@ void* g_scratch_addr[kMaxDevices] = {};
 
 // Device address of g_noalloc_scratch on the current device. In host code
 // the array's name is only a host-side stand-in, so the address must come
-// from cudaGetSymbolAddress, once per device, with that device current.
-int32_t scratch_address(void** out) {
+// from cudaGetSymbolAddress, with that device current. A call made outside
+// stream capture looks it up again (cheap once the module is loaded), so a
+// device reset, which reloads the module at a new address, never leaves a
+// stale address behind; a call under capture uses the address of the last
+// uncaptured call on that device, and fails without one.
+int32_t scratch_address(cudaStream_t stream, void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return OTTB_ERR_NO_DEVICE;
   if (dev < 0 || dev >= kMaxDevices) return OTTB_ERR_NO_DEVICE;
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) return OTTB_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_scratch_mu);
-  if (g_scratch_addr[dev] == nullptr) {
+  if (cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
     if (e != cudaSuccess || p == nullptr) return OTTB_ERR_CUDA;
     g_scratch_addr[dev] = p;
+  } else if (g_scratch_addr[dev] == nullptr) {
+    return OTTB_ERR_INVALID;  // first call on this device under capture
   }
   *out = g_scratch_addr[dev];
   return OTTB_OK;
@@ -56,7 +64,7 @@ extern "C" int32_t ottb_sinkhorn_pointcloud_noalloc(const ottb_problem* problems
   const size_t need = ottb_sinkhorn_workspace_size(problems, num_problems, d, cfg);
   if (need > (size_t)OTTB_NOALLOC_SCRATCH_BYTES) return OTTB_ERR_WORKSPACE;
   void* scratch = nullptr;
-  const int32_t st = scratch_address(&scratch);
+  const int32_t st = scratch_address((cudaStream_t)stream, &scratch);
   if (st != OTTB_OK) return st;
   // The solve writes every word of its workspace it later reads (the call
   // header, and the split-arrival counters it clears with cudaMemsetAsync),

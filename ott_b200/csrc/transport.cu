@@ -1054,19 +1054,24 @@ extern "C" int32_t ottb_apply_transport_plan(const float* x, const float* y, int
   const int st = make_apply_args(x, y, n, m, d, f, g, epsilon, inv_scale_cost, num_vec, axis,
                                  workspace, workspace_bytes, a);
   if (st != OTTB_OK) return st;
+  // the handle first, so that nothing is enqueued for a plan that cannot be kept
+  ottb_apply_product* h = new (std::nothrow) ottb_apply_product;
+  if (!h) return OTTB_ERR_HOST_MEMORY;
   if (a.bt) {
     // the centre, B transposed and the column terms, once (d <= 64 here)
     const int dp = d <= 8 ? 8 : d <= 16 ? 16 : d <= 32 ? 32 : 64;
     cudaStream_t s = (cudaStream_t)stream;
+    (void)cudaGetLastError();  // clear an error left by earlier, unrelated work
     apply_prep_center_kernel<<<dp, 256, 0, s>>>(a);
     const int64_t tot = (int64_t)dp * a.c_pad;
     apply_prep_b_kernel<<<(unsigned)std::min<int64_t>((tot + 255) / 256, 4096), 256, 0, s>>>(
         a, dp);
-    if (cudaGetLastError() != cudaSuccess) return OTTB_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) {
+      delete h;
+      return OTTB_ERR_CUDA;
+    }
     a.prepared = 1;
   }
-  ottb_apply_product* h = new (std::nothrow) ottb_apply_product;
-  if (!h) return OTTB_ERR_INVALID;
   h->a = a;
   *product = h;
   return OTTB_OK;

@@ -503,6 +503,16 @@ class _TransportMatrix(torch.autograd.Function):
             _cast(gg, g, need[3]), None)
 
 
+def _keep_until_done(*tensors: torch.Tensor) -> None:
+  """Marks tensors as in use on the current stream, so the caching allocator
+  does not hand their memory to another stream's work before the product
+  queued here has run (a product may run on a stream other than the one its
+  plan was made on)."""
+  st = torch.cuda.current_stream(tensors[0].device)
+  for t in tensors:
+    t.record_stream(st)
+
+
 class _SweepProduct:
   """One planned ``ottb_apply_transport_sweep`` product (the plan applied to
   vectors through zero-iteration solves on the solver's sweep engine). It
@@ -542,6 +552,7 @@ class _SweepProduct:
     out = torch.empty((self._num_vec, self._rows_out), dtype=torch.float32,
                       device=self._ws.device)
     pot = self._f if self._axis == 0 else self._g
+    _keep_until_done(self._ws, self._f, self._g)
     st = self._lib.ottb_apply_transport_sweep_run(self._handle, pot.data_ptr(), v2.data_ptr(),
                                                   out.data_ptr(), _arrays.stream_handle())
     _lib.check(st, "ottb_apply_transport_sweep_run")
@@ -587,6 +598,7 @@ class _ApplyProduct:
                        f"{(self._num_vec, self._rows_in)}")
     out = torch.empty((self._num_vec, self._rows_out), dtype=torch.float32,
                       device=self._ws.device)
+    _keep_until_done(self._ws, self._f, self._g)
     st = self._lib.ottb_apply_transport_run(self._handle, v2.data_ptr(), out.data_ptr(),
                                             _arrays.stream_handle())
     _lib.check(st, "ottb_apply_transport_run")

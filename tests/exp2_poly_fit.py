@@ -3,7 +3,7 @@ in engine_tc.cuh, minimising the maximum RELATIVE error (Remez exchange on
 the weighted error (p - 2^f) / 2^f), then rounds the coefficients to float32
 and reports the error of the float32 evaluation.
 
-    python ott_b200/csrc/exp2_poly_fit.py [degree]
+    python tests/exp2_poly_fit.py [degree]
 """
 import sys
 

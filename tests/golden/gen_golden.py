@@ -5,8 +5,9 @@ on ``ott.geometry.pointcloud.PointCloud``, then ``SinkhornOutput.apply`` on
 seeded vectors) over the NumPy stand-in for jax
 (``oracle/jaxshim.py``, loaded by ``oracle/reference_loader.py``), in float64
 (``jax_enable_x64`` semantics) and in float32, on seeded inputs from
-``tests/problems.py``. Needs the reference source tree (default
-/root/reference/src); the GPU machine only reads the committed ``*.npz``.
+``tests/problems.py``. Needs the reference source tree (the argument, else
+$OTT_REFERENCE_SRC, else ``reference/src`` beside this repository); the GPU
+machine only reads the committed ``*.npz``.
 
     python tests/golden/gen_golden.py [reference_src_root]
 """

@@ -28,6 +28,19 @@ def load(name, tag="f64"):
   return data, geom, dict(meta["solver"]), meta["init"]
 
 
+def oracle_run(data, geom, solver, init, n_iters):
+  """The float64 oracle on a case's inputs and arguments, run for exactly
+  n_iters iterations (threshold 0): the state a solve that stopped after
+  n_iters iterations should hold."""
+  from oracle import sinkhorn_np as oracle
+  kw = dict(geom)
+  kw.update(solver)
+  kw.update(threshold=0.0, max_iterations=n_iters)
+  if init == "restart":
+    kw["init"] = (data["f_init"], data["g_init"])
+  return oracle.solve(data["x"], data["y"], data["a"], data["b"], dtype=np.float64, **kw)
+
+
 def divergence_names():
   with open(os.path.join(HERE, "divergence_manifest.json")) as fh:
     return sorted(json.load(fh))

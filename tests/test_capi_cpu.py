@@ -31,9 +31,11 @@ def test_library_exports_every_declared_symbol():
 def test_status_strings_and_version():
   lib = _lib.load()
   assert lib.ottb_version().decode().count(".") == 2
-  for st in range(7):
-    assert lib.ottb_status_string(st)
+  for st in range(8):
+    assert lib.ottb_status_string(st) != b"unknown status"
+  assert lib.ottb_status_string(8) == b"unknown status"
   assert _lib.status_string(_lib.OTTB_ERR_TIMEOUT) == "device wait timed out"
+  assert _lib.status_string(_lib.OTTB_ERR_HOST_MEMORY) == "host memory allocation failed"
 
 
 def test_struct_layouts_match_header():

@@ -7,15 +7,15 @@ import warnings
 import numpy as np
 import pytest
 
+from oracle import reference_loader
 from tests import golden_cases
 
-ROOT = "/root/reference/src"
+ROOT = reference_loader.DEFAULT_ROOT
 
 
 @pytest.mark.skipif(not os.path.isdir(os.path.join(ROOT, "ott")),
                     reason="reference source tree not present")
 def test_golden_vectors_regenerate_from_reference():
-  from oracle import reference_loader
   warnings.filterwarnings("ignore")
   ref = reference_loader.load(ROOT, x64=True)
   data, _, _, _ = golden_cases.load("refprob_eps0.1", "f64")

@@ -148,3 +148,45 @@ def test_noalloc_refuses_problems_beyond_its_scratch():
                                             torch.cuda.current_stream().cuda_stream)
   assert st == L.OTTB_ERR_WORKSPACE
   torch.cuda.synchronize()
+
+
+def test_noalloc_calls_leave_free_device_memory_unchanged():
+  """The entry point's own claim: after one call (the address look-up and
+  module load), further calls change neither the device's free memory
+  (cudaMemGetInfo) nor torch's allocated bytes. Every buffer the calls use
+  is made before the first reading."""
+  import torch
+  L, lib = _lib()
+  x, y, a, b = problems.uniform_cloud_problem(3000, 2500, 3, seed=11)
+  p = _inputs(torch, [(x, y, a, b, 0.02)])[0]
+  n, m = x.shape[0], y.shape[0]
+  f = torch.empty(n, device="cuda")
+  g = torch.empty(m, device="cuda")
+  e = torch.empty(200, device="cuda")
+  arr = (L.OttbProblem * 1)()
+  q = arr[0]
+  q.x, q.y, q.a, q.b = p["x"].data_ptr(), p["y"].data_ptr(), p["a"].data_ptr(), p["b"].data_ptr()
+  q.f_init = q.g_init = None
+  q.f, q.g, q.errors = f.data_ptr(), g.data_ptr(), e.data_ptr()
+  q.n, q.m, q.epsilon, q.inv_scale_cost = n, m, 0.02, 1.0
+  cfg = _cfg(L)
+  res = torch.zeros(L.RESULT_BYTES, dtype=torch.uint8, device="cuda")
+  stream = torch.cuda.current_stream().cuda_stream
+
+  def call():
+    st = lib.ottb_sinkhorn_pointcloud_noalloc(arr, 1, 3, ctypes.byref(cfg), res.data_ptr(),
+                                              stream)
+    assert st == L.OTTB_OK, L.status_string(st)
+
+  call()
+  torch.cuda.synchronize()
+  free0, _ = torch.cuda.mem_get_info()
+  alloc0 = torch.cuda.memory_allocated()
+  call()
+  call()
+  torch.cuda.synchronize()
+  free1, _ = torch.cuda.mem_get_info()
+  assert free1 == free0, (free0, free1)
+  assert torch.cuda.memory_allocated() == alloc0
+  r = L.OttbResult.from_buffer_copy(res.cpu().numpy().tobytes()[:L.RESULT_BYTES])
+  assert r.status == 0 and r.n_iters > 0
