@@ -121,7 +121,7 @@ __global__ void init_potentials_kernel(InitArgs args) {
   const ProbDev& P = args.probs[p];
   const float* fi = args.init[2 * p];
   const float* gi = args.init[2 * p + 1];
-  const float wsh = 0.5f / P.inv_scale;
+  const float wsh = P.ws_t;
   // f over n_pad, then g over both g buffers' m_pad rows (padding rows get
   // the -inf column shift of the tensor-core path)
   const int64_t tot = P.n_pad + 2 * P.m_pad;
@@ -332,7 +332,9 @@ namespace ottb {
 
 // Tensor-core layout: centred points split into bf16 pairs, hi rows then lo
 // rows, [2][pad][dk] (zero padded in both dimensions), and scaled squared
-// norms of the centred FP32 points. blockIdx.y = problem, blockIdx.z = side.
+// norms of the centred FP32 points. The x side is multiplied by the exponent
+// scale s = 2 inv log2(e) / eps_target before the split, so the products
+// <x', y> come out in log2 units. blockIdx.y = problem, blockIdx.z = side.
 __global__ void prep_points_tc_kernel(PrepArgs args) {
   __shared__ float center[128];
   const int p = blockIdx.y;
@@ -344,6 +346,7 @@ __global__ void prep_points_tc_kernel(PrepArgs args) {
   __nv_bfloat16* dst = (__nv_bfloat16*)(side ? P.yh : P.xh);
   float* nrm = const_cast<float*>(side ? P.ny : P.nx);
   const int d = args.d, dk = args.dp;
+  const float scale = side ? 1.0f : 2.0f * P.inv_scale * P.ws_t;
   for (int k = threadIdx.x; k < d; k += blockDim.x) center[k] = P.center[k];
   __syncthreads();
   // one warp per row: lanes over the coordinates, so the bf16 stores of a
@@ -359,9 +362,10 @@ __global__ void prep_points_tc_kernel(PrepArgs args) {
     for (int k = lane; k < dk; k += 32) {
       const float v = (i < cnt && k < d) ? row[k] - center[k] : 0.f;
       s += (double)v * (double)v;
-      const __nv_bfloat16 h = __float2bfloat16_rn(v);
+      const float vs = v * scale;
+      const __nv_bfloat16 h = __float2bfloat16_rn(vs);
       hi[k] = h;
-      lo[k] = __float2bfloat16_rn(v - __bfloat162float(h));
+      lo[k] = __float2bfloat16_rn(vs - __bfloat162float(h));
     }
     for (int off = 16; off > 0; off >>= 1) s += __shfl_xor_sync(0xffffffffu, s, off);
     if (lane == 0) nrm[i] = (float)((double)P.inv_scale * s);

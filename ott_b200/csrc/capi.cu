@@ -221,7 +221,7 @@ struct ProbPlan {
   int64_t n, m, n_pad, m_pad;
   int rb_f, rb_g, split_f, split_g, smax_f, smax_g;
   size_t off_xt, off_yt, off_nx, off_ny, off_galt, off_pm, off_pl, off_arr, off_err,
-      off_msum, off_extx, off_exty, off_cen;
+      off_msum, off_extx, off_exty, off_cen, off_lprev;
 };
 
 // BF16 split-3 on tcgen05 when asked for, and by default where the inner
@@ -402,6 +402,8 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.off_extx = off; off = align_up(off + (plan.tc ? 16 * pp.n_pad : 0));
     pp.off_exty = off; off = align_up(off + (plan.tc ? 16 * 2 * pp.m_pad : 0));
     pp.off_cen = off; off = align_up(off + fsz * 128);
+    // tensor-core path: the rows' log-sum-exps of their last sweep
+    pp.off_lprev = off; off = align_up(off + (plan.tc ? fsz * (pp.n_pad + pp.m_pad) : 0));
   }
   plan.off_pristine = off; off = align_up(off + plan.header_bytes);
   plan.total = off;
@@ -462,6 +464,8 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
         return OTTB_ERR_CUDA;
       P.extx = ws + pp.off_extx;
       P.exty = ws + pp.off_exty;
+      P.lprev = (float*)(ws + pp.off_lprev);
+      P.dkey = &((ProbState*)(ws + plan.off_state))[t].dkey[0][0][0];
       std::memcpy(host.data() + plan.off_maps + sizeof(TcMaps) * t, &maps, sizeof(TcMaps));
       P.maps = ws + plan.off_maps + sizeof(TcMaps) * t;
     } else {
@@ -486,6 +490,8 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     P.smax_g = pp.smax_g;
     P.eps_target = q.epsilon;
     P.inv_scale = q.inv_scale_cost;
+    // sweep_wscale at multiplier 1, the same FP32 value the kernels derive
+    P.ws_t = (float)(kLog2eD / ((double)q.epsilon * 1.0));
     P.uid = plan.order[t];
     P.outer = outer;
     P.symmetric = q.symmetric;
@@ -493,6 +499,11 @@ int write_header(const ottb_problem* problems, int num_problems, const ottb_solv
     P.lse_out = lse_out ? lse_out[plan.order[t]] : nullptr;
     pd[t] = P;
     ps[t].active = 1;
+    for (int k = 0; k < 2; ++k)
+      for (int sl = 0; sl < 2; ++sl) {
+        ps[t].dkey[k][sl][0] = kDkeyEmptyMax;
+        ps[t].dkey[k][sl][1] = kDkeyEmptyMin;
+      }
     ps[t].split_f = pp.split_f;
     ps[t].split_g = pp.split_g;
     ids[t] = t;

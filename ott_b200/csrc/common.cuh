@@ -71,6 +71,12 @@ struct ProbDev {
   float* lse_out;      // [m] eps log sum_i exp((f_i + g_j - C_ij) / eps) - g_j of
                        // that sweep (apply_lse_kernel), or null
   float* center;       // [128] workspace: the common centre of the two point sets
+  // tensor-core path: base-2 log-sum-exp of every row in its last sweep
+  // ([n_pad] x rows from f-sweeps, then [m_pad] y rows from g-sweeps), and
+  // this problem's ProbState::dkey (bounds of the column shifts' changes)
+  float* lprev;
+  int* dkey;
+  float ws_t;          // log2(e) / eps_target in FP32 (sweep_wscale at multiplier 1)
 };
 
 // Operands of one sweep for one problem, resolved from the descriptor.
@@ -92,6 +98,11 @@ struct ProbState {
   int split_f;       // column split of this problem's f- and g-sweeps (set
   int split_g;       // by the host, grown at schedule rebuilds)
   double msum;
+  // Tensor-core path: order-preserving integer keys (fkey) of the largest
+  // and smallest change of the column shifts w_c seen by the next sweep of
+  // each kind, [consumer kind][slot][0 = max, 1 = min]; slot = parity of
+  // the consumer's sweep count. Empty: kDkeyEmptyMax / kDkeyEmptyMin.
+  int dkey[2][2][2];
 };
 
 // Work schedule of the current sweep, rebuilt by CTA 0 at block boundaries.
@@ -178,23 +189,57 @@ __device__ __forceinline__ f32x2 add2(f32x2 a, f32x2 b) {
   return r;
 }
 
+__device__ __forceinline__ f32x2 sub2(f32x2 a, f32x2 b) {
+  f32x2 r;
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
 // exp2_poly on a pair, the range reduction and the polynomial in packed
 // arithmetic (same operations, same results as two exp2_poly calls).
 __device__ __forceinline__ f32x2 exp2_poly2(f32x2 xp) {
   float x0, x1;
   unpack2(xp, x0, x1);
   const f32x2 x = pack2(fmaxf(x0, -126.0f), fmaxf(x1, -126.0f));
-  const f32x2 t = add2(x, pack2(kRoundShift, kRoundShift));
-  const f32x2 u = add2(t, pack2(-kRoundShift, -kRoundShift));
-  float u0, u1;
-  unpack2(u, u0, u1);
-  const f32x2 f = add2(x, pack2(-u0, -u1));
+  const f32x2 sh = pack2(kRoundShift, kRoundShift);
+  const f32x2 t = add2(x, sh);
+  const f32x2 f = sub2(x, sub2(t, sh));
   f32x2 p = pack2(kExp2C5, kExp2C5);
   p = fma2(p, f, pack2(kExp2C4, kExp2C4));
   p = fma2(p, f, pack2(kExp2C3, kExp2C3));
   p = fma2(p, f, pack2(kExp2C2, kExp2C2));
   p = fma2(p, f, pack2(kExp2C1, kExp2C1));
   p = fma2(p, f, pack2(kExp2C0, kExp2C0));
+  float p0, p1, t0, t1;
+  unpack2(p, p0, p1);
+  unpack2(t, t0, t1);
+  return pack2(__int_as_float(__float_as_int(p0) + (__float_as_int(t0) << 23)),
+               __int_as_float(__float_as_int(p1) + (__float_as_int(t1) << 23)));
+}
+
+// Degree-4 polynomial 2^f on [-1/2, 1/2] (tests/exp2_poly_fit.py 4: 2.6e-6
+// minimax relative error, 2.7e-6 evaluated in FP32), for the tensor-core
+// epilogue, whose products carry ~1e-5 relative error already (BF16
+// split-3 inner products scaled to exponents of tens).
+constexpr float kExp2D4C4 = 9.570102207e-03f;
+constexpr float kExp2D4C3 = 5.591785908e-02f;
+constexpr float kExp2D4C2 = 2.402474433e-01f;
+constexpr float kExp2D4C1 = 6.931217909e-01f;
+constexpr float kExp2D4C0 = 9.999992847e-01f;
+
+// exp2_poly2 with the degree-4 polynomial: one packed FMA fewer per pair.
+__device__ __forceinline__ f32x2 exp2_poly2_d4(f32x2 xp) {
+  float x0, x1;
+  unpack2(xp, x0, x1);
+  const f32x2 x = pack2(fmaxf(x0, -126.0f), fmaxf(x1, -126.0f));
+  const f32x2 sh = pack2(kRoundShift, kRoundShift);
+  const f32x2 t = add2(x, sh);
+  const f32x2 f = sub2(x, sub2(t, sh));
+  f32x2 p = pack2(kExp2D4C4, kExp2D4C4);
+  p = fma2(p, f, pack2(kExp2D4C3, kExp2D4C3));
+  p = fma2(p, f, pack2(kExp2D4C2, kExp2D4C2));
+  p = fma2(p, f, pack2(kExp2D4C1, kExp2D4C1));
+  p = fma2(p, f, pack2(kExp2D4C0, kExp2D4C0));
   float p0, p1, t0, t1;
   unpack2(p, p0, p1);
   unpack2(t, t0, t1);
@@ -215,6 +260,18 @@ __device__ __forceinline__ f32x2 exp2_poly2(f32x2 xp) {
 #ifndef OTTB_POLY_OF_8_TC
 #define OTTB_POLY_OF_8_TC 2
 #endif
+
+// Order-preserving map of non-NaN floats to ints (and back), for atomic
+// maxima and minima of floats of either sign.
+__host__ __device__ __forceinline__ int fkey_bits(int i) { return i >= 0 ? i : i ^ 0x7fffffff; }
+__device__ __forceinline__ int fkey(float f) { return fkey_bits(__float_as_int(f)); }
+__device__ __forceinline__ float fkey_value(int k) { return __int_as_float(fkey_bits(k)); }
+constexpr int kDkeyEmptyMax = (int)0x807fffff;  // fkey(-inf)
+constexpr int kDkeyEmptyMin = 0x7f800000;        // fkey(+inf)
+// Largest spread (log2 units) of the column shifts' changes for which a
+// sweep uses the bounded shift instead of running maxima: the row sums then
+// stay within [2^-kMaxShiftSpread, m] (see tc_unit).
+constexpr float kMaxShiftSpread = 60.0f;
 
 // Three-input maximum (sm_100 max.f32 with three sources; NaN operands are
 // ignored as by fmaxf).
@@ -239,10 +296,12 @@ __device__ __forceinline__ void two_sum_acc(float& s, float& c, float x) {
   c += err;
 }
 
-// One 16-byte column-shift row of the tensor-core path: w' = (pot - inv
-// |p|^2) / (2 inv) as three bf16 terms w1 + w2 + w3 (~24 bits) followed by
-// five zeros. A non-finite w' (zero-weight potentials, padding rows = -inf)
-// is carried by w1 alone, so no inf - inf = NaN appears.
+// One 16-byte column-shift row of the tensor-core path: the base-2 column
+// shift w = (pot - inv |p|^2) log2(e) / eps_target as three bf16 terms
+// w1 + w2 + w3 (~24 bits), then two ones (the factors of the row shift the
+// A operand's extension block may carry) and three zeros. A non-finite w
+// (zero-weight potentials, padding rows = -inf) is carried by w1 alone, so
+// no inf - inf = NaN appears.
 __device__ __forceinline__ void write_ext_row(void* row16, float w) {
   const bool fin = isfinite(w);
   const __nv_bfloat16 w1 = __float2bfloat16_rn(w);
@@ -250,9 +309,10 @@ __device__ __forceinline__ void write_ext_row(void* row16, float w) {
   const __nv_bfloat16 w2 = __float2bfloat16_rn(r1);
   const __nv_bfloat16 w3 = __float2bfloat16_rn(fin ? r1 - __bfloat162float(w2) : 0.f);
   uint4 v;
+  const uint32_t one = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(1.f));
   v.x = (uint32_t)__bfloat16_as_ushort(w1) | ((uint32_t)__bfloat16_as_ushort(w2) << 16);
-  v.y = (uint32_t)__bfloat16_as_ushort(w3);
-  v.z = 0u;
+  v.y = (uint32_t)__bfloat16_as_ushort(w3) | (one << 16);
+  v.z = one;
   v.w = 0u;
   *reinterpret_cast<uint4*>(row16) = v;
 }

@@ -38,6 +38,13 @@ struct SweepParams {
   int write;     // write the new potential
   int final_eval;  // use the eval list and each problem's final parity
   int parity;    // g parity of active problems
+  // tensor-core path: the rows' shifts may be bounded from their last sweep
+  // (set by persistent_main: multiplier 1 now and then, not the final
+  // evaluation); dkey slot this sweep reads, and slot of the other kind's
+  // next sweep its potential changes go to
+  int fast;
+  int rslot;
+  int wslot;
 };
 
 __device__ __forceinline__ float eps_mult(const ottb_solver_cfg& c, int it) {
@@ -100,6 +107,9 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
   const float ws = sweep_wscale(P, sp.mult);
   const double eps = kLog2eD / (double)ws;
   double err_t = 0.0, msum_t = 0.0;
+  // change of this row's potential, as the change of its column shift in the
+  // other kind's next sweep (log2 units), for the bound that sweep uses
+  float dmax = -INFINITY, dmin = INFINITY;
   const int64_t r = (int64_t)rb * kBM + t;
   if (t < kBM && r < R) {
     const float mv = rm[t], lv = rl[t];
@@ -115,6 +125,7 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
     // symmetric problem: Momentum(value=0.5) on the parallel update,
     // (1 - w) * where(isfinite(old), old, 0) + w * new (acceleration.py:168-170)
     if (P.symmetric) newp = 0.5 * (isfinite(old) ? old : 0.0) + 0.5 * newp;
+    if (P.lprev) P.lprev[(isG ? P.n_pad : 0) + r] = (float)lse2;
     if (sp.write) {
       const float nf = (float)newp;
       outp[r] = nf;
@@ -122,7 +133,16 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       void* ext = isG ? P.exty : P.extx;
       if (ext) {
         const int64_t row = isG ? (int64_t)(parity ^ 1) * P.m_pad + r : r;
-        write_ext_row((char*)ext + row * 16, (nf - na[r]) * (0.5f / P.inv_scale));
+        write_ext_row((char*)ext + row * 16, (nf - na[r]) * P.ws_t);
+      }
+      if (isfinite(nf) && isfinite(old)) {
+        const float dl = (nf - (float)old) * P.ws_t;
+        dmax = dl;
+        dmin = dl;
+      } else if (isfinite(nf) != isfinite(old)) {
+        // a potential became or stopped being -inf: no bound
+        dmax = INFINITY;
+        dmin = -INFINITY;
       }
     }
     if (sp.eval) {
@@ -134,6 +154,27 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       if (sp.final_eval && P.marg_out) P.marg_out[r] = (float)bh;
       if (sp.final_eval && P.lse_out) P.lse_out[r] = (float)app;  // eps LSE_i - |y_j|^2 term
     }
+  }
+  if (sp.write && P.dkey && !P.symmetric) {
+    // the row block's extremes, then one atomic each into the other kind's slot
+    for (int off = 16; off > 0; off >>= 1) {
+      dmax = fmaxf(dmax, __shfl_xor_sync(0xffffffffu, dmax, off));
+      dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
+    }
+    float* fr = reinterpret_cast<float*>(red);
+    if (t < kBM && (t & 31) == 0) {
+      fr[t >> 5] = dmax;
+      fr[4 + (t >> 5)] = dmin;
+    }
+    __syncthreads();
+    if (t == 0) {
+      const float mx = fmaxf(fmaxf(fr[0], fr[1]), fmaxf(fr[2], fr[3]));
+      const float mn = fminf(fminf(fr[4], fr[5]), fminf(fr[6], fr[7]));
+      int* slot = P.dkey + (((isG ? kSweepF : kSweepG) * 2 + sp.wslot) * 2);
+      if (mx > -INFINITY) atomicMax(slot, fkey(mx));
+      if (mn < INFINITY) atomicMin(slot + 1, fkey(mn));
+    }
+    __syncthreads();
   }
   if (sp.eval) {
     double e = block_sum_128(err_t, red);

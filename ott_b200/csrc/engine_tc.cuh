@@ -3,32 +3,44 @@
 // log-sum-exp as the CUDA-core engine.
 //
 // Points are stored as bf16 pairs v = hi + lo (hi = bf16(v), lo =
-// bf16(v - hi)), rows of DK (64 or 128) elements, hi rows then lo rows. A
-// tile is 128 rows of A by 256 columns of B: the three products hi*hi +
-// hi*lo + lo*hi accumulate into one TMEM tile (3 * DK / 16 MMAs of M = 128,
-// N = 256, K = 16); lo*lo (~2^-16 relative) is dropped. N = 256 because an
-// N = 128 MMA takes ~84 cycles on B200 where an N = 256 one takes 128 (the
-// full rate; measured with back-to-back MMAs, A in shared or tensor memory
-// alike). One more K = 16 MMA adds the column shift: A's extension block
-// holds ones in its first 3 K columns, B's holds
-// w'_c = (pot_c - inv |B_c|^2) / (2 inv) as 3 bf16 terms (~24 bits), so the
-// accumulator is acc = <a_r, b_c> + w'_c and the exponent is s * acc,
-// s = 2 inv log2(e) / eps. The epilogue needs no per-column data, and w' is
-// computed once per point per sweep: every potential update writes its
-// point's row of the global extension array (write_ext_row), which the
-// producer loads by TMA with the B tile.
+// bf16(v - hi)), rows of DK (64 or 128) elements, hi rows then lo rows; the
+// x points carry the exponent scale s = 2 inv log2(e) / eps_target (x' =
+// s x before the split), so <x', y> is already in log2 units. A tile is 128
+// rows of A by 256 columns of B: the three products hi*hi + hi*lo + lo*hi
+// accumulate into one TMEM tile (3 * DK / 16 MMAs of M = 128, N = 256,
+// K = 16); lo*lo (~2^-16 relative) is dropped. N = 256 because an N = 128
+// MMA takes ~84 cycles on B200 where an N = 256 one takes 128 (the full
+// rate; measured with back-to-back MMAs, A in shared or tensor memory
+// alike). One more K = 16 MMA adds the shifts: B's extension rows hold the
+// column shift w_c = (pot_c - inv |B_c|^2) log2(e) / eps_target as 3 bf16
+// terms (~24 bits) and two ones, A's hold three ones and -sigma_r as two
+// bf16 terms, so acc = s <a_r, b_c> + w_c - sigma_r, the base-2 exponent of
+// the entry less a row shift. w is computed once per point per sweep: every
+// potential update writes its point's row of the global extension array
+// (write_ext_row), which the producer loads by TMA with the B tile.
+//
+// Row shifts. A row's log-sum-exp changes between two sweeps of its kind by
+// at most D = max_c (change of w_c) (each term moves by its column's change),
+// and by at least the smallest change. So when the last sweep of the kind
+// ran at the same epsilon and its row log-sum-exps L_r are stored, sigma_r =
+// L_r + D bounds every exponent of the row from above (terms <= 1, sums
+// <= m), and while the spread of the changes is at most kMaxShiftSpread the
+// row sum stays >= 2^-kMaxShiftSpread: the epilogue needs no maxima and no
+// rescaling, only 2^acc and the sums. Otherwise (first sweeps, epsilon
+// decay, large moves) sigma_r = 0 and the epilogue keeps running maxima.
 //
 // Warp roles in the 576-thread CTA:
-//   warp 0      producer (lane 0): A tile once per unit; B tiles, one 64-wide
-//               K chunk (hi and lo) per shared-memory stage, and their
-//               column-shift rows with the last chunk, through a ring of
-//               kStages stages (TMA, no multicast).
+//   warp 0      producer: the row shifts of a unit into A's extension block
+//               (all lanes), then (lane 0) the A tile once per unit; B tiles,
+//               one 64-wide K chunk (hi and lo) per shared-memory stage, and
+//               their column-shift rows with the last chunk, through a ring
+//               of kStages stages (TMA, no multicast).
 //   warp 1      TMEM owner and MMA issuer (lane 0): two 256-column
 //               accumulators (all of TMEM), so MMAs of tile t+1 overlap the
 //               epilogue of t.
 //   warps 2-17  epilogue: warp w reads TMEM lanes 32*(w%4).. (its rows) and
 //               the 64-column group (w-2)/4 of each tile and keeps a running
-//               (max, sum) of 2^(s * acc) per row.
+//               (shift, sum) of 2^acc per row.
 // Every wait is bounded; a timeout marks the CTA and unwinds.
 #pragma once
 
@@ -175,6 +187,37 @@ __device__ __forceinline__ void tc_issue_ext(uint32_t d_tmem, const uint8_t* Aex
   tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, 1);
 }
 
+// The bounded row shift of one problem's units in a sweep (see the file
+// comment); on = false: sigma = 0 and running maxima.
+struct RowShift {
+  const float* lprev;  // the rows' log-sum-exps from their last sweep
+  float dmax;          // D
+  int64_t rows;        // rows of A (padding rows get sigma = 0)
+  bool on;
+};
+
+// sigma_r = L_r + D as two bf16 terms (sigma = p1 + p2 exactly in FP32), 0
+// for padding rows, rows whose L_r is not finite, or without a bound.
+__device__ __forceinline__ float row_shift(const RowShift& rs, int64_t row,
+                                           __nv_bfloat16& p1, __nv_bfloat16& p2) {
+  float sg = 0.f;
+  if (rs.on && row < rs.rows) {
+    const float lp = __ldcg(rs.lprev + row);
+    if (isfinite(lp)) sg = lp + rs.dmax;
+  }
+  p1 = __float2bfloat16_rn(sg);
+  p2 = __float2bfloat16_rn(sg - __bfloat162float(p1));
+  return __bfloat162float(p1) + __bfloat162float(p2);
+}
+
+// Of every 8 exponentials of a bounded-shift chunk, this many (even) go to
+// exp2_poly2_d4 (FMA pipe), the rest to ex2.approx (MUFU); measured in an
+// epilogue-only kernel, 4 of 8 (2019 cycles per tile) is slower than 2
+// (1841): the polynomial's issue slots then bind.
+#ifndef OTTB_POLY_OF_8_TC_FAST
+#define OTTB_POLY_OF_8_TC_FAST 2
+#endif
+
 // Operands of one tensor-core sweep for one problem.
 struct TcOperands {
   const CUtensorMap* mapA;
@@ -186,15 +229,16 @@ struct TcOperands {
 };
 
 // One work unit: rows row0..row0+127 of A against B tiles [t0, t1) of 256
-// columns. Leaves the per-row base-2 LSE state in sm.rm / sm.rl. Returns
-// false if a wait timed out.
+// columns. Leaves the per-row base-2 LSE state in sm.rm / sm.rl. r scales
+// the accumulator to the sweep's epsilon (1 at the target epsilon); rs is
+// the unit's row shift. Returns false if a wait timed out.
 //
 // Per ring stage st the producer fills one K chunk of B's hi/lo tiles (and,
 // with the last chunk, the first K half of B's extension block) by TMA;
 // full[st] completes on those bytes, empty[st] on the MMA commit.
 template <int DK>
 __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
-                        int t0, int t1, float s, uint64_t timeout_ns) {
+                        int t0, int t1, float s, const RowShift& rs, uint64_t timeout_ns) {
   constexpr int NS = TcCfg<DK>::kStages;
   constexpr int NB = TcCfg<DK>::kTmemBufs;
   constexpr int C = TcCfg<DK>::kChunks;
@@ -207,9 +251,22 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
   bool ok = true;
 
   if (warp == 0) {
+    // A tile and its extension block: wait until the previous unit's MMAs
+    // released them, then write the rows' -sigma terms (K columns 3, 4).
+    const bool freed = tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns);
+    if (freed) {
+      for (int i = lane; i < kBM; i += 32) {
+        __nv_bfloat16 p1, p2;
+        row_shift(rs, (int64_t)row0 + i, p1, p2);
+        __nv_bfloat16* e = reinterpret_cast<__nv_bfloat16*>(sm.Aext + i * 16);
+        e[3] = __hneg(p1);
+        e[4] = __hneg(p2);
+      }
+      tc::fence_proxy_async_smem();
+    }
+    __syncwarp();
     if (lane == 0) {
-      // A tile: wait until the previous unit's MMAs released it.
-      if (!tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns)) ok = false;
+      if (!freed) ok = false;
       if (ok) {
         tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK>::kABytes);
         tc_load_a<DK>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
@@ -267,6 +324,9 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
     const int cg = e >> 2;
     const int r = 32 * q + lane;
     float mrun = kNegSentinel, lrun = 0.f, lcmp = 0.f;
+    __nv_bfloat16 p1, p2;
+    const float sigma = row_shift(rs, (int64_t)row0 + r, p1, p2);
+    const bool fast = rs.on;
     for (int i = 0; ok && i < ntiles; ++i) {
       const uint32_t g = pp.tile + i;
       const uint32_t b = g % NB;
@@ -275,6 +335,56 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
         break;
       }
       tc::fence_after_sync();
+      if (fast) {
+        // acc is the exponent less sigma_r: every term <= 1, no maxima.
+        // 16-column loads, the next issued before the current one is
+        // reduced; scalar sums into 8 accumulators; the polynomial pairs in
+        // packed arithmetic. Measured per 128 x 256 tile in the solve at
+        // n = m = 65536: 1808 cycles (2026 with two 32-column loads per
+        // tile and packed sums, 2059 before that).
+        const uint32_t tb = sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg;
+        float acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+        auto reduce16 = [&](const float (&v)[16]) {
+#pragma unroll
+          for (int j = 0; j < 16; j += 8) {
+#pragma unroll
+            for (int k = 0; k < 8; k += 2) {
+              if (k >= 8 - OTTB_POLY_OF_8_TC_FAST) {
+                float e0, e1;
+                unpack2(exp2_poly2_d4(pack2(v[j + k], v[j + k + 1])), e0, e1);
+                acc[k] += e0;
+                acc[k + 1] += e1;
+              } else {
+                acc[k] += ex2_approx(v[j + k]);
+                acc[k + 1] += ex2_approx(v[j + k + 1]);
+              }
+            }
+          }
+        };
+        static_assert(CW == 64, "four 16-column loads per warp and tile");
+        float va[16], vb[16];
+        tc::tmem_ld16(tb, va);
+        tc::tmem_ld_wait();
+        tc::tmem_ld16(tb + 16, vb);
+        reduce16(va);
+        tc::tmem_ld_wait();
+        tc::tmem_ld16(tb + 32, va);
+        reduce16(vb);
+        tc::tmem_ld_wait();
+        tc::tmem_ld16(tb + 48, vb);
+        reduce16(va);
+        tc::tmem_ld_wait();
+        // The accumulator buffer can be refilled once every warp has read it.
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
+        reduce16(vb);
+        two_sum_acc(lrun, lcmp,
+                    ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+        continue;
+      }
 #pragma unroll 1
       for (int h = 0; h < CW / 32; ++h) {
         float v[32];
@@ -331,7 +441,7 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
         two_sum_acc(lrun, lcmp, ta + tb);
       }
     }
-    sm.part_m[cg][r] = mrun;
+    sm.part_m[cg][r] = fast ? sigma : mrun;
     sm.part_l[cg][r] = lrun + lcmp;
   }
   pp.tile += ntiles;

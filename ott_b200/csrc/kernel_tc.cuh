@@ -27,6 +27,29 @@ __device__ __forceinline__ TcOperands make_tc_operands(const ProbDev& P, int kin
   return op;
 }
 
+// Whether this problem's units of the sweep use the bounded row shift, and
+// the bound: D = the largest change of a column shift since the rows' last
+// sweep (0 when no potential changed), usable while the spread of those
+// changes stays within kMaxShiftSpread.
+__device__ __forceinline__ RowShift bounded_row_shift(const ProbDev& P, const SweepParams& sp) {
+  RowShift rs{nullptr, 0.f, 0, false};
+  if (!sp.fast || P.symmetric || !P.lprev || !P.dkey) return rs;
+  const int* slot = P.dkey + ((sp.kind * 2 + sp.rslot) * 2);
+  const int kmax = __ldcg(slot), kmin = __ldcg(slot + 1);
+  float dmax = 0.f, spread = 0.f;
+  if (kmax != kDkeyEmptyMax) {
+    if (kmin == kDkeyEmptyMin) return rs;
+    dmax = fkey_value(kmax);
+    spread = dmax - fkey_value(kmin);
+  }
+  if (!(spread <= kMaxShiftSpread) || !isfinite(dmax)) return rs;
+  rs.lprev = P.lprev + (sp.kind == kSweepG ? P.n_pad : 0);
+  rs.dmax = dmax;
+  rs.rows = sp.kind == kSweepG ? P.m : P.n;
+  rs.on = true;
+  return rs;
+}
+
 template <int DK>
 __global__ void __launch_bounds__(TcCfg<DK>::kThreads, 1)
 sinkhorn_tc_kernel(KernelArgs A) {
@@ -86,7 +109,11 @@ sinkhorn_tc_kernel(KernelArgs A) {
     auto unit = [&](const ProbDev& P, const float* gcur, int parity, int rb, int t0, int t1,
                     float s, float wscale) -> bool {
       const TcOperands op = make_tc_operands(P, sp.kind, parity);
-      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, s, A.timeout_ns);
+      // The x layout carries the exponent scale of the target epsilon; a
+      // sweep at another epsilon scales the accumulator by ws / ws_t.
+      const float r = wscale / P.ws_t;
+      RowShift rs = bounded_row_shift(P, sp);
+      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, r, rs, A.timeout_ns);
     };
     return sweep_units<TcCfg<DK>::kTileN>(A, sp, idx, cs, unit);
   };

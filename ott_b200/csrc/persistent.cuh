@@ -278,9 +278,32 @@ __device__ void persistent_main(const KernelArgs& A, SweepFn&& sweep) {
   unsigned sweep_idx = 0;
   int it = 0;
   int commits = 0;  // committed g-sweeps; identical in every CTA
+  // Per sweep kind: sweeps begun, and whether the last one ran at
+  // multiplier 1 (its row log-sum-exps, stored by finalize_rows, then bound
+  // the next one's rows; see tc_unit).
+  int nsw[2] = {0, 0};
+  int prev_one[2] = {0, 0};
+  auto begin_sweep = [&](SweepParams& sp) {
+    const int K = sp.kind;
+    sp.rslot = nsw[K] & 1;
+    sp.wslot = nsw[K ^ 1] & 1;
+    sp.fast = (!sp.final_eval && sp.mult == 1.0f && prev_one[K]) ? 1 : 0;
+    // The slot the sweep after next of this kind reads is free now (its
+    // previous reader has finished, its writers come after this sweep).
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+      const int nxt = (nsw[K] + 1) & 1;
+      for (int p = 0; p < A.num_problems; ++p) {
+        A.state[p].dkey[K][nxt][0] = kDkeyEmptyMax;
+        A.state[p].dkey[K][nxt][1] = kDkeyEmptyMin;
+      }
+    }
+    prev_one[K] = (!sp.final_eval && sp.mult == 1.0f) ? 1 : 0;
+    ++nsw[K];
+  };
 
 #define OTTB_SWEEP(sp)                                                           \
   do {                                                                           \
+    begin_sweep(sp);                                                             \
     if (!sweep((sp), sweep_idx++)) {                                             \
       if (threadIdx.x == 0) atomicExch(status, (int)OTTB_ERR_TIMEOUT);           \
       grid_barrier(A.gl, A.expected_arrivals, A.timeout_ns, status);             \
