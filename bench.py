@@ -67,8 +67,8 @@ def parse_args():
   p.add_argument("--pairs", type=int, default=8)
   p.add_argument("--stages", type=int, default=10)
   args = p.parse_args()
-  default_n, default_d = {"uniform2048": (2048, 2), "anneal": (16384, 128)}.get(
-      args.workload, (65536, 64))
+  default_n, default_d = {"uniform2048": (2048, 2), "anneal": (16384, 128),
+                          "divergence": (32768, 64)}.get(args.workload, (65536, 64))
   args.n = default_n if args.n is None else args.n
   args.d = default_d if args.d is None else args.d
   return args
@@ -621,6 +621,14 @@ def run_warmstart(args):
   e1.synchronize()
   train_s = e0.elapsed_time(e1) * 1e-3
   meta.mlp.check_status()
+  dims = meta.mlp.dims
+  mlp_flops = 3.0 * 2.0 * 512 * sum(dims[i] * dims[i + 1] for i in range(len(dims) - 1)) \
+      * args.train_steps
+  mp = load_peaks_json()
+  bf16_sust = mp.get("bf16_tflops_sustained") if mp else None
+  bf16_src = ("MEASURED_PEAKS.json bf16_tflops_sustained" if bf16_sust else
+              "fallback: 1.4 PFLOP/s sustained, an earlier B200 measurement (file absent)")
+  bf16_sust = bf16_sust or 1400.0
   del G
 
   # 3. held-out: zero init vs warm start (with fallback), same chunks
@@ -696,7 +704,13 @@ def run_warmstart(args):
       "cost_rel_diff": {"max": float(rel.max()), "median": float(np.median(rel))},
       "training": {"target_solve_s": gen_s, "target_mean_iters": float(it_train.mean()),
                    "train_s": train_s, "loss_first": float(losses[:20].mean()),
-                   "loss_last": float(losses[-100:].mean())},
+                   "loss_last": float(losses[-100:].mean()),
+                   "mlp_train_tflops": mlp_flops / train_s / 1e12,
+                   "mlp_train_frac_of_bf16_sustained": (
+                       mlp_flops / train_s / 1e12 / bf16_sust if bf16_sust else None),
+                   "bf16_sustained_source": bf16_src,
+                   "mlp_flops": "3 x forward GEMM flops (forward, data and weight "
+                                "gradients) x batch 512 x steps"},
       "clocks": clk,
   }
   print(json.dumps(line))

@@ -9,8 +9,10 @@
 // One CTA per 128 x 128 tile of D (M, N multiples of 128, K of 64). Warp 0
 // issues TMA loads of 64-wide K slabs of A and B through a 4-stage ring, warp
 // 1 the MMAs (M = N = 128, K = 16) into one TMEM accumulator, warps 2-5 read
-// it back (warp w: TMEM lanes 32*(w%4)..) and run the epilogue. Waits are
-// bounded; on a timeout the CTA sets *err and returns after draining.
+// it back (warp w: TMEM lanes 32*(w%4)..) and run the epilogue, staging
+// their rows in shared memory so the row-major outputs leave as whole rows.
+// Waits are bounded; on a timeout the CTA sets *err and returns after
+// draining.
 #pragma once
 
 #include <cuda_bf16.h>
@@ -37,9 +39,16 @@ struct GemmArgs {
 constexpr int kGemmStages = 4;
 constexpr int kGemmSlabBytes = 128 * 64 * 2;  // one [128][64] bf16 slab, 128-byte swizzle
 
+// Epilogue staging, per epilogue warp (its 32 rows of the tile): an fp32
+// [32][129] tile or two bf16-pair [32][65] tiles (the odd strides keep a
+// warp's row-per-lane writes free of bank conflicts), written out as whole
+// rows so every global store of a warp is contiguous.
+constexpr int kEpiWords = 32 * 130;
+
 struct GemmSmem {
   uint8_t A[kGemmStages][kGemmSlabBytes];
   uint8_t B[kGemmStages][kGemmSlabBytes];
+  uint32_t epi[4][kEpiWords];
   uint64_t full[kGemmStages];
   uint64_t empty[kGemmStages];
   uint64_t done;
@@ -123,13 +132,30 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA,
     }
     __syncwarp();
   } else {
-    // epilogue: row r of the tile, 128 columns in 4 chunks of 32
+    // epilogue: row r of the tile (this warp's 32 rows, one per lane), 128
+    // columns in 4 chunks of 32 from TMEM into the warp's staging tile,
+    // then out by whole rows (the transposed outputs go straight out: a
+    // column of the tile is contiguous there)
     const int q = warp & 3;
     const int r = 32 * q + lane;
     const int row = m0 + r;
+    uint32_t* st = sm.epi[q];
+    float* sf = reinterpret_cast<float*>(st);           // fp32 [32][129]
+    uint32_t* s0 = st;                                   // bf16 pairs [32][65]
+    uint32_t* s1 = st + 32 * 65;                         // bf16 pairs [32][65]
     if (!tc::mbar_wait(&sm.done, 0, g.timeout_ns)) ok = false;
     if (ok) {
       tc::fence_after_sync();
+      if (g.epi == kEpiBackHid) {
+        // the layer below's pre-activations of these rows, read as whole rows
+        for (int i = 0; i < 32; ++i) {
+          const uint32_t* src =
+              reinterpret_cast<const uint32_t*>(g.zprev + (int64_t)(m0 + 32 * q + i) * g.N + n0);
+          s1[i * 65 + lane] = src[lane];
+          s1[i * 65 + 32 + lane] = src[32 + lane];
+        }
+        __syncwarp();
+      }
       for (int c0 = 0; c0 < 128; c0 += 32) {
         float v[32];
         tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + c0, v);
@@ -137,28 +163,58 @@ gemm_bf16_tc_kernel(const __grid_constant__ CUtensorMap mapA,
         const int col0 = n0 + c0;
         if (g.epi == kEpiHidden) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float z = v[j] + g.bias[col0 + j];
-            const __nv_bfloat16 zb = __float2bfloat16_rn(z);
-            const __nv_bfloat16 hb = __float2bfloat16_rn(gelu_tanh(__bfloat162float(zb)));
-            g.out_z[(int64_t)row * g.N + col0 + j] = zb;
-            g.out_h[(int64_t)row * g.N + col0 + j] = hb;
-            g.out_ht[(int64_t)(col0 + j) * g.M + row] = hb;
+          for (int j = 0; j < 32; j += 2) {
+            const float z0 = v[j] + g.bias[col0 + j];
+            const float z1 = v[j + 1] + g.bias[col0 + j + 1];
+            const __nv_bfloat16 zb0 = __float2bfloat16_rn(z0), zb1 = __float2bfloat16_rn(z1);
+            const __nv_bfloat16 hb0 = __float2bfloat16_rn(gelu_tanh(__bfloat162float(zb0)));
+            const __nv_bfloat16 hb1 = __float2bfloat16_rn(gelu_tanh(__bfloat162float(zb1)));
+            s0[lane * 65 + (c0 + j) / 2] =
+                (uint32_t)__bfloat16_as_ushort(zb0) | ((uint32_t)__bfloat16_as_ushort(zb1) << 16);
+            s1[lane * 65 + (c0 + j) / 2] =
+                (uint32_t)__bfloat16_as_ushort(hb0) | ((uint32_t)__bfloat16_as_ushort(hb1) << 16);
+            g.out_ht[(int64_t)(col0 + j) * g.M + row] = hb0;
+            g.out_ht[(int64_t)(col0 + j + 1) * g.M + row] = hb1;
           }
-        } else if (g.epi == kEpiOutput) {
-#pragma unroll
-          for (int j = 0; j < 32; ++j) g.out_f32[(int64_t)row * g.N + col0 + j] = v[j] + g.bias[col0 + j];
         } else if (g.epi == kEpiBackHid) {
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            const float z = __bfloat162float(g.zprev[(int64_t)row * g.N + col0 + j]);
-            const __nv_bfloat16 db = __float2bfloat16_rn(v[j] * gelu_tanh_grad(z));
-            g.out_h[(int64_t)row * g.N + col0 + j] = db;
-            g.out_ht[(int64_t)(col0 + j) * g.M + row] = db;
+          for (int j = 0; j < 32; j += 2) {
+            const uint32_t zw = s1[lane * 65 + (c0 + j) / 2];
+            const float za = __bfloat162float(__ushort_as_bfloat16((unsigned short)(zw & 0xffffu)));
+            const float zc = __bfloat162float(__ushort_as_bfloat16((unsigned short)(zw >> 16)));
+            const __nv_bfloat16 d0 = __float2bfloat16_rn(v[j] * gelu_tanh_grad(za));
+            const __nv_bfloat16 d1 = __float2bfloat16_rn(v[j + 1] * gelu_tanh_grad(zc));
+            s0[lane * 65 + (c0 + j) / 2] =
+                (uint32_t)__bfloat16_as_ushort(d0) | ((uint32_t)__bfloat16_as_ushort(d1) << 16);
+            g.out_ht[(int64_t)(col0 + j) * g.M + row] = d0;
+            g.out_ht[(int64_t)(col0 + j + 1) * g.M + row] = d1;
           }
         } else {
+          const bool bias = g.epi == kEpiOutput;
 #pragma unroll
-          for (int j = 0; j < 32; ++j) g.out_f32[(int64_t)row * g.N + col0 + j] = v[j];
+          for (int j = 0; j < 32; ++j) sf[lane * 129 + c0 + j] = v[j] + (bias ? g.bias[col0 + j] : 0.f);
+        }
+      }
+      __syncwarp();
+      // whole rows out: a warp store covers 32 consecutive words of a row
+      // (bf16 pairs or floats), conflict-free shared-memory reads
+      for (int i = 0; i < 32; ++i) {
+        const int64_t grow = (int64_t)(m0 + 32 * q + i);
+        if (g.epi == kEpiHidden) {
+          uint32_t* dz = reinterpret_cast<uint32_t*>(g.out_z + grow * g.N + n0);
+          uint32_t* dh = reinterpret_cast<uint32_t*>(g.out_h + grow * g.N + n0);
+          dz[lane] = s0[i * 65 + lane];
+          dz[32 + lane] = s0[i * 65 + 32 + lane];
+          dh[lane] = s1[i * 65 + lane];
+          dh[32 + lane] = s1[i * 65 + 32 + lane];
+        } else if (g.epi == kEpiBackHid) {
+          uint32_t* dh = reinterpret_cast<uint32_t*>(g.out_h + grow * g.N + n0);
+          dh[lane] = s0[i * 65 + lane];
+          dh[32 + lane] = s0[i * 65 + 32 + lane];
+        } else {
+          float* d = g.out_f32 + grow * g.N + n0;
+#pragma unroll
+          for (int k = 0; k < 4; ++k) d[32 * k + lane] = sf[i * 129 + 32 * k + lane];
         }
       }
     }

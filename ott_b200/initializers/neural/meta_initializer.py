@@ -207,10 +207,13 @@ def fit(meta: MetaInitializer, a: torch.Tensor, b: torch.Tensor, g: torch.Tensor
   num = a.shape[0]
   lr0 = meta.lr
   losses = []
+  # every step's minibatch indices drawn at once and copied to the device
+  # once (no host-to-device copy per step)
+  idx_all = torch.randint(0, num, (steps, batch_size), generator=gen).to(a.device)
   for step in range(steps):
     if cosine:
       meta.lr = lr0 * 0.5 * (1.0 + math.cos(math.pi * step / steps))
-    idx = torch.randint(0, num, (batch_size,), generator=gen).to(a.device)
+    idx = idx_all[step]
     losses.append(meta.update(a[idx], b[idx], g[idx]))
     if log_every and (step + 1) % log_every == 0:
       print(f"step {step + 1}: loss {float(losses[-1]):.3e}", flush=True)
