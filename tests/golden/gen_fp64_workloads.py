@@ -12,8 +12,10 @@ the same points.
 
     python tests/golden/gen_fp64_workloads.py [name ...]
 
-The headline workload (n = m = 65536, d = 64) takes about 15 minutes on 8
-cores; the GPU machine only reads the committed files.
+The headline workload (n = m = 65536, d = 64) takes about 20 minutes on 8
+cores; the GPU machine only reads the committed files. ``ANNEALED`` adds an
+epsilon-annealed chain at a reduced size (the float64 reference of the
+annealing workload's accuracy).
 """
 import os
 import sys
@@ -38,6 +40,16 @@ WORKLOADS = {
     # epsilon = 0.05 * mean(C): the reference's CPU-runnable configuration
     "uniform2048_d2": (lambda: problems.uniform_cloud_problem(2048, 2048, 2, seed=0),
                        0.05, 1e-3),
+}
+
+
+# name -> (inputs, stages, start, final): epsilon-annealed chains, every
+# stage from the previous stage's potentials, threshold 1e-3 per stage
+ANNEALED = {
+    # two 8-component Gaussian mixtures in R^128, uniform weights (the
+    # annealing workload's family, pair seed 0) at n = m = 2048
+    "anneal_gmm8_n2048_d128": (lambda: problems.gmm8_pair(2048, 2048, 128, seed=0), 10, 1.0,
+                               1e-3),
 }
 
 
@@ -69,6 +81,29 @@ def generate(name, workers=None):
         f" -> {os.path.basename(path)}")
 
 
+def generate_annealed(name, workers=None):
+  make, stages, start, final = ANNEALED[name]
+  x, y, a, b = make()
+  x64, y64 = x.astype(np.float64), y.astype(np.float64)
+  mean_c = float(oracle.mean_cost_matrix(x64, y64))
+  mults = start * (final / start) ** (np.arange(stages) / max(1, stages - 1))
+  init, iters, t0 = None, [], time.time()
+  for m in mults:
+    geom = oracle.Geom(x64, y64, float(m * mean_c), workers=workers or os.cpu_count())
+    r = oracle.sinkhorn(geom, a, b, init=init, threshold=1e-3)
+    init = (r.f, r.g)
+    iters.append(r.n_iters)
+  path = os.path.join(HERE, f"{name}.fp64.npz")
+  np.savez_compressed(path, f=r.f, g=r.g, stage_iters=np.array(iters),
+                      reg_ot_cost=r.reg_ot_cost, epsilon=r.epsilon, mean_cost=mean_c,
+                      checksums=input_checksums(x, y, a, b))
+  print(f"{name}: stage iterations {iters}, final reg_ot_cost={r.reg_ot_cost:.12g} "
+        f"({time.time() - t0:.0f} s) -> {os.path.basename(path)}")
+
+
 if __name__ == "__main__":
-  for nm in (sys.argv[1:] or list(WORKLOADS)):
-    generate(nm)
+  for nm in (sys.argv[1:] or list(WORKLOADS) + list(ANNEALED)):
+    if nm in ANNEALED:
+      generate_annealed(nm)
+    else:
+      generate(nm)
