@@ -796,6 +796,12 @@ def run_batched(args):
   t_b, o_b = timed(graph.replay, args.steps, args.warmup)
   clk = clocks.stop()
   t_d, _ = timed(batch("auto", autotune=True), 1, 1)
+  # each tensor-core tile width pinned (the autotuner's other dimension)
+  tiles = {}
+  for tile in (256, 128):
+    sinkhorn.set_schedule(probs, sinkhorn.Sinkhorn(precision="auto"), waves=2, dynamic=1,
+                          tile_n=tile)
+    tiles[str(tile)] = timed(batch("auto"), 1, 1)[0]
   t_f, o_f = timed(batch("fp32"), 1, 1)
   t_s, o_s = timed(one_by_one("auto"), 1, 1)
   it_b = np.array([o.n_iters for o in o_b])
@@ -833,6 +839,7 @@ def run_batched(args):
       "max_iters": int(it_b.max()),
       "entries_per_s": odist.sum_over_ranks(entries) / t_b,  # whole job, all ranks
       "direct_call_no_graph": {"s": t_d},
+      "tile_width_s": tiles,
       "plain_fp32_batched": {"s": t_f, "mean_iters": float(it_f.mean())},
       "one_launch_per_problem": {"s": t_s},
       "speedup_vs_plain_fp32": t_f / t_b, "speedup_vs_per_problem": t_s / t_b,

@@ -153,7 +153,8 @@ int32_t ottb_sinkhorn_launch(const ottb_problem* problems, int32_t num_problems,
  * for one problem, the column split of each sweep (the heuristic choice
  * x1/2, x1, x2) and round-robin or queued dealing of work units; for
  * several problems, how far the column splits of the problems still
- * iterating may grow as others converge. Each candidate runs the whole
+ * iterating may grow as others converge; on the tensor cores each of those
+ * with tiles of 256 and of 128 columns. Each candidate runs the whole
  * solve twice (one untimed, one timed with CUDA events), writing the
  * problems' outputs and results; the call blocks until the trials finish
  * and refuses a stream under capture (OTTB_ERR_INVALID). Returns at once if
@@ -162,6 +163,21 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
                                int32_t d, const ottb_solver_cfg* cfg,
                                ottb_result* results, void* workspace,
                                size_t workspace_bytes, void* stream, int32_t force);
+
+/* Records a work schedule for calls with these shapes and this
+ * configuration on the current device, in the cache ottb_sinkhorn_autotune
+ * fills (no counterpart in the reference, where XLA schedules the loop):
+ * later plans of such calls use it without timing trials. split_scale: a
+ * single problem's column split is the heuristic one times split_scale / 4;
+ * waves: the splits of problems still iterating grow while fewer than
+ * waves x grid units remain (0: never); dynamic: 1 deals work units from an
+ * atomic queue, 0 round-robin (calls with several problems always queue);
+ * tile_n: columns of a tensor-core tile, 256 or 128 (ignored by the
+ * CUDA-core engine). OTTB_ERR_INVALID for values outside those ranges. */
+int32_t ottb_sinkhorn_set_schedule(const ottb_problem* problems, int32_t num_problems,
+                                   int32_t d, const ottb_solver_cfg* cfg,
+                                   int32_t split_scale, int32_t waves, int32_t dynamic,
+                                   int32_t tile_n);
 
 /* Transport plan of a point-cloud problem applied to num_vec vectors, from
  * its dual potentials, without materialising the plan

@@ -33,6 +33,7 @@ EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_prepare",
     "ottb_sinkhorn_launch",
     "ottb_sinkhorn_autotune",
+    "ottb_sinkhorn_set_schedule",
     "ottb_apply_transport_workspace_size",
     "ottb_apply_transport",
     "ottb_apply_transport_sweep_workspace_size",
@@ -180,6 +181,9 @@ def load() -> ctypes.CDLL:
         ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg),
         vp, vp, sz, vp, i32]
     lib.ottb_sinkhorn_autotune.restype = i32
+    lib.ottb_sinkhorn_set_schedule.argtypes = [
+        ctypes.POINTER(OttbProblem), i32, i32, ctypes.POINTER(OttbSolverCfg), i32, i32, i32, i32]
+    lib.ottb_sinkhorn_set_schedule.restype = i32
     f32_ = ctypes.c_float
     lib.ottb_apply_transport_workspace_size.argtypes = [i64, i64, i32, i32, i32]
     lib.ottb_apply_transport_workspace_size.restype = sz

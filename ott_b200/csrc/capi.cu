@@ -89,18 +89,25 @@ KernelChoice pick_simt(int dp) {
   return k;
 }
 
-// Tensor-core engine: DK = 64 or 128 (d padded with zeros).
-template <int DK>
+// Tensor-core engine: DK = 64 or 128 (d padded with zeros), tiles of TN =
+// 256 or 128 columns.
+template <int DK, int TN>
 struct TcKernel {
-  static void* fn() { return (void*)&sinkhorn_tc_kernel<DK>; }
-  static size_t smem() { return sizeof(TcSmem<DK>) + 1024; }  // + alignment slack
+  static void* fn() { return (void*)&sinkhorn_tc_kernel<DK, TN>; }
+  static size_t smem() { return sizeof(TcSmem<DK, TN>) + 1024; }  // + alignment slack
 };
 
-KernelChoice pick_tc(int dk) {
+// Points of the tensor-core layout are padded to this many (either tile
+// width divides it), so the workspace layout does not depend on the tile.
+constexpr int64_t kTcPad = 256;
+
+KernelChoice pick_tc(int dk, int tn) {
   KernelChoice k;
-  k.threads = dk == 64 ? TcCfg<64>::kThreads : TcCfg<128>::kThreads;
-  if (dk == 64) { k.fn = TcKernel<64>::fn(); k.smem = TcKernel<64>::smem(); }
-  if (dk == 128) { k.fn = TcKernel<128>::fn(); k.smem = TcKernel<128>::smem(); }
+  k.threads = TcCfg<64, 256>::kThreads;
+  if (dk == 64 && tn == 256) { k.fn = TcKernel<64, 256>::fn(); k.smem = TcKernel<64, 256>::smem(); }
+  if (dk == 64 && tn == 128) { k.fn = TcKernel<64, 128>::fn(); k.smem = TcKernel<64, 128>::smem(); }
+  if (dk == 128 && tn == 256) { k.fn = TcKernel<128, 256>::fn(); k.smem = TcKernel<128, 256>::smem(); }
+  if (dk == 128 && tn == 128) { k.fn = TcKernel<128, 128>::fn(); k.smem = TcKernel<128, 128>::smem(); }
   return k;
 }
 
@@ -185,10 +192,13 @@ int persistent_grid(const KernelChoice& k, int sms) {
 //                (0: never)
 //   dynamic      work units dealt from an atomic queue (1) or round-robin
 //                (0); calls with several problems always use the queue
+//   tile_n       columns of a tensor-core tile (256: two accumulators, full
+//                MMA rate; 128: four accumulators, smaller last tiles)
 struct Schedule {
   int split_scale = 4;
   int waves = 2;
   int dynamic = 0;
+  int tile_n = 256;  // tensor-core tile width (256 or 128); the CUDA-core engine ignores it
 };
 
 // Column splits of one sweep: enough units to keep every CTA busy with
@@ -315,7 +325,7 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
   plan.tc = wants_tc(cfg, d);
   if (plan.tc) {
     plan.dp = d <= 64 ? 64 : 128;
-    plan.kern = pick_tc(plan.dp);
+    plan.kern = pick_tc(plan.dp, 256);
   } else {
     plan.dp = simt_dp(d);
     plan.kern = pick_simt(plan.dp);
@@ -348,6 +358,16 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     if (tuned_schedule(tune_key(probs, num, plan), &t)) plan.sched = t;
   }
   if (num > 1) plan.sched.dynamic = 1;
+  if (plan.tc) {
+    if (plan.sched.tile_n != 256 && plan.sched.tile_n != 128) return OTTB_ERR_INVALID;
+    plan.kern = pick_tc(plan.dp, plan.sched.tile_n);
+    if (!plan.kern.fn) return OTTB_ERR_UNSUPPORTED;
+    if (need_grid) {
+      DeviceInfo di = device_info();
+      plan.grid = persistent_grid(plan.kern, di.sms);
+      if (plan.grid <= 0) return OTTB_ERR_CUDA;
+    }
+  }
   size_t off = 0;
   plan.off_globals = off; off = align_up(off + sizeof(Globals));
   plan.off_sched = off; off = align_up(off + sizeof(Sched));
@@ -368,7 +388,7 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     pp.m = q.m;
     // Points are padded to whole column tiles (128 columns on the CUDA
     // cores, 256 on the tensor cores); row blocks of 128 cover the real rows.
-    const int64_t tile_n = plan.tc ? TcCfg<64>::kTileN : kBN;
+    const int64_t tile_n = plan.tc ? kTcPad : kBN;
     pp.n_pad = round_up(q.n, tile_n);
     pp.m_pad = round_up(q.m, tile_n);
     pp.rb_f = (int)((q.n + kBM - 1) / kBM);
@@ -877,21 +897,27 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
   // Candidate schedules: initial split of a single problem (x1/2, x1, x2;
   // round-robin or queued units); for several problems, how far the splits
   // of the problems still iterating may grow (0, 1, 2, 4 waves of units).
+  // On the tensor cores each of these with 256- and with 128-column tiles.
   std::vector<Schedule> cands;
-  if (num_problems == 1) {
-    for (int scale : {4, 2, 8})
-      for (int dyn : {0, 1}) {
+  for (int tile : {256, 128}) {
+    if (tile != 256 && !base.tc) break;
+    if (num_problems == 1) {
+      for (int scale : {4, 2, 8})
+        for (int dyn : {0, 1}) {
+          Schedule c;
+          c.split_scale = scale;
+          c.dynamic = dyn;
+          c.tile_n = tile;
+          cands.push_back(c);
+        }
+    } else {
+      for (int w : {2, 0, 1, 4}) {
         Schedule c;
-        c.split_scale = scale;
-        c.dynamic = dyn;
+        c.waves = w;
+        c.dynamic = 1;
+        c.tile_n = tile;
         cands.push_back(c);
       }
-  } else {
-    for (int w : {2, 0, 1, 4}) {
-      Schedule c;
-      c.waves = w;
-      c.dynamic = 1;
-      cands.push_back(c);
     }
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -929,6 +955,31 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
   if (st != OTTB_OK) return st;
   std::lock_guard<std::mutex> lock(g_tune_mu);
   tune_cache()[key] = best;
+  return OTTB_OK;
+}
+
+int32_t ottb_sinkhorn_set_schedule(const ottb_problem* problems, int32_t num_problems,
+                                   int32_t d, const ottb_solver_cfg* cfg, int32_t split_scale,
+                                   int32_t waves, int32_t dynamic, int32_t tile_n) {
+  if (split_scale < 1 || split_scale > 128 || waves < 0 || waves > 64) return OTTB_ERR_INVALID;
+  if (dynamic != 0 && dynamic != 1) return OTTB_ERR_INVALID;
+  if (tile_n != 256 && tile_n != 128) return OTTB_ERR_INVALID;
+  int st = check_problems(problems, num_problems);
+  if (st != OTTB_OK) return st;
+  Plan base;
+  st = make_plan(problems, num_problems, d, cfg, true, base);
+  if (st != OTTB_OK) return st;
+  Schedule sc;
+  sc.split_scale = split_scale;
+  sc.waves = waves;
+  sc.dynamic = dynamic;
+  sc.tile_n = tile_n;
+  Plan check;  // the schedule must give a valid plan (and a launchable kernel)
+  st = make_plan(problems, num_problems, d, cfg, true, check, &sc);
+  if (st != OTTB_OK) return st;
+  const TuneKey key = tune_key(problems, num_problems, base);
+  std::lock_guard<std::mutex> lock(g_tune_mu);
+  tune_cache()[key] = sc;
   return OTTB_OK;
 }
 

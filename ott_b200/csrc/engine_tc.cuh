@@ -6,12 +6,14 @@
 // bf16(v - hi)), rows of DK (64 or 128) elements, hi rows then lo rows; the
 // x points carry the exponent scale s = 2 inv log2(e) / eps_target (x' =
 // s x before the split), so <x', y> is already in log2 units. A tile is 128
-// rows of A by 256 columns of B: the three products hi*hi + hi*lo + lo*hi
-// accumulate into one TMEM tile (3 * DK / 16 MMAs of M = 128, N = 256,
-// K = 16); lo*lo (~2^-16 relative) is dropped. N = 256 because an N = 128
-// MMA takes ~84 cycles on B200 where an N = 256 one takes 128 (the full
-// rate; measured with back-to-back MMAs, A in shared or tensor memory
-// alike). One more K = 16 MMA adds the shifts: B's extension rows hold the
+// rows of A by TN = 256 (or 128) columns of B: the three products hi*hi +
+// hi*lo + lo*hi accumulate into one TMEM tile (3 * DK / 16 MMAs of M = 128,
+// N = TN, K = 16); lo*lo (~2^-16 relative) is dropped. TN = 256 is the
+// default because an N = 128 MMA takes ~84 cycles on B200 where an N = 256
+// one takes 128 (the full rate; measured with back-to-back MMAs, A in
+// shared or tensor memory alike); TN = 128 gives four accumulators instead
+// of two and a 4-stage ring, and the autotuner times both. One more K = 16
+// MMA adds the shifts: B's extension rows hold the
 // column shift w_c = (pot_c - inv |B_c|^2) log2(e) / eps_target as 3 bf16
 // terms (~24 bits) and two ones, A's hold three ones and -sigma_r as two
 // bf16 terms, so acc = s <a_r, b_c> + w_c - sigma_r, the base-2 exponent of
@@ -51,16 +53,16 @@
 
 namespace ottb {
 
-template <int DK>
+template <int DK, int TN>
 struct TcCfg {
   static constexpr int kChunks = DK / 64;           // 64-wide K chunks (128-byte swizzle atoms)
-  static constexpr int kTileN = 256;                // columns of B per tile (MMA N)
+  static constexpr int kTileN = TN;                 // columns of B per tile (MMA N): 256 or 128
   static constexpr int kABlockBytes = 128 * 64 * 2;    // one [128][64] bf16 block
   static constexpr int kBBlockBytes = kTileN * 64 * 2; // one [256][64] bf16 block
   static constexpr int kABytes = 2 * kChunks * kABlockBytes;  // hi + lo, every chunk
   static constexpr int kStageBytes = 2 * kBBlockBytes;        // hi + lo of one chunk
-  static constexpr int kStages = 2;
-  static constexpr int kTmemBufs = 2;
+  static constexpr int kStages = 2 * 256 / TN;      // a 128 KB ring either way
+  static constexpr int kTmemBufs = 512 / TN;        // accumulators filling the 512 columns
   static constexpr int kTmemCols = 512;
   static constexpr int kColGroups = 4;    // epilogue warps per TMEM lane quarter
   static constexpr int kColsPerWarp = kTileN / kColGroups;
@@ -78,23 +80,23 @@ struct TcCfg {
   static constexpr uint32_t kExtSbo = 128;
 };
 
-template <int DK>
+template <int DK, int TN>
 struct TcSmem {
   // operand tiles first: the struct is placed at a 1024-byte boundary
-  uint8_t A[TcCfg<DK>::kABytes];
-  uint8_t B[TcCfg<DK>::kStages][TcCfg<DK>::kStageBytes];
+  uint8_t A[TcCfg<DK, TN>::kABytes];
+  uint8_t B[TcCfg<DK, TN>::kStages][TcCfg<DK, TN>::kStageBytes];
   // K = 16 extension blocks, no swizzle: [row groups][2 K halves][8 rows][8]
-  uint8_t Aext[TcCfg<DK>::kAExtBytes];
-  uint8_t Bext[TcCfg<DK>::kStages][TcCfg<DK>::kBExtBytes];
-  float part_m[TcCfg<DK>::kColGroups][kBM];
-  float part_l[TcCfg<DK>::kColGroups][kBM];
+  uint8_t Aext[TcCfg<DK, TN>::kAExtBytes];
+  uint8_t Bext[TcCfg<DK, TN>::kStages][TcCfg<DK, TN>::kBExtBytes];
+  float part_m[TcCfg<DK, TN>::kColGroups][kBM];
+  float part_l[TcCfg<DK, TN>::kColGroups][kBM];
   float rm[kBM];
   float rl[kBM];
   double red[8];
-  uint64_t full[TcCfg<DK>::kStages];
-  uint64_t empty[TcCfg<DK>::kStages];
-  uint64_t tfull[TcCfg<DK>::kTmemBufs];
-  uint64_t tempty[TcCfg<DK>::kTmemBufs];
+  uint64_t full[TcCfg<DK, TN>::kStages];
+  uint64_t empty[TcCfg<DK, TN>::kStages];
+  uint64_t tfull[TcCfg<DK, TN>::kTmemBufs];
+  uint64_t tempty[TcCfg<DK, TN>::kTmemBufs];
   uint64_t a_full;
   uint64_t a_empty;
   uint64_t drain;
@@ -128,37 +130,37 @@ struct TcMaps {
 };
 
 // A tile: 128 rows, every K chunk, hi and lo ([part][chunk] blocks).
-template <int DK>
+template <int DK, int TN>
 __device__ __forceinline__ void tc_load_a(uint8_t* dst, const CUtensorMap* map, uint64_t* bar,
                                           int32_t row, int32_t pad) {
-  constexpr int C = TcCfg<DK>::kChunks;
+  constexpr int C = TcCfg<DK, TN>::kChunks;
 #pragma unroll
   for (int part = 0; part < 2; ++part)
 #pragma unroll
     for (int c = 0; c < C; ++c)
-      tc::tma_load_2d(dst + (part * C + c) * TcCfg<DK>::kABlockBytes, map, bar, 64 * c,
+      tc::tma_load_2d(dst + (part * C + c) * TcCfg<DK, TN>::kABlockBytes, map, bar, 64 * c,
                       row + part * pad);
 }
 
 // One ring stage: K chunk c of 256 B rows from row, hi and lo ([part] blocks
 // of 256 rows, each loaded as two 128-row boxes).
-template <int DK>
+template <int DK, int TN>
 __device__ __forceinline__ void tc_load_b_chunk(uint8_t* dst, const CUtensorMap* map,
                                                 uint64_t* bar, int c, int32_t row, int32_t pad) {
 #pragma unroll
   for (int part = 0; part < 2; ++part)
 #pragma unroll
-    for (int h = 0; h < 2; ++h)
-      tc::tma_load_2d(dst + part * TcCfg<DK>::kBBlockBytes + h * TcCfg<DK>::kABlockBytes, map,
+    for (int h = 0; h < TN / 128; ++h)
+      tc::tma_load_2d(dst + part * TcCfg<DK, TN>::kBBlockBytes + h * TcCfg<DK, TN>::kABlockBytes, map,
                       bar, 64 * c, row + 128 * h + part * pad);
 }
 
 // Issues the 3 * 4 MMAs of K chunk c of one tile into the TMEM accumulator
 // d_tmem (first = the tile's first MMA, which overwrites the accumulator).
-template <int DK>
+template <int DK, int TN>
 __device__ __forceinline__ void tc_issue_chunk(uint32_t d_tmem, const uint8_t* A,
                                                const uint8_t* Bst, int c, bool first) {
-  constexpr int C = TcCfg<DK>::kChunks;
+  constexpr int C = TcCfg<DK, TN>::kChunks;
   const uint32_t a0 = tc::smem_u32(A), b0 = tc::smem_u32(Bst);
   // (A part, B part): hi*hi, hi*lo, lo*hi
   const int pa[3] = {0, 0, 1};
@@ -169,22 +171,22 @@ __device__ __forceinline__ void tc_issue_chunk(uint32_t d_tmem, const uint8_t* A
 #pragma unroll
     for (int kk = 0; kk < 4; ++kk) {
       const uint64_t ad =
-          tc::sw128_kmajor_desc(a0 + (pa[prod] * C + c) * TcCfg<DK>::kABlockBytes + kk * 32);
-      const uint64_t bd = tc::sw128_kmajor_desc(b0 + pb[prod] * TcCfg<DK>::kBBlockBytes + kk * 32);
-      tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, acc);
+          tc::sw128_kmajor_desc(a0 + (pa[prod] * C + c) * TcCfg<DK, TN>::kABlockBytes + kk * 32);
+      const uint64_t bd = tc::sw128_kmajor_desc(b0 + pb[prod] * TcCfg<DK, TN>::kBBlockBytes + kk * 32);
+      tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK, TN>::kIdesc, acc);
       acc = 1;
     }
 }
 
 // The column-shift MMA: D += Aext * Bext^T over K = 16.
-template <int DK>
+template <int DK, int TN>
 __device__ __forceinline__ void tc_issue_ext(uint32_t d_tmem, const uint8_t* Aext,
                                              const uint8_t* Bext) {
-  const uint64_t ad = tc::plain_kmajor_desc(tc::smem_u32(Aext), TcCfg<DK>::kAExtLbo,
-                                            TcCfg<DK>::kExtSbo);
-  const uint64_t bd = tc::plain_kmajor_desc(tc::smem_u32(Bext), TcCfg<DK>::kBExtLbo,
-                                            TcCfg<DK>::kExtSbo);
-  tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK>::kIdesc, 1);
+  const uint64_t ad = tc::plain_kmajor_desc(tc::smem_u32(Aext), TcCfg<DK, TN>::kAExtLbo,
+                                            TcCfg<DK, TN>::kExtSbo);
+  const uint64_t bd = tc::plain_kmajor_desc(tc::smem_u32(Bext), TcCfg<DK, TN>::kBExtLbo,
+                                            TcCfg<DK, TN>::kExtSbo);
+  tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK, TN>::kIdesc, 1);
 }
 
 // The bounded row shift of one problem's units in a sweep (see the file
@@ -236,15 +238,14 @@ struct TcOperands {
 // Per ring stage st the producer fills one K chunk of B's hi/lo tiles (and,
 // with the last chunk, the first K half of B's extension block) by TMA;
 // full[st] completes on those bytes, empty[st] on the MMA commit.
-template <int DK>
-__device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
+template <int DK, int TN>
+__device__ bool tc_unit(TcSmem<DK, TN>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
                         int t0, int t1, float s, const RowShift& rs, uint64_t timeout_ns) {
-  constexpr int NS = TcCfg<DK>::kStages;
-  constexpr int NB = TcCfg<DK>::kTmemBufs;
-  constexpr int C = TcCfg<DK>::kChunks;
-  constexpr int CG = TcCfg<DK>::kColGroups;
-  constexpr int CW = TcCfg<DK>::kColsPerWarp;  // columns per epilogue warp per tile
-  constexpr int TN = TcCfg<DK>::kTileN;
+  constexpr int NS = TcCfg<DK, TN>::kStages;
+  constexpr int NB = TcCfg<DK, TN>::kTmemBufs;
+  constexpr int C = TcCfg<DK, TN>::kChunks;
+  constexpr int CG = TcCfg<DK, TN>::kColGroups;
+  constexpr int CW = TcCfg<DK, TN>::kColsPerWarp;  // columns per epilogue warp per tile
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
   const int ntiles = t1 - t0;
@@ -268,8 +269,8 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
     if (lane == 0) {
       if (!freed) ok = false;
       if (ok) {
-        tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK>::kABytes);
-        tc_load_a<DK>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
+        tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK, TN>::kABytes);
+        tc_load_a<DK, TN>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
       }
       for (int i = 0; ok && i < ntiles; ++i) {
         const int32_t brow = (t0 + i) * TN;
@@ -278,13 +279,14 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
           const uint32_t st = g % NS;
           if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
           const bool last = c == C - 1;
-          tc::mbar_arrive_expect_tx(&sm.full[st], TcCfg<DK>::kStageBytes +
-                                                      (last ? TcCfg<DK>::kBExtHalfBytes : 0));
-          tc_load_b_chunk<DK>(sm.B[st], op.mapB, &sm.full[st], c, brow, op.padB);
+          tc::mbar_arrive_expect_tx(&sm.full[st], TcCfg<DK, TN>::kStageBytes +
+                                                      (last ? TcCfg<DK, TN>::kBExtHalfBytes : 0));
+          tc_load_b_chunk<DK, TN>(sm.B[st], op.mapB, &sm.full[st], c, brow, op.padB);
           if (last) {
-            tc::tma_load_2d(sm.Bext[st], op.mapBext, &sm.full[st], 0, op.extRow0 + brow);
-            tc::tma_load_2d(sm.Bext[st] + 128 * 16, op.mapBext, &sm.full[st], 0,
-                            op.extRow0 + brow + 128);
+#pragma unroll
+            for (int h = 0; h < TN / 128; ++h)
+              tc::tma_load_2d(sm.Bext[st] + h * 128 * 16, op.mapBext, &sm.full[st], 0,
+                              op.extRow0 + brow + 128 * h);
           }
           pp.last_full_stage = st;
           pp.last_full_parity = (g / NS) & 1;
@@ -306,8 +308,8 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
           const uint32_t st = g % NS;
           if (!tc::mbar_wait(&sm.full[st], (g / NS) & 1, timeout_ns)) { ok = false; break; }
           tc::fence_after_sync();
-          tc_issue_chunk<DK>(d, sm.A, sm.B[st], c, c == 0);
-          if (c == C - 1) tc_issue_ext<DK>(d, sm.Aext, sm.Bext[st]);
+          tc_issue_chunk<DK, TN>(d, sm.A, sm.B[st], c, c == 0);
+          if (c == C - 1) tc_issue_ext<DK, TN>(d, sm.Aext, sm.Bext[st]);
           tc::mma_commit(&sm.empty[st]);
         }
         if (!ok) break;
@@ -363,24 +365,24 @@ __device__ bool tc_unit(TcSmem<DK>& sm, TcPipe& pp, const TcOperands& op, int32_
             }
           }
         };
-        static_assert(CW == 64, "four 16-column loads per warp and tile");
+        constexpr int NCH = CW / 16;  // 16-column loads per warp and tile (4 or 2)
+        static_assert(NCH >= 2 && CW % 16 == 0, "at least two 16-column loads per tile");
         float va[16], vb[16];
         tc::tmem_ld16(tb, va);
         tc::tmem_ld_wait();
-        tc::tmem_ld16(tb + 16, vb);
-        reduce16(va);
-        tc::tmem_ld_wait();
-        tc::tmem_ld16(tb + 32, va);
-        reduce16(vb);
-        tc::tmem_ld_wait();
-        tc::tmem_ld16(tb + 48, vb);
-        reduce16(va);
-        tc::tmem_ld_wait();
+#pragma unroll
+        for (int c = 0; c + 1 < NCH; ++c) {
+          float(&cur)[16] = (c & 1) ? vb : va;
+          float(&nxt)[16] = (c & 1) ? va : vb;
+          tc::tmem_ld16(tb + 16 * (c + 1), nxt);
+          reduce16(cur);
+          tc::tmem_ld_wait();
+        }
         // The accumulator buffer can be refilled once every warp has read it.
         tc::fence_before_sync();
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
-        reduce16(vb);
+        reduce16(((NCH - 1) & 1) ? vb : va);
         two_sum_acc(lrun, lcmp,
                     ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
         continue;

@@ -50,21 +50,21 @@ __device__ __forceinline__ RowShift bounded_row_shift(const ProbDev& P, const Sw
   return rs;
 }
 
-template <int DK>
-__global__ void __launch_bounds__(TcCfg<DK>::kThreads, 1)
+template <int DK, int TN>
+__global__ void __launch_bounds__(TcCfg<DK, TN>::kThreads, 1)
 sinkhorn_tc_kernel(KernelArgs A) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   // The 128-byte swizzled operand tiles need 1024-byte alignment.
   const uint32_t base = tc::smem_u32(smem_raw);
   unsigned char* aligned = smem_raw + ((1024u - (base & 1023u)) & 1023u);
-  TcSmem<DK>& sm = *reinterpret_cast<TcSmem<DK>*>(aligned);
-  constexpr int NS = TcCfg<DK>::kStages;
-  constexpr int NB = TcCfg<DK>::kTmemBufs;
+  TcSmem<DK, TN>& sm = *reinterpret_cast<TcSmem<DK, TN>*>(aligned);
+  constexpr int NS = TcCfg<DK, TN>::kStages;
+  constexpr int NB = TcCfg<DK, TN>::kTmemBufs;
   const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
-    constexpr int NE = TcCfg<DK>::kEpiWarps;
+    constexpr int NE = TcCfg<DK, TN>::kEpiWarps;
     for (int i = 0; i < NS; ++i) {
       tc::mbar_init(&sm.full[i], 1);   // producer arrival + TMA bytes
       tc::mbar_init(&sm.empty[i], 1);  // MMA commit
@@ -80,16 +80,16 @@ sinkhorn_tc_kernel(KernelArgs A) {
     tc::fence_barrier_init();
   }
   if (warp == 1) {
-    tc::tmem_alloc(&sm.tmem_base, TcCfg<DK>::kTmemCols);
+    tc::tmem_alloc(&sm.tmem_base, TcCfg<DK, TN>::kTmemCols);
     tc::tmem_relinquish();
   }
   // Extension blocks: zero everywhere; A's first 3 K columns are ones.
   {
     uint32_t* a32 = reinterpret_cast<uint32_t*>(sm.Aext);
-    for (int i = threadIdx.x; i < TcCfg<DK>::kAExtBytes / 4; i += blockDim.x) a32[i] = 0u;
+    for (int i = threadIdx.x; i < TcCfg<DK, TN>::kAExtBytes / 4; i += blockDim.x) a32[i] = 0u;
     for (int st = 0; st < NS; ++st) {
       uint32_t* b32 = reinterpret_cast<uint32_t*>(sm.Bext[st]);
-      for (int i = threadIdx.x; i < TcCfg<DK>::kBExtBytes / 4; i += blockDim.x) b32[i] = 0u;
+      for (int i = threadIdx.x; i < TcCfg<DK, TN>::kBExtBytes / 4; i += blockDim.x) b32[i] = 0u;
     }
     __syncthreads();
     if (threadIdx.x < kBM) {
@@ -113,9 +113,9 @@ sinkhorn_tc_kernel(KernelArgs A) {
       // sweep at another epsilon scales the accumulator by ws / ws_t.
       const float r = wscale / P.ws_t;
       RowShift rs = bounded_row_shift(P, sp);
-      return tc_unit<DK>(sm, pp, op, rb * kBM, t0, t1, r, rs, A.timeout_ns);
+      return tc_unit<DK, TN>(sm, pp, op, rb * kBM, t0, t1, r, rs, A.timeout_ns);
     };
-    return sweep_units<TcCfg<DK>::kTileN>(A, sp, idx, cs, unit);
+    return sweep_units<TcCfg<DK, TN>::kTileN>(A, sp, idx, cs, unit);
   };
   persistent_main(A, sweep);
 
@@ -134,7 +134,7 @@ sinkhorn_tc_kernel(KernelArgs A) {
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  if (warp == 1) tc::tmem_dealloc(sm.tmem_base, TcCfg<DK>::kTmemCols);
+  if (warp == 1) tc::tmem_dealloc(sm.tmem_base, TcCfg<DK, TN>::kTmemCols);
 }
 
 }  // namespace ottb

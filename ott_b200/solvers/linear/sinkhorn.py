@@ -26,7 +26,7 @@ from ott_b200.initializers.linear import initializers as init_lib
 from ott_b200.problems.linear import linear_problem
 from ott_b200.solvers.linear import implicit_differentiation as implicit_lib
 
-__all__ = ["Sinkhorn", "SinkhornGraph", "SinkhornOutput", "run_batch"]
+__all__ = ["set_schedule", "Sinkhorn", "SinkhornGraph", "SinkhornOutput", "run_batch"]
 
 _PRECISIONS = {
     "auto": _lib.PRECISION_AUTO,
@@ -592,6 +592,13 @@ class _Call:
                                          self.ws_bytes, stream, 1 if force else 0)
     self._check(st, "ottb_sinkhorn_autotune")
 
+  def set_schedule(self, split_scale: int = 4, waves: int = 2, dynamic: int = 0,
+                   tile_n: int = 256) -> None:
+    st = self.lib.ottb_sinkhorn_set_schedule(self.arr, self.nprob, self.d,
+                                             ctypes.byref(self.cfg), split_scale, waves,
+                                             dynamic, tile_n)
+    self._check(st, "ottb_sinkhorn_set_schedule")
+
   def solve(self, stream: int) -> None:
     st = self.lib.ottb_sinkhorn_pointcloud(self.arr, self.nprob, self.d, ctypes.byref(self.cfg),
                                            self.res.data_ptr(), self.ws.data_ptr(),
@@ -668,6 +675,18 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
   if solver.progress_fn is not None:
     _replay_progress(solver, out)
   return out
+
+
+def set_schedule(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn, *,
+                 split_scale: int = 4, waves: int = 2, dynamic: int = 0,
+                 tile_n: int = 256) -> None:
+  """Pins the work schedule of calls with these problems' shapes and the
+  solver's configuration (``ottb_sinkhorn_set_schedule``): the choice
+  ``Sinkhorn(autotune=True)`` would otherwise time, including the
+  tensor-core tile width (256 or 128 columns)."""
+  if not probs:
+    raise ValueError("no problems")
+  _Call(probs, solver, None, None, {}, None).set_schedule(split_scale, waves, dynamic, tile_n)
 
 
 class SinkhornGraph:

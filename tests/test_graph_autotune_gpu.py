@@ -101,3 +101,36 @@ def test_autotuned_batch_keeps_parity():
     ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05)
     assert abs(out.n_iters - ref.n_iters) <= out.inner_iterations
     np.testing.assert_allclose(out.reg_ot_cost, ref.reg_ot_cost, rtol=1e-4)
+
+
+@pytest.mark.parametrize("specs", [[(1000, 1100)], [(300, 200), (129, 700), (900, 400)]])
+def test_tile_128_keeps_parity(specs):
+  """The 128-column tensor-core tile (four accumulators), pinned with
+  ottb_sinkhorn_set_schedule, keeps the tensor-core path's parity bars
+  against the float64 oracle, single and batched; its results equal the
+  256-column tile's within those bars."""
+  from ott_b200.solvers.linear import sinkhorn
+  probs, raw = _problems(specs, 64, 0.05, seed=40)
+  solver = sinkhorn.Sinkhorn(precision="bf16_split3")
+  wide = sinkhorn.run_batch(probs, solver)
+  sinkhorn.set_schedule(probs, solver, waves=2, dynamic=1 if len(specs) > 1 else 0,
+                        tile_n=128)
+  narrow = sinkhorn.run_batch(probs, solver)
+  for (x, y, a, b), o, w, p in zip(raw, narrow, wide, probs):
+    ref = helpers.oracle_solve(x, y, a, b, epsilon=0.05)
+    helpers.assert_parity(p.geom, o, ref, pot_tol=1e-3, cost_rtol=1e-4, iter_blocks=1,
+                          err_rtol=1e-2, err_atol=2e-3)
+    np.testing.assert_allclose(o.reg_ot_cost, w.reg_ot_cost, rtol=1e-4)
+  # restore the default schedule for these shapes
+  sinkhorn.set_schedule(probs, solver, waves=2, dynamic=1 if len(specs) > 1 else 0,
+                        tile_n=256)
+
+
+def test_set_schedule_rejects_bad_values():
+  from ott_b200 import _lib
+  from ott_b200.solvers.linear import sinkhorn
+  probs, _ = _problems([(200, 300)], 64, 0.05, seed=50)
+  solver = sinkhorn.Sinkhorn(precision="bf16_split3")
+  for kw in (dict(tile_n=64), dict(split_scale=0), dict(waves=-1), dict(dynamic=2)):
+    with pytest.raises(_lib.OttbError):
+      sinkhorn.set_schedule(probs, solver, **kw)
