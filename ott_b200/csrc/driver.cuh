@@ -74,25 +74,66 @@ __device__ __forceinline__ SweepOperands make_operands(const ProbDev& P, int kin
   return op;
 }
 
-// Block-wide sum of one double per thread (threads 0..kBM-1 contribute),
-// fixed-order tree so the result is deterministic.
-__device__ __forceinline__ double block_sum_128(double v, double* red) {
-  int t = threadIdx.x;
+// Thread groups that run the per-row-block steps (merges, potential
+// updates): the whole CTA, or the tensor-core kernel's epilogue warps
+// (threads 64.., synchronised by named barrier 1) while its producer and
+// MMA warps run ahead. tid() is the thread's index in the group; the rows
+// of a row block are handled by tids 0..kBM-1 (whole warps).
+struct CtaGroup {
+  static __device__ __forceinline__ int tid() { return threadIdx.x; }
+  static __device__ __forceinline__ int size() { return blockDim.x; }
+  static __device__ __forceinline__ void sync() { __syncthreads(); }
+};
+
+template <int FIRST, int COUNT>
+struct WarpGroup {
+  static __device__ __forceinline__ int tid() { return (int)threadIdx.x - FIRST; }
+  static __device__ __forceinline__ int size() { return COUNT; }
+  static __device__ __forceinline__ void sync() {
+    asm volatile("bar.sync 1, %0;" ::"n"(COUNT) : "memory");
+  }
+  // Barrier that also ORs a predicate over the group: every thread gets the
+  // same answer, so a decision to leave a loop is taken by all or none.
+  static __device__ __forceinline__ bool sync_or(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred pi, po;\n\t"
+        "setp.ne.u32 pi, %1, 0;\n\t"
+        "bar.red.or.pred po, 1, %2, pi;\n\t"
+        "selp.u32 %0, 1, 0, po;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v), "n"(COUNT)
+        : "memory");
+    return r != 0;
+  }
+};
+
+// Group-wide sum of one double per thread (tids 0..kBM-1 contribute),
+// fixed-order tree so the result is deterministic; tid 0 gets the sum.
+template <class G>
+__device__ __forceinline__ double group_sum_128(double v, double* red) {
+  const int t = G::tid();
   for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-  if (t < kBM && (t & 31) == 0) red[t >> 5] = v;
-  __syncthreads();
+  if (t >= 0 && t < kBM && (t & 31) == 0) red[t >> 5] = v;
+  G::sync();
   double r = 0.0;
   if (t == 0) r = (red[0] + red[1]) + (red[2] + red[3]);
-  __syncthreads();
+  G::sync();
   return r;
 }
 
+__device__ __forceinline__ double block_sum_128(double v, double* red) {
+  return group_sum_128<CtaGroup>(v, red);
+}
+
 // Potential update and (optionally) marginal for the rows of one row block,
-// from their base-2 LSE state. geometry.py:376-398 / :326-349.
-__device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parity,
-                              int rb, const float* rm, const float* rl,
-                              int norm_error, double* red) {
-  const int t = threadIdx.x;
+// from their base-2 LSE state. geometry.py:376-398 / :326-349. Run by every
+// thread of group G.
+template <class G>
+__device__ void finalize_rows_g(const ProbDev& P, const SweepParams& sp, int parity,
+                                int rb, const float* rm, const float* rl,
+                                int norm_error, double* red) {
+  const int t = G::tid();
   const bool isG = sp.kind == kSweepG;
   const int64_t R = isG ? P.m : P.n;
   const float* marg = isG ? P.b : P.a;
@@ -111,7 +152,7 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
   // other kind's next sweep (log2 units), for the bound that sweep uses
   float dmax = -INFINITY, dmin = INFINITY;
   const int64_t r = (int64_t)rb * kBM + t;
-  if (t < kBM && r < R) {
+  if (t >= 0 && t < kBM && r < R) {
     const float mv = rm[t], lv = rl[t];
     double lse2 = (lv > 0.f) ? (double)mv + log2((double)lv)
                              : (lv == 0.f ? -INFINITY : (double)NAN);
@@ -162,11 +203,11 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       dmin = fminf(dmin, __shfl_xor_sync(0xffffffffu, dmin, off));
     }
     float* fr = reinterpret_cast<float*>(red);
-    if (t < kBM && (t & 31) == 0) {
+    if (t >= 0 && t < kBM && (t & 31) == 0) {
       fr[t >> 5] = dmax;
       fr[4 + (t >> 5)] = dmin;
     }
-    __syncthreads();
+    G::sync();
     if (t == 0) {
       const float mx = fmaxf(fmaxf(fr[0], fr[1]), fmaxf(fr[2], fr[3]));
       const float mn = fminf(fminf(fr[4], fr[5]), fminf(fr[6], fr[7]));
@@ -174,16 +215,22 @@ __device__ void finalize_rows(const ProbDev& P, const SweepParams& sp, int parit
       if (mx > -INFINITY) atomicMax(slot, fkey(mx));
       if (mn < INFINITY) atomicMin(slot + 1, fkey(mn));
     }
-    __syncthreads();
+    G::sync();
   }
   if (sp.eval) {
-    double e = block_sum_128(err_t, red);
-    double s = block_sum_128(msum_t, red);
+    double e = group_sum_128<G>(err_t, red);
+    double s = group_sum_128<G>(msum_t, red);
     if (t == 0) {
       P.err_part[rb] = e;
       P.msum_part[rb] = s;
     }
   }
+}
+
+__device__ __forceinline__ void finalize_rows(const ProbDev& P, const SweepParams& sp,
+                                              int parity, int rb, const float* rm,
+                                              const float* rl, int norm_error, double* red) {
+  finalize_rows_g<CtaGroup>(P, sp, parity, rb, rm, rl, norm_error, red);
 }
 
 }  // namespace ottb

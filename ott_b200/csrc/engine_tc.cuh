@@ -80,6 +80,36 @@ struct TcCfg {
   static constexpr uint32_t kExtSbo = 128;
 };
 
+// The bounded row shift of one problem's units in a sweep (see the file
+// comment); on = false: sigma = 0 and running maxima.
+struct RowShift {
+  const float* lprev;  // the rows' log-sum-exps from their last sweep
+  float dmax;          // D
+  int64_t rows;        // rows of A (padding rows get sigma = 0)
+  bool on;
+};
+
+// Operands of one tensor-core sweep for one problem.
+struct TcOperands {
+  const CUtensorMap* mapA;
+  const CUtensorMap* mapB;
+  const CUtensorMap* mapBext;
+  int32_t padA, padB;
+  int32_t extRow0;  // first row of B's column-shift rows (g buffer of y)
+  int64_t rows, cols;
+};
+
+// One work unit of a tensor-core sweep as the epilogue warps deal it to the
+// producer and MMA warps: problem (table index), row block, column split
+// and tile range, g parity, accumulator scale, operands and row shift; end
+// marks the end of the sweep's units for this CTA.
+struct TcUnit {
+  TcOperands op;
+  RowShift rs;
+  int p, rb, sidx, S, parity, t0, t1, end;
+  float r;
+};
+
 template <int DK, int TN>
 struct TcSmem {
   // operand tiles first: the struct is placed at a 1024-byte boundary
@@ -88,6 +118,7 @@ struct TcSmem {
   // K = 16 extension blocks, no swizzle: [row groups][2 K halves][8 rows][8]
   uint8_t Aext[TcCfg<DK, TN>::kAExtBytes];
   uint8_t Bext[TcCfg<DK, TN>::kStages][TcCfg<DK, TN>::kBExtBytes];
+  TcUnit units[2];  // ring of unit descriptors (kernel_tc.cuh, tc_sweep)
   float part_m[TcCfg<DK, TN>::kColGroups][kBM];
   float part_l[TcCfg<DK, TN>::kColGroups][kBM];
   float rm[kBM];
@@ -100,10 +131,14 @@ struct TcSmem {
   uint64_t a_full;
   uint64_t a_empty;
   uint64_t drain;
+  uint64_t unit_full[2];   // a unit descriptor was written (the dealer arrives)
+  uint64_t unit_empty[2];  // the producer and MMA warps have read it
   uint32_t tmem_base;
   int unit;
   int last;
   int err;
+  int deal_rr;      // the dealer's round-robin position in the current sweep
+  int deal_ended;   // the dealer has written the sweep's end marker
 };
 
 // Pipeline positions, one copy per thread, advanced identically by every
@@ -115,6 +150,8 @@ struct TcPipe {
   uint32_t last_full_stage;  // producer: most recent stage issued
   uint32_t last_full_parity;
   int issued;
+  uint32_t desc;   // unit descriptors consumed so far (end markers included)
+  uint32_t wdesc;  // dealer: unit descriptors written so far
 };
 
 // Tensor maps of a problem, stored in global memory: the point sets
@@ -189,14 +226,6 @@ __device__ __forceinline__ void tc_issue_ext(uint32_t d_tmem, const uint8_t* Aex
   tc::mma_bf16(d_tmem, ad, bd, TcCfg<DK, TN>::kIdesc, 1);
 }
 
-// The bounded row shift of one problem's units in a sweep (see the file
-// comment); on = false: sigma = 0 and running maxima.
-struct RowShift {
-  const float* lprev;  // the rows' log-sum-exps from their last sweep
-  float dmax;          // D
-  int64_t rows;        // rows of A (padding rows get sigma = 0)
-  bool on;
-};
 
 // sigma_r = L_r + D as two bf16 terms (sigma = p1 + p2 exactly in FP32), 0
 // for padding rows, rows whose L_r is not finite, or without a bound.
@@ -220,246 +249,261 @@ __device__ __forceinline__ float row_shift(const RowShift& rs, int64_t row,
 #define OTTB_POLY_OF_8_TC_FAST 2
 #endif
 
-// Operands of one tensor-core sweep for one problem.
-struct TcOperands {
-  const CUtensorMap* mapA;
-  const CUtensorMap* mapB;
-  const CUtensorMap* mapBext;
-  int32_t padA, padB;
-  int32_t extRow0;  // first row of B's column-shift rows (g buffer of y)
-  int64_t rows, cols;
-};
 
-// One work unit: rows row0..row0+127 of A against B tiles [t0, t1) of 256
-// columns. Leaves the per-row base-2 LSE state in sm.rm / sm.rl. r scales
-// the accumulator to the sweep's epsilon (1 at the target epsilon); rs is
-// the unit's row shift. Returns false if a wait timed out.
+
+// The three roles of one work unit: rows row0 = u.rb * 128 .. +127 of A
+// against B tiles [u.t0, u.t1) of TN columns. Each role advances its own
+// copy of the pipeline positions pp over the same sequence of units and
+// returns false if one of its waits timed out (after marking sm.err).
 //
 // Per ring stage st the producer fills one K chunk of B's hi/lo tiles (and,
 // with the last chunk, the first K half of B's extension block) by TMA;
 // full[st] completes on those bytes, empty[st] on the MMA commit.
+// Producer (warp 0, all lanes; lane 0 issues the copies).
 template <int DK, int TN>
-__device__ bool tc_unit(TcSmem<DK, TN>& sm, TcPipe& pp, const TcOperands& op, int32_t row0,
-                        int t0, int t1, float s, const RowShift& rs, uint64_t timeout_ns) {
+__device__ bool tc_produce(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u, uint64_t timeout_ns) {
   constexpr int NS = TcCfg<DK, TN>::kStages;
-  constexpr int NB = TcCfg<DK, TN>::kTmemBufs;
   constexpr int C = TcCfg<DK, TN>::kChunks;
-  constexpr int CG = TcCfg<DK, TN>::kColGroups;
-  constexpr int CW = TcCfg<DK, TN>::kColsPerWarp;  // columns per epilogue warp per tile
-  const int warp = threadIdx.x >> 5;
   const int lane = threadIdx.x & 31;
-  const int ntiles = t1 - t0;
+  const TcOperands& op = u.op;
+  const int32_t row0 = u.rb * kBM;
+  const int t0 = u.t0;
+  const int ntiles = u.t1 - u.t0;
   bool ok = true;
-
-  if (warp == 0) {
-    // A tile and its extension block: wait until the previous unit's MMAs
-    // released them, then write the rows' -sigma terms (K columns 3, 4).
-    const bool freed = tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns);
-    if (freed) {
-      for (int i = lane; i < kBM; i += 32) {
-        __nv_bfloat16 p1, p2;
-        row_shift(rs, (int64_t)row0 + i, p1, p2);
-        __nv_bfloat16* e = reinterpret_cast<__nv_bfloat16*>(sm.Aext + i * 16);
-        e[3] = __hneg(p1);
-        e[4] = __hneg(p2);
-      }
-      tc::fence_proxy_async_smem();
+  // A tile and its extension block: wait until the previous unit's MMAs
+  // released them, then write the rows' -sigma terms (K columns 3, 4).
+  const bool freed = tc::mbar_wait(&sm.a_empty, (pp.unit & 1) ^ 1, timeout_ns);
+  if (freed) {
+    for (int i = lane; i < kBM; i += 32) {
+      __nv_bfloat16 p1, p2;
+      row_shift(u.rs, (int64_t)row0 + i, p1, p2);
+      __nv_bfloat16* e = reinterpret_cast<__nv_bfloat16*>(sm.Aext + i * 16);
+      e[3] = __hneg(p1);
+      e[4] = __hneg(p2);
     }
-    __syncwarp();
-    if (lane == 0) {
-      if (!freed) ok = false;
-      if (ok) {
-        tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK, TN>::kABytes);
-        tc_load_a<DK, TN>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
-      }
-      for (int i = 0; ok && i < ntiles; ++i) {
-        const int32_t brow = (t0 + i) * TN;
-        for (int c = 0; c < C; ++c) {
-          const uint32_t g = pp.chunk + i * C + c;
-          const uint32_t st = g % NS;
-          if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
-          const bool last = c == C - 1;
-          tc::mbar_arrive_expect_tx(&sm.full[st], TcCfg<DK, TN>::kStageBytes +
-                                                      (last ? TcCfg<DK, TN>::kBExtHalfBytes : 0));
-          tc_load_b_chunk<DK, TN>(sm.B[st], op.mapB, &sm.full[st], c, brow, op.padB);
-          if (last) {
-#pragma unroll
-            for (int h = 0; h < TN / 128; ++h)
-              tc::tma_load_2d(sm.Bext[st] + h * 128 * 16, op.mapBext, &sm.full[st], 0,
-                              op.extRow0 + brow + 128 * h);
-          }
-          pp.last_full_stage = st;
-          pp.last_full_parity = (g / NS) & 1;
-          pp.issued = 1;
-        }
-      }
-    }
-    __syncwarp();
-  } else if (warp == 1) {
-    if (lane == 0) {
-      if (!tc::mbar_wait(&sm.a_full, pp.unit & 1, timeout_ns)) ok = false;
-      for (int i = 0; ok && i < ntiles; ++i) {
-        const uint32_t gt = pp.tile + i;
-        const uint32_t b = gt % NB;
-        if (!tc::mbar_wait(&sm.tempty[b], ((gt / NB) & 1) ^ 1, timeout_ns)) { ok = false; break; }
-        const uint32_t d = sm.tmem_base + b * TN;
-        for (int c = 0; c < C; ++c) {
-          const uint32_t g = pp.chunk + i * C + c;
-          const uint32_t st = g % NS;
-          if (!tc::mbar_wait(&sm.full[st], (g / NS) & 1, timeout_ns)) { ok = false; break; }
-          tc::fence_after_sync();
-          tc_issue_chunk<DK, TN>(d, sm.A, sm.B[st], c, c == 0);
-          if (c == C - 1) tc_issue_ext<DK, TN>(d, sm.Aext, sm.Bext[st]);
-          tc::mma_commit(&sm.empty[st]);
-        }
-        if (!ok) break;
-        tc::mma_commit(&sm.tfull[b]);
-      }
-      if (ok) tc::mma_commit(&sm.a_empty);
-    }
-    __syncwarp();
-  } else {
-    // epilogue: warp e reads TMEM lane quarter q (its 32 rows) and column
-    // group cg (CW columns, two 32-column loads) of every tile
-    const int e = warp - 2;
-    const int q = warp & 3;
-    const int cg = e >> 2;
-    const int r = 32 * q + lane;
-    float mrun = kNegSentinel, lrun = 0.f, lcmp = 0.f;
-    __nv_bfloat16 p1, p2;
-    const float sigma = row_shift(rs, (int64_t)row0 + r, p1, p2);
-    const bool fast = rs.on;
-    for (int i = 0; ok && i < ntiles; ++i) {
-      const uint32_t g = pp.tile + i;
-      const uint32_t b = g % NB;
-      if (!tc::mbar_wait(&sm.tfull[b], (g / NB) & 1, timeout_ns)) {
-        ok = false;
-        break;
-      }
-      tc::fence_after_sync();
-      if (fast) {
-        // acc is the exponent less sigma_r: every term <= 1, no maxima.
-        // 16-column loads, the next issued before the current one is
-        // reduced; scalar sums into 8 accumulators; the polynomial pairs in
-        // packed arithmetic. Measured per 128 x 256 tile in the solve at
-        // n = m = 65536: 1808 cycles (2026 with two 32-column loads per
-        // tile and packed sums, 2059 before that).
-        const uint32_t tb = sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg;
-        float acc[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = 0.f;
-        auto reduce16 = [&](const float (&v)[16]) {
-#pragma unroll
-          for (int j = 0; j < 16; j += 8) {
-#pragma unroll
-            for (int k = 0; k < 8; k += 2) {
-              if (k >= 8 - OTTB_POLY_OF_8_TC_FAST) {
-                float e0, e1;
-                unpack2(exp2_poly2_d4(pack2(v[j + k], v[j + k + 1])), e0, e1);
-                acc[k] += e0;
-                acc[k + 1] += e1;
-              } else {
-                acc[k] += ex2_approx(v[j + k]);
-                acc[k + 1] += ex2_approx(v[j + k + 1]);
-              }
-            }
-          }
-        };
-        constexpr int NCH = CW / 16;  // 16-column loads per warp and tile (4 or 2)
-        static_assert(NCH >= 2 && CW % 16 == 0, "at least two 16-column loads per tile");
-        float va[16], vb[16];
-        tc::tmem_ld16(tb, va);
-        tc::tmem_ld_wait();
-#pragma unroll
-        for (int c = 0; c + 1 < NCH; ++c) {
-          float(&cur)[16] = (c & 1) ? vb : va;
-          float(&nxt)[16] = (c & 1) ? va : vb;
-          tc::tmem_ld16(tb + 16 * (c + 1), nxt);
-          reduce16(cur);
-          tc::tmem_ld_wait();
-        }
-        // The accumulator buffer can be refilled once every warp has read it.
-        tc::fence_before_sync();
-        __syncwarp();
-        if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
-        reduce16(((NCH - 1) & 1) ? vb : va);
-        two_sum_acc(lrun, lcmp,
-                    ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
-        continue;
-      }
-#pragma unroll 1
-      for (int h = 0; h < CW / 32; ++h) {
-        float v[32];
-        tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg + 32 * h, v);
-        tc::tmem_ld_wait();
-        if (h == CW / 32 - 1) {
-          // The accumulator buffer can be refilled once every warp has read it.
-          tc::fence_before_sync();
-          __syncwarp();
-          if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
-        }
-        // tree maximum (depth 4) instead of a 31-step dependent chain
-        float t11[11];
-#pragma unroll
-        for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
-        t11[10] = fmaxf(v[30], v[31]);
-        const float u0 = fmax3(t11[0], t11[1], t11[2]);
-        const float u1 = fmax3(t11[3], t11[4], t11[5]);
-        const float u2 = fmax3(t11[6], t11[7], t11[8]);
-        const float amax = fmaxf(fmax3(u0, u1, u2), fmaxf(t11[9], t11[10]));
-        const float cm = amax * s;  // s > 0
-        if (cm > mrun + kTau) {
-          const float sc = ex2_approx(mrun - cm);
-          lrun *= sc;
-          lcmp *= sc;
-          mrun = cm;
-        }
-        const float negm = -mrun;
-        // Packed pairs (v[j + 2k], v[j + 2k + 1]) in 4 accumulator pairs; of
-        // every 8 columns the last OTTB_POLY_OF_8_TC go to exp2_poly2 (FMA
-        // pipe), the rest to ex2.approx (MUFU).
-        const f32x2 s2 = pack2(s, s), m2 = pack2(negm, negm);
-        f32x2 acc[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) acc[k] = 0ull;
-#pragma unroll
-        for (int j = 0; j < 32; j += 8) {
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const f32x2 x = fma2(pack2(v[j + 2 * k], v[j + 2 * k + 1]), s2, m2);
-            f32x2 e;
-            if (2 * k >= 8 - OTTB_POLY_OF_8_TC) {
-              e = exp2_poly2(x);
-            } else {
-              float x0, x1;
-              unpack2(x, x0, x1);
-              e = pack2(ex2_approx(x0), ex2_approx(x1));
-            }
-            acc[k] = add2(acc[k], e);
-          }
-        }
-        float ta, tb;
-        unpack2(add2(add2(acc[0], acc[1]), add2(acc[2], acc[3])), ta, tb);
-        two_sum_acc(lrun, lcmp, ta + tb);
-      }
-    }
-    sm.part_m[cg][r] = fast ? sigma : mrun;
-    sm.part_l[cg][r] = lrun + lcmp;
+    tc::fence_proxy_async_smem();
   }
+  __syncwarp();
+  if (lane == 0) {
+    if (!freed) ok = false;
+    if (ok) {
+      tc::mbar_arrive_expect_tx(&sm.a_full, TcCfg<DK, TN>::kABytes);
+      tc_load_a<DK, TN>(sm.A, op.mapA, &sm.a_full, row0, op.padA);
+    }
+    for (int i = 0; ok && i < ntiles; ++i) {
+      const int32_t brow = (t0 + i) * TN;
+      for (int c = 0; c < C; ++c) {
+        const uint32_t g = pp.chunk + i * C + c;
+        const uint32_t st = g % NS;
+        if (!tc::mbar_wait(&sm.empty[st], ((g / NS) & 1) ^ 1, timeout_ns)) { ok = false; break; }
+        const bool last = c == C - 1;
+        tc::mbar_arrive_expect_tx(&sm.full[st], TcCfg<DK, TN>::kStageBytes +
+                                                    (last ? TcCfg<DK, TN>::kBExtHalfBytes : 0));
+        tc_load_b_chunk<DK, TN>(sm.B[st], op.mapB, &sm.full[st], c, brow, op.padB);
+        if (last) {
+#pragma unroll
+          for (int h = 0; h < TN / 128; ++h)
+            tc::tma_load_2d(sm.Bext[st] + h * 128 * 16, op.mapBext, &sm.full[st], 0,
+                            op.extRow0 + brow + 128 * h);
+        }
+        pp.last_full_stage = st;
+        pp.last_full_parity = (g / NS) & 1;
+        pp.issued = 1;
+      }
+    }
+  }
+  __syncwarp();
   pp.tile += ntiles;
   pp.chunk += ntiles * C;
   pp.unit += 1;
   if (!ok) atomicExch(&sm.err, 1);
-  __syncthreads();
-  if (threadIdx.x < kBM) {
-    float mv = sm.part_m[0][threadIdx.x], lv = sm.part_l[0][threadIdx.x];
-#pragma unroll
-    for (int k = 1; k < CG; ++k) lse_merge(mv, lv, sm.part_m[k][threadIdx.x], sm.part_l[k][threadIdx.x]);
-    sm.rm[threadIdx.x] = mv;
-    sm.rl[threadIdx.x] = lv;
+  return ok;
+}
+
+// MMA issuer (warp 1, all lanes; lane 0 issues).
+template <int DK, int TN>
+__device__ bool tc_mma(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u, uint64_t timeout_ns) {
+  constexpr int NS = TcCfg<DK, TN>::kStages;
+  constexpr int NB = TcCfg<DK, TN>::kTmemBufs;
+  constexpr int C = TcCfg<DK, TN>::kChunks;
+  const int lane = threadIdx.x & 31;
+  const int ntiles = u.t1 - u.t0;
+  bool ok = true;
+  if (lane == 0) {
+    if (!tc::mbar_wait(&sm.a_full, pp.unit & 1, timeout_ns)) ok = false;
+    for (int i = 0; ok && i < ntiles; ++i) {
+      const uint32_t gt = pp.tile + i;
+      const uint32_t b = gt % NB;
+      if (!tc::mbar_wait(&sm.tempty[b], ((gt / NB) & 1) ^ 1, timeout_ns)) { ok = false; break; }
+      const uint32_t d = sm.tmem_base + b * TN;
+      for (int c = 0; c < C; ++c) {
+        const uint32_t g = pp.chunk + i * C + c;
+        const uint32_t st = g % NS;
+        if (!tc::mbar_wait(&sm.full[st], (g / NS) & 1, timeout_ns)) { ok = false; break; }
+        tc::fence_after_sync();
+        tc_issue_chunk<DK, TN>(d, sm.A, sm.B[st], c, c == 0);
+        if (c == C - 1) tc_issue_ext<DK, TN>(d, sm.Aext, sm.Bext[st]);
+        tc::mma_commit(&sm.empty[st]);
+      }
+      if (!ok) break;
+      tc::mma_commit(&sm.tfull[b]);
+    }
+    if (ok) tc::mma_commit(&sm.a_empty);
   }
-  __syncthreads();
-  return sm.err == 0;
+  __syncwarp();
+  pp.tile += ntiles;
+  pp.chunk += ntiles * C;
+  pp.unit += 1;
+  if (!ok) atomicExch(&sm.err, 1);
+  return ok;
+}
+
+// Epilogue (warps 2-17): each warp's rows and column group of every tile
+// into sm.part_m / sm.part_l.
+template <int DK, int TN>
+__device__ bool tc_epilogue(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u,
+                            uint64_t timeout_ns) {
+  constexpr int NB = TcCfg<DK, TN>::kTmemBufs;
+  constexpr int C = TcCfg<DK, TN>::kChunks;
+  constexpr int CW = TcCfg<DK, TN>::kColsPerWarp;  // columns per epilogue warp per tile
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const RowShift& rs = u.rs;
+  const int32_t row0 = u.rb * kBM;
+  const int ntiles = u.t1 - u.t0;
+  const float s = u.r;
+  bool ok = true;
+  // epilogue: warp e reads TMEM lane quarter q (its 32 rows) and column
+  // group cg (CW columns, two 32-column loads) of every tile
+  const int e = warp - 2;
+  const int q = warp & 3;
+  const int cg = e >> 2;
+  const int r = 32 * q + lane;
+  float mrun = kNegSentinel, lrun = 0.f, lcmp = 0.f;
+  __nv_bfloat16 p1, p2;
+  const float sigma = row_shift(rs, (int64_t)row0 + r, p1, p2);
+  const bool fast = rs.on;
+  for (int i = 0; ok && i < ntiles; ++i) {
+    const uint32_t g = pp.tile + i;
+    const uint32_t b = g % NB;
+    if (!tc::mbar_wait(&sm.tfull[b], (g / NB) & 1, timeout_ns)) {
+      ok = false;
+      break;
+    }
+    tc::fence_after_sync();
+    if (fast) {
+      // acc is the exponent less sigma_r: every term <= 1, no maxima.
+      // 16-column loads, the next issued before the current one is
+      // reduced; scalar sums into 8 accumulators; the polynomial pairs in
+      // packed arithmetic. Measured per 128 x 256 tile in the solve at
+      // n = m = 65536: 1808 cycles (2026 with two 32-column loads per
+      // tile and packed sums, 2059 before that).
+      const uint32_t tb = sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg;
+      float acc[8];
+#pragma unroll
+      for (int k = 0; k < 8; ++k) acc[k] = 0.f;
+      auto reduce16 = [&](const float (&v)[16]) {
+#pragma unroll
+        for (int j = 0; j < 16; j += 8) {
+#pragma unroll
+          for (int k = 0; k < 8; k += 2) {
+            if (k >= 8 - OTTB_POLY_OF_8_TC_FAST) {
+              float e0, e1;
+              unpack2(exp2_poly2_d4(pack2(v[j + k], v[j + k + 1])), e0, e1);
+              acc[k] += e0;
+              acc[k + 1] += e1;
+            } else {
+              acc[k] += ex2_approx(v[j + k]);
+              acc[k + 1] += ex2_approx(v[j + k + 1]);
+            }
+          }
+        }
+      };
+      constexpr int NCH = CW / 16;  // 16-column loads per warp and tile (4 or 2)
+      static_assert(NCH >= 2 && CW % 16 == 0, "at least two 16-column loads per tile");
+      float va[16], vb[16];
+      tc::tmem_ld16(tb, va);
+      tc::tmem_ld_wait();
+#pragma unroll
+      for (int c = 0; c + 1 < NCH; ++c) {
+        float(&cur)[16] = (c & 1) ? vb : va;
+        float(&nxt)[16] = (c & 1) ? va : vb;
+        tc::tmem_ld16(tb + 16 * (c + 1), nxt);
+        reduce16(cur);
+        tc::tmem_ld_wait();
+      }
+      // The accumulator buffer can be refilled once every warp has read it.
+      tc::fence_before_sync();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
+      reduce16(((NCH - 1) & 1) ? vb : va);
+      two_sum_acc(lrun, lcmp,
+                  ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7])));
+      continue;
+    }
+#pragma unroll 1
+    for (int h = 0; h < CW / 32; ++h) {
+      float v[32];
+      tc::tmem_ld32(sm.tmem_base + ((uint32_t)(32 * q) << 16) + b * TN + CW * cg + 32 * h, v);
+      tc::tmem_ld_wait();
+      if (h == CW / 32 - 1) {
+        // The accumulator buffer can be refilled once every warp has read it.
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&sm.tempty[b]);
+      }
+      // tree maximum (depth 4) instead of a 31-step dependent chain
+      float t11[11];
+#pragma unroll
+      for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
+      t11[10] = fmaxf(v[30], v[31]);
+      const float u0 = fmax3(t11[0], t11[1], t11[2]);
+      const float u1 = fmax3(t11[3], t11[4], t11[5]);
+      const float u2 = fmax3(t11[6], t11[7], t11[8]);
+      const float amax = fmaxf(fmax3(u0, u1, u2), fmaxf(t11[9], t11[10]));
+      const float cm = amax * s;  // s > 0
+      if (cm > mrun + kTau) {
+        const float sc = ex2_approx(mrun - cm);
+        lrun *= sc;
+        lcmp *= sc;
+        mrun = cm;
+      }
+      const float negm = -mrun;
+      // Packed pairs (v[j + 2k], v[j + 2k + 1]) in 4 accumulator pairs; of
+      // every 8 columns the last OTTB_POLY_OF_8_TC go to exp2_poly2 (FMA
+      // pipe), the rest to ex2.approx (MUFU).
+      const f32x2 s2 = pack2(s, s), m2 = pack2(negm, negm);
+      f32x2 acc[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) acc[k] = 0ull;
+#pragma unroll
+      for (int j = 0; j < 32; j += 8) {
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const f32x2 x = fma2(pack2(v[j + 2 * k], v[j + 2 * k + 1]), s2, m2);
+          f32x2 e;
+          if (2 * k >= 8 - OTTB_POLY_OF_8_TC) {
+            e = exp2_poly2(x);
+          } else {
+            float x0, x1;
+            unpack2(x, x0, x1);
+            e = pack2(ex2_approx(x0), ex2_approx(x1));
+          }
+          acc[k] = add2(acc[k], e);
+        }
+      }
+      float ta, tb;
+      unpack2(add2(add2(acc[0], acc[1]), add2(acc[2], acc[3])), ta, tb);
+      two_sum_acc(lrun, lcmp, ta + tb);
+    }
+  }
+  sm.part_m[cg][r] = fast ? sigma : mrun;
+  sm.part_l[cg][r] = lrun + lcmp;
+  pp.tile += ntiles;
+  pp.chunk += ntiles * C;
+  pp.unit += 1;
+  if (!ok) atomicExch(&sm.err, 1);
+  return ok;
 }
 
 }  // namespace ottb
