@@ -31,7 +31,7 @@
 // rescaling, only 2^acc and the sums. Otherwise (first sweeps, epsilon
 // decay, large moves) sigma_r = 0 and the epilogue keeps running maxima.
 //
-// Warp roles in the 576-thread CTA:
+// Warp roles in the 640-thread CTA:
 //   warp 0      producer: the row shifts of a unit into A's extension block
 //               (all lanes), then (lane 0) the A tile once per unit; B tiles,
 //               one 64-wide K chunk (hi and lo) per shared-memory stage, and
@@ -40,8 +40,14 @@
 //   warp 1      TMEM owner and MMA issuer (lane 0): two 256-column
 //               accumulators (all of TMEM), so MMAs of tile t+1 overlap the
 //               epilogue of t.
-//   warps 2-17  epilogue: warp w reads TMEM lanes 32*(w%4).. (its rows) and
-//               the 64-column group (w-2)/4 of each tile and keeps a running
+//   warp 2      dealer: takes the sweep's work units (round-robin or from
+//               the sweep's atomic queue) and publishes each as a descriptor
+//               in a ring of kDescSlots slots in shared memory.
+//   warp 3      finalizer: merges the epilogue's per-row (shift, sum) of a
+//               unit, combines column splits and updates the rows'
+//               potentials, while the epilogue warps reduce the next unit.
+//   warps 4-19  epilogue: warp w reads TMEM lanes 32*(w%4).. (its rows) and
+//               the column group (w-4)/4 of each tile and keeps a running
 //               (shift, sum) of 2^acc per row.
 // Every wait is bounded; a timeout marks the CTA and unwinds.
 #pragma once
@@ -67,7 +73,10 @@ struct TcCfg {
   static constexpr int kColGroups = 4;    // epilogue warps per TMEM lane quarter
   static constexpr int kColsPerWarp = kTileN / kColGroups;
   static constexpr int kEpiWarps = 4 * kColGroups;
-  static constexpr int kThreads = 64 + 32 * kEpiWarps;
+  static constexpr int kCtrlWarps = 4;    // producer, MMA, dealer, finalizer
+  static constexpr int kEpiWarp0 = kCtrlWarps;
+  static constexpr int kThreads = 32 * (kCtrlWarps + kEpiWarps);
+  static constexpr int kDescSlots = 4;    // unit descriptors in flight
   static constexpr uint32_t kIdesc = tc::idesc_bf16_f32(128, kTileN);
   // extension blocks: R rows x 16 bf16, K-major without swizzle: K half 0
   // (elements 0-7) of all rows first, rows 16 B apart (8-row groups 128 B
@@ -118,12 +127,11 @@ struct TcSmem {
   // K = 16 extension blocks, no swizzle: [row groups][2 K halves][8 rows][8]
   uint8_t Aext[TcCfg<DK, TN>::kAExtBytes];
   uint8_t Bext[TcCfg<DK, TN>::kStages][TcCfg<DK, TN>::kBExtBytes];
-  TcUnit units[2];  // ring of unit descriptors (kernel_tc.cuh, tc_sweep)
-  float part_m[TcCfg<DK, TN>::kColGroups][kBM];
-  float part_l[TcCfg<DK, TN>::kColGroups][kBM];
-  float rm[kBM];
-  float rl[kBM];
-  double red[8];
+  TcUnit units[TcCfg<DK, TN>::kDescSlots];  // ring of unit descriptors
+  // per-row (shift, sum) of each column group, epilogue -> finalizer,
+  // double-buffered by unit
+  float part_m[2][TcCfg<DK, TN>::kColGroups][kBM];
+  float part_l[2][TcCfg<DK, TN>::kColGroups][kBM];
   uint64_t full[TcCfg<DK, TN>::kStages];
   uint64_t empty[TcCfg<DK, TN>::kStages];
   uint64_t tfull[TcCfg<DK, TN>::kTmemBufs];
@@ -131,14 +139,12 @@ struct TcSmem {
   uint64_t a_full;
   uint64_t a_empty;
   uint64_t drain;
-  uint64_t unit_full[2];   // a unit descriptor was written (the dealer arrives)
-  uint64_t unit_empty[2];  // the producer and MMA warps have read it
+  uint64_t unit_full[TcCfg<DK, TN>::kDescSlots];   // descriptor written (dealer)
+  uint64_t unit_empty[TcCfg<DK, TN>::kDescSlots];  // producer, MMA and finalizer done with it
+  uint64_t epi_done[2];   // the epilogue warps wrote part buffer b
+  uint64_t part_free[2];  // the finalizer has read part buffer b
   uint32_t tmem_base;
-  int unit;
-  int last;
   int err;
-  int deal_rr;      // the dealer's round-robin position in the current sweep
-  int deal_ended;   // the dealer has written the sweep's end marker
 };
 
 // Pipeline positions, one copy per thread, advanced identically by every
@@ -358,8 +364,9 @@ __device__ bool tc_mma(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u, uint64_t
   return ok;
 }
 
-// Epilogue (warps 2-17): each warp's rows and column group of every tile
-// into sm.part_m / sm.part_l.
+// Epilogue (warps 4-19): each warp's rows and column group of every tile
+// into part buffer (units so far) & 1 of sm.part_m / sm.part_l, handed to
+// the finalizer by epi_done.
 template <int DK, int TN>
 __device__ bool tc_epilogue(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u,
                             uint64_t timeout_ns) {
@@ -375,7 +382,7 @@ __device__ bool tc_epilogue(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u,
   bool ok = true;
   // epilogue: warp e reads TMEM lane quarter q (its 32 rows) and column
   // group cg (CW columns, two 32-column loads) of every tile
-  const int e = warp - 2;
+  const int e = warp - TcCfg<DK, TN>::kEpiWarp0;
   const int q = warp & 3;
   const int cg = e >> 2;
   const int r = 32 * q + lane;
@@ -497,8 +504,15 @@ __device__ bool tc_epilogue(TcSmem<DK, TN>& sm, TcPipe& pp, const TcUnit& u,
       two_sum_acc(lrun, lcmp, ta + tb);
     }
   }
-  sm.part_m[cg][r] = fast ? sigma : mrun;
-  sm.part_l[cg][r] = lrun + lcmp;
+  // the part buffer is free once the finalizer has read it two units ago
+  const uint32_t pb = pp.unit & 1;
+  if (ok && pp.unit >= 2 &&
+      !tc::mbar_wait(&sm.part_free[pb], ((pp.unit - 2) >> 1) & 1, timeout_ns))
+    ok = false;
+  sm.part_m[pb][cg][r] = fast ? sigma : mrun;
+  sm.part_l[pb][cg][r] = lrun + lcmp;
+  __syncwarp();
+  if (ok && lane == 0) tc::mbar_arrive(&sm.epi_done[pb]);
   pp.tile += ntiles;
   pp.chunk += ntiles * C;
   pp.unit += 1;

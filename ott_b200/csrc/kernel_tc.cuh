@@ -2,15 +2,15 @@
 // engine. One CTA per SM (its shared memory exceeds half an SM), so the
 // 512-column TMEM allocation never waits on another CTA.
 //
-// A sweep's work units run pipelined across units: the epilogue warps deal
-// the units (round-robin or from the sweep's atomic queue) and publish each
-// as a descriptor in a two-slot ring in shared memory; the producer and MMA
-// warps consume the descriptors in order, so they load the next unit's A
-// tile and B tiles and issue its MMAs while the epilogue warps still finish
-// the current unit (its last tiles, the column-group merge, the split
-// combine and the potential update, synchronised among the epilogue warps
-// by named barrier 1). Only the sweep's end, a grid barrier, joins all
-// warps.
+// A sweep's work units run pipelined across units and roles: the dealer
+// warp takes the units (round-robin or from the sweep's atomic queue) and
+// publishes each as a descriptor in a ring of four slots in shared memory;
+// the producer and MMA warps consume the descriptors in order, so they load
+// the next unit's A tile and B tiles and issue its MMAs while the epilogue
+// warps still reduce the current unit's last tiles; the finalizer warp
+// merges, combines and applies each unit's row results while the epilogue
+// warps reduce the next one. Only the sweep's end, a grid barrier, joins
+// all warps.
 #pragma once
 
 #include "engine_tc.cuh"
@@ -60,32 +60,184 @@ __device__ __forceinline__ RowShift bounded_row_shift(const ProbDev& P, const Sw
   return rs;
 }
 
+// The problem of unit u in a sweep's unit list: the last q with
+// prefix[q] <= u (prefix[count] = total > u), by a 32-way search over the
+// warp's lanes (two rounds for up to 1024 problems).
+__device__ __forceinline__ int warp_find_problem(const int* prefix, int count, int u) {
+  const int lane = threadIdx.x & 31;
+  int lo = 0, hi = count;
+  while (hi - lo > 1) {
+    const int step = (hi - lo + 31) >> 5;
+    const int idx = lo + lane * step;
+    const bool le = idx < hi && __ldcg(prefix + idx) <= u;
+    const unsigned bal = __ballot_sync(0xffffffffu, le);  // lane 0 (idx = lo) is set
+    lo += (31 - __clz(bal)) * step;
+    hi = min(hi, lo + step);
+  }
+  return lo;
+}
+
 // One sweep on the tensor cores (see the file comment). Returns false,
 // uniformly over the CTA, if any wait timed out.
 template <int DK, int TN>
 __device__ bool tc_sweep(const KernelArgs& A, const SweepParams& sp, unsigned sweep_idx,
                          TcSmem<DK, TN>& sm, TcPipe& pp) {
-  constexpr int kEpiThreads = TcCfg<DK, TN>::kEpiWarps * 32;
   constexpr int CG = TcCfg<DK, TN>::kColGroups;
-  using G = WarpGroup<64, kEpiThreads>;
+  constexpr uint32_t NSLOT = TcCfg<DK, TN>::kDescSlots;
   const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
   const volatile int* err = &sm.err;
   const uint64_t tmo = A.timeout_ns;
 
-  if (warp < 2) {
-    // producer (warp 0) and MMA issuer (warp 1): consume unit descriptors
-    // until this sweep's end marker
-    const int lane = threadIdx.x & 31;
-    bool ok = true;
-    while (ok) {
+  if (warp == 2) {
+    // dealer: every unit of this CTA, then the end marker
+    const int* ids = sp.final_eval ? A.eval_ids : A.active_ids;
+    const int* pre = sp.final_eval ? A.eval_prefix
+                                   : (A.prefix + (sp.kind == kSweepG ? 0 : A.num_problems + 1));
+    const int count = sp.final_eval ? ld_sched(&A.sched->num_eval)
+                                    : ld_sched(&A.sched->num_active);
+    const int total = sp.final_eval ? ld_sched(&A.sched->eval_units)
+                                    : ld_sched(&A.sched->total_units[sp.kind == kSweepG ? 0 : 1]);
+    const bool dynamic = ld_sched(&A.sched->dynamic_units) != 0;
+    unsigned* ctr = &A.gl->unit_ctr[sweep_idx % 3];
+    if (blockIdx.x == 0 && lane == 0) A.gl->unit_ctr[(sweep_idx + 1) % 3] = 0u;
+    int rr = blockIdx.x;
+    bool ended = false;
+    while (!ended) {
+      const uint32_t w = pp.wdesc++;
+      const uint32_t slot = w % NSLOT;
+      bool ok = w < NSLOT || tc::mbar_wait(&sm.unit_empty[slot], ((w - NSLOT) / NSLOT) & 1, tmo);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(&sm.err, 1);
+        break;
+      }
+      TcUnit& u = sm.units[slot];
+      int ui = 0;
+      if (lane == 0) ui = dynamic ? (int)atomicAdd(ctr, 1u) : rr;
+      ui = __shfl_sync(0xffffffffu, ui, 0);
+      rr += gridDim.x;
+      // after an error the end marker lets the other roles unwind at once
+      if (ui >= total || __any_sync(0xffffffffu, *err != 0)) {
+        ended = true;
+        if (lane == 0) u.end = 1;
+      } else {
+        const int q = warp_find_problem(pre, count, ui);
+        if (lane == 0) {
+          const int p = __ldcg(ids + q);
+          const ProbDev& P = A.probs[p];
+          const int local = ui - __ldcg(pre + q);
+          const int S = split_of(A.state[p], sp.kind);
+          u.end = 0;
+          u.p = p;
+          u.S = S;
+          u.rb = local / S;
+          u.sidx = local % S;
+          u.parity = sp.final_eval ? __ldcg(&A.state[p].final_parity) : sp.parity;
+          const int64_t cols = sp.kind == kSweepG ? P.n : P.m;
+          const int ntiles = (int)((cols + TN - 1) / TN);
+          u.t0 = (int)(((int64_t)ntiles * u.sidx) / S);
+          u.t1 = (int)(((int64_t)ntiles * (u.sidx + 1)) / S);
+          // The x layout carries the exponent scale of the target epsilon; a
+          // sweep at another epsilon scales the accumulator by ws / ws_t.
+          u.r = sweep_wscale(P, sp.mult) / P.ws_t;
+          u.op = make_tc_operands(P, sp.kind, u.parity);
+          u.rs = bounded_row_shift(P, sp);
+        }
+      }
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&sm.unit_full[slot]);
+    }
+  } else if (warp == 3) {
+    // finalizer: per unit, merge the column groups' (shift, sum) of each row
+    // (lane l: rows l + 32 k), combine the column splits of a row block
+    // (the CTA that completes its last split finishes it, as sweep_units)
+    // and update the rows' potentials
+    while (true) {
       const uint32_t d = pp.desc++;
-      const int slot = d & 1;
-      ok = __all_sync(0xffffffffu, tc::mbar_wait(&sm.unit_full[slot], (d >> 1) & 1, tmo));
-      if (!ok) break;
-      // read in place: the dealer rewrites this slot only after both warps
-      // arrive on unit_empty, which they do once they are done with the unit
+      const uint32_t slot = d % NSLOT;
+      bool ok = tc::mbar_wait(&sm.unit_full[slot], (d / NSLOT) & 1, tmo);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) atomicExch(&sm.err, 1);
+        break;
+      }
       const TcUnit& u = sm.units[slot];
-      bool stop = u.end || *err;
+      const bool stop = u.end != 0 || __any_sync(0xffffffffu, *err != 0);
+      if (!stop) {
+        const uint32_t pb = pp.unit & 1;
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(&sm.epi_done[pb], (pp.unit >> 1) & 1, tmo));
+        ++pp.unit;
+        if (!ok) {
+          if (lane == 0) atomicExch(&sm.err, 1);
+          break;
+        }
+        float mv[4], lv[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const int r = lane + 32 * k;
+          mv[k] = sm.part_m[pb][0][r];
+          lv[k] = sm.part_l[pb][0][r];
+#pragma unroll
+          for (int c = 1; c < CG; ++c) lse_merge(mv[k], lv[k], sm.part_m[pb][c][r], sm.part_l[pb][c][r]);
+        }
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&sm.part_free[pb]);
+        const ProbDev& P = A.probs[u.p];
+        const int64_t R = sp.kind == kSweepG ? P.m : P.n;
+        const int64_t rbase = (int64_t)u.rb * kBM;
+        bool do_final = true;
+        if (u.S > 1) {
+#pragma unroll
+          for (int k = 0; k < 4; ++k) {
+            const int64_t row = rbase + lane + 32 * k;
+            if (row < R) {
+              P.part_m[(int64_t)u.sidx * R + row] = mv[k];
+              P.part_l[(int64_t)u.sidx * R + row] = lv[k];
+            }
+          }
+          __threadfence();
+          __syncwarp();
+          int last = 0;
+          if (lane == 0) {
+            const int prev = atomicAdd(&P.arrive[u.rb], 1);
+            last = prev == u.S - 1;
+            if (last) atomicExch(&P.arrive[u.rb], 0);
+          }
+          do_final = __shfl_sync(0xffffffffu, last, 0) != 0;
+          if (do_final) {
+            __threadfence();
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              const int64_t row = rbase + lane + 32 * k;
+              mv[k] = kNegSentinel;
+              lv[k] = 0.f;
+              if (row < R) {
+                for (int j = 0; j < u.S; ++j)
+                  lse_merge(mv[k], lv[k], __ldcg(P.part_m + (int64_t)j * R + row),
+                            __ldcg(P.part_l + (int64_t)j * R + row));
+              }
+            }
+          }
+        }
+        if (do_final) finalize_rows_warp(P, sp, u.parity, u.rb, mv, lv, A.cfg.norm_error);
+      }
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&sm.unit_empty[slot]);
+      if (stop) break;
+    }
+  } else if (warp < 2) {
+    // producer (warp 0) and MMA issuer (warp 1)
+    while (true) {
+      const uint32_t d = pp.desc++;
+      const uint32_t slot = d % NSLOT;
+      bool ok = __all_sync(0xffffffffu, tc::mbar_wait(&sm.unit_full[slot], (d / NSLOT) & 1, tmo));
+      if (!ok) {
+        if (lane == 0) atomicExch(&sm.err, 1);
+        break;
+      }
+      // read in place: the dealer rewrites this slot only after this warp,
+      // the other control warp and the finalizer have arrived on unit_empty
+      const TcUnit& u = sm.units[slot];
+      const bool stop = u.end != 0 || __any_sync(0xffffffffu, *err != 0);
       if (!stop) {
         const bool r = warp == 0 ? tc_produce<DK, TN>(sm, pp, u, tmo)
                                  : tc_mma<DK, TN>(sm, pp, u, tmo);
@@ -93,131 +245,22 @@ __device__ bool tc_sweep(const KernelArgs& A, const SweepParams& sp, unsigned sw
       }
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&sm.unit_empty[slot]);
-      if (stop) break;
+      if (stop || !ok) break;
     }
-    if (!ok) atomicExch(&sm.err, 1);
   } else {
-    // epilogue warps: deal the units, reduce their tiles, finish each unit
-    const int t = G::tid();
-    const bool leader = t == 0;
-    // Writes the next descriptor into its ring slot (leader only; its
-    // round-robin position and end flag live in shared memory).
-    auto deal = [&]() -> bool {
-      if (sm.deal_ended) return true;
-      const int* ids = sp.final_eval ? A.eval_ids : A.active_ids;
-      const int* pre = sp.final_eval ? A.eval_prefix
-                                     : (A.prefix + (sp.kind == kSweepG ? 0 : A.num_problems + 1));
-      const int count = sp.final_eval ? ld_sched(&A.sched->num_eval)
-                                      : ld_sched(&A.sched->num_active);
-      const int total = sp.final_eval
-                            ? ld_sched(&A.sched->eval_units)
-                            : ld_sched(&A.sched->total_units[sp.kind == kSweepG ? 0 : 1]);
-      const uint32_t w = pp.wdesc;
-      const int slot = w & 1;
-      if (w >= 2 && !tc::mbar_wait(&sm.unit_empty[slot], ((w - 2) >> 1) & 1, tmo)) return false;
-      TcUnit& u = sm.units[slot];
-      const int ui = ld_sched(&A.sched->dynamic_units) != 0
-                         ? (int)atomicAdd(&A.gl->unit_ctr[sweep_idx % 3], 1u)
-                         : sm.deal_rr;
-      sm.deal_rr += gridDim.x;
-      if (ui >= total) {
-        u.end = 1;
-        sm.deal_ended = 1;
-      } else {
-        const int q = find_problem(pre, count, ui);
-        const int p = __ldcg(ids + q);
-        const ProbDev& P = A.probs[p];
-        const int local = ui - __ldcg(pre + q);
-        const int S = split_of(A.state[p], sp.kind);
-        u.end = 0;
-        u.p = p;
-        u.S = S;
-        u.rb = local / S;
-        u.sidx = local % S;
-        u.parity = sp.final_eval ? __ldcg(&A.state[p].final_parity) : sp.parity;
-        const int64_t cols = sp.kind == kSweepG ? P.n : P.m;
-        const int ntiles = (int)((cols + TN - 1) / TN);
-        u.t0 = (int)(((int64_t)ntiles * u.sidx) / S);
-        u.t1 = (int)(((int64_t)ntiles * (u.sidx + 1)) / S);
-        // The x layout carries the exponent scale of the target epsilon; a
-        // sweep at another epsilon scales the accumulator by ws / ws_t.
-        u.r = sweep_wscale(P, sp.mult) / P.ws_t;
-        u.op = make_tc_operands(P, sp.kind, u.parity);
-        u.rs = bounded_row_shift(P, sp);
-      }
-      ++pp.wdesc;
-      tc::mbar_arrive(&sm.unit_full[slot]);
-      return true;
-    };
-    if (leader) {
-      if (blockIdx.x == 0) A.gl->unit_ctr[(sweep_idx + 1) % 3] = 0u;
-      sm.deal_rr = blockIdx.x;
-      sm.deal_ended = 0;
-      if (!deal() || !deal()) atomicExch(&sm.err, 1);
-    }
+    // epilogue warps, each on its own: reduce every unit's tiles into the
+    // part buffers
     while (true) {
       const uint32_t d = pp.desc++;
-      const int slot = d & 1;
-      if (!tc::mbar_wait(&sm.unit_full[slot], (d >> 1) & 1, tmo)) atomicExch(&sm.err, 1);
-      // read in place: the dealer rewrites this slot only after this unit
+      const uint32_t slot = d % NSLOT;
+      bool ok = __all_sync(0xffffffffu, tc::mbar_wait(&sm.unit_full[slot], (d / NSLOT) & 1, tmo));
+      if (!ok) {
+        if (lane == 0) atomicExch(&sm.err, 1);
+        break;
+      }
       const TcUnit& u = sm.units[slot];
-      // err may be set by the producer or MMA warp at any time: the group
-      // decides together whether to stop
-      if (G::sync_or(*err != 0 || u.end != 0)) break;
-      tc_epilogue<DK, TN>(sm, pp, u, tmo);
-      if (G::sync_or(*err != 0)) break;
-      // the column groups' (shift, sum) of each row merged
-      if (t < kBM) {
-        float mv = sm.part_m[0][t], lv = sm.part_l[0][t];
-#pragma unroll
-        for (int k = 1; k < CG; ++k) lse_merge(mv, lv, sm.part_m[k][t], sm.part_l[k][t]);
-        sm.rm[t] = mv;
-        sm.rl[t] = lv;
-      }
-      G::sync();
-      // a row block split over S column ranges is finished by the CTA that
-      // completes its last range (as sweep_units)
-      const ProbDev& P = A.probs[u.p];
-      const int64_t R = sp.kind == kSweepG ? P.m : P.n;
-      bool do_final = true;
-      if (u.S > 1) {
-        const int64_t rbase = (int64_t)u.rb * kBM;
-        for (int i = t; i < kBM; i += kEpiThreads) {
-          if (rbase + i < R) {
-            P.part_m[(int64_t)u.sidx * R + rbase + i] = sm.rm[i];
-            P.part_l[(int64_t)u.sidx * R + rbase + i] = sm.rl[i];
-          }
-        }
-        __threadfence();
-        G::sync();
-        if (leader) {
-          const int prev = atomicAdd(&P.arrive[u.rb], 1);
-          sm.last = (prev == u.S - 1);
-          if (sm.last) atomicExch(&P.arrive[u.rb], 0);
-        }
-        G::sync();
-        do_final = sm.last != 0;
-        if (do_final) {
-          __threadfence();
-          for (int i = t; i < kBM; i += kEpiThreads) {
-            float mv = kNegSentinel, lv = 0.f;
-            if (rbase + i < R) {
-              for (int k = 0; k < u.S; ++k) {
-                const float m2 = __ldcg(P.part_m + (int64_t)k * R + rbase + i);
-                const float l2 = __ldcg(P.part_l + (int64_t)k * R + rbase + i);
-                lse_merge(mv, lv, m2, l2);
-              }
-            }
-            sm.rm[i] = mv;
-            sm.rl[i] = lv;
-          }
-          G::sync();
-        }
-      }
-      if (do_final)
-        finalize_rows_g<G>(P, sp, u.parity, u.rb, sm.rm, sm.rl, A.cfg.norm_error, sm.red);
-      G::sync();
-      if (leader && !deal()) atomicExch(&sm.err, 1);
+      if (u.end != 0 || __any_sync(0xffffffffu, *err != 0)) break;
+      if (!__all_sync(0xffffffffu, tc_epilogue<DK, TN>(sm, pp, u, tmo))) break;
     }
   }
   __syncthreads();
@@ -250,9 +293,13 @@ sinkhorn_tc_kernel(KernelArgs A) {
     tc::mbar_init(&sm.a_full, 1);
     tc::mbar_init(&sm.a_empty, 1);
     tc::mbar_init(&sm.drain, 1);
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < TcCfg<DK, TN>::kDescSlots; ++i) {
       tc::mbar_init(&sm.unit_full[i], 1);   // the dealer
-      tc::mbar_init(&sm.unit_empty[i], 2);  // producer and MMA warps
+      tc::mbar_init(&sm.unit_empty[i], 3);  // producer, MMA and finalizer warps
+    }
+    for (int i = 0; i < 2; ++i) {
+      tc::mbar_init(&sm.epi_done[i], NE);   // one arrival per epilogue warp
+      tc::mbar_init(&sm.part_free[i], 1);   // the finalizer
     }
     sm.err = 0;
     tc::fence_barrier_init();
