@@ -36,6 +36,8 @@ EXPORTED_SYMBOLS = (
     "ottb_sinkhorn_set_schedule",
     "ottb_apply_transport_workspace_size",
     "ottb_apply_transport",
+    "ottb_apply_transport_tc_workspace_size",
+    "ottb_apply_transport_tc",
     "ottb_apply_transport_sweep_workspace_size",
     "ottb_apply_transport_sweep",
     "ottb_apply_lse_kernel_workspace_size",
@@ -190,6 +192,11 @@ def load() -> ctypes.CDLL:
     lib.ottb_apply_transport.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, i32,
                                          i32, vp, vp, sz, vp]
     lib.ottb_apply_transport.restype = i32
+    lib.ottb_apply_transport_tc_workspace_size.argtypes = [i64, i64, i32, i32, i32]
+    lib.ottb_apply_transport_tc_workspace_size.restype = sz
+    lib.ottb_apply_transport_tc.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, i32,
+                                            i32, vp, vp, sz, vp]
+    lib.ottb_apply_transport_tc.restype = i32
     lib.ottb_apply_transport_sweep_workspace_size.argtypes = [i64, i64, i32, i32, i32, i32]
     lib.ottb_apply_transport_sweep_workspace_size.restype = sz
     lib.ottb_apply_transport_sweep.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp,

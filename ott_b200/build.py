@@ -60,6 +60,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
   if force or not up_to_date(OUT, deps):
     _nvcc_shared([os.path.join(CSRC, "capi.cu"), os.path.join(CSRC, "noalloc.cu"),
                   os.path.join(CSRC, "mlp.cu"), os.path.join(CSRC, "transport.cu"),
+                  os.path.join(CSRC, "transport_tc.cu"),
                   os.path.join(CSRC, "krylov.cu")], OUT,
                  verbose)
   peaks = os.path.join(CSRC, "peaks", "peaks.cu")

@@ -22,6 +22,7 @@
 #include "aux_kernels.cuh"
 #include "kernel_simt.cuh"
 #include "kernel_tc.cuh"
+#include "tmap.cuh"
 
 using namespace ottb;
 
@@ -109,27 +110,6 @@ KernelChoice pick_tc(int dk, int tn) {
   if (dk == 128 && tn == 256) { k.fn = TcKernel<128, 256>::fn(); k.smem = TcKernel<128, 256>::smem(); }
   if (dk == 128 && tn == 128) { k.fn = TcKernel<128, 128>::fn(); k.smem = TcKernel<128, 128>::smem(); }
   return k;
-}
-
-// cuTensorMapEncodeTiled, resolved through the runtime (no libcuda link).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled_fn() {
-  static std::mutex mu;
-  static EncodeTiledFn fn = nullptr;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeTiledFn)p;
-  }
-  return fn;
 }
 
 // Tensor map over a [2 * pad][dk] bf16 array (hi rows, then lo rows): boxes

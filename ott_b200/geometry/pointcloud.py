@@ -15,6 +15,11 @@ import torch
 from ott_b200 import _arrays, _lib
 from ott_b200.geometry import costs, geometry
 
+# Below these the tensor-core application's fixed cost (its log-sum-exp
+# pass and operand preparation) outweighs its faster products.
+TC_PRODUCT_MIN_VECTORS = 8
+TC_PRODUCT_MIN_ENTRIES = 1 << 22
+
 
 class PointCloud(geometry.Geometry):
   """Two point clouds ``x [n, d]`` and ``y [m, d]`` (``y=None`` uses ``x``).
@@ -147,6 +152,8 @@ class PointCloud(geometry.Geometry):
     sweep = {"bf16_split3": _lib.PRECISION_BF16_SPLIT3, "sweep_fp32": _lib.PRECISION_FP32}
     if precision == "auto" and self.dim >= 32:
       precision = "bf16_split3"
+    if precision == "bf16_split3_tc":
+      return self._apply_tc(fd, gd, v2, axis, out)
     if precision in sweep:
       code = sweep[precision]
       ws_bytes = _sweep_ws_bytes(n, m, self.dim, v2.shape[0], axis, code)
@@ -170,6 +177,23 @@ class PointCloud(geometry.Geometry):
     _lib.check(st, "ottb_apply_transport")
     return out
 
+  def _apply_tc(self, fd: torch.Tensor, gd: torch.Tensor, v2: torch.Tensor, axis: int,
+                out: torch.Tensor) -> torch.Tensor:
+    """``ottb_apply_transport_tc``: both products of the application on the
+    tensor cores (BF16 split-3, FP32 accumulation), for many vectors."""
+    lib = _lib.load()
+    n, m = self.shape
+    ws_bytes = int(lib.ottb_apply_transport_tc_workspace_size(n, m, self.dim, v2.shape[0], axis))
+    if ws_bytes == 0:
+      raise NotImplementedError("problem sizes not supported by ottb_apply_transport_tc")
+    ws = torch.empty(ws_bytes, dtype=torch.uint8, device=v2.device)
+    st = lib.ottb_apply_transport_tc(
+        self.x.data_ptr(), self.y.data_ptr(), n, m, self.dim, fd.data_ptr(), gd.data_ptr(),
+        ctypes.c_float(self.epsilon), ctypes.c_float(self.inv_scale_cost), v2.data_ptr(),
+        v2.shape[0], axis, out.data_ptr(), ws.data_ptr(), ws_bytes, _arrays.stream_handle())
+    _lib.check(st, "ottb_apply_transport_tc")
+    return out
+
   def _sweep_product(self, f: torch.Tensor, g: torch.Tensor, axis: int, precision: str,
                      num_vec: int = 1) -> Optional["_SweepProduct"]:
     """``_apply_raw`` on the sweep route planned once for fixed potentials
@@ -191,12 +215,18 @@ class PointCloud(geometry.Geometry):
     return _ApplyProduct(self, f, g, axis, num_vec)
 
   def apply_transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor, vec: Any,
-                                      axis: int = 0) -> torch.Tensor:
+                                      axis: int = 0, precision: str = "fp32") -> torch.Tensor:
     """Applies ``P_ij = exp((f_i + g_j - C_ij) / eps)`` to ``vec`` without
     forming P (geometry.py:444-486): ``axis=0`` sums over rows
     (``vec [..., n] -> [..., m]``), ``axis=1`` over columns
     (``vec [..., m] -> [..., n]``). ``vec`` may be 1-D or a batch.
-    Differentiable w.r.t. the points, ``f``, ``g`` and ``vec``."""
+    Differentiable w.r.t. the points, ``f``, ``g`` and ``vec``.
+
+    ``precision`` (not in the reference): "fp32" (FP32 on the CUDA cores),
+    or "bf16_split3" / "auto" (d >= 32), which takes batches of at least
+    ``TC_PRODUCT_MIN_VECTORS`` vectors on problems of at least
+    ``TC_PRODUCT_MIN_ENTRIES`` plan entries to the tensor cores
+    (``ottb_apply_transport_tc``) and the rest to FP32."""
     if axis not in (0, 1):
       raise ValueError("axis must be 0 or 1")
     n, m = self.shape
@@ -208,11 +238,24 @@ class PointCloud(geometry.Geometry):
       raise ValueError(f"vec has length {v2.shape[1]}, expected {n if axis == 0 else m}")
     f = _arrays.as_f32(f, dev)
     g = _arrays.as_f32(g, dev)
+    prec = self._product_precision(precision, v2.shape[0])
     if _needs_grad(self.x, self.y, f, g, v2):
-      out = _ApplyTransport.apply(self.x, self.y, f, g, v2, self, axis)
+      out = _ApplyTransport.apply(self.x, self.y, f, g, v2, self, axis, precision)
     else:
-      out = self._apply_raw(f, g, v2, axis)
+      out = self._apply_raw(f, g, v2, axis, prec)
     return out[0] if one else out.reshape(*v.shape[:-1], out.shape[-1])
+
+  def _product_precision(self, precision: str, num_vec: int) -> str:
+    """``_apply_raw``'s route for a batch of ``num_vec`` vectors under the
+    public ``precision`` of ``apply_transport_from_potentials``."""
+    if precision not in ("fp32", "auto", "bf16_split3"):
+      raise ValueError("precision must be 'fp32', 'auto' or 'bf16_split3'")
+    if precision == "fp32" or (precision == "auto" and self.dim < 32):
+      return "fp32"
+    n, m = self.shape
+    if num_vec >= TC_PRODUCT_MIN_VECTORS and n * m >= TC_PRODUCT_MIN_ENTRIES:
+      return "bf16_split3_tc"
+    return "fp32"
 
   def transport_from_potentials(self, f: torch.Tensor, g: torch.Tensor) -> torch.Tensor:
     """The plan ``[n, m]`` (geometry.py:361-365); differentiable w.r.t. the
@@ -258,7 +301,7 @@ class PointCloud(geometry.Geometry):
     return gx, gy
 
   def _plan_vjp(self, f: torch.Tensor, g: torch.Tensor, alpha: torch.Tensor,
-                beta: torch.Tensor, points: bool = True):
+                beta: torch.Tensor, points: bool = True, precision: str = "fp32"):
     """Backward of the plan for a cotangent of the low-rank form
     ``dL/dP = sum_t alpha_t beta_t^T`` (``alpha [T, n]``, ``beta [T, m]``),
     without forming P. Returns ``(gx, gy, u, w)`` in float64: ``u = P
@@ -272,9 +315,10 @@ class PointCloud(geometry.Geometry):
     d = self.dim
     T = alpha.shape[0]
     alpha, beta = alpha.double(), beta.double()
+    route = lambda k: self._product_precision(precision, k)  # noqa: E731
     if not points:
-      u = self._apply_raw(f, g, beta, 1).double()
-      w = self._apply_raw(f, g, alpha, 0).double()
+      u = self._apply_raw(f, g, beta, 1, route(T)).double()
+      w = self._apply_raw(f, g, alpha, 0, route(T)).double()
       return None, None, u, w
     x, y = self.x.detach().double(), self.y.detach().double()
     mean = self._scale_cost == "mean"
@@ -282,11 +326,13 @@ class PointCloud(geometry.Geometry):
     if mean:
       parts.append((beta * (y * y).sum(1)[None])[:, None, :])
     k_r = len(parts) - 1 + d
-    r = self._apply_raw(f, g, torch.cat(parts, 1).reshape(T * k_r, m), 1).double()
+    r = self._apply_raw(f, g, torch.cat(parts, 1).reshape(T * k_r, m), 1,
+                        route(T * k_r)).double()
     r = r.reshape(T, k_r, n)
     u, py = r[:, 0], r[:, 1:1 + d]
     c = self._apply_raw(f, g, torch.cat([alpha[:, None, :], alpha[:, None, :] * x.t()[None]],
-                                        1).reshape(T * (1 + d), n), 0).double()
+                                        1).reshape(T * (1 + d), n), 0,
+                        route(T * (1 + d))).double()
     c = c.reshape(T, 1 + d, m)
     w, ptx = c[:, 0], c[:, 1:]
     # G = dL/dC = -(1/eps) sum_t diag(alpha_t) P diag(beta_t)
@@ -445,9 +491,9 @@ class _ApplyTransport(torch.autograd.Function):
   (``PointCloud._plan_vjp``)."""
 
   @staticmethod
-  def forward(ctx, x, y, f, g, v2, geom, axis):  # pylint: disable=arguments-differ
-    out = geom._apply_raw(f, g, v2, axis)
-    ctx.geom, ctx.axis = geom, axis
+  def forward(ctx, x, y, f, g, v2, geom, axis, precision):  # pylint: disable=arguments-differ
+    out = geom._apply_raw(f, g, v2, axis, geom._product_precision(precision, v2.shape[0]))
+    ctx.geom, ctx.axis, ctx.precision = geom, axis, precision
     ctx.save_for_backward(f, g, v2)
     return out
 
@@ -461,12 +507,13 @@ class _ApplyTransport(torch.autograd.Function):
     W, V = gout.double(), v2.double()
     # axis 0: out_k = P^T v_k, dL/dP = sum_k v_k W_k^T; axis 1: out_k = P v_k
     alpha, beta = (V, W) if axis == 0 else (W, V)
-    gx, gy, u, w = geom._plan_vjp(f, g, alpha, beta, points=need[0] or need[1])
+    gx, gy, u, w = geom._plan_vjp(f, g, alpha, beta, points=need[0] or need[1],
+                                  precision=ctx.precision)
     gf = (alpha * u).sum(0) / eps
     gg = (beta * w).sum(0) / eps
     gv = u if axis == 0 else w
     return (_cast(gx, geom.x, need[0]), _cast(gy, geom.y, need[1]), _cast(gf, f, need[2]),
-            _cast(gg, g, need[3]), _cast(gv, v2, need[4]), None, None)
+            _cast(gg, g, need[3]), _cast(gv, v2, need[4]), None, None, None)
 
 
 class _TransportMatrix(torch.autograd.Function):

@@ -71,6 +71,7 @@ class SinkhornOutput(NamedTuple):
   inner_iterations: Optional[int] = None
   symmetric: bool = False  # solved with the symmetric update (f = g, x = y)
   use_danskin: bool = True  # gradient of reg_ot_cost with f, g held fixed
+  precision: str = "fp32"  # the solve's arithmetic; plan applications follow it
 
   def _res(self) -> _lib.OttbResult:
     results, k = self.reg_ot_cost_
@@ -232,8 +233,11 @@ class SinkhornOutput(NamedTuple):
 
   def apply(self, inputs: Any, axis: int = 0) -> torch.Tensor:
     """The plan applied to ``inputs`` (sinkhorn.py:455-469); ``axis=0``
-    maps ``[..., n]`` to ``[..., m]``, ``axis=1`` the transpose."""
-    return self.geom.apply_transport_from_potentials(self.f, self.g, inputs, axis=axis)
+    maps ``[..., n]`` to ``[..., m]``, ``axis=1`` the transpose. After a
+    tensor-core solve (precision "bf16_split3", or "auto" at d >= 32) large
+    batches of vectors are applied on the tensor cores too."""
+    return self.geom.apply_transport_from_potentials(self.f, self.g, inputs, axis=axis,
+                                                     precision=self.precision)
 
   def marginal(self, axis: int) -> torch.Tensor:
     """sinkhorn.py:471-472."""
@@ -628,7 +632,8 @@ class _Call:
                                 ot_prob=p, threshold=self.solver.threshold,
                                 inner_iterations=self.solver.inner_iterations,
                                 symmetric=bool(self.arr[k].symmetric),
-                                use_danskin=self.solver.use_danskin))
+                                use_danskin=self.solver.use_danskin,
+                                precision=self.solver.precision))
     return out
 
   def keep_alive(self, stream: torch.cuda.Stream) -> None:
