@@ -10,6 +10,10 @@
 //   S = s <A_r, B_c> + w_c - sigma_r      (M = 128 rows, N = 128 columns, K = d,
 //                                          + one K = 16 MMA for the shifts)
 //   O += 2^S V^T                           (M = 128 rows, N = vectors, K = 128 columns)
+// The second product's split is two MMAs per K slab, not three: the hi and
+// lo rows of V are stacked along N, so P_hi [V_hi | V_lo] fills two
+// accumulator halves at once, P_lo V_hi adds into the first, and O is the
+// sum of the halves (an MMA costs about the same from N = 16 to N = 128).
 // with s = 2 inv log2(e) / eps on A's centred points, w_c = (g_c - inv |B_c|^2)
 // log2(e) / eps and sigma_r the row's base-2 log-sum-exp, which the first
 // pass (ottb_apply_lse_kernel, one sweep of the solver's engine) provides.
@@ -23,18 +27,22 @@
 // in columns 32 (j / 2) + 8 (j % 2) (hi) and + 16 (lo)), so the second MMA
 // takes P straight from tensor memory as its A operand. Two S/P buffers
 // (TMEM columns 0-255) let the MMAs of tile t + 1 run while the epilogue
-// turns tile t into weights; O takes columns 256 up to 256 + 96.
+// turns tile t into weights; O's two halves take columns 256 up to 256 +
+// 2 * 96. (Measured at n = m = 65536, d = 64, 65 vectors: a third S/P
+// buffer, or loading the next tile's S before forming the current tile's
+// weights, made the kernel slower; stacking V's hi and lo rows saved a
+// quarter of its time.)
 //
-// Warp roles in the 576-thread CTA (one work unit: a 128-row block, a
+// Warp roles in the 608-thread CTA (one work unit: a 128-row block, a
 // range of 128-column tiles, a chunk of up to 96 vectors):
-//   warp 0      producer: the rows' shift block, the A tile, then per tile
+//   warp 0      producer of the rows' shift block, the A tile and per tile
 //               B (one 64-wide K chunk, hi and lo, per ring stage) with its
-//               shift rows, and V's hi and lo rows of the vector chunk (TMA,
-//               no multicast).
+//               shift rows (TMA, no multicast).
 //   warp 1      TMEM owner and MMA issuer (lane 0): S of tile t, then the
 //               P V MMAs of tile t - 1.
-//   warps 2-17  epilogue: warp w reads TMEM lanes 32 (w % 4).. and the
-//               column group (w - 2) / 4 of each tile; at the end the same
+//   warp 2      producer of V's hi and lo rows of the vector chunk, per tile.
+//   warps 3-18  epilogue: warp w reads TMEM lanes 32 (w % 4).. and the
+//               column group (w - 3) / 4 of each tile; at the end the same
 //               warps scale O and write it out (or a column split's part).
 // Every wait is bounded; a timeout sets the error flag and unwinds.
 #include <cuda_bf16.h>
@@ -54,9 +62,10 @@ namespace {
 
 constexpr int kAtcRows = 128;      // output rows per unit (MMA M)
 constexpr int kAtcCols = 128;      // summed columns per tile (S's N, P V's K)
-constexpr int kAtcWarps = 18;
+constexpr int kAtcWarps = 19;
 constexpr int kAtcThreads = 32 * kAtcWarps;
-constexpr int kAtcEpiWarp0 = 2;
+constexpr int kAtcEpiWarp0 = 3;
+constexpr int kAtcSBufs = 2;       // S/P buffers in TMEM (128 columns each)
 constexpr int kAtcStages = 2;      // B ring (one 64-wide K chunk per stage)
 constexpr int kAtcVStages = 2;     // V ring (one tile per stage)
 constexpr int kAtcSplitsMax = 32;
@@ -70,7 +79,7 @@ struct AtcCfg {
   static constexpr int kABytes = 2 * kChunks * kBlock;  // hi + lo, every chunk
   static constexpr int kStageBytes = 2 * kBlock;        // hi + lo of one chunk of 128 B rows
   static constexpr int kVBlock = kKvMax * 128;          // [kv][64] bf16 (one column half)
-  static constexpr int kVStageBytes = 4 * kVBlock;      // [part][half]
+  static constexpr int kVStageBytes = 4 * kVBlock;      // [half][part], KVP rows each
   static constexpr int kExtBytes = 128 * 16 * 2;        // K = 16 shift block, 128 rows
   static constexpr int kExtHalf = 128 * 16;             // its TMA-loaded K half
 };
@@ -84,7 +93,7 @@ struct AtcSmem {
   uint8_t Bext[kAtcStages][AtcCfg<DK>::kExtBytes];
   uint64_t bfull[kAtcStages], bempty[kAtcStages];
   uint64_t vfull[kAtcVStages], vempty[kAtcVStages];
-  uint64_t sfull[2], pfull[2];
+  uint64_t sfull[kAtcSBufs], pfull[kAtcSBufs];
   uint64_t a_full, ofull;
   uint32_t tmem_base;
   int err;
@@ -151,6 +160,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
   const int kv = min(a.KV, a.K - ch * a.KV);  // vectors of this chunk
   const uint32_t idesc_s = tc::idesc_bf16_f32(128, kAtcCols);
   const uint32_t idesc_o = tc::idesc_bf16_f32(128, a.KVP);
+  const uint32_t idesc_o2 = tc::idesc_bf16_f32(128, 2 * a.KVP);
   const uint32_t vbytes = 4u * (uint32_t)a.KVP * 128u;
 
   if (threadIdx.x == 0) {
@@ -162,7 +172,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
       tc::mbar_init(&sm.vfull[i], 1);
       tc::mbar_init(&sm.vempty[i], 1);
     }
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < kAtcSBufs; ++i) {
       tc::mbar_init(&sm.sfull[i], 1);
       tc::mbar_init(&sm.pfull[i], kAtcWarps - kAtcEpiWarp0);
     }
@@ -185,7 +195,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = sm.tmem_base;
-  const uint32_t tO = tbase + 2 * kAtcCols;
+  const uint32_t tO = tbase + kAtcSBufs * kAtcCols;
 
   bool ok = true;
   if (warp == 0) {
@@ -233,16 +243,24 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
                             (int32_t)(col + part * a.C_pad));
           if (last) tc::tma_load_2d(sm.Bext[st], &mapBext, &sm.bfull[st], 0, col);
         }
-        if (!ok) break;
+      }
+    }
+    __syncwarp();
+  } else if (warp == 2) {
+    // ---- producer of the vector tiles
+    if (lane == 0) {
+      for (int i = 0; ok && i < T; ++i) {
+        const int32_t col = (t0 + i) * kAtcCols;
         const uint32_t vs = i % kAtcVStages;
         if (!tc::mbar_wait(&sm.vempty[vs], ((i / kAtcVStages) & 1) ^ 1, a.timeout_ns)) {
           ok = false;
           break;
         }
         tc::mbar_arrive_expect_tx(&sm.vfull[vs], vbytes);
-        for (int part = 0; part < 2; ++part)
-          for (int h = 0; h < 2; ++h)
-            tc::tma_load_2d(sm.V[vs] + (part * 2 + h) * Cfg::kVBlock, &mapV, &sm.vfull[vs],
+        // block (column half h, part): the hi and lo rows of a half adjacent
+        for (int h = 0; h < 2; ++h)
+          for (int part = 0; part < 2; ++part)
+            tc::tma_load_2d(sm.V[vs] + (h * 2 + part) * a.KVP * 128, &mapV, &sm.vfull[vs],
                             col + 64 * h, (int32_t)(part * a.Kpad + (int64_t)ch * a.KVP));
       }
     }
@@ -252,11 +270,11 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
     if (lane == 0) {
       if (!tc::mbar_wait(&sm.a_full, 0, a.timeout_ns)) ok = false;
       const uint32_t a0 = tc::smem_u32(sm.A);
-      for (int i = 0; ok && i <= T; ++i) {
+      for (int i = 0; ok && i < T + kAtcSBufs - 1; ++i) {
         if (i < T) {
-          // S of tile i into buffer i & 1 (its P was consumed by the P V
+          // S of tile i into buffer i % 2 (its P was consumed by the P V
           // MMAs of tile i - 2, issued before these)
-          const uint32_t d = tbase + (i & 1) * kAtcCols;
+          const uint32_t d = tbase + (i % kAtcSBufs) * kAtcCols;
           for (int c = 0; ok && c < C; ++c) {
             const uint32_t g = i * C + c;
             const uint32_t st = g % kAtcStages;
@@ -282,13 +300,13 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
             tc::mma_commit(&sm.bempty[st]);
           }
           if (!ok) break;
-          tc::mma_commit(&sm.sfull[i & 1]);
+          tc::mma_commit(&sm.sfull[i % kAtcSBufs]);
         }
-        if (i >= 1) {
+        if (i >= kAtcSBufs - 1) {
           // O += P V^T for tile j = i - 1: P from TMEM, V from the ring
-          const int j = i - 1;
-          const uint32_t b = j & 1, vs = j % kAtcVStages;
-          if (!tc::mbar_wait(&sm.pfull[b], (j >> 1) & 1, a.timeout_ns) ||
+          const int j = i - (kAtcSBufs - 1);
+          const uint32_t b = j % kAtcSBufs, vs = j % kAtcVStages;
+          if (!tc::mbar_wait(&sm.pfull[b], (j / kAtcSBufs) & 1, a.timeout_ns) ||
               !tc::mbar_wait(&sm.vfull[vs], (j / kAtcVStages) & 1, a.timeout_ns)) {
             ok = false;
             break;
@@ -297,10 +315,9 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
           const uint32_t v0 = tc::smem_u32(sm.V[vs]);
           for (int s = 0; s < kAtcCols / 16; ++s) {
             const uint32_t ahi = tbase + b * kAtcCols + 32 * (s >> 1) + 8 * (s & 1);
-            const uint32_t vhi = v0 + (0 * 2 + (s >> 2)) * Cfg::kVBlock + (s & 3) * 32;
-            const uint32_t vlo = v0 + (1 * 2 + (s >> 2)) * Cfg::kVBlock + (s & 3) * 32;
-            tc::mma_bf16_ts(tO, ahi, tc::sw128_kmajor_desc(vhi), idesc_o, (j | s) ? 1u : 0u);
-            tc::mma_bf16_ts(tO, ahi, tc::sw128_kmajor_desc(vlo), idesc_o, 1u);
+            // V_hi rows of the slab's column half, its V_lo rows right after
+            const uint32_t vhi = v0 + (s >> 2) * 2 * a.KVP * 128 + (s & 3) * 32;
+            tc::mma_bf16_ts(tO, ahi, tc::sw128_kmajor_desc(vhi), idesc_o2, (j | s) ? 1u : 0u);
             tc::mma_bf16_ts(tO, ahi + 16, tc::sw128_kmajor_desc(vhi), idesc_o, 1u);
           }
           tc::mma_commit(&sm.vempty[vs]);
@@ -318,8 +335,8 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
     const int64_t row = (int64_t)rb * kAtcRows + 32 * q + lane;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
     for (int i = 0; ok && i < T; ++i) {
-      const uint32_t b = i & 1;
-      if (!tc::mbar_wait(&sm.sfull[b], (i >> 1) & 1, a.timeout_ns)) {
+      const uint32_t b = i % kAtcSBufs;
+      if (!tc::mbar_wait(&sm.sfull[b], (i / kAtcSBufs) & 1, a.timeout_ns)) {
         ok = false;
         break;
       }
@@ -361,9 +378,13 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
       }
       const float scf = (float)sc;
       for (int jc = cg; jc < a.KVP / 16; jc += 4) {
-        float o[16];
+        // O = its first half (P_hi V_hi + P_lo V_hi) + its second (P_hi V_lo)
+        float o[16], o2[16];
         tc::tmem_ld16(tO + lane_off + 16 * jc, o);
+        tc::tmem_ld16(tO + lane_off + a.KVP + 16 * jc, o2);
         tc::tmem_ld_wait();
+#pragma unroll
+        for (int t = 0; t < 16; ++t) o[t] += o2[t];
         if (row < a.R) {
 #pragma unroll
           for (int t = 0; t < 16; ++t) {

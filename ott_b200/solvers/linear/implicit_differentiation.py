@@ -494,7 +494,7 @@ class ImplicitDiff:
     beta2 = torch.where(sb, lb * self._derivative(geom, one(mb, sb)), zero)
     alpha = torch.stack([alpha1, torch.ones(n, dtype=torch.float64, device=dev)])
     beta = torch.stack([torch.ones(m, dtype=torch.float64, device=dev), beta2])
-    gx, gy, _, _ = geom._plan_vjp(f, g, alpha, beta, points=True)
+    gx, gy, _, _ = geom._plan_vjp(f, g, alpha, beta, points=True, precision=precision)
     ga = torch.where(a > 0, -la * self._derivative(geom, one(a, a > 0)), zero)
     gb = torch.where(b > 0, -lb * self._derivative(geom, one(b, b > 0)), zero)
     return gx, gy, ga, gb

@@ -432,10 +432,13 @@ def test_device_minres_matches_host_minres(case):
 def test_tensor_core_products_give_the_fp32_gradient():
   """Above 2^25 plan entries at d >= 32 the chosen precision runs the
   backward's one-vector products as planned zero-iteration solves on the
-  tensor-core sweep (``ottb_apply_transport_sweep_plan`` / ``_run``). At
+  tensor-core sweep (``ottb_apply_transport_sweep_plan`` / ``_run``) and
+  the pullback's many-vector products on ``ottb_apply_transport_tc``. At
   the same potentials and cotangent its input cotangents agree with those
-  of the FP32 products within 5e-3 of each one's largest entry (products
-  within ~1.5e-4 relative, amplified by the system's conditioning)."""
+  of the FP32 products within 1e-2 of each one's largest entry (products
+  within ~1.5e-4 relative, amplified by the system's conditioning; the
+  points' cotangents also carry the pullback products' BF16 split-3
+  exponent error, ~1e-3 in log2 units at this epsilon: measured 7.0e-3)."""
   import torch
   from ott_b200.geometry import pointcloud
   from ott_b200.problems.linear import linear_problem
@@ -457,4 +460,4 @@ def test_tensor_core_products_give_the_fp32_gradient():
   assert tc_steps > 0
   for got, want in zip(tc, ref):
     want = want.detach().cpu().numpy()
-    assert _rel(got, want) < 5e-3, _rel(got, want)
+    assert _rel(got, want) < 1e-2, _rel(got, want)
