@@ -222,6 +222,29 @@ def load_peaks_json():
     return None
 
 
+def bf16_peak_tflops():
+  """The measured cuBLAS bf16 burst peak (MEASURED_PEAKS.json) and its source,
+  else the 1.59 PFLOP/s fallback, an earlier B200 measurement."""
+  mp = load_peaks_json()
+  if mp and mp.get("bf16_tflops"):
+    return float(mp["bf16_tflops"]), "MEASURED_PEAKS.json bf16_tflops (burst)"
+  return 1590.0, "fallback: 1.59 PFLOP/s, an earlier B200 measurement (file absent)"
+
+
+def tc_apply_flops_per_entry(d, k):
+  """BF16 tensor flops that ottb_apply_transport_tc executes per plan entry
+  for k vectors: its log-sum-exp sweep and its cost tile (each 3 DK / 16 + 1
+  MMAs of K = 16, 2 flops per multiply-add) and the P V products of each
+  vector chunk (P_hi [V_hi | V_lo] and P_lo V_hi: 3 products of the chunk's
+  padded width); the cost tile is recomputed for every chunk."""
+  dk = 64 if d <= 64 else 128
+  kvmax = 96 if dk == 64 else 64
+  nch = -(-k // kvmax)
+  kvp = -(-(-(-k // nch)) // 16) * 16
+  cost = 2 * 16 * (3 * dk // 16 + 1)
+  return cost + nch * (cost + 2 * 3 * kvp)
+
+
 def ncu_traffic(name):
   """Per-launch DRAM bytes of a kernel from the committed ncu summary."""
   path = os.path.join(ROOT, "profiles", "traffic.json")
@@ -1030,19 +1053,34 @@ def run_divergence(args):
     fw.append(a)
     bw.append(b_)
   clk = clocks.stop()
+  gx, gy = xt.grad.clone(), yt.grad.clone()
+  step("fp32")  # warm-up of the FP32 arm
   pf, pb, pdiv, pout = step("fp32")
+  grad_diff = max(float((gx - xt.grad).abs().max() / xt.grad.abs().max()),
+                  float((gy - yt.grad).abs().max() / yt.grad.abs().max()))
   n, d = args.n, args.d
   iters = list(out.n_iters)
   fwd_s = statistics.median(fw) * 1e-3
   bwd_s = statistics.median(bw) * 1e-3
   # backward: 4 applications of an n x n plan to d + 1 vectors (2 for the
-  # (x, y) term, 1 for each symmetric term, whose plan is symmetric); per
-  # plan entry 2 d flops (cost) + 2 (d + 1) flops (P V) on the FP32 pipe
-  bwd_flops = 4.0 * n * n * (2 * d + 2 * (d + 1))
-  roof = {"bound": "fp32_fma", "kernel": "apply_transport_kernel",
-          "achieved": bwd_flops / bwd_s / 1e12, "peak": 2 * peaks["ffma_per_s"] / 1e12,
-          "unit": "TFLOP/s", "frac": bwd_flops / bwd_s / (2 * peaks["ffma_per_s"]),
-          "peak_source": "measured in bench.py (FFMA probe kernel)"}
+  # (x, y) term, 1 for each symmetric term, whose plan is symmetric). The
+  # chosen form runs each on ottb_apply_transport_tc: a log-sum-exp sweep
+  # and the product kernel, both tcgen05 BF16 split-3 (tensor flops per
+  # plan entry from tc_apply_flops_per_entry); FP32 (the plain arm): 2 d +
+  # 2 (d + 1) flops per entry on the FMA pipe
+  tc_flops = 4.0 * n * n * tc_apply_flops_per_entry(d, d + 1)
+  bf16_peak, bf16_src = bf16_peak_tflops()
+  roof = {"bound": "tensor", "kernel": "apply_tc_kernel + its log-sum-exp sweep",
+          "achieved": tc_flops / bwd_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
+          "frac": tc_flops / bwd_s / 1e12 / bf16_peak, "peak_source": bf16_src,
+          "work_per_backward": f"{tc_flops:.3e} BF16 tensor flops (4 applications to "
+                               f"{d + 1} vectors, split-3 products)"}
+  fp32_flops = 4.0 * n * n * (2 * d + 2 * (d + 1))
+  roof_fp32 = {"bound": "fp32_fma", "kernel": "apply_pipelined_kernel",
+               "achieved": fp32_flops / (pb * 1e-3) / 1e12,
+               "peak": 2 * peaks["ffma_per_s"] / 1e12, "unit": "TFLOP/s",
+               "frac": fp32_flops / (pb * 1e-3) / (2 * peaks["ffma_per_s"]),
+               "peak_source": "measured in bench.py (FFMA probe kernel)"}
   line = {
       "metric": "s per Sinkhorn divergence (3 solves to 1e-3 in one launch) and its gradient",
       "value": fwd_s + bwd_s, "unit": "s", "higher_is_better": False, "n_gpus": 1,
@@ -1053,9 +1091,11 @@ def run_divergence(args):
                  "l2": "flushed before each step (256 MiB write)"},
       "forward_s": fwd_s, "backward_s": bwd_s, "divergence": div, "n_iters": iters,
       "plain_fp32": {"forward_s": pf * 1e-3, "backward_s": pb * 1e-3, "divergence": pdiv,
-                     "n_iters": list(pout.n_iters)},
+                     "n_iters": list(pout.n_iters), "roofline_backward": roof_fp32},
       "divergence_rel_diff_vs_fp32": abs(div - pdiv) / abs(pdiv),
+      "grad_rel_diff_vs_fp32": grad_diff,
       "speedup_forward_vs_plain_fp32": pf * 1e-3 / fwd_s,
+      "speedup_backward_vs_plain_fp32": pb * 1e-3 / bwd_s,
       "roofline_backward": roof, "clocks": clk,
   }
   print(json.dumps(line))
