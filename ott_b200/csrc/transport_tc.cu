@@ -438,22 +438,34 @@ struct AtcPrep {
 
 // Common centre of both point sets: the mean of up to 256 points of each
 // at a fixed stride (any centre gives the same plan; a central one keeps
-// the expanded |a|^2 + |b|^2 - 2 <a, b> small).
+// the expanded |a|^2 + |b|^2 - 2 <a, b> small). One CTA per coordinate,
+// one sample per thread, a fixed-order tree sum.
 __global__ void atc_center_kernel(AtcPrep p) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
+  __shared__ float red[2][8];
+  const int k = blockIdx.x, t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int64_t na = p.R < 256 ? p.R : 256, nb = p.C < 256 ? p.C : 256;
   const int64_t sa = p.R / na, sb = p.C / nb;
-  for (int k = warp; k < p.DK; k += warps) {
-    float ma = 0.f, mb = 0.f;
-    if (k < p.d) {
-      for (int64_t i = lane; i < na; i += 32) ma += p.A[i * sa * p.d + k];
-      for (int64_t i = lane; i < nb; i += 32) mb += p.B[i * sb * p.d + k];
+  float ma = 0.f, mb = 0.f;
+  if (k < p.d) {
+    if (t < na) ma = p.A[t * sa * p.d + k];
+    if (t < nb) mb = p.B[t * sb * p.d + k];
+  }
+  for (int off = 16; off > 0; off >>= 1) {
+    ma += __shfl_xor_sync(0xffffffffu, ma, off);
+    mb += __shfl_xor_sync(0xffffffffu, mb, off);
+  }
+  if (lane == 0) {
+    red[0][warp] = ma;
+    red[1][warp] = mb;
+  }
+  __syncthreads();
+  if (t == 0) {
+    float sa2 = 0.f, sb2 = 0.f;
+    for (int w = 0; w < 8; ++w) {
+      sa2 += red[0][w];
+      sb2 += red[1][w];
     }
-    for (int off = 16; off > 0; off >>= 1) {
-      ma += __shfl_xor_sync(0xffffffffu, ma, off);
-      mb += __shfl_xor_sync(0xffffffffu, mb, off);
-    }
-    if (lane == 0) p.cen[k] = k < p.d ? 0.5f * (ma / (float)na + mb / (float)nb) : 0.f;
+    p.cen[k] = k < p.d ? 0.5f * (sa2 / (float)na + sb2 / (float)nb) : 0.f;
   }
 }
 
@@ -674,7 +686,7 @@ extern "C" int32_t ottb_apply_transport_tc(const float* x, const float* y, int64
                              OTTB_PRECISION_AUTO, lse, ws + L.lse_ws, L.lse_ws_bytes, stream);
   if (st != OTTB_OK) return st;
 
-  atc_center_kernel<<<1, 256, 0, stream>>>(p);
+  atc_center_kernel<<<L.DK, 256, 0, stream>>>(p);
   {
     const int64_t warps = std::max(L.R_pad, L.C_pad);
     dim3 grid((unsigned)((warps * 32 + 255) / 256), 2);
