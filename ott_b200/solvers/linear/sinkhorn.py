@@ -16,6 +16,7 @@ from __future__ import annotations
 
 import ctypes
 import math
+import time
 from typing import Any, List, NamedTuple, Optional, Sequence, Tuple
 
 import torch
@@ -507,8 +508,12 @@ class _Call:
   def __init__(self, probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
                inits: Optional[Sequence[Optional[Tuple[Any, Any]]]],
                f_from_g: Optional[bool], init_kwargs: dict,
-               symmetric: Optional[Sequence[bool]] = None):
+               symmetric: Optional[Sequence[bool]] = None, live_errors: bool = False):
     self.lib = _lib.load()
+    # live_errors: the kernel writes each block's error into pinned host
+    # memory (device-accessible under unified addressing) that the host
+    # reads while the solve runs; copied to the device buffers afterwards
+    self.host_errors: List[torch.Tensor] = []
     self.probs = list(probs)
     self.solver = solver
     inits = list(inits) if inits is not None else [None] * len(probs)
@@ -561,7 +566,12 @@ class _Call:
       q.g_init = None if gi is None else gi.data_ptr()
       q.f = f.data_ptr()
       q.g = g.data_ptr()
-      q.errors = errors.data_ptr()
+      if live_errors:
+        host = torch.full((max(outer, 1),), -1.0, dtype=torch.float32, pin_memory=True)
+        self.host_errors.append(host)
+        q.errors = host.data_ptr()
+      else:
+        q.errors = errors.data_ptr()
       q.n = n
       q.m = m
       q.epsilon = float(p.geom.epsilon)
@@ -670,15 +680,16 @@ def run_batch(probs: Sequence[linear_problem.LinearProblem], solver: Sinkhorn,
   """
   if not probs:
     return []
-  call = _Call(probs, solver, inits, f_from_g, init_kwargs, symmetric)
+  live = solver.progress_fn is not None
+  call = _Call(probs, solver, inits, f_from_g, init_kwargs, symmetric, live_errors=live)
   stream = _arrays.stream_handle()
   if solver.autotune:
     call.autotune(stream)
   call.solve(stream)
+  if live:
+    _live_progress(solver, call)
   out = call.outputs()
   call.keep_alive(torch.cuda.current_stream())
-  if solver.progress_fn is not None:
-    _replay_progress(solver, out)
   return out
 
 
@@ -742,14 +753,45 @@ class SinkhornGraph:
     return out
 
 
-def _replay_progress(solver: Sinkhorn, outs: List[SinkhornOutput]) -> None:
-  """Calls ``progress_fn`` once per recorded block after the solve.
+class _LiveState(NamedTuple):
+  """The solver state a live ``progress_fn`` call sees: the errors buffer so
+  far (-1 where a block has not been reached, sinkhorn.py:1008-1013)."""
+  errors: torch.Tensor
 
-  The reference calls it from inside the loop every iteration
-  (sinkhorn.py:933-937); the persistent kernel does not return to the host
-  mid-solve, so the per-block errors are replayed afterwards with the final
-  potentials in the state.
-  """
+
+def _live_progress(solver: Sinkhorn, call: "_Call", poll_s: float = 2e-4) -> None:
+  """Calls ``progress_fn`` while the solve runs, as the reference does from
+  inside its loop (sinkhorn.py:933-937): the persistent kernel writes each
+  block's error into pinned host memory as the block ends; this polls it
+  until the solve's stream work completes and makes one call per new block
+  of each problem, in block order, then copies the errors into the
+  outputs' device buffers."""
+  done = torch.cuda.Event()
+  done.record()
+  inner = solver.inner_iterations
+  seen = [0] * len(call.host_errors)
+  while True:
+    finished = done.query()
+    for k, host in enumerate(call.host_errors):
+      errs = host.numpy()
+      nb = seen[k]
+      while nb < errs.shape[0] and errs[nb] != -1.0:
+        nb += 1
+      for blk in range(seen[k], nb):
+        state = _LiveState(errors=host.clone())
+        solver.progress_fn(((blk + 1) * inner - 1, inner, solver.max_iterations, state))
+      seen[k] = nb
+    if finished:
+      break
+    time.sleep(poll_s)
+  for (_, _, dev_err), host in zip(call.bufs, call.host_errors):
+    dev_err.copy_(host[:dev_err.shape[0]], non_blocking=True)
+
+
+def _replay_progress(solver: Sinkhorn, outs: List[SinkhornOutput]) -> None:
+  """Calls ``progress_fn`` once per recorded block after a replayed CUDA
+  graph (``SinkhornGraph``), with the final potentials in the state; direct
+  solves call it live (``_live_progress``)."""
   for o in outs:
     errs = o.errors.cpu()
     for blk in range(int((errs != -1).sum())):

@@ -1,10 +1,12 @@
 """Progress callbacks for ``Sinkhorn(progress_fn=...)`` (ott/utils.py:105-231).
 
 The callbacks receive ``(iteration, inner_iterations, max_iterations,
-state)`` with ``state.errors`` the errors buffer; here the solver calls them
-after its single launch, once per error block (the iterations
+state)`` with ``state.errors`` the errors buffer so far (-1 where a block
+has not been reached). The solver calls them while its persistent launch
+runs, once per error block as the block ends (the iterations
 ``inner_iterations - 1``, ``2 inner_iterations - 1``, ...), which are the
-calls on which these callbacks act in the reference too.
+calls on which these callbacks act in the reference too; the kernel writes
+each block's error into pinned host memory, which the calling thread polls.
 """
 from __future__ import annotations
 

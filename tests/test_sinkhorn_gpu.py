@@ -258,3 +258,34 @@ def test_progress_callbacks():
                                                           stream=stream),
                min_iterations=0, inner_iterations=7, max_iterations=14)
   assert stream.getvalue().startswith("foo 7/14"), stream.getvalue()
+
+
+def test_progress_callbacks_run_while_the_solve_runs():
+  """progress_fn is called live, from the errors the persistent kernel
+  writes into pinned host memory at each block's end (the reference calls
+  it from inside its loop, sinkhorn.py:933-937): the first calls come
+  while the solve's stream is still busy, every block is reported once and
+  in order, each call's state holds that block's error, and the output's
+  errors (device) equal what the calls saw."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.solvers import linear
+  n, d = 16384, 64
+  x, y, _, _ = problems.gaussian_shift_problem(n, n, d, seed=4)
+  geom = pointcloud.PointCloud(torch.as_tensor(x).cuda(), torch.as_tensor(y).cuda(),
+                               epsilon=0.002, relative_epsilon="mean")
+  calls = []
+
+  def progress_fn(status):
+    iteration, inner, total, state = status
+    blk = (int(iteration) + 1) // int(inner) - 1
+    calls.append((int(iteration), float(state.errors[blk]),
+                  bool(torch.cuda.current_stream().query())))
+
+  out = linear.solve(geom, progress_fn=progress_fn, threshold=1e-12, inner_iterations=10,
+                     max_iterations=600)
+  assert [c[0] for c in calls] == [10 * k + 9 for k in range(60)]
+  assert not calls[0][2], "the first call came after the solve had finished"
+  errs = out.errors.cpu().numpy()
+  np.testing.assert_array_equal(errs, np.array([c[1] for c in calls], dtype=np.float32))
+  assert out.n_iters == 600
