@@ -398,6 +398,14 @@ int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x,
 int32_t ottb_mlp_adam(const ottb_mlp* net, float lr, float beta1, float beta2,
                       float eps, int32_t step, void* stream);
 
+/* The same step with the learning rate and the bias corrections read from
+ * device memory, hyper = {lr, 1 - beta1^step, 1 - beta2^step}, so that a
+ * training step can be captured once in a CUDA graph and replayed with a
+ * different row of a schedule each time (meta_initializer.py:101-135,
+ * the update). */
+int32_t ottb_mlp_adam_device(const ottb_mlp* net, const float* hyper, float beta1,
+                             float beta2, float eps, void* stream);
+
 /* Refreshes the bf16 copies (w_bf16, wt_bf16) from the FP32 weights. */
 int32_t ottb_mlp_sync_bf16(const ottb_mlp* net, void* stream);
 

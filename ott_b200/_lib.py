@@ -57,6 +57,7 @@ EXPORTED_SYMBOLS = (
     "ottb_mlp_forward",
     "ottb_mlp_gradients",
     "ottb_mlp_adam",
+    "ottb_mlp_adam_device",
     "ottb_mlp_sync_bf16",
     "ottb_status_string",
     "ottb_version",
@@ -241,6 +242,8 @@ def load() -> ctypes.CDLL:
     lib.ottb_mlp_gradients.restype = i32
     lib.ottb_mlp_adam.argtypes = [mlp, f32, f32, f32, f32, i32, vp]
     lib.ottb_mlp_adam.restype = i32
+    lib.ottb_mlp_adam_device.argtypes = [mlp, vp, f32, f32, f32, vp]
+    lib.ottb_mlp_adam_device.restype = i32
     lib.ottb_mlp_sync_bf16.argtypes = [mlp, vp]
     lib.ottb_mlp_sync_bf16.restype = i32
     lib.ottb_status_string.argtypes = [i32]

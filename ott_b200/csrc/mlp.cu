@@ -43,12 +43,13 @@ EncodeFn encode_fn() {
 }
 
 // [rows][cols] bf16, K = cols contiguous: boxes 64 x 128, 128-byte swizzle.
-bool operand_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols) {
+bool operand_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols,
+                 uint32_t box_rows = 128) {
   EncodeFn fn = encode_fn();
   if (!fn) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {64, 128};
+  const cuuint32_t box[2] = {64, box_rows};
   const cuuint32_t estr[2] = {1, 1};
   return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
             estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
@@ -56,22 +57,38 @@ bool operand_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols)
          CUDA_SUCCESS;
 }
 
-size_t gemm_smem() { return sizeof(GemmSmem) + 1024; }
+template <int TN>
+size_t gemm_smem() { return sizeof(GemmSmem<TN>) + 1024; }
 
-// D[M, N] = A[M, K] B[N, K]^T with the given epilogue.
-int gemm(const void* A, const void* B, GemmArgs g, cudaStream_t stream) {
-  if (g.M % 128 || g.N % 128 || g.K % 64 || g.K < 64) return OTTB_ERR_UNSUPPORTED;
-  CUtensorMap ma, mb;
-  if (!operand_map(&ma, A, g.M, g.K) || !operand_map(&mb, B, g.N, g.K)) return OTTB_ERR_CUDA;
+template <int TN>
+int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, const GemmArgs& g,
+                cudaStream_t stream) {
   static std::once_flag once;
   static cudaError_t attr = cudaSuccess;
   std::call_once(once, [] {
-    attr = cudaFuncSetAttribute((const void*)gemm_bf16_tc_kernel,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)gemm_smem());
+    attr = cudaFuncSetAttribute((const void*)gemm_bf16_tc_kernel<TN>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)gemm_smem<TN>());
   });
   if (attr != cudaSuccess) return OTTB_ERR_CUDA;
-  gemm_bf16_tc_kernel<<<dim3(g.N / 128, g.M / 128), 192, gemm_smem(), stream>>>(ma, mb, g);
+  gemm_bf16_tc_kernel<TN><<<dim3(g.N / TN, g.M / 128), 192, gemm_smem<TN>(), stream>>>(ma, mb, g);
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+// D[M, N] = A[M, K] B[N, K]^T with the given epilogue. The tile width is
+// the widest of 128, 64, 32 columns that still gives 96 or more CTAs (all
+// three when M N is small), since one 128 x 128 tile per CTA leaves most
+// of the 148 SMs idle on the batch-512 layers.
+int gemm(const void* A, const void* B, GemmArgs g, cudaStream_t stream) {
+  if (g.M % 128 || g.N % 128 || g.K % 64 || g.K < 64) return OTTB_ERR_UNSUPPORTED;
+  const int64_t tiles128 = (int64_t)(g.M / 128) * (g.N / 128);
+  const int tn = tiles128 >= 96 ? 128 : tiles128 * 2 >= 96 ? 64 : 32;
+  CUtensorMap ma, mb;
+  if (!operand_map(&ma, A, g.M, g.K) || !operand_map(&mb, B, g.N, g.K, (uint32_t)tn))
+    return OTTB_ERR_CUDA;
+  if (tn == 128) return launch_gemm<128>(ma, mb, g, stream);
+  if (tn == 64) return launch_gemm<64>(ma, mb, g, stream);
+  return launch_gemm<32>(ma, mb, g, stream);
 }
 
 // Workspace layout of one batch: input, activations, gradients.
@@ -213,7 +230,7 @@ int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x, const float* tar
     gw.out_f32 = ly.w_grad;
     st = gemm(dzt, actt, gw, stream);
     if (st != OTTB_OK) return st;
-    colsum_bf16_kernel<<<(ly.out + 255) / 256, 256, 0, stream>>>(
+    colsum_bf16_kernel<<<(ly.out + 63) / 64, 256, 0, stream>>>(
         (const __nv_bfloat16*)dz, batch, ly.out, ly.b_grad);
     if (l == 0) break;
     // dz_{l-1}[B, in] = (dz_l [B, out] x W_l^T ... as A B^T with B = W_l^T [in, out])
@@ -230,26 +247,46 @@ int32_t ottb_mlp_gradients(const ottb_mlp* net, const float* x, const float* tar
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }
 
-int32_t ottb_mlp_adam(const ottb_mlp* net, float lr, float beta1, float beta2, float eps,
-                      int32_t step, void* stream_ptr) {
-  if (!net || net->num_layers < 1 || net->num_layers > OTTB_MLP_MAX_LAYERS || step < 1)
+}  // extern "C"
+
+namespace {
+
+int adam_all(const ottb_mlp* net, float lr, float beta1, float beta2, float eps, float c1,
+             float c2, const float* hyper, cudaStream_t stream) {
+  if (!net || net->num_layers < 1 || net->num_layers > OTTB_MLP_MAX_LAYERS)
     return OTTB_ERR_INVALID;
-  cudaStream_t stream = (cudaStream_t)stream_ptr;
-  const float c1 = 1.f - powf(beta1, (float)step);
-  const float c2 = 1.f - powf(beta2, (float)step);
   for (int l = 0; l < net->num_layers; ++l) {
     const ottb_mlp_layer& ly = net->layers[l];
     if (!ly.w || !ly.w_m || !ly.w_v || !ly.w_grad || !ly.b || !ly.b_m || !ly.b_v || !ly.b_grad)
       return OTTB_ERR_INVALID;
-    const int64_t nw = (int64_t)ly.out * ly.in;
-    adam_kernel<<<(unsigned)std::min<int64_t>((nw + 255) / 256, 4096), 256, 0, stream>>>(
-        ly.w, ly.w_m, ly.w_v, ly.w_grad, nw, ly.in, lr, beta1, beta2, eps, c1, c2,
-        (__nv_bfloat16*)ly.w_bf16, (__nv_bfloat16*)ly.wt_bf16, ly.out);
-    adam_kernel<<<(ly.out + 255) / 256, 256, 0, stream>>>(ly.b, ly.b_m, ly.b_v, ly.b_grad,
-                                                          ly.out, ly.out, lr, beta1, beta2, eps,
-                                                          c1, c2, nullptr, nullptr, 1);
+    const dim3 block(32, 8);
+    adam_kernel<<<dim3((ly.in + 31) / 32, (ly.out + 31) / 32), block, 0, stream>>>(
+        ly.w, ly.w_m, ly.w_v, ly.w_grad, ly.out, ly.in, lr, beta1, beta2, eps, c1, c2, hyper,
+        (__nv_bfloat16*)ly.w_bf16, (__nv_bfloat16*)ly.wt_bf16);
+    adam_kernel<<<dim3((ly.out + 31) / 32, 1), block, 0, stream>>>(
+        ly.b, ly.b_m, ly.b_v, ly.b_grad, 1, ly.out, lr, beta1, beta2, eps, c1, c2, hyper,
+        nullptr, nullptr);
   }
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t ottb_mlp_adam(const ottb_mlp* net, float lr, float beta1, float beta2, float eps,
+                      int32_t step, void* stream_ptr) {
+  if (step < 1) return OTTB_ERR_INVALID;
+  // bias corrections in double, rounded once
+  const float c1 = (float)(1.0 - pow((double)beta1, (double)step));
+  const float c2 = (float)(1.0 - pow((double)beta2, (double)step));
+  return adam_all(net, lr, beta1, beta2, eps, c1, c2, nullptr, (cudaStream_t)stream_ptr);
+}
+
+int32_t ottb_mlp_adam_device(const ottb_mlp* net, const float* hyper, float beta1, float beta2,
+                             float eps, void* stream_ptr) {
+  if (!hyper) return OTTB_ERR_INVALID;
+  return adam_all(net, 0.f, beta1, beta2, eps, 1.f, 1.f, hyper, (cudaStream_t)stream_ptr);
 }
 
 int32_t ottb_mlp_sync_bf16(const ottb_mlp* net, void* stream_ptr) {

@@ -110,6 +110,14 @@ class MLP:
     _lib.check(self.lib.ottb_mlp_adam(ctypes.byref(self.net), lr, b1, b2, eps, self.step,
                                       _arrays.stream_handle()), "ottb_mlp_adam")
 
+  def adam_device(self, hyper: torch.Tensor, b1=0.9, b2=0.999, eps=1e-8):
+    """An Adam step whose learning rate and bias corrections are read from
+    the device (``hyper`` = float32 ``[lr, 1 - b1^t, 1 - b2^t]``), for a
+    step captured in a CUDA graph; the caller keeps the step count."""
+    _lib.check(self.lib.ottb_mlp_adam_device(ctypes.byref(self.net), hyper.data_ptr(), b1, b2,
+                                             eps, _arrays.stream_handle()),
+               "ottb_mlp_adam_device")
+
   def check_status(self):
     st = int(self.status.item())
     if st != _lib.OTTB_OK:
@@ -159,16 +167,22 @@ class MetaInitializer(initializers.SinkhornInitializer):
     b2 = (b if b.ndim == 2 else b[None]).float()
     return float(self.geom.epsilon) * torch.log(b2)
 
-  def update(self, a: torch.Tensor, b: torch.Tensor, g_target: torch.Tensor) -> torch.Tensor:
-    """One Adam step on a batch (batch a multiple of 128) regressing the g
-    of solved problems. Returns the batch-mean loss (device scalar)."""
+  def _loss_gradients(self, a: torch.Tensor, b: torch.Tensor,
+                      g_target: torch.Tensor) -> torch.Tensor:
+    """Network inputs, regression targets and weights of a batch, then the
+    gradients into the layers; returns the per-sample losses."""
     x = self._inputs(a, b)
     b = b.float()
     pos = b > 0
     t = torch.where(pos, g_target.float() - self._eps_log(b), torch.zeros_like(b))
     m = b.shape[1]
     w = pos.float() if self.mass_floor is None else pos * (m * b + self.mass_floor)
-    loss = self.mlp.gradients(x, t, w)
+    return self.mlp.gradients(x, t, w)
+
+  def update(self, a: torch.Tensor, b: torch.Tensor, g_target: torch.Tensor) -> torch.Tensor:
+    """One Adam step on a batch (batch a multiple of 128) regressing the g
+    of solved problems. Returns the batch-mean loss (device scalar)."""
+    loss = self._loss_gradients(a, b, g_target)
     self.mlp.adam(lr=self.lr)
     return loss.mean()
 
@@ -199,26 +213,70 @@ class MetaInitializer(initializers.SinkhornInitializer):
 
 
 def fit(meta: MetaInitializer, a: torch.Tensor, b: torch.Tensor, g: torch.Tensor, steps: int,
-        batch_size: int = 512, seed: int = 0, cosine: bool = True, log_every: int = 0):
+        batch_size: int = 512, seed: int = 0, cosine: bool = True, log_every: int = 0,
+        graph: bool = True):
   """Adam steps on random minibatches of solved problems (rows of a, b and
   their solved g), the learning rate decayed from ``meta.lr`` to 0 along a
-  cosine when ``cosine``. Returns the per-step batch losses (device)."""
+  cosine when ``cosine``. Returns the per-step batch losses (device).
+
+  With ``graph`` (and no ``log_every``) the first step runs directly and one
+  training step (minibatch gather by a device step counter, inputs and
+  targets, the MLP's forward and backward, Adam with the step's learning
+  rate and bias corrections read from a device schedule) is captured in a
+  CUDA graph and replayed for the others: the same kernels on the same
+  values in the same order as the direct loop, without its ~40 host-side
+  launches per step."""
   gen = torch.Generator(device="cpu").manual_seed(seed)
   num = a.shape[0]
   lr0 = meta.lr
-  losses = []
   # every step's minibatch indices drawn at once and copied to the device
   # once (no host-to-device copy per step)
   idx_all = torch.randint(0, num, (steps, batch_size), generator=gen).to(a.device)
-  for step in range(steps):
-    if cosine:
-      meta.lr = lr0 * 0.5 * (1.0 + math.cos(math.pi * step / steps))
-    idx = idx_all[step]
-    losses.append(meta.update(a[idx], b[idx], g[idx]))
-    if log_every and (step + 1) % log_every == 0:
-      print(f"step {step + 1}: loss {float(losses[-1]):.3e}", flush=True)
-  meta.lr = lr0
-  return torch.stack(losses)
+  lrs = [lr0 * 0.5 * (1.0 + math.cos(math.pi * s / steps)) if cosine else lr0
+         for s in range(steps)]
+  if not graph or log_every or steps < 2:
+    losses = []
+    for step in range(steps):
+      meta.lr = lrs[step]
+      idx = idx_all[step]
+      losses.append(meta.update(a[idx], b[idx], g[idx]))
+      if log_every and (step + 1) % log_every == 0:
+        print(f"step {step + 1}: loss {float(losses[-1]):.3e}", flush=True)
+    meta.lr = lr0
+    return torch.stack(losses)
+  mlp = meta.mlp
+  b1, b2 = 0.9, 0.999
+  t0 = mlp.step
+  # Adam's schedule per step: lr, 1 - b1^t, 1 - b2^t, as ottb_mlp_adam
+  # forms them (the float32 betas, powers in double, rounded once)
+  fb1, fb2 = float(np.float32(b1)), float(np.float32(b2))
+  hyper = torch.tensor(np.array(
+      [[lrs[s], 1.0 - fb1 ** float(t0 + s + 1), 1.0 - fb2 ** float(t0 + s + 1)]
+       for s in range(steps)], dtype=np.float64).astype(np.float32), device=a.device)
+  losses = torch.empty(steps, dtype=torch.float32, device=a.device)
+  step_t = torch.zeros(1, dtype=torch.int64, device=a.device)
+  hyper_cur = torch.empty(3, dtype=torch.float32, device=a.device)
+
+  def body():
+    idx = idx_all.index_select(0, step_t).reshape(-1)
+    loss = meta._loss_gradients(a.index_select(0, idx), b.index_select(0, idx),
+                                g.index_select(0, idx))
+    hyper_cur.copy_(hyper.index_select(0, step_t).reshape(-1))
+    mlp.adam_device(hyper_cur, b1, b2)
+    losses.index_copy_(0, step_t, loss.mean().reshape(1))
+    step_t.add_(1)
+
+  body()  # the first step, directly: also warms up every kernel
+  side = torch.cuda.Stream()
+  side.wait_stream(torch.cuda.current_stream())
+  gr = torch.cuda.CUDAGraph()
+  with torch.cuda.graph(gr, stream=side):
+    body()
+  torch.cuda.current_stream().wait_stream(side)
+  for _ in range(steps - 1):
+    gr.replay()
+  mlp.step = t0 + steps
+  return losses
 
 
 def solve_warm_started(geom, a: torch.Tensor, b: torch.Tensor, meta: MetaInitializer,

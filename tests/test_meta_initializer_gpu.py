@@ -65,6 +65,64 @@ def test_mlp_gradients_match_oracle(weighted):
     assert _rel(gb, grads[l][1]) < 3e-2, (l, _rel(gb, grads[l][1]))
 
 
+@pytest.mark.parametrize("batch,width,tile", [(512, 1024, 32), (768, 1024, 64),
+                                              (1536, 1024, 128)])
+def test_mlp_gradients_every_tile_width(batch, width, tile):
+  """The GEMMs' tile width (128, 64 or 32 columns, the widest giving 96 or
+  more CTAs) follows M N: the layer GEMMs of these shapes take the given
+  width for the forward and data-gradient products (M = batch, N =
+  width). Forward output and every gradient against the float64 oracle on
+  the same bf16 operands."""
+  import torch
+  tiles128 = (batch // 128) * (width // 128)
+  assert (128 if tiles128 >= 96 else 64 if 2 * tiles128 >= 96 else 32) == tile
+  dims = [256, width, 128]
+  net = _mlp(dims, seed=4)
+  rng = np.random.default_rng(5)
+  x = rng.standard_normal((batch, 256)).astype(np.float32)
+  t = rng.standard_normal((batch, 128)).astype(np.float32)
+  loss = net.gradients(torch.tensor(x, device="cuda"), torch.tensor(t, device="cuda"), None)
+  loss = loss.cpu().numpy()
+  net.check_status()
+  params = net.params_numpy()
+  bparams = [(mlp_np.bf16(wt).astype(np.float64), b) for wt, b in params]
+  loss_ref, grads = mlp_np.loss_and_grads(bparams, mlp_np.bf16(x).astype(np.float64),
+                                          t.astype(np.float64), None)
+  np.testing.assert_allclose(loss, loss_ref, rtol=2e-2)
+  for l, tens in enumerate(net.tensors):
+    assert _rel(tens["w_grad"].cpu().numpy(), grads[l][0]) < 3e-2, l
+    assert _rel(tens["b_grad"].cpu().numpy(), grads[l][1]) < 3e-2, l
+  y = net.forward(torch.tensor(x, device="cuda")).cpu().numpy()
+  y_emul, _ = mlp_np.forward_bf16(params, x)
+  assert _rel(y, y_emul) < 2e-3
+
+
+def test_fit_graph_replay_matches_direct_steps():
+  """meta_initializer.fit with the training step captured in a CUDA graph
+  (device step counter, device Adam schedule) against the direct loop on
+  the same data and minibatches: the same kernels on the same values, so
+  the same losses and weights."""
+  import torch
+  from ott_b200.geometry import pointcloud
+  from ott_b200.initializers.neural import meta_initializer
+  grid = problems.grid_support(16)
+  geom = pointcloud.PointCloud(torch.tensor(grid).cuda(), epsilon=1e-2)
+  W = problems.grid_mixture_weights(2 * 640, grid, seed=3, device="cuda")
+  A, B = W[0::2].contiguous(), W[1::2].contiguous()
+  G = torch.randn(A.shape, device="cuda") * 1e-2
+  res = []
+  for graph in (False, True):
+    meta = meta_initializer.MetaInitializer(geom, dims=(256,), seed=7)
+    losses = meta_initializer.fit(meta, A, B, G, steps=25, batch_size=128, graph=graph)
+    res.append((losses.cpu().numpy(), [t["w"].cpu().numpy() for t in meta.mlp.tensors],
+                meta.mlp.step))
+  (l0, w0, s0), (l1, w1, s1) = res
+  assert s0 == s1 == 25
+  np.testing.assert_array_equal(l1, l0)
+  for u, v in zip(w1, w0):
+    np.testing.assert_array_equal(u, v)
+
+
 def test_mlp_adam_step_matches_oracle():
   import torch
   net = _mlp([128, 256, 128], seed=3)
