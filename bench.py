@@ -233,16 +233,17 @@ def bf16_peak_tflops():
 
 def tc_apply_flops_per_entry(d, k):
   """BF16 tensor flops that ottb_apply_transport_tc executes per plan entry
-  for k vectors: its log-sum-exp sweep and its cost tile (each 3 DK / 16 + 1
-  MMAs of K = 16, 2 flops per multiply-add) and the P V products of each
-  vector chunk (P_hi [V_hi | V_lo] and P_lo V_hi: 3 products of the chunk's
-  padded width); the cost tile is recomputed for every chunk."""
+  for k vectors: its first pass (the hi*hi product and the shift block, DK
+  / 16 + 1 MMAs of K = 16, 2 flops per multiply-add), the cost tile of each
+  vector chunk (3 DK / 16 + 1 MMAs) and its P V products (P_hi [V_hi |
+  V_lo] and P_lo V_hi: 3 products of the chunk's padded width)."""
   dk = 64 if d <= 64 else 128
   kvmax = 96 if dk == 64 else 64
   nch = -(-k // kvmax)
   kvp = -(-(-(-k // nch)) // 16) * 16
+  first = 2 * 16 * (dk // 16 + 1)
   cost = 2 * 16 * (3 * dk // 16 + 1)
-  return cost + nch * (cost + 2 * 3 * kvp)
+  return first + nch * (cost + 2 * 3 * kvp)
 
 
 def ncu_traffic(name):
@@ -1064,13 +1065,13 @@ def run_divergence(args):
   bwd_s = statistics.median(bw) * 1e-3
   # backward: 4 applications of an n x n plan to d + 1 vectors (2 for the
   # (x, y) term, 1 for each symmetric term, whose plan is symmetric). The
-  # chosen form runs each on ottb_apply_transport_tc: a log-sum-exp sweep
-  # and the product kernel, both tcgen05 BF16 split-3 (tensor flops per
-  # plan entry from tc_apply_flops_per_entry); FP32 (the plain arm): 2 d +
+  # chosen form runs each on ottb_apply_transport_tc: the kernel's max-only
+  # first pass and its product, both tcgen05 BF16 (tensor flops per plan
+  # entry from tc_apply_flops_per_entry); FP32 (the plain arm): 2 d +
   # 2 (d + 1) flops per entry on the FMA pipe
   tc_flops = 4.0 * n * n * tc_apply_flops_per_entry(d, d + 1)
   bf16_peak, bf16_src = bf16_peak_tflops()
-  roof = {"bound": "tensor", "kernel": "apply_tc_kernel + its log-sum-exp sweep",
+  roof = {"bound": "tensor", "kernel": "apply_tc_kernel (its first pass and the product)",
           "achieved": tc_flops / bwd_s / 1e12, "peak": bf16_peak, "unit": "TFLOP/s",
           "frac": tc_flops / bwd_s / 1e12 / bf16_peak, "peak_source": bf16_src,
           "work_per_backward": f"{tc_flops:.3e} BF16 tensor flops (4 applications to "

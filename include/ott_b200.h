@@ -210,12 +210,12 @@ int32_t ottb_apply_transport(const float* x, const float* y, int64_t n, int64_t 
  * implicit_differentiation.py:262-287): both products are tcgen05 BF16
  * split-3 MMAs with FP32 accumulation, S = <x, y> (+ the potentials) into
  * tensor memory, its weights 2^S written back there as bf16 hi/lo pairs and
- * O += P V^T taken with P straight from tensor memory. A first pass
- * (ottb_apply_lse_kernel) gives every output row its log-sum-exp, so the
- * weights need no running maximum. d <= 128; the workspace
- * (ottb_apply_transport_tc_workspace_size bytes, 256-byte aligned) holds
- * the bf16 operands, the first pass's workspace and the column splits'
- * partial sums. Its first int32 is a status word, 0 after the call's
+ * O += P V^T taken with P straight from tensor memory. A first pass of the
+ * same kernel (the hi*hi product only) gives every output row its largest
+ * exponent, so the weights need no running maximum. d <= 128; the
+ * workspace (ottb_apply_transport_tc_workspace_size bytes, 256-byte
+ * aligned) holds the bf16 operands, the rows' maxima and the column
+ * splits' partial sums. Its first int32 is a status word, 0 after the call's
  * kernels complete normally and 1 if one of the kernel's bounded waits gave
  * up (the output is then not valid). */
 size_t ottb_apply_transport_tc_workspace_size(int64_t n, int64_t m, int32_t d, int32_t num_vec,

@@ -15,11 +15,16 @@
 // accumulator halves at once, P_lo V_hi adds into the first, and O is the
 // sum of the halves (an MMA costs about the same from N = 16 to N = 128).
 // with s = 2 inv log2(e) / eps on A's centred points, w_c = (g_c - inv |B_c|^2)
-// log2(e) / eps and sigma_r the row's base-2 log-sum-exp, which the first
-// pass (ottb_apply_lse_kernel, one sweep of the solver's engine) provides.
-// With that shift every weight 2^S of a row is <= 1 and they sum to 1, so P
-// never overflows, never needs a running maximum, and out = 2^(u_r + sigma_r)
-// O_r with u_r = (f_r - inv |A_r|^2) log2(e) / eps, applied once per row.
+// log2(e) / eps and sigma_r the row's largest exponent s <A_r, B_c> + w_c,
+// which a first pass of the same kernel provides (MAXP: the hi*hi product
+// and the shift block only, 5 MMAs a tile instead of 13 at d <= 64, row
+// maxima instead of weights, combined across column splits with an integer
+// atomicMax). Its products drop the hi*lo and lo*hi terms, so its maxima
+// are good to about one log2 unit; the weights need no more: with that
+// shift every weight 2^S of a row is at most a few units, no row sum
+// overflows, no running maximum or rescale is needed, and out =
+// 2^(u_r + sigma_r) O_r with u_r = (f_r - inv |A_r|^2) log2(e) / eps,
+// applied once per row with the sigma_r the weights were formed with.
 //
 // The weights never leave the SM: each epilogue thread owns one TMEM lane
 // (one row), reads its 32 columns of S, and writes 2^S back into the same
@@ -109,7 +114,7 @@ struct AtcArgs {
   int splits;       // column splits (1: write out directly)
   int nt;           // 128-column tiles of B
   const float* potA;
-  const float* lse;     // [R] eps log sum_c exp((potB_c - C_rc) / eps)
+  int* smax;            // [R_pad] order-preserving keys (fkey) of the rows' largest exponent
   const double* nrmA;   // [R_pad] |A_r - centre|^2
   float lf;             // log2(e) / eps (FP32)
   float inv;
@@ -119,25 +124,23 @@ struct AtcArgs {
   uint64_t timeout_ns;
 };
 
-// Row shift sigma_r = log2 sum_c 2^(w_c + s <A_r, B_c>) as two bf16 terms
-// (sigma = p1 + p2 exactly in FP32); 0 for padding rows and rows whose
-// log-sum-exp is not finite.
+// Row shift sigma_r = the first pass's max_c (w_c + s <A_r, B_c>) as two
+// bf16 terms (sigma = p1 + p2 exactly in FP32); 0 for padding rows, rows
+// whose maximum is not finite, and in the first pass itself.
+template <bool MAXP>
 __device__ __forceinline__ float atc_sigma(const AtcArgs& a, int64_t row, __nv_bfloat16& p1,
                                            __nv_bfloat16& p2) {
   float sg = 0.f;
-  if (row < a.R) {
-    const float l = __ldg(a.lse + row);
-    if (isfinite(l)) {
-      const double t = ((double)l + (double)a.inv * a.nrmA[row]) * (double)a.lf;
-      if (isfinite(t)) sg = (float)t;
-    }
+  if (!MAXP && row < a.R) {
+    const float mx = fkey_value(__ldcg(a.smax + row));
+    if (isfinite(mx)) sg = mx;
   }
   p1 = __float2bfloat16_rn(sg);
   p2 = __float2bfloat16_rn(sg - __bfloat162float(p1));
   return __bfloat162float(p1) + __bfloat162float(p2);
 }
 
-template <int DK>
+template <int DK, bool MAXP>
 __global__ void __launch_bounds__(kAtcThreads, 1)
 apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                 const __grid_constant__ CUtensorMap mapBext,
@@ -210,7 +213,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
     const uint32_t one = (uint32_t)__bfloat16_as_ushort(__float2bfloat16_rn(1.f));
     for (int i = lane; i < kAtcRows; i += 32) {
       __nv_bfloat16 p1, p2;
-      atc_sigma(a, (int64_t)rb * kAtcRows + i, p1, p2);
+      atc_sigma<MAXP>(a, (int64_t)rb * kAtcRows + i, p1, p2);
       uint4 v;
       v.x = one | (one << 16);
       v.y = one | ((uint32_t)__bfloat16_as_ushort(__hneg(p1)) << 16);
@@ -248,7 +251,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
     __syncwarp();
   } else if (warp == 2) {
     // ---- producer of the vector tiles
-    if (lane == 0) {
+    if (!MAXP && lane == 0) {
       for (int i = 0; ok && i < T; ++i) {
         const int32_t col = (t0 + i) * kAtcCols;
         const uint32_t vs = i % kAtcVStages;
@@ -273,7 +276,16 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
       for (int i = 0; ok && i < T + kAtcSBufs - 1; ++i) {
         if (i < T) {
           // S of tile i into buffer i % 2 (its P was consumed by the P V
-          // MMAs of tile i - 2, issued before these)
+          // MMAs of tile i - 2, issued before these; in the first pass the
+          // epilogue releases the buffer once it has read tile i - 2)
+          if (MAXP && i >= kAtcSBufs) {
+            const int j = i - kAtcSBufs;
+            if (!tc::mbar_wait(&sm.pfull[j % kAtcSBufs], (j / kAtcSBufs) & 1, a.timeout_ns)) {
+              ok = false;
+              break;
+            }
+            tc::fence_after_sync();
+          }
           const uint32_t d = tbase + (i % kAtcSBufs) * kAtcCols;
           for (int c = 0; ok && c < C; ++c) {
             const uint32_t g = i * C + c;
@@ -287,7 +299,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
             // (A part, B part): hi*hi, hi*lo, lo*hi
             const int pa[3] = {0, 0, 1};
             const int pb[3] = {0, 1, 0};
-            for (int prod = 0; prod < 3; ++prod)
+            for (int prod = 0; prod < (MAXP ? 1 : 3); ++prod)
               for (int kk = 0; kk < 4; ++kk)
                 tc::mma_bf16(d,
                              tc::sw128_kmajor_desc(a0 + (pa[prod] * C + c) * Cfg::kBlock + kk * 32),
@@ -302,7 +314,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
           if (!ok) break;
           tc::mma_commit(&sm.sfull[i % kAtcSBufs]);
         }
-        if (i >= kAtcSBufs - 1) {
+        if (!MAXP && i >= kAtcSBufs - 1) {
           // O += P V^T for tile j = i - 1: P from TMEM, V from the ring
           const int j = i - (kAtcSBufs - 1);
           const uint32_t b = j % kAtcSBufs, vs = j % kAtcVStages;
@@ -334,6 +346,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
     const int cg = e >> 2;
     const int64_t row = (int64_t)rb * kAtcRows + 32 * q + lane;
     const uint32_t lane_off = (uint32_t)(32 * q) << 16;
+    float rmax = -INFINITY;  // first pass: this row's largest exponent so far
     for (int i = 0; ok && i < T; ++i) {
       const uint32_t b = i % kAtcSBufs;
       if (!tc::mbar_wait(&sm.sfull[b], (i / kAtcSBufs) & 1, a.timeout_ns)) {
@@ -345,6 +358,19 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
       float v[32];
       tc::tmem_ld32(ta, v);
       tc::tmem_ld_wait();
+      if (MAXP) {
+        // the buffer is free once read
+        tc::fence_before_sync();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&sm.pfull[b]);
+        float t11[11];
+#pragma unroll
+        for (int j = 0; j < 10; ++j) t11[j] = fmax3(v[3 * j], v[3 * j + 1], v[3 * j + 2]);
+        t11[10] = fmaxf(v[30], v[31]);
+        rmax = fmaxf(rmax, fmax3(fmax3(t11[0], t11[1], t11[2]), fmax3(t11[3], t11[4], t11[5]),
+                                 fmaxf(fmax3(t11[6], t11[7], t11[8]), fmaxf(t11[9], t11[10]))));
+        continue;
+      }
       uint32_t hi[16], lo[16];
 #pragma unroll
       for (int t = 0; t < 16; ++t) {
@@ -363,14 +389,20 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&sm.pfull[b]);
     }
-    if (ok && !tc::mbar_wait(&sm.ofull, 0, a.timeout_ns)) ok = false;
-    if (ok) {
+    if (MAXP) {
+      // every column group's maximum of the row into the row's key (the
+      // column splits' CTAs combine there too)
+      if (ok && row < a.R && rmax > -INFINITY) atomicMax(a.smax + row, fkey(rmax));
+    } else if (ok && !tc::mbar_wait(&sm.ofull, 0, a.timeout_ns)) {
+      ok = false;
+    }
+    if (!MAXP && ok) {
       tc::fence_after_sync();
       // the row's scale 2^(u_r + sigma_r), u_r = (potA_r - inv |A_r|^2) lf
       double sc = 0.0;
       if (row < a.R) {
         __nv_bfloat16 p1, p2;
-        const float sig = atc_sigma(a, row, p1, p2);
+        const float sig = atc_sigma<false>(a, row, p1, p2);
         const double pa = (double)__ldg(a.potA + row);
         const double ex =
             (pa - (double)a.inv * a.nrmA[row]) * (double)a.lf + (double)sig;
@@ -518,6 +550,12 @@ __global__ void atc_prep_vec_kernel(AtcPrep p) {
   }
 }
 
+// Every row's key of its largest exponent starts as fkey(-inf).
+__global__ void atc_fill_keys_kernel(int* keys, int64_t n) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) keys[i] = kDkeyEmptyMax;
+}
+
 // out[k][r] = sum over the column splits of their parts (fixed order).
 __global__ void atc_combine_kernel(const float* part, int splits, int64_t KR, float* out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < KR;
@@ -545,8 +583,7 @@ struct AtcLayout {
   int K, KV, KVP, nch;
   int64_t Kpad;
   int splits, nt;
-  size_t status, cen, abuf, bbuf, bext, nrmA, lse, vbuf, part, lse_ws, total;
-  size_t lse_ws_bytes;
+  size_t status, cen, abuf, bbuf, bext, nrmA, smax, vbuf, part, total;
 };
 
 // Column splits: the fewest waves x (tiles per unit + 2 for the pipeline's
@@ -595,31 +632,28 @@ int atc_layout(int64_t n, int64_t m, int d, int K, int axis, AtcLayout& L) {
   L.bbuf = take(2 * (size_t)L.C_pad * L.DK * 2);
   L.bext = take((size_t)L.C_pad * 16);
   L.nrmA = take(sizeof(double) * (size_t)L.R_pad);
-  L.lse = take(sizeof(float) * (size_t)L.R);
+  L.smax = take(sizeof(int32_t) * (size_t)L.R_pad);
   L.vbuf = take(2 * (size_t)L.Kpad * L.C_pad * 2);
   L.part = take(L.splits > 1 ? sizeof(float) * (size_t)L.splits * K * L.R : 0);
-  L.lse_ws_bytes = ottb_apply_lse_kernel_workspace_size(n, m, d, axis, OTTB_PRECISION_AUTO);
-  if (L.lse_ws_bytes == 0) return OTTB_ERR_UNSUPPORTED;
-  L.lse_ws = take(L.lse_ws_bytes);
   L.total = off;
   return OTTB_OK;
 }
 
-template <int DK>
+template <int DK, bool MAXP>
 int atc_launch(const CUtensorMap* maps, const AtcArgs& args, int units, cudaStream_t stream) {
   const size_t smem = sizeof(AtcSmem<DK>) + 1024;
   static bool attr_set[64] = {};  // per device
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OTTB_ERR_NO_DEVICE;
   if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute((const void*)apply_tc_kernel<DK>,
+    if (cudaFuncSetAttribute((const void*)apply_tc_kernel<DK, MAXP>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess)
       return OTTB_ERR_CUDA;
     attr_set[dev] = true;
   }
-  apply_tc_kernel<DK><<<units, kAtcThreads, smem, stream>>>(maps[0], maps[1], maps[2], maps[3],
-                                                             args);
+  apply_tc_kernel<DK, MAXP><<<units, kAtcThreads, smem, stream>>>(maps[0], maps[1], maps[2],
+                                                                   maps[3], args);
   return cudaPeekAtLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }
 
@@ -679,13 +713,6 @@ extern "C" int32_t ottb_apply_transport_tc(const float* x, const float* y, int64
   p.nrmA = (double*)(ws + L.nrmA);
   p.vbuf = (__nv_bfloat16*)(ws + L.vbuf);
 
-  // first pass: the rows' log-sum-exps (ottb_apply_lse_kernel's axis is the
-  // summed side's: axis 1 sums over y with g, axis 0 over x with f)
-  float* lse = (float*)(ws + L.lse);
-  st = ottb_apply_lse_kernel(x, y, n, m, d, axis == 1 ? g : f, epsilon, inv_scale_cost, axis,
-                             OTTB_PRECISION_AUTO, lse, ws + L.lse_ws, L.lse_ws_bytes, stream);
-  if (st != OTTB_OK) return st;
-
   atc_center_kernel<<<L.DK, 256, 0, stream>>>(p);
   {
     const int64_t warps = std::max(L.R_pad, L.C_pad);
@@ -725,7 +752,7 @@ extern "C" int32_t ottb_apply_transport_tc(const float* x, const float* y, int64
   a.splits = L.splits;
   a.nt = L.nt;
   a.potA = axis == 1 ? f : g;
-  a.lse = lse;
+  a.smax = (int*)(ws + L.smax);
   a.nrmA = p.nrmA;
   a.lf = p.lf;
   a.inv = inv_scale_cost;
@@ -733,8 +760,20 @@ extern "C" int32_t ottb_apply_transport_tc(const float* x, const float* y, int64
   a.part = L.splits > 1 ? (float*)(ws + L.part) : nullptr;
   a.err = status;
   a.timeout_ns = 20ull * 1000000000ull;
+  // first pass: the rows' largest exponents (one vector chunk's worth of
+  // units), then the product
+  {
+    AtcArgs a1 = a;
+    a1.nch = 1;
+    const int units1 = (int)((L.R_pad / kAtcRows) * L.splits);
+    atc_fill_keys_kernel<<<(unsigned)((L.R_pad + 255) / 256), 256, 0, stream>>>(a.smax, L.R_pad);
+    st = L.DK == 64 ? atc_launch<64, true>(maps, a1, units1, stream)
+                    : atc_launch<128, true>(maps, a1, units1, stream);
+    if (st != OTTB_OK) return st;
+  }
   const int units = (int)((L.R_pad / kAtcRows) * L.nch * L.splits);
-  st = L.DK == 64 ? atc_launch<64>(maps, a, units, stream) : atc_launch<128>(maps, a, units, stream);
+  st = L.DK == 64 ? atc_launch<64, false>(maps, a, units, stream)
+                  : atc_launch<128, false>(maps, a, units, stream);
   if (st != OTTB_OK) return st;
   if (L.splits > 1) {
     const int64_t KR = (int64_t)num_vec * L.R;
