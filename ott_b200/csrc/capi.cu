@@ -115,31 +115,15 @@ KernelChoice pick_tc(int dk, int tn) {
 // Tensor map over a [2 * pad][dk] bf16 array (hi rows, then lo rows): boxes
 // of 64 elements (128 bytes) x 128 rows, 128-byte swizzle.
 bool encode_points_map(CUtensorMap* map, void* base, int64_t pad, int dk) {
-  EncodeTiledFn fn = encode_tiled_fn();
-  if (!fn) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)dk, (cuuint64_t)(2 * pad)};
-  const cuuint64_t strides[1] = {(cuuint64_t)dk * 2};
-  const cuuint32_t box[2] = {64, 128};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
-         CUDA_SUCCESS;
+  return encode_bf16_2d(map, base, 2 * pad, dk, 64, 128, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B);
 }
 
 // Tensor map over column-shift rows [rows][8] bf16: boxes of 8 x 128, no
 // swizzle (the K-major core-matrix layout of an MMA extension block).
 bool encode_ext_map(CUtensorMap* map, void* base, int64_t rows) {
-  EncodeTiledFn fn = encode_tiled_fn();
-  if (!fn) return false;
-  const cuuint64_t dims[2] = {8, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {16};
-  const cuuint32_t box[2] = {8, 128};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, dims, strides, box, estr,
-            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
-         CUDA_SUCCESS;
+  return encode_bf16_2d(map, base, rows, 8, 8, 128, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_128B);
 }
 
 // Grid size of the persistent launch: all CTAs co-resident. Computed once

@@ -14,6 +14,8 @@
 
 #include "../../include/ott_b200.h"
 #include "gemm_tc.cuh"
+#include "launch.cuh"
+#include "tmap.cuh"
 
 using namespace ottb;
 
@@ -22,39 +24,11 @@ namespace {
 constexpr size_t kAlign = 256;
 inline size_t align_up(size_t v) { return (v + kAlign - 1) / kAlign * kAlign; }
 
-typedef CUresult (*EncodeFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
-                             const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
-                             const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
-                             CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeFn encode_fn() {
-  static std::mutex mu;
-  static EncodeFn fn = nullptr;
-  std::lock_guard<std::mutex> lock(mu);
-  if (!fn) {
-    void* p = nullptr;
-    cudaDriverEntryPointQueryResult q;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
-            cudaSuccess &&
-        q == cudaDriverEntryPointSuccess)
-      fn = (EncodeFn)p;
-  }
-  return fn;
-}
-
-// [rows][cols] bf16, K = cols contiguous: boxes 64 x 128, 128-byte swizzle.
+// [rows][cols] bf16, K = cols contiguous: boxes of 64 x box_rows, 128-byte swizzle.
 bool operand_map(CUtensorMap* map, const void* base, int64_t rows, int64_t cols,
                  uint32_t box_rows = 128) {
-  EncodeFn fn = encode_fn();
-  if (!fn) return false;
-  const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
-  const cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-  const cuuint32_t box[2] = {64, box_rows};
-  const cuuint32_t estr[2] = {1, 1};
-  return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box,
-            estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
-            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
-         CUDA_SUCCESS;
+  return encode_bf16_2d(map, const_cast<void*>(base), rows, cols, 64, box_rows,
+                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B);
 }
 
 template <int TN>
@@ -63,14 +37,8 @@ size_t gemm_smem() { return sizeof(GemmSmem<TN>) + 1024; }
 template <int TN>
 int launch_gemm(const CUtensorMap& ma, const CUtensorMap& mb, const GemmArgs& g,
                 cudaStream_t stream) {
-  static std::once_flag once;
-  static cudaError_t attr = cudaSuccess;
-  std::call_once(once, [] {
-    attr = cudaFuncSetAttribute((const void*)gemm_bf16_tc_kernel<TN>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)gemm_smem<TN>());
-  });
-  if (attr != cudaSuccess) return OTTB_ERR_CUDA;
+  if (!ensure_dynamic_smem((const void*)gemm_bf16_tc_kernel<TN>, gemm_smem<TN>()))
+    return OTTB_ERR_CUDA;
   gemm_bf16_tc_kernel<TN><<<dim3(g.N / TN, g.M / 128), 192, gemm_smem<TN>(), stream>>>(ma, mb, g);
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }

@@ -59,6 +59,7 @@
 
 #include "../../include/ott_b200.h"
 #include "common.cuh"
+#include "launch.cuh"
 #include "tc_ptx.cuh"
 #include "tmap.cuh"
 
@@ -642,16 +643,7 @@ int atc_layout(int64_t n, int64_t m, int d, int K, int axis, AtcLayout& L) {
 template <int DK, bool MAXP>
 int atc_launch(const CUtensorMap* maps, const AtcArgs& args, int units, cudaStream_t stream) {
   const size_t smem = sizeof(AtcSmem<DK>) + 1024;
-  static bool attr_set[64] = {};  // per device
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return OTTB_ERR_NO_DEVICE;
-  if (!attr_set[dev]) {
-    if (cudaFuncSetAttribute((const void*)apply_tc_kernel<DK, MAXP>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)smem) != cudaSuccess)
-      return OTTB_ERR_CUDA;
-    attr_set[dev] = true;
-  }
+  if (!ensure_dynamic_smem((const void*)apply_tc_kernel<DK, MAXP>, smem)) return OTTB_ERR_CUDA;
   apply_tc_kernel<DK, MAXP><<<units, kAtcThreads, smem, stream>>>(maps[0], maps[1], maps[2],
                                                                    maps[3], args);
   return cudaPeekAtLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
