@@ -179,10 +179,12 @@ class ClockSampler:
       return None
     sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
     mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+    pw = [float(r[3]) for r in rows if r[3].replace(".", "").isdigit()]
     names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
     reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k] == "Active"})
     return {"sm_mhz": statistics.median(sm) if sm else None,
             "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+            "power_w_median": statistics.median(pw) if pw else None,
             "samples": len(rows)}
 
 
