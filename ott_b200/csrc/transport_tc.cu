@@ -49,7 +49,8 @@
 //   warps 3-18  epilogue: warp w reads TMEM lanes 32 (w % 4).. and the
 //               column group (w - 3) / 4 of each tile; at the end the same
 //               warps scale O and write it out (or a column split's part).
-// Every wait is bounded; a timeout sets the error flag and unwinds.
+// Every wait is bounded; a timeout sets the error flag, the producers wait
+// (again bounded) for their copies in flight, and the CTA unwinds.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -230,6 +231,7 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
         for (int c = 0; c < C; ++c)
           tc::tma_load_2d(sm.A + (part * C + c) * Cfg::kBlock, &mapA, &sm.a_full, 64 * c,
                           (int32_t)(rb * kAtcRows + part * a.R_pad));
+      int issued = -1;  // the last ring stage given a copy
       for (int i = 0; ok && i < T; ++i) {
         const int32_t col = (t0 + i) * kAtcCols;
         for (int c = 0; c < C; ++c) {
@@ -246,13 +248,21 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
             tc::tma_load_2d(sm.B[st] + part * Cfg::kBlock, &mapB, &sm.bfull[st], 64 * c,
                             (int32_t)(col + part * a.C_pad));
           if (last) tc::tma_load_2d(sm.Bext[st], &mapBext, &sm.bfull[st], 0, col);
+          issued = (int)g;
         }
+      }
+      // after a timeout: wait (bounded) for this warp's copies in flight
+      if (!ok) {
+        tc::mbar_wait(&sm.a_full, 0, 1000000000ull);
+        for (int g = issued - kAtcStages + 1; g <= issued; ++g)
+          if (g >= 0) tc::mbar_wait(&sm.bfull[g % kAtcStages], (g / kAtcStages) & 1, 1000000000ull);
       }
     }
     __syncwarp();
   } else if (warp == 2) {
     // ---- producer of the vector tiles
     if (!MAXP && lane == 0) {
+      int issued = -1;  // the last vector tile given a copy
       for (int i = 0; ok && i < T; ++i) {
         const int32_t col = (t0 + i) * kAtcCols;
         const uint32_t vs = i % kAtcVStages;
@@ -266,7 +276,12 @@ apply_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant_
           for (int part = 0; part < 2; ++part)
             tc::tma_load_2d(sm.V[vs] + (h * 2 + part) * a.KVP * 128, &mapV, &sm.vfull[vs],
                             col + 64 * h, (int32_t)(part * a.Kpad + (int64_t)ch * a.KVP));
+        issued = i;
       }
+      if (!ok)
+        for (int i = issued - kAtcVStages + 1; i <= issued; ++i)
+          if (i >= 0)
+            tc::mbar_wait(&sm.vfull[i % kAtcVStages], (i / kAtcVStages) & 1, 1000000000ull);
     }
     __syncwarp();
   } else if (warp == 1) {
