@@ -589,10 +589,6 @@ def run_ours(args):
       "clocks": clk, "gpu_launches": launches_per_solve * args.steps,
       "pipe_peaks": peaks,
   }
-  if clk and clk.get("power_w_median"):
-    # at the board's power cap the solve's rate is its energy per cost entry
-    line["energy"] = {"power_w_median": clk["power_w_median"],
-                      "entries_per_joule": entries / t / clk["power_w_median"]}
   if rank == 0:
     print(json.dumps(line))
   if world > 1:
