@@ -1161,6 +1161,15 @@ def run_implicit(args):
   bwd_s = statistics.median(bw) * 1e-3
   pf, pb, pout, _, pinfo, pgrad = step("fp32")
   grad_diff = float((grad - pgrad).abs().max() / pgrad.abs().max())
+  # the same backward with its MINRES steps replayed from a CUDA graph in
+  # blocks of 4 instead of issued one by one from the host
+  block = imp.MINRES_GRAPH_BLOCK
+  imp.MINRES_GRAPH_BLOCK = 4
+  try:
+    gb = [step(args.precision)[1] for _ in range(max(1, min(args.steps, 3)))]
+  finally:
+    imp.MINRES_GRAPH_BLOCK = block
+  bwd_graph_s = statistics.median(gb) * 1e-3
   # one single-vector product of the backward, timed alone, in both forms
   f, g = out.f.detach(), out.g.detach()
   vec = torch.randn(1, n, device="cuda")
@@ -1213,6 +1222,7 @@ def run_implicit(args):
                              "eps=0.01*mean(C), thr=1e-3",
                  "l2": "flushed before each step (256 MiB write)"},
       "forward_s": fwd_s, "backward_s": bwd_s, "n_iters": out.n_iters,
+      "minres_graph_block": block, "backward_s_graph_replayed_blocks_of_4": bwd_graph_s,
       "minres_steps": steps, "minres_rel_residual": info.get("rel_residual"),
       "recomputed_rel_residual": info.get("true_rel_residual"),
       "single_vector_products": n_app1, "single_vector_product_s": t_app,

@@ -170,7 +170,9 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
  * later plans of such calls use it without timing trials. split_scale: a
  * single problem's column split is the heuristic one times split_scale / 4;
  * waves: the splits of problems still iterating grow while fewer than
- * waves x grid units remain (0: never); dynamic: 1 deals work units from an
+ * waves x grid units remain (0: never; unpinned, a single problem on the
+ * tensor cores runs with 0 and its split from a cost model of one sweep);
+ * dynamic: 1 deals work units from an
  * atomic queue, 0 round-robin (calls with several problems always queue);
  * tile_n: columns of a tensor-core tile, 256 or 128 (ignored by the
  * CUDA-core engine). OTTB_ERR_INVALID for values outside those ranges. */
@@ -429,6 +431,20 @@ int32_t ottb_minres_step(double* state, int32_t step, int32_t window, const doub
                          double* y, const double* r1, const double* r2, const double* w,
                          double* w_prev, double* x, double* v_next, double* history,
                          int64_t history_len, int64_t s, void* stream);
+
+/* ottb_minres_step with the step number kept on the device: the step run is
+ * state[steps] + 1, and a call once that would reach history_len clears
+ * active (the step cap) instead. The launch then has no host-side
+ * argument that changes from step to step, so a fixed sequence of steps
+ * and their operator products can be captured into a CUDA graph and
+ * replayed; calls after the stop return at once. Same state layout and
+ * initial values as ottb_minres_step; history_len >= 2. Replaces the same
+ * reference solve as ottb_minres_step (implicit_differentiation.py:156-233,
+ * lineax_implicit.py:49-101). */
+int32_t ottb_minres_step_next(double* state, int32_t window, const double* v, double* y,
+                              const double* r1, const double* r2, const double* w,
+                              double* w_prev, double* x, double* v_next, double* history,
+                              int64_t history_len, int64_t s, void* stream);
 
 /* Human-readable text of a status code. */
 const char* ottb_status_string(int32_t status);

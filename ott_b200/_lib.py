@@ -49,6 +49,7 @@ EXPORTED_SYMBOLS = (
     "ottb_apply_transport_sweep_free",
     "ottb_apply_lse_kernel",
     "ottb_minres_step",
+    "ottb_minres_step_next",
     "ottb_transport_matrix",
     "ottb_cost_stats_workspace_size",
     "ottb_cost_stats",
@@ -226,6 +227,9 @@ def load() -> ctypes.CDLL:
     lib.ottb_minres_step.argtypes = [vp, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64,
                                      i64, vp]
     lib.ottb_minres_step.restype = i32
+    lib.ottb_minres_step_next.argtypes = [vp, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, i64, i64,
+                                          vp]
+    lib.ottb_minres_step_next.restype = i32
     lib.ottb_transport_matrix.argtypes = [vp, vp, i64, i64, i32, vp, vp, f32_, f32_, vp, vp]
     lib.ottb_transport_matrix.restype = i32
     lib.ottb_cost_stats_workspace_size.argtypes = [i64, i64, i32]

@@ -150,10 +150,12 @@ int persistent_grid(const KernelChoice& k, int sms) {
 
 // Work schedule knobs of a call: the autotuner's search space.
 //   split_scale  the initial column split of a single problem is the
-//                heuristic choice (choose_split) times split_scale / 4
+//                heuristic choice (choose_split; choose_split_tc on the
+//                tensor cores) times split_scale / 4
 //   waves        the kernel grows the splits of the still-active problems
 //                whenever they offer fewer than waves * grid units per sweep
-//                (0: never)
+//                (0: never; without a tuned or pinned schedule a single
+//                problem on the tensor cores takes 0)
 //   dynamic      work units dealt from an atomic queue (1) or round-robin
 //                (0); calls with several problems always use the queue
 //   tile_n       columns of a tensor-core tile (256: two accumulators, full
@@ -179,6 +181,34 @@ int choose_split(int rb, int ntiles, int grid, int num_problems) {
     const double score = eff - 0.004 * s;
     if (score > best_score + 1e-9) {
       best_score = score;
+      best = s;
+    }
+  }
+  return best;
+}
+
+// Column splits of a single problem on the tensor cores: the split that
+// minimises a cost model of one sweep, in units of one 128 x 256 tile's
+// time (about 1.5 us at the power-capped clock). A work unit costs about
+// 4.2 tiles beyond its own tiles (filling the TMA/MMA pipeline, the first
+// accumulator round trip through tensor memory, handing its row results to
+// the merge), units run in waves of the grid, and merging s splits of a row
+// block adds about 0.33 s tiles per unit. Fitted to B200 sweeps of the
+// split at d = 64 (n = m = 2048 ... 65536): it keeps the splits of 32768
+// and 65536 (4 and 2) and takes fewer, longer units from 2048 to 16384,
+// where more units than one wave cost up to twice the time (n = m = 8192:
+// 2 splits, 3.5 ms to 1e-3, against 6.9 ms with 9).
+int choose_split_tc(int rb, int ntiles, int grid) {
+  if (grid <= 0) return 1;
+  int best = 1;
+  double best_t = -1.0;
+  const int smax = std::max(1, std::min(ntiles, 32));
+  for (int s = 1; s <= smax; ++s) {
+    const double units = (double)rb * s;
+    const double waves = std::ceil(units / grid);
+    const double t = waves * (4.2 + std::ceil((double)ntiles / s)) + 0.33 * units * s / grid;
+    if (best_t < 0.0 || t < best_t - 1e-9) {
+      best_t = t;
       best = s;
     }
   }
@@ -319,7 +349,10 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     plan.sched = *sched_override;
   } else if (need_grid) {
     Schedule t;
-    if (tuned_schedule(tune_key(probs, num, plan), &t)) plan.sched = t;
+    if (tuned_schedule(tune_key(probs, num, plan), &t))
+      plan.sched = t;
+    else if (num == 1 && plan.tc)
+      plan.sched.waves = 0;  // a single problem keeps choose_split_tc's split
   }
   if (num > 1) plan.sched.dynamic = 1;
   if (plan.tc) {
@@ -363,8 +396,13 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     auto scaled = [&](int s0, int smax) {
       return std::max(1, std::min(smax, (s0 * plan.sched.split_scale + 2) / 4));
     };
-    pp.split_f = scaled(choose_split(pp.rb_f, (int)(pp.m_pad / tile_n), plan.grid, num), pp.smax_f);
-    pp.split_g = scaled(choose_split(pp.rb_g, (int)(pp.n_pad / tile_n), plan.grid, num), pp.smax_g);
+    auto base = [&](int rb, int64_t pad) {
+      const int nt = (int)(pad / tile_n);
+      return plan.tc && num == 1 ? choose_split_tc(rb, nt, plan.grid)
+                                 : choose_split(rb, nt, plan.grid, num);
+    };
+    pp.split_f = scaled(base(pp.rb_f, pp.m_pad), pp.smax_f);
+    pp.split_g = scaled(base(pp.rb_g, pp.n_pad), pp.smax_g);
     const size_t fsz = sizeof(float);
     // FP32 engine: transposed [DP][pad] floats; tensor cores: [2][pad][DK] bf16
     const size_t elt = plan.tc ? 2 * 2 : fsz;
@@ -859,9 +897,10 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
   if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) return OTTB_ERR_CUDA;
   if (cap != cudaStreamCaptureStatusNone) return OTTB_ERR_INVALID;  // trials synchronise
   // Candidate schedules: initial split of a single problem (x1/2, x1, x2;
-  // round-robin or queued units); for several problems, how far the splits
-  // of the problems still iterating may grow (0, 1, 2, 4 waves of units).
-  // On the tensor cores each of these with 256- and with 128-column tiles.
+  // round-robin or queued units; on the tensor cores the split stays as
+  // chosen); for several problems, how far the splits of the problems still
+  // iterating may grow (0, 1, 2, 4 waves of units). On the tensor cores each
+  // of these with 256- and with 128-column tiles.
   std::vector<Schedule> cands;
   for (int tile : {256, 128}) {
     if (tile != 256 && !base.tc) break;
@@ -872,6 +911,7 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
           c.split_scale = scale;
           c.dynamic = dyn;
           c.tile_n = tile;
+          if (base.tc) c.waves = 0;
           cands.push_back(c);
         }
     } else {

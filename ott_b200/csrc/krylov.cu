@@ -4,7 +4,10 @@
 // search direction, the iterate and the next Lanczos vector, in one launch.
 // The solver's scalars live in a small device array, so the host issues the
 // products of successive steps back to back and reads only the previous
-// step's stop flag while the current step runs. Used by the implicit backward of the Sinkhorn potentials, whose
+// step's stop flag while the current step runs; with the step number kept
+// on the device too (ottb_minres_step_next), a block of steps and their
+// products is one fixed sequence of launches that a CUDA graph replays.
+// Used by the implicit backward of the Sinkhorn potentials, whose
 // linear system (implicit_differentiation.py:156-233) is solved here in a
 // symmetric form.
 //
@@ -58,18 +61,28 @@ __device__ double block_sum(double v, double* red) {
 
 // y holds op(v) on entry and the new Lanczos residual r2' on exit. w_prev
 // holds the direction before w on entry and the new direction on exit.
+// step == 0: the step number is state[steps] + 1, and a step past
+// hist_len - 1 clears the active flag instead of running.
 __global__ void __launch_bounds__(kThreads)
 minres_step_kernel(double* __restrict__ st, int step, int window,
                    const double* __restrict__ v, double* __restrict__ y,
                    const double* __restrict__ r1, const double* __restrict__ r2,
                    const double* __restrict__ w, double* __restrict__ w_prev,
                    double* __restrict__ x, double* __restrict__ v_next,
-                   double* __restrict__ hist, int64_t s) {
+                   double* __restrict__ hist, int64_t hist_len, int64_t s) {
   __shared__ double red[kWarps + 1];
   __shared__ double sc[5];
-  // every thread reads the flag before thread 0 can write it (it writes
-  // only after the reductions' barriers)
+  // every thread reads the flag and the step count before thread 0 can
+  // write them (it writes only after the reductions' barriers)
   if (st[kActive] == 0.0) return;
+  if (step == 0) {
+    const int64_t next = (int64_t)st[kSteps] + 1;
+    if (next >= hist_len) {
+      if (threadIdx.x == 0) st[kActive] = 0.0;  // the step cap: every thread returns here
+      return;
+    }
+    step = (int)next;
+  }
   const double beta = st[kBeta];
   // y = op(v) - (beta / oldb) r1 (not on the first step), alfa = <v, y>
   const double c1 = step >= 2 ? beta / st[kOldBeta] : 0.0;
@@ -144,7 +157,20 @@ int32_t ottb_minres_step(double* state, int32_t step, int32_t window, const doub
     return OTTB_ERR_INVALID;
   if (s < 1 || step < 1 || window < 1 || step >= history_len) return OTTB_ERR_INVALID;
   ottb::minres_step_kernel<<<1, ottb::kThreads, 0, (cudaStream_t)stream>>>(
-      state, step, window, v, y, r1, r2, w, w_prev, x, v_next, history, s);
+      state, step, window, v, y, r1, r2, w, w_prev, x, v_next, history, history_len, s);
+  return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
+}
+
+int32_t ottb_minres_step_next(double* state, int32_t window, const double* v, double* y,
+                              const double* r1, const double* r2, const double* w,
+                              double* w_prev, double* x, double* v_next, double* history,
+                              int64_t history_len, int64_t s, void* stream) {
+  if (!state || !v || !y || !r1 || !r2 || !w || !w_prev || !x || !v_next || !history)
+    return OTTB_ERR_INVALID;
+  if (s < 1 || window < 1 || history_len < 2 || history_len > (int64_t)INT32_MAX)
+    return OTTB_ERR_INVALID;
+  ottb::minres_step_kernel<<<1, ottb::kThreads, 0, (cudaStream_t)stream>>>(
+      state, 0, window, v, y, r1, r2, w, w_prev, x, v_next, history, history_len, s);
   return cudaGetLastError() == cudaSuccess ? OTTB_OK : OTTB_ERR_CUDA;
 }
 

@@ -94,15 +94,30 @@ def _minres(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
 # ottb_minres_step's state slots read back by the host
 _ST_PHIBAR, _ST_ACTIVE, _ST_STEPS = 4, 9, 10
 
+# Steps that one CUDA graph replay runs (a multiple of 4, the period of the
+# graph path's buffer rotation); 0 issues every step from the host. Off by
+# default: on B200 at d = 64 the replayed blocks gave the same gradients bit
+# for bit but no steady gain (n = m = 4096: 21.8 ms either way; 8192: 47-59
+# ms against 52-53 ms; 65536: 0.877 s against 0.850 s, where up to a block
+# of 2.9 ms products runs past the stop), since the plan products' own
+# device time, not the host's issue time, bounds a step.
+MINRES_GRAPH_BLOCK = 0
+
 
 def _minres_device(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
-                   window: int = 50) -> torch.Tensor:
+                   window: int = 50, graph_block: Optional[int] = None) -> torch.Tensor:
   """``_minres_host``'s iteration with its scalars on the device: per step
   the product ``op(v)`` and one ``ottb_minres_step`` launch, which freezes
   the iterate once the stop test fires, then an asynchronous copy of the
   stop flag to pinned memory. After issuing step k the host waits for step
   k - 1's flag only, so step k keeps the GPU busy meanwhile; the one step
-  issued past the stop is discarded work, not a change of the result."""
+  issued past the stop is discarded work, not a change of the result.
+
+  With ``graph_block`` (default ``MINRES_GRAPH_BLOCK``) > 0 the steps run
+  in blocks replayed from one CUDA graph instead (``_minres_graph``)."""
+  block = MINRES_GRAPH_BLOCK if graph_block is None else int(graph_block)
+  if block > 0:
+    return _minres_graph(op, rhs, rtol, max_steps, window, block)
   from ott_b200 import _arrays, _lib
   lib = _lib.load()
   rhs = rhs.to(torch.float64).contiguous()
@@ -149,6 +164,116 @@ def _minres_device(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int,
       if float(flags[(step - 1) % 2]) == 0.0:
         break
   steps, phibar = state[[_ST_STEPS, _ST_PHIBAR]].tolist()
+  true_res = float(torch.linalg.vector_norm(rhs - op(x))) / beta1
+  last_solve_info.update(steps=int(steps), rel_residual=phibar / beta1,
+                         true_rel_residual=true_res)
+  return x
+
+
+def _minres_graph(op: LinOp, rhs: torch.Tensor, rtol: float, max_steps: int, window: int,
+                  block: int) -> torch.Tensor:
+  """``_minres_device`` with its steps in blocks of ``block`` replayed from
+  one CUDA graph, so that the host's issue time of a step (the products'
+  launches, the MINRES launch, the small vector kernels around them) is
+  paid once, at capture, instead of at every step.
+
+  ``ottb_minres_step_next`` counts the steps on the device, and every step
+  reads and writes fixed buffers (the Lanczos vectors in a ring of four, v
+  and the search directions in pairs), so a block that starts at step
+  4j + 1 is one fixed sequence of launches. The first block runs
+  uncaptured: it plans the products and initialises whatever the operator
+  calls. After it the host replays the graph, copies the stop flag to
+  pinned memory behind each replay and waits for the previous replay's
+  flag only; at most one block past the stop runs, as frozen steps that
+  leave the iterate unchanged. Steps left over at the step cap run
+  uncaptured, and so does every step after an operator that cannot be
+  captured. The arithmetic is ``_minres_device``'s, launch for launch."""
+  from ott_b200 import _arrays, _lib
+  lib = _lib.load()
+  if block < 4 or block % 4:
+    raise ValueError("graph_block must be a positive multiple of 4")
+  rhs = rhs.to(torch.float64).contiguous()
+  s = rhs.numel()
+  beta1 = float(torch.linalg.vector_norm(rhs))
+  x = torch.zeros_like(rhs)
+  last_solve_info.clear()
+  last_solve_info.update(steps=0, rel_residual=1.0, true_rel_residual=1.0)
+  if beta1 == 0.0 or max_steps < 1:
+    if beta1 == 0.0:
+      last_solve_info.update(rel_residual=0.0, true_rel_residual=0.0)
+    return x
+  dev = rhs.device
+  state = torch.tensor([beta1, 0.0, 0.0, 0.0, beta1, -1.0, 0.0, beta1, float(rtol), 1.0, 0.0]
+                       + [0.0] * 5, dtype=torch.float64).to(dev)
+  hist = torch.zeros(max_steps + 1, dtype=torch.float64, device=dev)
+  hist[0] = beta1
+  vs = [rhs / beta1, torch.empty_like(rhs)]
+  dirs = [torch.zeros_like(rhs), torch.zeros_like(rhs)]
+  rs = [rhs.clone()] + [torch.empty_like(rhs) for _ in range(3)]
+
+  def step(k: int) -> None:
+    # step k: v = vs[(k-1)%2] -> v_next = vs[k%2]; direction w = dirs[(k-1)%2],
+    # the new one into dirs[k%2]; y = op(v) in rs[k%4], r2 = rs[(k-1)%4],
+    # r1 = rs[(k-2)%4] (unused at step 1); the stream is read at every call,
+    # the capture's own while capturing
+    v, y = vs[(k - 1) % 2], rs[k % 4]
+    y.copy_(op(v).reshape(s))
+    st = lib.ottb_minres_step_next(
+        state.data_ptr(), int(window), v.data_ptr(), y.data_ptr(), rs[(k - 2) % 4].data_ptr(),
+        rs[(k - 1) % 4].data_ptr(), dirs[(k - 1) % 2].data_ptr(), dirs[k % 2].data_ptr(),
+        x.data_ptr(), vs[k % 2].data_ptr(), hist.data_ptr(), hist.numel(), s,
+        _arrays.stream_handle())
+    _lib.check(st, "ottb_minres_step_next")
+
+  def capture(k0: int) -> Optional[torch.cuda.CUDAGraph]:
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(device=dev)
+    try:
+      with torch.cuda.stream(side):
+        graph.capture_begin()
+        try:
+          for j in range(block):
+            step(k0 + 1 + j)
+        except BaseException:
+          try:
+            graph.capture_end()
+          except RuntimeError:
+            pass
+          raise
+        graph.capture_end()
+    except RuntimeError:
+      return None
+    return graph
+
+  flags = torch.ones(2, dtype=torch.float64).pin_memory()
+  done = [torch.cuda.Event(), torch.cuda.Event()]
+
+  def mark(i: int) -> None:
+    flags[i % 2].copy_(state[_ST_ACTIVE], non_blocking=True)
+    done[i % 2].record()
+
+  k = 0
+  for _ in range(min(block, max_steps)):
+    k += 1
+    step(k)
+  mark(0)
+  graph = capture(k) if max_steps - k >= block else None
+  i = 0
+  while k < max_steps:
+    i += 1
+    if graph is not None and max_steps - k >= block:
+      graph.replay()
+      k += block
+    else:
+      for _ in range(min(block, max_steps - k)):
+        k += 1
+        step(k)
+    mark(i)
+    done[(i - 1) % 2].synchronize()
+    if float(flags[(i - 1) % 2]) == 0.0:
+      break
+  steps, phibar = state[[_ST_STEPS, _ST_PHIBAR]].tolist()  # waits for every step issued
+  del graph
   true_res = float(torch.linalg.vector_norm(rhs - op(x))) / beta1
   last_solve_info.update(steps=int(steps), rel_residual=phibar / beta1,
                          true_rel_residual=true_res)

@@ -135,6 +135,15 @@ def test_invalid_arguments_rejected_without_device():
   assert step(step=11) == _lib.OTTB_ERR_INVALID
   assert step(window=0) == _lib.OTTB_ERR_INVALID
   assert step(s=0) == _lib.OTTB_ERR_INVALID
+  # the device-counted step: the same refusals, and a history of fewer than
+  # two entries (no step fits)
+  def step_next(*, ptrs=p, window=50, hist_len=11, s=8):
+    return lib.ottb_minres_step_next(ptrs[0], window, *ptrs[1:], hist_len, s, None)
+  assert step_next(ptrs=[None] + p[1:]) == _lib.OTTB_ERR_INVALID
+  assert step_next(ptrs=p[:9] + [None]) == _lib.OTTB_ERR_INVALID
+  assert step_next(hist_len=1) == _lib.OTTB_ERR_INVALID
+  assert step_next(window=0) == _lib.OTTB_ERR_INVALID
+  assert step_next(s=0) == _lib.OTTB_ERR_INVALID
 
 
 def test_mlp_shape_checks_without_device():

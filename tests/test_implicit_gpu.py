@@ -427,6 +427,19 @@ def test_device_minres_matches_host_minres(case):
   # the public dispatch takes the device loop for CUDA tensors
   xp = imp._minres(op, b, rtol, max_steps, window)
   assert _rel(xp, xd.cpu().numpy()) < 1e-12
+  # blocks of 4 and 8 steps replayed from a CUDA graph
+  # (ottb_minres_step_next, the step count on the device) give the step
+  # count and iterate of the steps issued one by one from the host
+  # (ottb_minres_step): the same launches in the same order (frozen steps
+  # past the stop change nothing; the operator's own library products may
+  # round differently when captured, hence the host-loop tolerances)
+  for block in (4, 8):
+    xb = imp._minres_device(op, b, rtol, max_steps, window, graph_block=block)
+    ib = dict(imp.last_solve_info)
+    assert abs(ib["steps"] - idv["steps"]) <= tol_steps, (block, ib, idv)
+    assert _rel(xb, xd.cpu().numpy()) < 1e-9, block
+    assert abs(ib["rel_residual"] - idv["rel_residual"]) <= 1e-9 * max(idv["rel_residual"],
+                                                                       1e-3)
 
 
 def test_tensor_core_products_give_the_fp32_gradient():
