@@ -170,8 +170,9 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
  * later plans of such calls use it without timing trials. split_scale: a
  * single problem's column split is the heuristic one times split_scale / 4;
  * waves: the splits of problems still iterating grow while fewer than
- * waves x grid units remain (0: never; unpinned, a single problem on the
- * tensor cores runs with 0 and its split from a cost model of one sweep);
+ * waves x grid units remain (0: never; unpinned, a single problem runs
+ * with 0, on the tensor cores with its split from a cost model of one
+ * sweep);
  * dynamic: 1 deals work units from an
  * atomic queue, 0 round-robin (calls with several problems always queue);
  * tile_n: columns of a tensor-core tile, 256 or 128 (ignored by the

@@ -155,7 +155,9 @@ int persistent_grid(const KernelChoice& k, int sms) {
 //   waves        the kernel grows the splits of the still-active problems
 //                whenever they offer fewer than waves * grid units per sweep
 //                (0: never; without a tuned or pinned schedule a single
-//                problem on the tensor cores takes 0)
+//                problem takes 0: on B200 growth cost a single FP32 solve
+//                1.42x at n = m = 4096 and 1.24x at 8192, nothing at 2048
+//                and 16384)
 //   dynamic      work units dealt from an atomic queue (1) or round-robin
 //                (0); calls with several problems always use the queue
 //   tile_n       columns of a tensor-core tile (256: two accumulators, full
@@ -351,8 +353,8 @@ int make_plan(const ottb_problem* probs, int num, int d, const ottb_solver_cfg* 
     Schedule t;
     if (tuned_schedule(tune_key(probs, num, plan), &t))
       plan.sched = t;
-    else if (num == 1 && plan.tc)
-      plan.sched.waves = 0;  // a single problem keeps choose_split_tc's split
+    else if (num == 1)
+      plan.sched.waves = 0;  // a single problem keeps its first split
   }
   if (num > 1) plan.sched.dynamic = 1;
   if (plan.tc) {
@@ -897,8 +899,8 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
   if (cudaStreamIsCapturing(stream, &cap) != cudaSuccess) return OTTB_ERR_CUDA;
   if (cap != cudaStreamCaptureStatusNone) return OTTB_ERR_INVALID;  // trials synchronise
   // Candidate schedules: initial split of a single problem (x1/2, x1, x2;
-  // round-robin or queued units; on the tensor cores the split stays as
-  // chosen); for several problems, how far the splits of the problems still
+  // round-robin or queued units; the split stays as chosen); for several
+  // problems, how far the splits of the problems still
   // iterating may grow (0, 1, 2, 4 waves of units). On the tensor cores each
   // of these with 256- and with 128-column tiles.
   std::vector<Schedule> cands;
@@ -911,7 +913,7 @@ int32_t ottb_sinkhorn_autotune(const ottb_problem* problems, int32_t num_problem
           c.split_scale = scale;
           c.dynamic = dyn;
           c.tile_n = tile;
-          if (base.tc) c.waves = 0;
+          c.waves = 0;
           cands.push_back(c);
         }
     } else {
